@@ -1,0 +1,388 @@
+/*
+ * svpf.h -- C ABI of the B200 SVPF step engine (libsvpf_b200.so).
+ *
+ * Drop-in for the reference's include/svpf.cuh: same type names, same field
+ * names for every SVPFState field a caller configures, same entry points and
+ * argument meaning.  Field offsets differ: callers recompile against this
+ * header.  Plain C types only (cudaStream_t is an opaque pointer).
+ *
+ * Every tick of a filter runs as ONE kernel launch: predict, EKF guide,
+ * bandwidth, the annealed Newton-Stein loop with KSD, rejuvenation and the
+ * output moments, with particles resident in shared memory.  The batch API
+ * runs many independent filters (own N, own theta) in one persistent launch
+ * per tick.
+ */
+#ifndef SVPF_B200_H
+#define SVPF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#ifndef __cplusplus
+#include <stdbool.h>
+#endif
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- constants (include/svpf.cuh:47-64) ---------------------------------- */
+#define SVPF_DEFAULT_PARTICLES     512
+#define SVPF_DEFAULT_STEIN_STEPS   5
+#define SVPF_DEFAULT_NU            5.0f
+#define SVPF_STEIN_STEP_SIZE       0.1f
+#define SVPF_H_MIN                 -15.0f
+#define SVPF_H_MAX                 5.0f
+#define SVPF_SMOOTH_MAX_LAG        8
+#define SVPF_STEIN_SIGN_LEGACY     0
+#define SVPF_STEIN_SIGN_PAPER      1
+#ifndef SVPF_STEIN_SIGN_DEFAULT
+#define SVPF_STEIN_SIGN_DEFAULT    SVPF_STEIN_SIGN_LEGACY
+#endif
+
+/* Engine limits. */
+#define SVPF_MAX_PARTICLES         8192   /* per filter */
+#define SVPF_MAX_ANNEAL_STEPS      16
+
+/* Error codes returned by svpf_last_error() and the batch API. */
+#define SVPF_OK                    0
+#define SVPF_ERR_INVALID_ARG       1
+#define SVPF_ERR_CUDA              2
+#define SVPF_ERR_NOT_INITIALIZED   3
+#define SVPF_ERR_TAPE_SHORT        4   /* noise tape has fewer slots than the tick draws */
+#define SVPF_ERR_NONFINITE         5   /* NaN/Inf seen in an observation or the outputs */
+#define SVPF_ERR_UNSUPPORTED       6
+
+/* ---- model parameters (include/svpf.cuh:257-262) ------------------------- */
+typedef struct {
+    float rho;
+    float sigma_z;
+    float mu;
+    float gamma;
+} SVPFParams;
+
+/* ---- step result (include/svpf.cuh:552-558) ------------------------------ */
+typedef struct {
+    float log_lik_increment;
+    float vol_mean;
+    float vol_std;
+    float h_mean;
+    float mu_estimate;
+} SVPFResult;
+
+/* ---- per-filter configuration ---------------------------------------------
+ * Field names and meaning follow the SVPFState configuration fields of the
+ * reference (include/svpf.cuh:337-545).  Used directly by the batch API; the
+ * single-filter API keeps the same fields inside SVPFState.                */
+#define SVPF_CONFIG_FIELDS(X_INT, X_FLOAT)                                     \
+    X_INT(n_stein_steps) X_FLOAT(nu) X_FLOAT(student_t_implied_offset)        \
+    X_FLOAT(lik_offset) X_INT(use_exact_gradient) X_INT(use_svld)             \
+    X_INT(use_annealing) X_INT(use_adaptive_beta) X_INT(n_anneal_steps)       \
+    X_FLOAT(temperature) X_FLOAT(rmsprop_rho) X_FLOAT(rmsprop_eps)            \
+    X_INT(use_mim) X_FLOAT(mim_jump_prob) X_FLOAT(mim_jump_scale)             \
+    X_INT(use_local_params) X_FLOAT(delta_rho) X_FLOAT(delta_sigma)           \
+    X_INT(use_asymmetric_rho) X_FLOAT(rho_up) X_FLOAT(rho_down)               \
+    X_INT(use_newton) X_INT(use_full_newton) X_INT(use_guided)                \
+    X_FLOAT(guided_alpha_base) X_FLOAT(guided_alpha_shock)                    \
+    X_FLOAT(guided_innovation_threshold) X_INT(use_rejuvenation)              \
+    X_FLOAT(rejuv_ksd_threshold) X_FLOAT(rejuv_prob) X_FLOAT(rejuv_blend)     \
+    X_INT(use_guide) X_INT(use_guide_preserving) X_FLOAT(guide_strength)      \
+    X_INT(use_adaptive_guide) X_FLOAT(guide_strength_base)                    \
+    X_FLOAT(guide_strength_max) X_FLOAT(guide_innovation_threshold)           \
+    X_INT(use_adaptive_mu) X_FLOAT(mu_process_var) X_FLOAT(mu_obs_var_scale)  \
+    X_FLOAT(mu_min) X_FLOAT(mu_max) X_INT(use_adaptive_sigma)                 \
+    X_FLOAT(sigma_boost_threshold) X_FLOAT(sigma_boost_max)                   \
+    X_INT(stein_repulsive_sign) X_INT(use_fan_mode) X_INT(stein_min_steps)    \
+    X_INT(stein_max_steps) X_FLOAT(ksd_improvement_threshold)                 \
+    X_INT(use_student_t_state) X_FLOAT(nu_state) X_INT(use_smoothing)         \
+    X_INT(smooth_lag) X_INT(smooth_output_lag) X_INT(use_heun)
+
+#define SVPF_DECL_INT_(f) int f;
+#define SVPF_DECL_FLOAT_(f) float f;
+typedef struct {
+    SVPF_CONFIG_FIELDS(SVPF_DECL_INT_, SVPF_DECL_FLOAT_)
+} svpf_config_t;
+
+/* Per-filter control record carried from tick to tick (device resident in the
+ * batch engine; mirrored into SVPFState fields for the single-filter API). */
+typedef struct {
+    double guide_mean;        /* EKF posterior mean (FP64 recursion) */
+    double guide_var;         /* EKF posterior variance (FP64 recursion) */
+    double guide_K;
+    double loglik_sum;        /* FP64 sum of per-tick log-likelihoods */
+    int    timestep;
+    int    guide_initialized;
+    int    stein_steps_used;
+    int    smooth_head;
+    float  ksd_prev;          /* KSD of the previous tick: budget, beta, rejuvenation */
+    float  ksd_last;          /* last KSD computed */
+    float  vol_prev;
+    float  h_mean_prev;
+    float  bw;
+    float  bw_sq;
+    float  return_ema;
+    float  return_var;
+    float  sigma_z_effective;
+    float  mu_state;
+    float  mu_var;
+    float  y_prev;
+    float  smooth_h_mean[SVPF_SMOOTH_MAX_LAG];
+    float  smooth_h_var[SVPF_SMOOTH_MAX_LAG];
+    float  smooth_y[SVPF_SMOOTH_MAX_LAG];
+    int    status;            /* SVPF_OK or an SVPF_ERR_* code of the last tick */
+    int    reserved;
+} svpf_ctl_t;
+
+/* Per-tick outputs of one filter. */
+typedef struct {
+    float loglik;
+    float vol;
+    float h_mean;             /* smoothed when use_smoothing */
+    float h_mean_raw;
+    float bw;
+    float ksd;
+    int   steps_used;
+    int   rejuv_fired;
+} svpf_out_t;
+
+/* ---- single-filter state (include/svpf.cuh:290-547) ---------------------- */
+typedef struct {
+    /* particle arrays (device, [n_particles]) */
+    float* h;
+    float* h_prev;
+    float* h_pred;            /* kept for source compatibility; not written */
+    float* grad_log_p;        /* kept for source compatibility; not written */
+    float* log_weights;       /* log importance weights of the last gradient pass */
+    float* d_grad_v;          /* RMSProp second moment */
+    void*  rng_states;        /* unused: the engine's RNG is counter based */
+
+    int    n_particles;
+    int    n_stein_steps;
+    float  nu;
+    float  student_t_const;
+    float  student_t_implied_offset;
+    int    timestep;
+    float  y_prev;
+    cudaStream_t stream;
+
+    float lik_offset;
+    int   use_exact_gradient;
+    int   use_svld;
+    int   use_annealing;
+    int   use_adaptive_beta;
+    int   n_anneal_steps;
+    float temperature;
+    float rmsprop_rho;
+    float rmsprop_eps;
+    int   use_mim;
+    float mim_jump_prob;
+    float mim_jump_scale;
+    int   use_local_params;
+    float delta_rho;
+    float delta_sigma;
+    int   use_asymmetric_rho;
+    float rho_up;
+    float rho_down;
+    int   use_newton;
+    int   use_full_newton;
+    int   use_guided;
+    float guided_alpha_base;
+    float guided_alpha_shock;
+    float guided_innovation_threshold;
+    int   use_rejuvenation;
+    float rejuv_ksd_threshold;
+    float rejuv_prob;
+    float rejuv_blend;
+    int   use_guide;
+    int   use_guide_preserving;
+    float guide_strength;
+    float guide_mean;
+    float guide_var;
+    float guide_K;
+    int   guide_initialized;
+    int   use_adaptive_guide;
+    float guide_strength_base;
+    float guide_strength_max;
+    float guide_innovation_threshold;
+    float vol_prev;
+    int   use_adaptive_mu;
+    float mu_state;
+    float mu_var;
+    float mu_process_var;
+    float mu_obs_var_scale;
+    float mu_min;
+    float mu_max;
+    int   use_adaptive_sigma;
+    float sigma_boost_threshold;
+    float sigma_boost_max;
+    float sigma_z_effective;
+    int   stein_repulsive_sign;
+    int   use_fan_mode;
+    int   stein_min_steps;
+    int   stein_max_steps;
+    float ksd_improvement_threshold;
+    float ksd_prev;
+    int   stein_steps_used;
+    int   use_student_t_state;
+    float nu_state;
+    int   use_smoothing;
+    int   smooth_lag;
+    int   smooth_output_lag;
+    int   smooth_head;
+    float smooth_h_mean[SVPF_SMOOTH_MAX_LAG];
+    float smooth_h_var[SVPF_SMOOTH_MAX_LAG];
+    float smooth_y[SVPF_SMOOTH_MAX_LAG];
+    int   use_persistent_kernel;   /* accepted, no effect: every tick is one launch */
+    int   persistent_kernel_supported;
+    int   use_heun;
+    int   use_two_factor;          /* not supported by this engine: step reports SVPF_ERR_UNSUPPORTED */
+
+    void* impl;                    /* engine-private state */
+} SVPFState;
+
+/* ---- core API (include/svpf.cuh:573-603, src/svpf_optimized_graph.cu) ---- */
+
+/* svpf_create (include/svpf.cuh:573): allocates the filter; NULL on failure
+ * (n_particles outside [1, SVPF_MAX_PARTICLES], no device, out of memory). */
+SVPFState* svpf_create(int n_particles, int n_stein_steps, float nu, cudaStream_t stream);
+
+/* svpf_destroy (include/svpf.cuh:578). NULL is a no-op. */
+void svpf_destroy(SVPFState* state);
+
+/* svpf_initialize (include/svpf.cuh:587): particles from the stationary law;
+ * synchronous.  The seed keys the engine's counter-based Philox generator. */
+void svpf_initialize(SVPFState* state, const SVPFParams* params, unsigned long long seed);
+
+/* svpf_step (include/svpf.cuh:597): one tick with y_prev = state->y_prev. */
+void svpf_step(SVPFState* state, float y_t, const SVPFParams* params, SVPFResult* result);
+
+/* svpf_step_seeded (include/svpf.cuh:602-603): as svpf_step, but this tick's
+ * noise is keyed by rng_seed (the reference ignores the seed; here the same
+ * seed and state reproduce the same tick). */
+void svpf_step_seeded(SVPFState* state, float y_t, const SVPFParams* params,
+                      unsigned long long rng_seed, SVPFResult* result);
+
+/* svpf_step_adaptive (include/svpf.cuh:768-776): same as svpf_step_graph. */
+void svpf_step_adaptive(SVPFState* state, float y_t, float y_prev, const SVPFParams* params,
+                        float* h_loglik_out, float* h_vol_out, float* h_mean_out);
+
+/* svpf_step_graph (include/svpf.cuh:843-851): the production tick.  Blocking;
+ * NULL output pointers are allowed.  One kernel launch per call. */
+void svpf_step_graph(SVPFState* state, float y_t, float y_prev, const SVPFParams* params,
+                     float* h_loglik_out, float* h_vol_out, float* h_mean_out);
+
+/* svpf_run_sequence[_device] (include/svpf.cuh:689-708). */
+void svpf_run_sequence(SVPFState* state, const float* h_observations, int T,
+                       const SVPFParams* params, float* h_loglik_out, float* h_vol_out);
+void svpf_run_sequence_device(SVPFState* state, const float* d_observations, int T,
+                              const SVPFParams* params, float* d_loglik_out, float* d_vol_out);
+
+/* diagnostics (include/svpf.cuh:795-811, src/svpf_optimized_graph.cu:1490) */
+void  svpf_get_particles(const SVPFState* state, float* h_out);
+void  svpf_get_stats(const SVPFState* state, float* h_mean, float* h_std);
+float svpf_get_ess(const SVPFState* state);
+void  svpf_get_ksd_stats(const SVPFState* state, float* ksd_out, int* steps_used_out);
+
+/* graph API (include/svpf.cuh:856-869).  A tick is already one launch; these
+ * report/drop the cached launch configuration. */
+bool svpf_graph_is_captured(SVPFState* state);
+void svpf_graph_invalidate(SVPFState* state);
+void svpf_optimized_cleanup_state(SVPFState* state);
+
+/* sign / Fan mode setters (include/svpf.cuh:626-673) */
+static inline void svpf_set_stein_sign_mode(SVPFState* state, int mode) {
+    state->stein_repulsive_sign = (mode == SVPF_STEIN_SIGN_PAPER) ? 1 : 0;
+}
+static inline int svpf_get_stein_sign_mode(const SVPFState* state) {
+    return state->stein_repulsive_sign;
+}
+static inline void svpf_set_fan_mode(SVPFState* state, int enable) {
+    state->use_fan_mode = enable ? 1 : 0;
+    if (enable) state->stein_repulsive_sign = SVPF_STEIN_SIGN_PAPER;
+}
+static inline int svpf_get_fan_mode(const SVPFState* state) { return state->use_fan_mode; }
+
+/* ---- additions (no reference counterpart) -------------------------------- */
+
+/* Error of the last call on this state (the reference's step returns void). */
+int svpf_last_error(const SVPFState* state);
+
+/* Fill cfg with the svpf_create defaults for (n_stein_steps, nu), including
+ * the create-time Student-t implied offset.  Needs no device. */
+void svpf_config_init(svpf_config_t* cfg, int n_stein_steps, float nu);
+
+/* Copy the configuration fields of the state into a svpf_config_t and back. */
+void svpf_get_config(const SVPFState* state, svpf_config_t* cfg);
+void svpf_set_config(SVPFState* state, const svpf_config_t* cfg);
+
+/* Full state snapshot / restore: control record plus host arrays [n].  Used for
+ * checkpointing and for per-tick parity checks with state re-sync. */
+int svpf_get_state(const SVPFState* state, svpf_ctl_t* ctl, float* h, float* h_prev,
+                   float* v, float* log_w);
+int svpf_set_state(SVPFState* state, const svpf_ctl_t* ctl, const float* h,
+                   const float* h_prev, const float* v, const float* log_w);
+
+/* Test hook: drive the next ticks' noise from a host tape instead of Philox.
+ * normals[k*n + i] is the k-th normal of particle i within a tick; uniforms
+ * likewise.  Pass NULL to return to Philox.  The tape is copied. */
+int svpf_set_noise_tape(SVPFState* state, const float* normals, int n_normal_slots,
+                        const float* uniforms, int n_uniform_slots);
+
+/* Last tick's full outputs. */
+int svpf_get_last_output(const SVPFState* state, svpf_out_t* out);
+
+/* Cluster size used by the single-filter kernel for this state (0 = auto). */
+int svpf_set_cluster_size(SVPFState* state, int cluster_ctas);
+
+/* ---- batch API: many independent filters, one persistent launch per tick -- */
+typedef struct svpf_batch svpf_batch_t;
+
+/* Create a batch of n_filters filters; filter f has ns[f] particles,
+ * configuration cfgs[f] and parameters params[f].  stream may be NULL. */
+svpf_batch_t* svpf_batch_create(int n_filters, const int* ns, const svpf_config_t* cfgs,
+                                const SVPFParams* params, cudaStream_t stream);
+void svpf_batch_destroy(svpf_batch_t* b);
+
+/* Stationary initialisation of every filter; filter f is keyed by (seed, f). */
+int svpf_batch_initialize(svpf_batch_t* b, unsigned long long seed);
+
+/* One tick of every filter from HOST observations y_t[f], y_prev[f]; outputs
+ * (may be NULL) land in host arrays [n_filters].  Copies in and out are part
+ * of the call.  Blocking. */
+int svpf_batch_step(svpf_batch_t* b, const float* y_t, const float* y_prev,
+                    float* loglik, float* vol, float* h_mean);
+
+/* One tick from DEVICE observations (d_y_t/d_y_prev [n_filters]); outputs go
+ * to device arrays (may be NULL).  Asynchronous on the batch stream. */
+int svpf_batch_step_device(svpf_batch_t* b, const float* d_y_t, const float* d_y_prev,
+                           svpf_out_t* d_out);
+
+/* Capture one device tick in a CUDA graph and replay it: the observations are
+ * read from d_y_t/d_y_prev (fixed device buffers the caller refills). */
+int svpf_batch_graph_launch(svpf_batch_t* b, const float* d_y_t, const float* d_y_prev,
+                            svpf_out_t* d_out);
+
+int svpf_batch_sync(svpf_batch_t* b);
+int svpf_batch_n_filters(const svpf_batch_t* b);
+int svpf_batch_kernel_launches(const svpf_batch_t* b);  /* launches issued so far */
+int svpf_batch_get_ctl(const svpf_batch_t* b, svpf_ctl_t* ctl_host);          /* [n_filters] */
+int svpf_batch_get_particles(const svpf_batch_t* b, int filter, float* h_out);
+int svpf_batch_set_noise_tape(svpf_batch_t* b, const float* normals, int n_normal_slots,
+                              const float* uniforms, int n_uniform_slots);   /* same tape for all, [k][n_max] */
+/* Tile shape (rows per thread R, column split S) used for filters of size n;
+ * -1 when no choice was made. */
+int svpf_batch_tile_of(const svpf_batch_t* b, int n, int* rows_per_thread, int* col_split);
+
+/* Autotuner: time each compiled tile shape on a synthetic filter of each
+ * particle count in ns[] and keep the fastest per size for this process. */
+int svpf_autotune(const int* ns, int count, int ticks);
+int svpf_tile_choice(int n, int* rows_per_thread, int* col_split);
+
+/* Library facts. */
+const char* svpf_build_info(void);
+int svpf_debug_philox(uint32_t k0, uint32_t k1, const uint32_t* ctr4, uint32_t* out4, int count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

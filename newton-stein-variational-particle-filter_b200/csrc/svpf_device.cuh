@@ -1,0 +1,664 @@
+// svpf_device.cuh -- device side of the B200 SVPF step engine.
+//
+// One SVPF tick of one filter is executed by a "team": one CTA (batch engine)
+// or a thread-block cluster of C CTAs (low-latency single-filter kernel).
+// All particle data of a tick live in shared memory:
+//
+//   h[2][N]   particle positions, double buffered (Jacobi transport: every row
+//             reads the pre-iteration positions; the reference updates in place
+//             and races across blocks, svpf_opt_kernels.cu:545-598)
+//   g[N]      transport score (raw gradient, or the Newton-preconditioned one)
+//   c[N]      curvature (full Newton) or its reciprocal (plain Newton)
+//   mu[M]     prior means mu_k = mu + rho (h_prev,k - mu) + leverage_k, sorted
+//             once per tick; M >= N padded with a far value
+//   v[L]      RMSProp second moment of the team member's own rows
+//
+// Rows (particles) are split across the team; within a CTA a tile <R, S>
+// gives each thread R rows and 1/S of the columns (S lanes of a warp share a
+// row and combine their partial sums with shuffles).  After the gradient pass
+// g/c are all-gathered across the cluster through distributed shared memory,
+// after the transport pass the new h is; every exchange is followed by one
+// cluster barrier.  There are no spin waits anywhere.
+#pragma once
+
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "svpf.h"
+
+namespace svpf {
+namespace cg = cooperative_groups;
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr float kMuPad = 1e18f;   // sorted-prior pad: exp weight is exactly 0, products stay finite
+constexpr float kHPad = 1e15f;    // particle pad column: K ~ 1e-34, K^2 flushes to 0, no inf/NaN
+constexpr int kMaxCluster = 16;
+
+// ---------------------------------------------------------------------------
+// Hardware approximations, as PTX instructions.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float lg2_approx(float x) {
+    float r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr float kLn2 = 0.6931471805599453f;
+
+__device__ __forceinline__ float clamp_h(float h) { return fminf(fmaxf(h, SVPF_H_MIN), SVPF_H_MAX); }
+__device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+
+// ---------------------------------------------------------------------------
+// Counter-based RNG: Philox4x32-10 (Salmon et al., SC'11), written from the
+// paper's round function.  key = (seed_lo, seed_hi + 0x9E3779B9 * filter),
+// counter = (particle, draw index, tick, stream); stream 0 normals, 1
+// uniforms, 2 the initial draw.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint4 philox10(uint2 key, uint4 c) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ key.x, lo1, hi0 ^ c.w ^ key.y, lo0);
+        key.x += 0x9E3779B9u;
+        key.y += 0xBB67AE85u;
+    }
+    return c;
+}
+
+__device__ __forceinline__ uint2 philox_key(unsigned long long seed, int filter) {
+    return make_uint2((uint32_t)seed, (uint32_t)(seed >> 32) + 0x9E3779B9u * (uint32_t)filter);
+}
+
+// Box-Muller on 24-bit uniforms: u1 in (0,1], u2 in [0,1).
+__device__ __forceinline__ float normal_from_bits(uint32_t a, uint32_t b) {
+    const float u1 = (float)((a >> 8) + 1u) * (1.0f / 16777216.0f);
+    const float u2 = (float)(b >> 8) * (1.0f / 16777216.0f);
+    return sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+}
+__device__ __forceinline__ float uniform_from_bits(uint32_t a) {
+    return (float)((a >> 8) + 1u) * (1.0f / 16777216.0f);
+}
+
+// Noise of one filter for one tick: Philox, or a pre-drawn tape (test mode).
+struct Noise {
+    uint2 key;
+    uint32_t tick;
+    const float* tape_n;   // [slots_n][n] or nullptr
+    const float* tape_u;   // [slots_u][n]
+    int slots_n, slots_u, stride;
+    int* flag;             // shared flag: set to SVPF_ERR_TAPE_SHORT on overrun
+
+    __device__ __forceinline__ float normal(int i, int k) const {
+        if (tape_n != nullptr) {
+            if (k >= slots_n) { *flag = SVPF_ERR_TAPE_SHORT; return 0.0f; }
+            return tape_n[(size_t)k * stride + i];
+        }
+        const uint4 r = philox10(key, make_uint4((uint32_t)i, (uint32_t)k, tick, 0u));
+        return normal_from_bits(r.x, r.y);
+    }
+    __device__ __forceinline__ float uniform(int i, int k) const {
+        if (tape_u != nullptr) {
+            if (k >= slots_u) { *flag = SVPF_ERR_TAPE_SHORT; return 1.0f; }
+            return tape_u[(size_t)k * stride + i];
+        }
+        const uint4 r = philox10(key, make_uint4((uint32_t)i, (uint32_t)k, tick, 1u));
+        return uniform_from_bits(r.x);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Tick plan: every scalar decision of a tick, made by one thread before the
+// particle phases (the reference makes them on the host between launches,
+// svpf_optimized_graph.cu:933-1138, 1328-1341).
+// ---------------------------------------------------------------------------
+struct Plan {
+    float mu_eff, sz_eff, stc, off;
+    float rho_up, rho_dn, drho, dsig;
+    float gs, guide_mean, gstd;
+    float eps_step, temp;
+    float y_t, y_prev;
+    float bw, inv_bw, inv_bw2;
+    float beta[SVPF_MAX_ANNEAL_STEPS];
+    int budget, na, si_base;
+    int rejuv;
+    int kn_pred;
+    int uses_uniform_predict;
+    int transport;         // 0 vanilla, 1 Newton, 2 full Newton
+    int fan;
+    int flag;              // tape overrun etc.
+    float red[4][kWarps];  // block reduction scratch
+    float ksd_slot[kMaxCluster];
+};
+
+// Adaptive beta (svpf_optimized_graph.cu:1066-1092).
+__device__ __forceinline__ float adaptive_beta(float ksd_prev, int ai, int na) {
+    if (ai == na - 1) return 1.0f;
+    float b;
+    if (ksd_prev > 0.50f) b = 0.30f;
+    else if (ksd_prev < 0.05f) b = 0.80f;
+    else b = 0.30f + (0.50f - ksd_prev) / (0.50f - 0.05f) * (0.80f - 0.30f);
+    b *= 0.5f + 0.5f * ((float)(ai + 1) / (float)na);
+    return clampf(b, 0.1f, 1.0f);
+}
+
+// Scalar control of a tick; writes the updated EKF/sigma fields into ctl.
+__device__ inline void make_plan(const svpf_config_t& c, const SVPFParams& p, svpf_ctl_t& s,
+                          float y_t, float y_prev, Plan& pl) {
+    const int t = s.timestep;
+    pl.y_t = y_t;
+    pl.y_prev = y_prev;
+    // effective parameters (:933-948)
+    pl.mu_eff = c.use_adaptive_mu ? s.mu_state : p.mu;
+    pl.sz_eff = p.sigma_z;
+    if (c.use_adaptive_sigma && t > 0) {
+        const float ve = fmaxf(s.vol_prev, 1e-4f);
+        const float z = fabsf(y_t) / ve;
+        float boost = 1.0f;
+        if (z > c.sigma_boost_threshold) {
+            const float sev = fminf((z - c.sigma_boost_threshold) / 3.0f, 1.0f);
+            boost = 1.0f + (c.sigma_boost_max - 1.0f) * sev;
+        }
+        pl.sz_eff = p.sigma_z * boost;
+        s.sigma_z_effective = pl.sz_eff;
+    }
+    // Student-t normaliser (:951-953) and the create-time implied offset
+    pl.stc = lgammaf((c.nu + 1.0f) * 0.5f) - lgammaf(c.nu * 0.5f) - 0.5f * logf(3.14159265358979f * c.nu);
+    pl.off = c.student_t_implied_offset;
+    pl.rho_up = c.use_asymmetric_rho ? c.rho_up : p.rho;
+    pl.rho_dn = c.use_asymmetric_rho ? c.rho_down : p.rho;
+    pl.drho = c.use_local_params ? c.delta_rho : 0.0f;
+    pl.dsig = c.use_local_params ? c.delta_sigma : 0.0f;
+    // adaptive guide strength (:1006-1021)
+    pl.gs = c.guide_strength_base;
+    if (c.use_guide && c.use_adaptive_guide && t > 0) {
+        const float ve = fmaxf(s.vol_prev, 1e-4f);
+        const float z = fabsf(y_t) / ve;
+        const float ih = logf(y_t * y_t + 1e-8f) + pl.off;
+        const float he = logf(ve * ve + 1e-8f);
+        if (ih - he > 0.0f && z > c.guide_innovation_threshold) {
+            const float sev = fminf((z - c.guide_innovation_threshold) / 3.0f, 1.0f);
+            pl.gs = c.guide_strength_base + (c.guide_strength_max - c.guide_strength_base) * sev;
+        }
+    }
+    // EKF guide on log y^2 (include/svpf_kernels.cuh:509-541), FP64 recursion
+    if (c.use_guide) {
+        const double mu = (double)pl.mu_eff, rho = (double)p.rho, sz = (double)p.sigma_z;
+        double m = s.guide_mean, P = s.guide_var;
+        if (!s.guide_initialized) {
+            m = mu;
+            P = sz * sz / (1.0 - rho * rho);
+            s.guide_initialized = 1;
+        }
+        const double m_pred = mu + rho * (m - mu);
+        const double P_pred = rho * rho * P + sz * sz;
+        const double log_y2 = log((double)y_t * (double)y_t + 1e-8);
+        const double S = P_pred + (4.93 + 2.0);
+        const double K = P_pred / (S + 1e-8);
+        s.guide_mean = m_pred + K * (log_y2 - (m_pred - (double)pl.off));
+        s.guide_var = (1.0 - K) * P_pred;
+        s.guide_K = K;
+    }
+    pl.guide_mean = (float)s.guide_mean;
+    pl.gstd = sqrtf(fmaxf((float)s.guide_var, 1e-6f));
+    // Stein budget from the previous tick's KSD (:1096-1112), split over stages
+    const int na = c.use_annealing ? max(min(c.n_anneal_steps, SVPF_MAX_ANNEAL_STEPS), 1) : 1;
+    int budget;
+    if (t < 10) {
+        budget = c.stein_max_steps;
+    } else {
+        float kn = (s.ksd_prev - 0.05f) / (0.50f - 0.05f);
+        kn = fminf(fmaxf(kn, 0.0f), 1.0f);
+        budget = c.stein_min_steps + (int)(kn * (float)(c.stein_max_steps - c.stein_min_steps));
+    }
+    pl.budget = max(budget, 0);
+    pl.na = na;
+    pl.si_base = pl.budget / na;
+    for (int ai = 0; ai < na; ++ai) {
+        float beta;
+        if (!c.use_annealing) beta = 1.0f;
+        else if (c.use_adaptive_beta) beta = adaptive_beta(s.ksd_prev, ai, na);
+        else beta = (ai % 3 == 0) ? 0.30f : (ai % 3 == 1) ? 0.65f : 1.0f;
+        pl.beta[ai] = beta;
+    }
+    pl.eps_step = SVPF_STEIN_STEP_SIZE * (c.use_guide ? 0.5f : 1.0f);
+    pl.temp = c.use_svld ? c.temperature : 0.0f;
+    pl.rejuv = (c.use_rejuvenation && c.use_guide && t > 10 && s.ksd_prev > c.rejuv_ksd_threshold) ? 1 : 0;
+    // draws consumed by predict (svpf_opt_kernels.cu:31-53, 187-193)
+    if (c.use_student_t_state && c.nu_state <= 30.0f) {
+        const int nu_int = max((int)(c.nu_state + 0.5f), 3);
+        pl.kn_pred = 1 + nu_int;
+    } else {
+        pl.kn_pred = 1;
+    }
+    pl.uses_uniform_predict = (c.use_mim || c.use_guided) ? 1 : 0;
+    pl.transport = c.use_newton ? (c.use_full_newton ? 2 : 1) : 0;
+    pl.fan = c.use_fan_mode;
+}
+
+// Stage of Stein iteration `it` and its beta (budget split :1136-1138).
+__device__ __forceinline__ int stage_of(const Plan& pl, int it) {
+    if (pl.si_base == 0) return pl.na - 1;
+    const int a = it / pl.si_base;
+    return a < pl.na - 1 ? a : pl.na - 1;
+}
+
+// ---------------------------------------------------------------------------
+// Team: one CTA or one cluster.
+// ---------------------------------------------------------------------------
+struct Team {
+    int rank, size;
+    __device__ __forceinline__ void sync() const {
+        if (size == 1) __syncthreads();
+        else cg::this_cluster().sync();
+    }
+    template <class T>
+    __device__ __forceinline__ T* at(T* local, int r) const {
+        if (size == 1) return local;
+        return cg::this_cluster().map_shared_rank(local, r);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Block reductions (kThreads threads).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Reduce up to four values (op per slot: 0 sum, 1 max, 2 min); result visible
+// to all threads.  Contains two __syncthreads.
+template <int K>
+__device__ __forceinline__ void block_reduce(float (&v)[K], const int (&op)[K], Plan& pl) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        v[k] = op[k] == 0 ? warp_sum(v[k]) : op[k] == 1 ? warp_max(v[k]) : warp_min(v[k]);
+        if (lane == 0) pl.red[k][w] = v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        float a = pl.red[k][0];
+        for (int i = 1; i < kWarps; ++i) {
+            const float b = pl.red[k][i];
+            a = op[k] == 0 ? a + b : op[k] == 1 ? fmaxf(a, b) : fminf(a, b);
+        }
+        v[k] = a;
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Bitonic sort of m[0..P) ascending (P a power of two), whole CTA.
+// ---------------------------------------------------------------------------
+__device__ inline void bitonic_sort(float* m, int P) {
+    for (int k = 2; k <= P; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < P; i += kThreads) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const float a = m[i], b = m[ixj];
+                    const bool up = (i & k) == 0;
+                    if ((a > b) == up) { m[i] = b; m[ixj] = a; }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Largest log-responsibility of row value x: attained at the nearest prior
+// mean, found by binary search in the sorted means (the reference scans all N,
+// svpf_opt_kernels.cu:453-459; the value is the same).
+__device__ __forceinline__ float nearest_lmax_gauss(const float* m, int n, float x, float inv2) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (m[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    float best = -1e10f;
+    if (lo < n) { const float d = x - m[lo]; best = fmaxf(best, -d * d * inv2); }
+    if (lo > 0) { const float d = x - m[lo - 1]; best = fmaxf(best, -d * d * inv2); }
+    return best;
+}
+__device__ __forceinline__ float nearest_lmax_student(const float* m, int n, float x, float inv_nus2,
+                                                      float half_np1) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (m[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    float best = -1e10f;
+    if (lo < n) { const float d = x - m[lo]; best = fmaxf(best, -half_np1 * kLn2 * lg2_approx(1.0f + d * d * inv_nus2)); }
+    if (lo > 0) { const float d = x - m[lo - 1]; best = fmaxf(best, -half_np1 * kLn2 * lg2_approx(1.0f + d * d * inv_nus2)); }
+    return best;
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory view of one tick.
+// ---------------------------------------------------------------------------
+struct Smem {
+    float* h[2];
+    float* g;
+    float* c;
+    float* mu;
+    float* v;
+    float* phi0;        // Heun: operator at the start point, own rows
+    float* phi1;        // Heun: operator at the predicted point, own rows
+    int n, np, m_len, p2;   // particles, padded row length, padded prior length, sort length
+    int row0, row1;     // rows owned by this team member
+};
+
+__host__ __device__ inline int pow2_at_least(int n) {
+    int p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+__host__ __device__ inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+// Floats of dynamic shared memory for N particles on a team of C CTAs.
+__host__ __device__ inline int smem_floats(int n, int C) {
+    const int np = round_up(n, 64);
+    const int p2 = pow2_at_least(n);
+    const int m_len = round_up(p2 > np ? p2 : np, 64);
+    const int L = round_up((n + C - 1) / C, 4);
+    return 2 * np + np + np + m_len + 3 * L;
+}
+
+__device__ inline Smem carve(float* base, int n, int C, int rank) {
+    Smem s;
+    const int np = round_up(n, 64);
+    s.n = n;
+    s.p2 = pow2_at_least(n);
+    s.m_len = round_up(s.p2 > np ? s.p2 : np, 64);
+    s.h[0] = base;
+    s.h[1] = base + np;
+    s.g = base + 2 * np;
+    s.c = base + 3 * np;
+    s.mu = base + 4 * np;
+    s.np = np;
+    const int L = (n + C - 1) / C;
+    const int Lp = round_up(L, 4);
+    s.v = s.mu + s.m_len;
+    s.phi0 = s.v + Lp;
+    s.phi1 = s.phi0 + Lp;
+    s.row0 = min(rank * L, n);
+    s.row1 = min(s.row0 + L, n);
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// Gradient pass (svpf_fused_gradient_kernel, svpf_opt_kernels.cu:354-521) for
+// the team member's rows.  Mixture prior over all N sorted prior means in one
+// exp per pair (the row maximum comes from the nearest mean), likelihood,
+// beta-combine and clamp, curvature.  Writes g/c on every team member and the
+// log-weights to global memory.
+// ---------------------------------------------------------------------------
+template <int R, int S, bool STUDENT>
+__device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_config_t& cfg,
+                          float beta, float* __restrict__ lw_out, const Team& team) {
+    constexpr int G = kThreads / S;
+    const int grp = threadIdx.x / S, q = threadIdx.x % S;
+    const float* __restrict__ hc = sm.h[cur];
+    const float* __restrict__ mu = sm.mu;
+    const int nloc = sm.row1 - sm.row0;
+    const int nv = round_up(sm.n, 4 * S);
+    const float s2 = pl.sz_eff * pl.sz_eff;
+    const float inv2 = 0.5f / s2, inv_s2 = 1.0f / s2;
+    const float nu = cfg.nu;
+    // Student-t prior constants (:406-447)
+    const float nus2 = cfg.nu_state * s2, inv_nus2 = 1.0f / nus2, np1 = cfg.nu_state + 1.0f;
+    const float half_np1 = 0.5f * np1;
+
+    for (int base = 0; base < nloc; base += G * R) {
+        float hj[R], lmax[R], sr[R], wg[R], wh[R];
+        int jl[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            jl[r] = base + r * G + grp;
+            const int j = sm.row0 + min(jl[r], nloc - 1);
+            hj[r] = hc[j];
+            lmax[r] = STUDENT ? nearest_lmax_student(mu, sm.n, hj[r], inv_nus2, half_np1)
+                              : nearest_lmax_gauss(mu, sm.n, hj[r], inv2);
+            sr[r] = 0.0f; wg[r] = 0.0f; wh[r] = 0.0f;
+        }
+        // exponent in base 2: r = 2^((-d^2 c - lmax) log2 e)
+        const float c2 = -inv2 * kLog2e;
+        float l2[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) l2[r] = -lmax[r] * kLog2e;
+
+        for (int cb = q * 4; cb < nv; cb += 4 * S) {
+            const float4 m4 = *reinterpret_cast<const float4*>(mu + cb);
+            const float mm[4] = {m4.x, m4.y, m4.z, m4.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const float d = hj[r] - mm[e];
+                    if (!STUDENT) {
+                        const float w = ex2_approx(fmaf(d * d, c2, l2[r]));
+                        sr[r] += w;
+                        wg[r] = fmaf(w, d, wg[r]);
+                    } else {
+                        const float d2 = d * d;
+                        const float den = nus2 + d2;
+                        const float lr = -half_np1 * kLn2 * lg2_approx(fmaf(d2, inv_nus2, 1.0f));
+                        const float w = ex2_approx((lr - lmax[r]) * kLog2e);
+                        const float iden = rcp_approx(den);
+                        sr[r] += w;
+                        wg[r] = fmaf(w * d, iden, wg[r]);
+                        wh[r] = fmaf(w * (nus2 - d2), iden * iden, wh[r]);
+                    }
+                }
+            }
+        }
+        // combine the S column slices
+#pragma unroll
+        for (int o = S / 2; o > 0; o >>= 1) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                sr[r] += __shfl_xor_sync(0xffffffffu, sr[r], o);
+                wg[r] += __shfl_xor_sync(0xffffffffu, wg[r], o);
+                if (STUDENT) wh[r] += __shfl_xor_sync(0xffffffffu, wh[r], o);
+            }
+        }
+        if (q == 0) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (jl[r] >= nloc) continue;
+                const int j = sm.row0 + jl[r];
+                const float h = hj[r];
+                float gp, hp;
+                if (!STUDENT) {
+                    gp = -wg[r] * inv_s2 / (sr[r] + 1e-8f);
+                    hp = -inv_s2;
+                } else {
+                    gp = -np1 * wg[r] / (sr[r] + 1e-8f);
+                    hp = -np1 * wh[r] / (sr[r] + 1e-8f);
+                }
+                // likelihood (:475-499)
+                const float vol = expf(fminf(h, 20.0f));
+                const float y2 = pl.y_t * pl.y_t;
+                const float A = y2 / (vol + 1e-8f) / nu;
+                const float opA = 1.0f + A;
+                const float lw = pl.fan ? 0.0f
+                                        : pl.stc - 0.5f * h - (nu + 1.0f) * 0.5f * log1pf(fmaxf(A, -0.999f));
+                float glik;
+                if (cfg.use_exact_gradient) glik = -0.5f + 0.5f * (nu + 1.0f) * A / opA - cfg.lik_offset;
+                else glik = (logf(y2 + 1e-10f) - h + cfg.lik_offset) / 1.4f;
+                const float eb = pl.fan ? 1.0f : beta;
+                const float gg = clampf(gp + eb * glik, -10.0f, 10.0f);
+                float score = gg, cc = 0.0f;
+                if (pl.transport != 0) {
+                    const float hl = -0.5f * (nu + 1.0f) * A / (opA * opA);
+                    const float curv = clampf(-(hl + hp), 0.1f, 100.0f);
+                    if (pl.transport == 2) {
+                        cc = curv;
+                    } else {
+                        score = 0.7f * gg / curv;   // precond_grad (:519)
+                        cc = 1.0f / curv;           // 1/curvature (:765)
+                    }
+                }
+                for (int rk = 0; rk < team.size; ++rk) {
+                    team.at(sm.g, rk)[j] = score;
+                    team.at(sm.c, rk)[j] = cc;
+                }
+                lw_out[j] = lw;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Transport pass (svpf_fused_stein_transport*_kernel, svpf_opt_kernels.cu:527-
+// 1103): IMQ kernel K = 1 / (1 + d^2/bw^2), attraction K*score and repulsion
+// 2 d/bw^2 K^2 (sign by stein_repulsive_sign), Newton scaling, optional KSD
+// row sum, RMSProp, drift, SVLD diffusion, clamp.  KIND 0 vanilla, 1 Newton
+// (precondition per column), 2 full Newton (kernel-weighted Hessian per row).
+// Returns this thread's KSD row sums.
+// ---------------------------------------------------------------------------
+enum { kTransport = 0, kPhiOnly = 1, kKsdOnly = 2 };
+
+template <int R, int S, int KIND, bool KSD, int MODE = kTransport>
+__device__ float transport_pass(const Smem& sm, int cur, const Plan& pl, const svpf_config_t& cfg,
+                                float bf, const Noise& nz, int kn, const Team& team,
+                                float* __restrict__ phi_out = nullptr) {
+    constexpr int G = kThreads / S;
+    const int grp = threadIdx.x / S, q = threadIdx.x % S;
+    const float* __restrict__ hc = sm.h[cur];
+    float* __restrict__ hn = sm.h[cur ^ 1];
+    const float* __restrict__ gs = sm.g;
+    const float* __restrict__ cs = sm.c;
+    const int n = sm.n;
+    const int nloc = sm.row1 - sm.row0;
+    const int nv = round_up(n, 4 * S);
+    const float inv_bw = pl.inv_bw, inv_bw2 = pl.inv_bw2;
+    const float sign = cfg.stein_repulsive_sign == 1 ? 1.0f : -1.0f;
+    const float inv_n = 1.0f / (float)n;
+    const float es = pl.eps_step * bf;
+    const float rr = cfg.rmsprop_rho;
+    float ksd_thread = 0.0f;
+
+    for (int base = 0; base < nloc; base += G * R) {
+        float hi[R], si[R];
+        float ks[R], kg[R], gk[R], kc[R], nk[R], gkr[R], gdk[R], hs[R];
+        int il[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            il[r] = base + r * G + grp;
+            const int i = sm.row0 + min(il[r], nloc - 1);
+            hi[r] = hc[i];
+            si[r] = gs[i];
+            ks[r] = kg[r] = gk[r] = kc[r] = nk[r] = gkr[r] = gdk[r] = hs[r] = 0.0f;
+        }
+        for (int cb = q * 4; cb < nv; cb += 4 * S) {
+            const float4 h4 = *reinterpret_cast<const float4*>(hc + cb);
+            const float4 g4 = *reinterpret_cast<const float4*>(gs + cb);
+            float4 c4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (KIND != 0) c4 = *reinterpret_cast<const float4*>(cs + cb);
+            const float hh[4] = {h4.x, h4.y, h4.z, h4.w};
+            const float gg[4] = {g4.x, g4.y, g4.z, g4.w};
+            const float cc[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                // columns past n hold h = kHPad, g = c = 0: their terms vanish
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const float d = hi[r] - hh[e];
+                    const float u = d * inv_bw;
+                    const float base_ = fmaf(u, u, 1.0f);
+                    const float K = rcp_approx(base_);
+                    const float K2 = K * K;
+                    kg[r] = fmaf(K, gg[e], kg[r]);
+                    const float dk2 = d * K2;
+                    if (KIND == 1) gk[r] = fmaf(dk2, cc[e], gk[r]);
+                    else gk[r] += dk2;
+                    if (KIND == 2) {
+                        ks[r] += K;
+                        kc[r] = fmaf(K, cc[e], kc[r]);
+                        nk[r] = fmaf(K2, fabsf(fmaf(3.0f, base_, -4.0f)), nk[r]);   // |3 d^2/bw^2 - 1|
+                    }
+                    if (KSD) {
+                        if (KIND == 1) gkr[r] += dk2;
+                        gdk[r] = fmaf(gg[e], dk2, gdk[r]);
+                        hs[r] = fmaf(K2, fmaf(-4.0f, K, 3.0f), hs[r]);           // 4 (d^2/bw^2) K - 1 = 3 - 4K
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int o = S / 2; o > 0; o >>= 1) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                kg[r] += __shfl_xor_sync(0xffffffffu, kg[r], o);
+                gk[r] += __shfl_xor_sync(0xffffffffu, gk[r], o);
+                if (KIND == 2) {
+                    ks[r] += __shfl_xor_sync(0xffffffffu, ks[r], o);
+                    kc[r] += __shfl_xor_sync(0xffffffffu, kc[r], o);
+                    nk[r] += __shfl_xor_sync(0xffffffffu, nk[r], o);
+                }
+                if (KSD) {
+                    if (KIND == 1) gkr[r] += __shfl_xor_sync(0xffffffffu, gkr[r], o);
+                    gdk[r] += __shfl_xor_sync(0xffffffffu, gdk[r], o);
+                    hs[r] += __shfl_xor_sync(0xffffffffu, hs[r], o);
+                }
+            }
+        }
+        if (q == 0) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (il[r] >= nloc) continue;
+                const int i = sm.row0 + il[r];
+                float phi = (kg[r] + sign * 2.0f * inv_bw2 * gk[r]) * inv_n;
+                if (KIND == 2) {
+                    float H = (kc[r] + 2.0f * inv_bw2 * nk[r]) / fmaxf(ks[r], 1e-6f);
+                    H = clampf(H, 0.1f, 100.0f);
+                    phi = phi * (1.0f / H) * 0.7f;
+                }
+                if (KSD) {
+                    const float gsum = (KIND == 1) ? gkr[r] : gk[r];
+                    ksd_thread += si[r] * kg[r] + 2.0f * inv_bw2 * (si[r] * gsum - gdk[r] + hs[r]);
+                }
+                const int li = i - sm.row0;
+                if (MODE == kPhiOnly) { phi_out[li] = phi; continue; }
+                if (MODE == kKsdOnly) continue;
+                const float vn = rr * sm.v[li] + (1.0f - rr) * phi * phi;
+                sm.v[li] = vn;
+                const float drift = es * phi * rsqrtf(vn + cfg.rmsprop_eps);
+                float diff = 0.0f;
+                if (pl.temp > 1e-6f) diff = sqrtf(2.0f * es * pl.temp) * nz.normal(i, kn);
+                const float h_new = clamp_h(hi[r] + drift + diff);
+                for (int rk = 0; rk < team.size; ++rk) team.at(hn, rk)[i] = h_new;
+            }
+        }
+    }
+    return ksd_thread;
+}
+
+}  // namespace svpf

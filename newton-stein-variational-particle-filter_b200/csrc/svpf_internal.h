@@ -1,0 +1,99 @@
+// svpf_internal.h -- launch interface between the C ABI (svpf_capi.cu) and
+// the kernels (svpf_kernels.cu).  Host-only declarations.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "svpf.h"
+
+namespace svpf {
+
+// Tile shapes <rows per thread R, column split S> compiled into the kernels.
+struct TileShape { int R, S; };
+constexpr int kNumTiles = 7;
+constexpr TileShape kTiles[kNumTiles] = {{1, 8}, {1, 4}, {1, 2}, {1, 1}, {2, 1}, {4, 1}, {8, 1}};
+// The batch kernel compiles tiles [kBatchTileLo, kNumTiles).
+constexpr int kBatchTileLo = 1;
+
+struct SingleArgs {
+    svpf_config_t cfg;
+    SVPFParams prm;
+    svpf_ctl_t ctl;
+    float y_t, y_prev;
+    float* h;
+    float* hp;
+    float* v;
+    float* lw;
+    int n;
+    unsigned long long seed;
+    const float* tape_n;
+    const float* tape_u;
+    int slots_n, slots_u;
+    svpf_ctl_t* ctl_out;   // host-mapped
+    svpf_out_t* out;       // host-mapped
+};
+
+struct BatchArgs {
+    int F;
+    const int* order;      // work order (largest cost first)
+    int* queue;            // work counter, zero before each launch
+    const int* n;
+    const long long* off;
+    const uint8_t* tile;
+    const svpf_config_t* cfg;
+    const SVPFParams* prm;
+    svpf_ctl_t* ctl;
+    float* h;
+    float* hp;
+    float* v;
+    float* lw;
+    const float* y_t;
+    const float* y_prev;
+    svpf_out_t* out;
+    unsigned long long seed;
+    const float* tape_n;
+    const float* tape_u;
+    int slots_n, slots_u, tape_stride;
+};
+
+struct InitArgs {
+    float* h;
+    float* hp;
+    float* v;
+    const long long* off;   // nullptr: single filter at offset 0
+    const int* n;           // per filter (or single n in n0)
+    int n0;
+    int F;
+    const float* mu;        // per filter [F] or nullptr (mu0)
+    const float* sd;        // per filter [F] or nullptr (sd0)
+    float mu0, sd0;
+    unsigned long long seed;
+    const float* tape0;     // optional [n] initial normals (single filter)
+};
+
+// Dynamic shared-memory bytes of a tick kernel for n particles on C CTAs.
+size_t tick_smem_bytes(int n, int C);
+// Largest dynamic shared memory a CTA may use on this device.
+size_t max_dyn_smem();
+
+// Default tile of the single-filter kernel for n particles on C CTAs, and of
+// the batch kernel for n particles.
+int default_single_tile(int n, int C);
+int default_batch_tile(int n);
+// Default cluster size of the single-filter kernel for n particles.
+int default_cluster(int n);
+
+cudaError_t launch_single(const SingleArgs& a, int C, int tile, cudaStream_t s);
+cudaError_t launch_single_small(const SingleArgs& a, int C, int tile, cudaStream_t s);
+cudaError_t launch_single_large(const SingleArgs& a, int C, int tile, cudaStream_t s);
+cudaError_t launch_batch(const BatchArgs& a, size_t smem_bytes, int grid, cudaStream_t s);
+cudaError_t launch_init(const InitArgs& a, cudaStream_t s);
+int batch_grid(size_t smem_bytes);
+cudaError_t debug_philox(uint32_t k0, uint32_t k1, const uint32_t* d_ctr, uint32_t* d_out, int count);
+
+// Process-wide tuner table: tile chosen for a particle count (-1 = none yet).
+int tuned_batch_tile(int n);
+void set_tuned_batch_tile(int n, int tile);
+
+}  // namespace svpf

@@ -1,0 +1,118 @@
+// svpf_kernels.cu -- initialisation and debug kernels, launch helpers and the
+// tile-shape table of the B200 SVPF engine.  The tick kernels themselves:
+//
+//   single_tick_kernel<R,S>  (svpf_single_*.cu) one filter, one tick, a
+//                            cluster of C <= 16 CTAs sharing particles via DSMEM
+//   batch_tick_kernel        (svpf_batch_kernel.cu) many filters, one tick, a
+//                            persistent grid pulling filters largest-first
+#include <cstdio>
+#include <mutex>
+#include <unordered_map>
+
+#include "svpf_internal.h"
+#include "svpf_tick.cuh"
+
+namespace svpf {
+
+__global__ void init_kernel(const InitArgs a) {
+    // one CTA per filter
+    const int f = blockIdx.x;
+    const int n = a.n ? a.n[f] : a.n0;
+    const long long off = a.off ? a.off[f] : 0;
+    const float mu = a.mu ? a.mu[f] : a.mu0;
+    const float sd = a.sd ? a.sd[f] : a.sd0;
+    const uint2 key = philox_key(a.seed, f);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        float z;
+        if (a.tape0 != nullptr) {
+            z = a.tape0[i];
+        } else {
+            const uint4 r = philox10(key, make_uint4((uint32_t)i, 0u, 0u, 2u));
+            z = normal_from_bits(r.x, r.y);
+        }
+        const float h = clamp_h(mu + sd * z);
+        a.h[off + i] = h;
+        a.hp[off + i] = h;
+        a.v[off + i] = 0.0f;
+    }
+}
+
+__global__ void philox_kernel(uint32_t k0, uint32_t k1, const uint32_t* ctr, uint32_t* out, int count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const uint4 r = philox10(make_uint2(k0, k1), make_uint4(ctr[4 * i], ctr[4 * i + 1], ctr[4 * i + 2], ctr[4 * i + 3]));
+    out[4 * i] = r.x; out[4 * i + 1] = r.y; out[4 * i + 2] = r.z; out[4 * i + 3] = r.w;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+size_t tick_smem_bytes(int n, int C) { return (size_t)smem_floats(n, C) * sizeof(float); }
+
+size_t max_dyn_smem() {
+    static size_t cached = 0;
+    if (cached == 0) {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        const size_t static_bytes = sizeof(Plan) + sizeof(svpf_ctl_t) + sizeof(svpf_config_t) +
+                                    sizeof(SVPFParams) + sizeof(svpf_out_t) + 64;
+        cached = (size_t)v > static_bytes ? (size_t)v - static_bytes : 0;
+    }
+    return cached;
+}
+
+int default_cluster(int n) {
+    int C = 1;
+    while (C < kMaxCluster && n / (2 * C) >= 32) C <<= 1;
+    return C;
+}
+
+static int rows_per_sweep(int tile) { return kTiles[tile].R * (kThreads / kTiles[tile].S); }
+
+int default_single_tile(int n, int C) {
+    const int L = (n + C - 1) / C;
+    for (int t = 0; t < kNumTiles; ++t)
+        if (rows_per_sweep(t) >= L) return t;
+    return kNumTiles - 1;
+}
+
+int default_batch_tile(int n) {
+    for (int t = kBatchTileLo; t < kNumTiles; ++t)
+        if (rows_per_sweep(t) >= n) return t;
+    return kNumTiles - 1;
+}
+
+cudaError_t launch_single(const SingleArgs& a, int C, int tile, cudaStream_t s) {
+    if (C < 1 || C > kMaxCluster || a.n < 1) return cudaErrorInvalidValue;
+    if (tick_smem_bytes(a.n, C) > max_dyn_smem()) return cudaErrorInvalidValue;
+    return tile <= 3 ? launch_single_small(a, C, tile, s) : launch_single_large(a, C, tile, s);
+}
+
+cudaError_t launch_init(const InitArgs& a, cudaStream_t s) {
+    if (a.F < 1) return cudaErrorInvalidValue;
+    init_kernel<<<a.F, kThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t debug_philox(uint32_t k0, uint32_t k1, const uint32_t* d_ctr, uint32_t* d_out, int count) {
+    if (count <= 0) return cudaSuccess;
+    philox_kernel<<<(count + 255) / 256, 256>>>(k0, k1, d_ctr, d_out, count);
+    return cudaGetLastError();
+}
+
+static std::mutex g_tune_mu;
+static std::unordered_map<int, int> g_tune;
+
+int tuned_batch_tile(int n) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(n);
+    return it == g_tune.end() ? -1 : it->second;
+}
+
+void set_tuned_batch_tile(int n, int tile) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[n] = tile;
+}
+
+}  // namespace svpf

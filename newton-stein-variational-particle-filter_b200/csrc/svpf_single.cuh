@@ -1,0 +1,76 @@
+// svpf_single.cuh -- the single-filter tick kernel template (one cluster of
+// C <= 16 CTAs per tick) and its launcher; instantiated per tile shape in
+// svpf_single_small.cu / svpf_single_large.cu.
+#pragma once
+
+#include "svpf_internal.h"
+#include "svpf_tick.cuh"
+
+namespace svpf {
+
+// Cooperative copy of a POD struct by 4-byte words.
+template <class T>
+__device__ __forceinline__ void copy_words(T* dst, const T* src) {
+    static_assert(sizeof(T) % 4 == 0, "word copy");
+    const int* s = reinterpret_cast<const int*>(src);
+    int* d = reinterpret_cast<int*>(dst);
+    for (int k = threadIdx.x; k < (int)(sizeof(T) / 4); k += kThreads) d[k] = s[k];
+}
+
+template <int R, int S>
+__global__ void __launch_bounds__(kThreads) single_tick_kernel(const __grid_constant__ SingleArgs a) {
+    extern __shared__ __align__(16) float smem[];
+    __shared__ Plan pl;
+    __shared__ svpf_ctl_t ctl;
+    __shared__ svpf_config_t cfg;
+    __shared__ SVPFParams prm;
+    __shared__ svpf_out_t out;
+    cg::cluster_group cl = cg::this_cluster();
+    const Team team{(int)cl.block_rank(), (int)cl.num_blocks()};
+    copy_words(&ctl, &a.ctl);
+    copy_words(&cfg, &a.cfg);
+    copy_words(&prm, &a.prm);
+    __syncthreads();
+    const Smem sm = carve(smem, a.n, team.size, team.rank);
+    const Noise nz{philox_key(a.seed, 0), (uint32_t)ctl.timestep, a.tape_n, a.tape_u,
+                   a.slots_n, a.slots_u, a.n, &pl.flag};
+    const FilterIO io{a.h, a.hp, a.v, a.lw, a.n};
+    run_tick<R, S>(cfg, prm, ctl, a.y_t, a.y_prev, io, nz, sm, pl, team, out);
+    if (team.rank == 0) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            *a.ctl_out = ctl;
+            *a.out = out;
+        }
+    }
+}
+
+template <int R, int S>
+static cudaError_t launch_single_t(const SingleArgs& a, int C, cudaStream_t s) {
+    const size_t smem = tick_smem_bytes(a.n, C);
+    auto kern = single_tick_kernel<R, S>;
+    static bool configured[kMaxCluster + 1] = {};
+    cudaError_t e;
+    if (!configured[0]) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn_smem());
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+        configured[0] = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C, 1, 1);
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, a);
+}
+
+}  // namespace svpf

@@ -1,0 +1,533 @@
+"""Host-side mirror of the reference's Python binding over libsvpf_b200.so.
+
+``SVPF`` keeps the method names, defaults and argument meaning of the
+reference's ``pysvpf.SVPF`` (py-torch/svpf_python.cpp:483-653): ``initialize``,
+``step``, ``run``, ``reset``, the ``set_*`` configuration calls, ``nu`` /
+``lik_offset`` properties, ``get_particles``, ``get_ess``.  ``Batch`` drives
+many independent filters with one persistent kernel launch per tick.
+
+Everything runs through the C ABI declared in include/svpf.h; there is no
+CPU path.  If the library has not been built this module raises on import of
+the library instead of falling back.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsvpf_b200.so")
+SMOOTH_MAX_LAG = 8
+
+SVPF_OK = 0
+ERRORS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "not initialized",
+          4: "noise tape too short", 5: "non-finite observation or output", 6: "unsupported"}
+
+_I, _F = C.c_int, C.c_float
+CONFIG_FIELDS = [
+    ("n_stein_steps", _I), ("nu", _F), ("student_t_implied_offset", _F), ("lik_offset", _F),
+    ("use_exact_gradient", _I), ("use_svld", _I), ("use_annealing", _I), ("use_adaptive_beta", _I),
+    ("n_anneal_steps", _I), ("temperature", _F), ("rmsprop_rho", _F), ("rmsprop_eps", _F),
+    ("use_mim", _I), ("mim_jump_prob", _F), ("mim_jump_scale", _F), ("use_local_params", _I),
+    ("delta_rho", _F), ("delta_sigma", _F), ("use_asymmetric_rho", _I), ("rho_up", _F),
+    ("rho_down", _F), ("use_newton", _I), ("use_full_newton", _I), ("use_guided", _I),
+    ("guided_alpha_base", _F), ("guided_alpha_shock", _F), ("guided_innovation_threshold", _F),
+    ("use_rejuvenation", _I), ("rejuv_ksd_threshold", _F), ("rejuv_prob", _F), ("rejuv_blend", _F),
+    ("use_guide", _I), ("use_guide_preserving", _I), ("guide_strength", _F), ("use_adaptive_guide", _I),
+    ("guide_strength_base", _F), ("guide_strength_max", _F), ("guide_innovation_threshold", _F),
+    ("use_adaptive_mu", _I), ("mu_process_var", _F), ("mu_obs_var_scale", _F), ("mu_min", _F),
+    ("mu_max", _F), ("use_adaptive_sigma", _I), ("sigma_boost_threshold", _F),
+    ("sigma_boost_max", _F), ("stein_repulsive_sign", _I), ("use_fan_mode", _I),
+    ("stein_min_steps", _I), ("stein_max_steps", _I), ("ksd_improvement_threshold", _F),
+    ("use_student_t_state", _I), ("nu_state", _F), ("use_smoothing", _I), ("smooth_lag", _I),
+    ("smooth_output_lag", _I), ("use_heun", _I),
+]
+
+
+class Config(C.Structure):
+    """svpf_config_t (include/svpf.h)."""
+    _fields_ = CONFIG_FIELDS
+
+    def to_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in CONFIG_FIELDS}
+
+    def update(self, **kw):
+        for k, v in kw.items():
+            if k not in dict(CONFIG_FIELDS):
+                raise KeyError(f"unknown configuration field {k!r}")
+            setattr(self, k, v)
+        return self
+
+
+class Params(C.Structure):
+    """SVPFParams (include/svpf.cuh:257-262 of the reference)."""
+    _fields_ = [("rho", _F), ("sigma_z", _F), ("mu", _F), ("gamma", _F)]
+
+
+class Ctl(C.Structure):
+    """svpf_ctl_t: per-filter control record."""
+    _fields_ = [
+        ("guide_mean", C.c_double), ("guide_var", C.c_double), ("guide_K", C.c_double),
+        ("loglik_sum", C.c_double), ("timestep", _I), ("guide_initialized", _I),
+        ("stein_steps_used", _I), ("smooth_head", _I), ("ksd_prev", _F), ("ksd_last", _F),
+        ("vol_prev", _F), ("h_mean_prev", _F), ("bw", _F), ("bw_sq", _F), ("return_ema", _F),
+        ("return_var", _F), ("sigma_z_effective", _F), ("mu_state", _F), ("mu_var", _F),
+        ("y_prev", _F), ("smooth_h_mean", _F * SMOOTH_MAX_LAG), ("smooth_h_var", _F * SMOOTH_MAX_LAG),
+        ("smooth_y", _F * SMOOTH_MAX_LAG), ("status", _I), ("reserved", _I),
+    ]
+
+
+class Out(C.Structure):
+    """svpf_out_t: per-tick outputs of one filter."""
+    _fields_ = [("loglik", _F), ("vol", _F), ("h_mean", _F), ("h_mean_raw", _F), ("bw", _F),
+                ("ksd", _F), ("steps_used", _I), ("rejuv_fired", _I)]
+
+
+_FP = C.POINTER(C.c_float)
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The engine library.  Raises if it is missing: there is no fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is not built (run build.py); the SVPF engine has no CPU fallback")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    sig = {
+        "svpf_create": (vp, [_I, _I, _F, vp]),
+        "svpf_destroy": (None, [vp]),
+        "svpf_initialize": (None, [vp, C.POINTER(Params), C.c_ulonglong]),
+        "svpf_step_graph": (None, [vp, _F, _F, C.POINTER(Params), _FP, _FP, _FP]),
+        "svpf_step_seeded": (None, [vp, _F, C.POINTER(Params), C.c_ulonglong, vp]),
+        "svpf_run_sequence": (None, [vp, _FP, _I, C.POINTER(Params), _FP, _FP]),
+        "svpf_get_particles": (None, [vp, _FP]),
+        "svpf_get_stats": (None, [vp, _FP, _FP]),
+        "svpf_get_ess": (_F, [vp]),
+        "svpf_get_ksd_stats": (None, [vp, _FP, C.POINTER(_I)]),
+        "svpf_graph_is_captured": (C.c_bool, [vp]),
+        "svpf_graph_invalidate": (None, [vp]),
+        "svpf_last_error": (_I, [vp]),
+        "svpf_get_config": (None, [vp, C.POINTER(Config)]),
+        "svpf_config_init": (None, [C.POINTER(Config), _I, _F]),
+        "svpf_set_config": (None, [vp, C.POINTER(Config)]),
+        "svpf_get_state": (_I, [vp, C.POINTER(Ctl), _FP, _FP, _FP, _FP]),
+        "svpf_set_state": (_I, [vp, C.POINTER(Ctl), _FP, _FP, _FP, _FP]),
+        "svpf_set_noise_tape": (_I, [vp, _FP, _I, _FP, _I]),
+        "svpf_get_last_output": (_I, [vp, C.POINTER(Out)]),
+        "svpf_set_cluster_size": (_I, [vp, _I]),
+        "svpf_batch_create": (vp, [_I, C.POINTER(_I), C.POINTER(Config), C.POINTER(Params), vp]),
+        "svpf_batch_destroy": (None, [vp]),
+        "svpf_batch_initialize": (_I, [vp, C.c_ulonglong]),
+        "svpf_batch_step": (_I, [vp, _FP, _FP, _FP, _FP, _FP]),
+        "svpf_batch_step_device": (_I, [vp, vp, vp, vp]),
+        "svpf_batch_graph_launch": (_I, [vp, vp, vp, vp]),
+        "svpf_batch_sync": (_I, [vp]),
+        "svpf_batch_n_filters": (_I, [vp]),
+        "svpf_batch_kernel_launches": (_I, [vp]),
+        "svpf_batch_get_ctl": (_I, [vp, C.POINTER(Ctl)]),
+        "svpf_batch_get_particles": (_I, [vp, _I, _FP]),
+        "svpf_batch_set_noise_tape": (_I, [vp, _FP, _I, _FP, _I]),
+        "svpf_batch_tile_of": (_I, [vp, _I, C.POINTER(_I), C.POINTER(_I)]),
+        "svpf_autotune": (_I, [C.POINTER(_I), _I, _I]),
+        "svpf_tile_choice": (_I, [_I, C.POINTER(_I), C.POINTER(_I)]),
+        "svpf_build_info": (C.c_char_p, []),
+        "svpf_debug_philox": (_I, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), _I]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(_FP)
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def default_config(n_stein_steps: int = 8, nu: float = 30.0) -> Config:
+    """The reference's svpf_create defaults (svpf_optimized_graph.cu:116-283)."""
+    c = Config()
+    lib().svpf_config_init(C.byref(c), int(n_stein_steps), float(nu))
+    return c
+
+
+def production_config(nu: float = 30.0, max_steps: int = 8) -> Config:
+    """The batched/plain production configuration used by the benchmarks:
+    svpf_create defaults plus full Newton, at most ``max_steps`` Stein
+    iterations over 3 annealing stages."""
+    return default_config(max_steps, nu).update(use_newton=1, use_full_newton=1, stein_min_steps=4,
+                                                stein_max_steps=max_steps, n_anneal_steps=3)
+
+
+@dataclass
+class SVPFResult:
+    """Mirror of pysvpf.SVPFResult."""
+    log_lik: float
+    vol_mean: float
+    vol_std: float
+    h_mean: float
+    mu_estimate: float
+
+
+class SVPF:
+    """One filter; mirror of pysvpf.SVPF (py-torch/svpf_python.cpp:57-480)."""
+
+    def __init__(self, n_particles: int = 400, n_stein: int = 8, nu: float = 30.0, stream=None):
+        self._s = lib().svpf_create(int(n_particles), int(n_stein), float(nu), stream)
+        if not self._s:
+            raise RuntimeError("Failed to create SVPF filter")
+        self._n = int(n_particles)
+        self._n_stein = int(n_stein)
+        self.params = Params(0.97, 0.15, -3.5, -0.5)
+        self._y_prev = 0.0
+        self._initialized = False
+        self.set_defaults()
+
+    def close(self):
+        if getattr(self, "_s", None):
+            lib().svpf_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- configuration -----------------------------------------------------
+    @property
+    def config(self) -> Config:
+        c = Config()
+        lib().svpf_get_config(self._s, C.byref(c))
+        return c
+
+    def configure(self, **kw) -> "SVPF":
+        c = self.config.update(**kw)
+        lib().svpf_set_config(self._s, C.byref(c))
+        return self
+
+    def _ctl(self) -> Ctl:
+        c = Ctl()
+        self._check(lib().svpf_get_state(self._s, C.byref(c), None, None, None, None))
+        return c
+
+    def _set_ctl(self, **kw):
+        c = self._ctl()
+        for k, v in kw.items():
+            setattr(c, k, v)
+        self._check(lib().svpf_set_state(self._s, C.byref(c), None, None, None, None))
+
+    def set_defaults(self):
+        """Production defaults of the reference binding (svpf_python.cpp:90-176)."""
+        self.configure(
+            nu=30.0, lik_offset=0.345, use_asymmetric_rho=1, rho_up=0.98, rho_down=0.93, use_svld=1,
+            temperature=0.45, rmsprop_rho=0.9, rmsprop_eps=1e-6, use_annealing=1, n_anneal_steps=5,
+            use_mim=1, mim_jump_prob=0.25, mim_jump_scale=9.0, use_adaptive_beta=1, use_rejuvenation=1,
+            rejuv_ksd_threshold=0.05, rejuv_prob=0.30, rejuv_blend=0.30, use_newton=1, use_full_newton=1,
+            use_exact_gradient=1, stein_min_steps=8, stein_max_steps=16, ksd_improvement_threshold=0.05,
+            use_guided=1, guided_alpha_base=0.0, guided_alpha_shock=0.40, guided_innovation_threshold=1.5,
+            use_guide=1, use_guide_preserving=1, guide_strength=0.05, use_adaptive_guide=1,
+            guide_strength_base=0.05, guide_strength_max=0.30, guide_innovation_threshold=1.0,
+            use_adaptive_mu=1, mu_process_var=0.001, mu_obs_var_scale=11.0, mu_min=-4.0, mu_max=-1.0,
+            use_adaptive_sigma=1, sigma_boost_threshold=0.95, sigma_boost_max=3.2, use_local_params=0,
+            delta_rho=0.0, delta_sigma=0.0)
+        self._set_ctl(guide_mean=0.0, guide_var=0.0, guide_K=0.0, guide_initialized=0, mu_state=-3.5,
+                      mu_var=1.0, sigma_z_effective=0.10)
+
+    def set_adaptive_mu(self, enabled=True, process_var=0.001, obs_var_scale=11.0, mu_min=-4.0, mu_max=-1.0):
+        self.configure(use_adaptive_mu=int(enabled), mu_process_var=process_var,
+                       mu_obs_var_scale=obs_var_scale, mu_min=mu_min, mu_max=mu_max)
+
+    def set_adaptive_sigma(self, enabled=True, threshold=0.95, max_boost=3.2):
+        self.configure(use_adaptive_sigma=int(enabled), sigma_boost_threshold=threshold, sigma_boost_max=max_boost)
+
+    def set_adaptive_guide(self, enabled=True, base=0.05, max=0.30, threshold=1.0):  # noqa: A002
+        self.configure(use_adaptive_guide=int(enabled), guide_strength_base=base, guide_strength_max=max,
+                       guide_innovation_threshold=threshold)
+
+    def set_asymmetric_rho(self, enabled=True, rho_up=0.98, rho_down=0.93):
+        self.configure(use_asymmetric_rho=int(enabled), rho_up=rho_up, rho_down=rho_down)
+
+    def set_mim(self, enabled=True, jump_prob=0.25, jump_scale=9.0):
+        self.configure(use_mim=int(enabled), mim_jump_prob=jump_prob, mim_jump_scale=jump_scale)
+
+    def set_svld(self, enabled=True, temperature=0.45):
+        self.configure(use_svld=int(enabled), temperature=temperature)
+
+    def set_annealing(self, enabled=True, n_steps=5):
+        self.configure(use_annealing=int(enabled), n_anneal_steps=n_steps)
+
+    def set_newton(self, enabled=True):
+        self.configure(use_newton=int(enabled))
+
+    def set_guide(self, enabled=True, strength=0.05):
+        self.configure(use_guide=int(enabled), guide_strength=strength)
+
+    def set_adaptive_beta(self, enabled=True):
+        self.configure(use_adaptive_beta=int(enabled))
+
+    def set_full_newton(self, enabled=True):
+        self.configure(use_full_newton=int(enabled))
+
+    def set_exact_gradient(self, enabled=True):
+        self.configure(use_exact_gradient=int(enabled))
+
+    def set_stein_steps(self, min_steps=8, max_steps=16, ksd_threshold=0.05):
+        self.configure(stein_min_steps=min_steps, stein_max_steps=max_steps, ksd_improvement_threshold=ksd_threshold)
+
+    def set_guided_innovation(self, alpha_base=0.0, alpha_shock=0.40, threshold=1.5):
+        self.configure(guided_alpha_base=alpha_base, guided_alpha_shock=alpha_shock,
+                       guided_innovation_threshold=threshold)
+
+    def set_rejuvenation(self, enabled=True, ksd_threshold=0.05, prob=0.30, blend=0.30):
+        self.configure(use_rejuvenation=int(enabled), rejuv_ksd_threshold=ksd_threshold, rejuv_prob=prob,
+                       rejuv_blend=blend)
+
+    def set_params(self, rho, sigma_z, mu, gamma):
+        self.params = Params(rho, sigma_z, mu, gamma)
+        self.invalidate_graph()
+
+    @property
+    def nu(self) -> float:
+        return self.config.nu
+
+    @nu.setter
+    def nu(self, value: float):
+        # the reference setter recomputes only the normaliser; the implied
+        # offset stays at its create-time value (svpf_python.cpp:259-266)
+        self.configure(nu=float(value))
+
+    @property
+    def lik_offset(self) -> float:
+        return self.config.lik_offset
+
+    @lik_offset.setter
+    def lik_offset(self, value: float):
+        self.configure(lik_offset=float(value))
+
+    @property
+    def n_particles(self) -> int:
+        return self._n
+
+    @property
+    def n_stein_steps(self) -> int:
+        return self._n_stein
+
+    # -- core ----------------------------------------------------------------
+    def _check(self, rc: int):
+        if rc != SVPF_OK:
+            raise RuntimeError(f"svpf error {rc}: {ERRORS.get(rc, '?')}")
+
+    def initialize(self, rho=0.97, sigma_z=0.15, mu=-3.5, gamma=-0.5, seed=42):
+        self.params = Params(rho, sigma_z, mu, gamma)
+        lib().svpf_initialize(self._s, C.byref(self.params), int(seed))
+        self._check(lib().svpf_last_error(self._s))
+        if self.config.use_adaptive_mu:
+            self._set_ctl(mu_state=mu, mu_var=0.01)
+        self._y_prev = 0.0
+        self._initialized = True
+
+    def step(self, y_t: float) -> SVPFResult:
+        if not self._initialized:
+            raise RuntimeError("Filter not initialized. Call initialize() first.")
+        ll, vol, hm = C.c_float(), C.c_float(), C.c_float()
+        lib().svpf_step_graph(self._s, float(y_t), float(self._y_prev), C.byref(self.params),
+                              C.byref(ll), C.byref(vol), C.byref(hm))
+        rc = lib().svpf_last_error(self._s)
+        if rc not in (SVPF_OK, 5):
+            self._check(rc)
+        self._y_prev = float(y_t)
+        mu_est = self._ctl().mu_state if self.config.use_adaptive_mu else self.params.mu
+        return SVPFResult(ll.value, vol.value, 0.0, hm.value, mu_est)
+
+    def run(self, observations):
+        if not self._initialized:
+            raise RuntimeError("Filter not initialized. Call initialize() first.")
+        obs = _f32(observations)
+        if obs.ndim != 1:
+            raise RuntimeError("Observations must be 1-dimensional")
+        T = obs.shape[0]
+        vol, hm, ll = (np.empty(T, np.float32) for _ in range(3))
+        p = C.byref(self.params)
+        for t in range(T):
+            a, b, c = C.c_float(), C.c_float(), C.c_float()
+            lib().svpf_step_graph(self._s, float(obs[t]), float(self._y_prev), p, C.byref(a), C.byref(b), C.byref(c))
+            ll[t], vol[t], hm[t] = a.value, b.value, c.value
+            self._y_prev = float(obs[t])
+        return vol, hm, ll
+
+    def reset(self, seed=42):
+        lib().svpf_initialize(self._s, C.byref(self.params), int(seed))
+        if self.config.use_adaptive_mu:
+            self._set_ctl(mu_state=self.params.mu, mu_var=0.01)
+        self._y_prev = 0.0
+
+    def get_particles(self) -> np.ndarray:
+        out = np.empty(self._n, np.float32)
+        lib().svpf_get_particles(self._s, _fp(out))
+        return out
+
+    def get_ess(self) -> float:
+        return float(lib().svpf_get_ess(self._s))
+
+    def invalidate_graph(self):
+        lib().svpf_graph_invalidate(self._s)
+
+    def is_graph_captured(self) -> bool:
+        return bool(lib().svpf_graph_is_captured(self._s))
+
+    # -- engine extras (no reference counterpart) ------------------------------
+    def last_error(self) -> int:
+        return int(lib().svpf_last_error(self._s))
+
+    def last_output(self) -> Out:
+        o = Out()
+        self._check(lib().svpf_get_last_output(self._s, C.byref(o)))
+        return o
+
+    def get_state(self):
+        ctl = Ctl()
+        h, hp, v, lw = (np.empty(self._n, np.float32) for _ in range(4))
+        self._check(lib().svpf_get_state(self._s, C.byref(ctl), _fp(h), _fp(hp), _fp(v), _fp(lw)))
+        return ctl, h, hp, v, lw
+
+    def set_state(self, ctl: Ctl, h, hp, v, lw):
+        arrs = [_f32(a) for a in (h, hp, v, lw)]
+        self._check(lib().svpf_set_state(self._s, C.byref(ctl), *[_fp(a) for a in arrs]))
+
+    def set_noise_tape(self, normals=None, uniforms=None):
+        if normals is None:
+            self._check(lib().svpf_set_noise_tape(self._s, None, 0, None, 0))
+            return
+        self._tape = (_f32(normals), _f32(uniforms))
+        nrm, uni = self._tape
+        self._check(lib().svpf_set_noise_tape(self._s, _fp(nrm), nrm.shape[0], _fp(uni), uni.shape[0]))
+
+    def set_cluster_size(self, ctas: int):
+        self._check(lib().svpf_set_cluster_size(self._s, int(ctas)))
+
+    def step_raw(self, y_t: float, y_prev: float):
+        """One svpf_step_graph call with explicit y_prev; returns the full outputs."""
+        lib().svpf_step_graph(self._s, float(y_t), float(y_prev), C.byref(self.params), None, None, None)
+        rc = lib().svpf_last_error(self._s)
+        return rc, self.last_output()
+
+
+class Batch:
+    """Many independent filters; one persistent kernel launch per tick."""
+
+    def __init__(self, ns, configs, params, stream=None):
+        ns = np.ascontiguousarray(ns, dtype=np.int32)
+        F = int(ns.shape[0])
+        if isinstance(configs, Config):
+            configs = [configs] * F
+        if isinstance(params, Params):
+            params = [params] * F
+        self._cfgs = (Config * F)(*configs)
+        self._prms = (Params * F)(*params)
+        self._ns = ns
+        self._b = lib().svpf_batch_create(F, ns.ctypes.data_as(C.POINTER(_I)), self._cfgs, self._prms, stream)
+        if not self._b:
+            raise RuntimeError("svpf_batch_create failed")
+        self.F = F
+
+    def close(self):
+        if getattr(self, "_b", None):
+            lib().svpf_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != SVPF_OK:
+            raise RuntimeError(f"svpf batch error {rc}: {ERRORS.get(rc, '?')}")
+
+    def initialize(self, seed: int = 0):
+        self._check(lib().svpf_batch_initialize(self._b, int(seed)))
+
+    def step(self, y_t, y_prev):
+        """One tick from host observations; returns host (loglik, vol, h_mean)."""
+        yt, yp = _f32(y_t), _f32(y_prev)
+        ll, vol, hm = (np.empty(self.F, np.float32) for _ in range(3))
+        self._check(lib().svpf_batch_step(self._b, _fp(yt), _fp(yp), _fp(ll), _fp(vol), _fp(hm)))
+        return ll, vol, hm
+
+    def step_device(self, d_y_t: int, d_y_prev: int, d_out: int | None = None):
+        """One tick from device pointers (asynchronous)."""
+        self._check(lib().svpf_batch_step_device(self._b, d_y_t, d_y_prev, d_out))
+
+    def graph_launch(self, d_y_t: int, d_y_prev: int, d_out: int | None = None):
+        self._check(lib().svpf_batch_graph_launch(self._b, d_y_t, d_y_prev, d_out))
+
+    def sync(self):
+        self._check(lib().svpf_batch_sync(self._b))
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(lib().svpf_batch_kernel_launches(self._b))
+
+    def ctl(self):
+        arr = (Ctl * self.F)()
+        self._check(lib().svpf_batch_get_ctl(self._b, arr))
+        return arr
+
+    def get_particles(self, f: int) -> np.ndarray:
+        out = np.empty(int(self._ns[f]), np.float32)
+        self._check(lib().svpf_batch_get_particles(self._b, int(f), _fp(out)))
+        return out
+
+    def set_noise_tape(self, normals=None, uniforms=None):
+        if normals is None:
+            self._check(lib().svpf_batch_set_noise_tape(self._b, None, 0, None, 0))
+            return
+        self._tape = (_f32(normals), _f32(uniforms))
+        nrm, uni = self._tape
+        self._check(lib().svpf_batch_set_noise_tape(self._b, _fp(nrm), nrm.shape[0], _fp(uni), uni.shape[0]))
+
+    def tile_of(self, n: int):
+        r, s = C.c_int(), C.c_int()
+        lib().svpf_batch_tile_of(self._b, int(n), C.byref(r), C.byref(s))
+        return r.value, s.value
+
+
+def autotune(ns, ticks: int = 2):
+    arr = np.ascontiguousarray(sorted(set(int(n) for n in ns)), dtype=np.int32)
+    rc = lib().svpf_autotune(arr.ctypes.data_as(C.POINTER(_I)), int(arr.shape[0]), int(ticks))
+    if rc != SVPF_OK:
+        raise RuntimeError(f"autotune failed: {ERRORS.get(rc, rc)}")
+    out = {}
+    for n in arr:
+        r, s = C.c_int(), C.c_int()
+        lib().svpf_tile_choice(int(n), C.byref(r), C.byref(s))
+        out[int(n)] = (r.value, s.value)
+    return out
+
+
+def philox(k0: int, k1: int, counters: np.ndarray) -> np.ndarray:
+    """Philox4x32-10 blocks computed on the GPU (for bit-exact checks)."""
+    ctr = np.ascontiguousarray(counters, dtype=np.uint32).reshape(-1, 4)
+    out = np.empty_like(ctr)
+    rc = lib().svpf_debug_philox(k0, k1, ctr.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                 out.ctypes.data_as(C.POINTER(C.c_uint32)), ctr.shape[0])
+    if rc != SVPF_OK:
+        raise RuntimeError(f"philox failed: {ERRORS.get(rc, rc)}")
+    return out
+
+
+def build_info() -> str:
+    return lib().svpf_build_info().decode()

@@ -1,0 +1,305 @@
+"""Oracle bindings -- TEST INFRASTRUCTURE ONLY.
+
+ctypes access to
+  * ``liboracle_svpf.so``: the CPU restatement of one SVPF tick (FP64 oracle,
+    FP32 CPU baseline), built from ``svpf_oracle.cpp``;
+  * ``_ref/libsvpf_ref_tape.so`` / ``_ref/libsvpf_ref_stock.so``: the
+    reference's own CUDA step compiled in place (see ``Makefile``), driven
+    through ``ref_harness.cu``.
+
+Only ``tests/``, the smoke check and the CPU-baseline leg of ``bench.py`` use
+this module.  The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SMOOTH_MAX_LAG = 8
+
+CONFIG_FIELDS = [
+    ("n_stein_steps", C.c_int), ("nu", C.c_float), ("student_t_implied_offset", C.c_float),
+    ("lik_offset", C.c_float), ("use_exact_gradient", C.c_int), ("use_svld", C.c_int),
+    ("use_annealing", C.c_int), ("use_adaptive_beta", C.c_int), ("n_anneal_steps", C.c_int),
+    ("temperature", C.c_float), ("rmsprop_rho", C.c_float), ("rmsprop_eps", C.c_float),
+    ("use_mim", C.c_int), ("mim_jump_prob", C.c_float), ("mim_jump_scale", C.c_float),
+    ("use_local_params", C.c_int), ("delta_rho", C.c_float), ("delta_sigma", C.c_float),
+    ("use_asymmetric_rho", C.c_int), ("rho_up", C.c_float), ("rho_down", C.c_float),
+    ("use_newton", C.c_int), ("use_full_newton", C.c_int), ("use_guided", C.c_int),
+    ("guided_alpha_base", C.c_float), ("guided_alpha_shock", C.c_float),
+    ("guided_innovation_threshold", C.c_float), ("use_rejuvenation", C.c_int),
+    ("rejuv_ksd_threshold", C.c_float), ("rejuv_prob", C.c_float), ("rejuv_blend", C.c_float),
+    ("use_guide", C.c_int), ("use_guide_preserving", C.c_int), ("guide_strength", C.c_float),
+    ("use_adaptive_guide", C.c_int), ("guide_strength_base", C.c_float),
+    ("guide_strength_max", C.c_float), ("guide_innovation_threshold", C.c_float),
+    ("use_adaptive_mu", C.c_int), ("mu_process_var", C.c_float), ("mu_obs_var_scale", C.c_float),
+    ("mu_min", C.c_float), ("mu_max", C.c_float), ("use_adaptive_sigma", C.c_int),
+    ("sigma_boost_threshold", C.c_float), ("sigma_boost_max", C.c_float),
+    ("stein_repulsive_sign", C.c_int), ("use_fan_mode", C.c_int), ("stein_min_steps", C.c_int),
+    ("stein_max_steps", C.c_int), ("ksd_improvement_threshold", C.c_float),
+    ("use_student_t_state", C.c_int), ("nu_state", C.c_float), ("use_smoothing", C.c_int),
+    ("smooth_lag", C.c_int), ("smooth_output_lag", C.c_int), ("use_heun", C.c_int),
+]
+
+
+class OracleConfig(C.Structure):
+    _fields_ = CONFIG_FIELDS
+
+
+class OracleParams(C.Structure):
+    _fields_ = [("rho", C.c_float), ("sigma_z", C.c_float), ("mu", C.c_float), ("gamma", C.c_float)]
+
+
+class OracleCtl(C.Structure):
+    _fields_ = [
+        ("guide_mean", C.c_double), ("guide_var", C.c_double), ("guide_K", C.c_double),
+        ("loglik_sum", C.c_double), ("timestep", C.c_int), ("guide_initialized", C.c_int),
+        ("stein_steps_used", C.c_int), ("smooth_head", C.c_int), ("ksd_prev", C.c_float),
+        ("ksd_last", C.c_float), ("vol_prev", C.c_float), ("h_mean_prev", C.c_float),
+        ("bw", C.c_float), ("bw_sq", C.c_float), ("return_ema", C.c_float),
+        ("return_var", C.c_float), ("sigma_z_effective", C.c_float), ("mu_state", C.c_float),
+        ("mu_var", C.c_float), ("y_prev", C.c_float),
+        ("smooth_h_mean", C.c_float * SMOOTH_MAX_LAG), ("smooth_h_var", C.c_float * SMOOTH_MAX_LAG),
+        ("smooth_y", C.c_float * SMOOTH_MAX_LAG), ("status", C.c_int), ("reserved", C.c_int),
+    ]
+
+
+class OracleOut(C.Structure):
+    _fields_ = [("loglik", C.c_float), ("vol", C.c_float), ("h_mean", C.c_float),
+                ("h_mean_raw", C.c_float), ("bw", C.c_float), ("ksd", C.c_float),
+                ("steps_used", C.c_int), ("rejuv_fired", C.c_int)]
+
+
+class OracleNoise(C.Structure):
+    _fields_ = [("mode", C.c_int), ("n_normal_slots", C.c_int), ("n_uniform_slots", C.c_int),
+                ("filter_id", C.c_int), ("normals", C.POINTER(C.c_float)),
+                ("uniforms", C.POINTER(C.c_float)), ("seed", C.c_uint64), ("tick", C.c_uint64)]
+
+
+CTL_SCALARS = [f for f, _ in OracleCtl._fields_ if f not in ("smooth_h_mean", "smooth_h_var", "smooth_y")]
+
+
+def ctl_to_dict(c) -> dict:
+    d = {f: getattr(c, f) for f in CTL_SCALARS}
+    for f in ("smooth_h_mean", "smooth_h_var", "smooth_y"):
+        d[f] = list(getattr(c, f))
+    return d
+
+
+def ctl_from_dict(d: dict, cls=None):
+    c = (cls or OracleCtl)()
+    for f in CTL_SCALARS:
+        if f in d:
+            setattr(c, f, type(getattr(c, f))(d[f]))
+    for f in ("smooth_h_mean", "smooth_h_var", "smooth_y"):
+        if f in d:
+            arr = getattr(c, f)
+            for i, v in enumerate(d[f]):
+                arr[i] = v
+    return c
+
+
+def config_to_dict(c) -> dict:
+    return {f: getattr(c, f) for f, _ in CONFIG_FIELDS}
+
+
+def config_from_dict(d: dict, cls=None):
+    c = (cls or OracleConfig)()
+    for f, _ in CONFIG_FIELDS:
+        setattr(c, f, d[f])
+    return c
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _fptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def build(quiet: bool = True) -> None:
+    """Compile the oracle (and, where the reference tree exists, the reference build)."""
+    out = subprocess.DEVNULL if quiet else None
+    subprocess.run(["make", "-C", HERE, "all"], check=True, stdout=out)
+    if os.path.isdir("/root/reference/src"):
+        subprocess.run(["make", "-C", HERE, "ref"], check=True, stdout=out)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle_svpf.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        L.svpf_oracle_tick.restype = C.c_int
+        L.svpf_oracle_tick.argtypes = [C.POINTER(OracleConfig), C.POINTER(OracleParams),
+                                       C.POINTER(OracleCtl), C.c_int] + [C.POINTER(C.c_double)] * 4 + [
+            C.c_float, C.c_float, C.POINTER(OracleNoise), C.POINTER(OracleOut), C.c_int]
+        L.svpf_oracle_initialize.restype = C.c_int
+        L.svpf_oracle_initialize.argtypes = [C.POINTER(OracleConfig), C.POINTER(OracleParams),
+                                             C.POINTER(OracleCtl), C.c_int] + [C.POINTER(C.c_double)] * 3 + [
+            C.POINTER(C.c_float), C.c_uint64, C.c_int]
+        L.svpf_oracle_ctl_defaults.argtypes = [C.POINTER(OracleCtl)]
+        L.svpf_oracle_config_defaults.argtypes = [C.POINTER(OracleConfig), C.c_int, C.c_float]
+        L.svpf_oracle_philox.argtypes = [C.c_uint32] * 6 + [C.POINTER(C.c_uint32)]
+        L.svpf_oracle_batch_tick_f32.restype = C.c_int
+        L.svpf_oracle_batch_tick_f32.argtypes = [
+            C.c_int, C.POINTER(OracleConfig), C.POINTER(OracleParams), C.POINTER(OracleCtl),
+            C.POINTER(C.c_int), C.c_int] + [C.POINTER(C.c_float)] * 6 + [
+            C.c_uint64, C.c_uint64, C.c_int, C.POINTER(OracleOut)]
+        _lib = L
+    return _lib
+
+
+def default_config(n_stein_steps: int = 8, nu: float = 30.0) -> OracleConfig:
+    c = OracleConfig()
+    lib().svpf_oracle_config_defaults(C.byref(c), n_stein_steps, nu)
+    return c
+
+
+def default_ctl() -> OracleCtl:
+    c = OracleCtl()
+    lib().svpf_oracle_ctl_defaults(C.byref(c))
+    return c
+
+
+def philox(k0, k1, c0, c1, c2, c3):
+    out = (C.c_uint32 * 4)()
+    lib().svpf_oracle_philox(k0, k1, c0, c1, c2, c3, out)
+    return list(out)
+
+
+class OracleFilter:
+    """One filter driven by the oracle, state in float64 numpy arrays."""
+
+    def __init__(self, n: int, cfg: OracleConfig, params: OracleParams, precision: int = 0):
+        self.n = n
+        self.cfg = cfg
+        self.params = params
+        self.ctl = default_ctl()
+        self.h = np.zeros(n)
+        self.h_prev = np.zeros(n)
+        self.v = np.zeros(n)
+        self.log_w = np.zeros(n)
+        self.precision = precision
+
+    def initialize(self, init_normals=None, seed: int = 0, filter_id: int = 0):
+        ptr = _fptr(np.ascontiguousarray(init_normals, np.float32)) if init_normals is not None else None
+        keep = np.ascontiguousarray(init_normals, np.float32) if init_normals is not None else None
+        rc = lib().svpf_oracle_initialize(C.byref(self.cfg), C.byref(self.params), C.byref(self.ctl),
+                                          self.n, _dptr(self.h), _dptr(self.h_prev), _dptr(self.v),
+                                          _fptr(keep) if keep is not None else ptr, seed, filter_id)
+        assert rc == 0, rc
+
+    def step(self, y_t, y_prev, normals=None, uniforms=None, seed=0, tick=0, filter_id=0):
+        nz = OracleNoise()
+        keep = []
+        if normals is not None:
+            nrm = np.ascontiguousarray(normals, np.float32)
+            uni = np.ascontiguousarray(uniforms, np.float32)
+            keep += [nrm, uni]
+            nz.mode = 0
+            nz.n_normal_slots = nrm.shape[0]
+            nz.n_uniform_slots = uni.shape[0]
+            nz.normals = _fptr(nrm)
+            nz.uniforms = _fptr(uni)
+        else:
+            nz.mode = 1
+        nz.seed = seed
+        nz.tick = tick
+        nz.filter_id = filter_id
+        out = OracleOut()
+        rc = lib().svpf_oracle_tick(C.byref(self.cfg), C.byref(self.params), C.byref(self.ctl), self.n,
+                                    _dptr(self.h), _dptr(self.h_prev), _dptr(self.v), _dptr(self.log_w),
+                                    float(y_t), float(y_prev), C.byref(nz), C.byref(out), self.precision)
+        if rc != 0:
+            raise RuntimeError(f"oracle tick failed rc={rc}")
+        return out
+
+
+# ---------------------------------------------------------------------------
+# Reference CUDA step (GPU only)
+# ---------------------------------------------------------------------------
+class RefLib:
+    def __init__(self, kind: str = "tape"):
+        path = os.path.join(HERE, "_ref", f"libsvpf_ref_{kind}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        L = C.CDLL(path)
+        L.svpf_ref_create.restype = C.c_void_p
+        L.svpf_ref_create.argtypes = [C.c_int, C.c_int, C.c_float]
+        L.svpf_ref_destroy.argtypes = [C.c_void_p]
+        L.svpf_ref_apply_config.argtypes = [C.c_void_p, C.POINTER(OracleConfig)]
+        L.svpf_ref_read_config.argtypes = [C.c_void_p, C.POINTER(OracleConfig)]
+        L.svpf_ref_initialize.restype = C.c_int
+        L.svpf_ref_initialize.argtypes = [C.c_void_p, C.POINTER(OracleParams), C.POINTER(C.c_float)]
+        L.svpf_ref_set_state.restype = C.c_int
+        L.svpf_ref_set_state.argtypes = [C.c_void_p, C.POINTER(OracleCtl)] + [C.POINTER(C.c_double)] * 4
+        L.svpf_ref_get_state.restype = C.c_int
+        L.svpf_ref_get_state.argtypes = [C.c_void_p, C.POINTER(OracleCtl)] + [C.POINTER(C.c_double)] * 4
+        L.svpf_ref_step.restype = C.c_int
+        L.svpf_ref_step.argtypes = [C.c_void_p, C.c_float, C.c_float, C.POINTER(OracleParams),
+                                    C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_float), C.c_int,
+                                    C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.svpf_ref_time_steps.restype = C.c_int
+        L.svpf_ref_time_steps.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int,
+                                          C.POINTER(OracleParams), C.POINTER(C.c_float)]
+        self.L = L
+
+
+class RefFilter:
+    """The reference's svpf_step_graph on one filter, via the harness."""
+
+    def __init__(self, reflib: RefLib, n: int, n_stein: int, nu: float):
+        self.L = reflib.L
+        self.n = n
+        self.s = self.L.svpf_ref_create(n, n_stein, nu)
+        if not self.s:
+            raise RuntimeError("svpf_create failed")
+
+    def close(self):
+        if self.s:
+            self.L.svpf_ref_destroy(self.s)
+            self.s = None
+
+    def read_config(self) -> OracleConfig:
+        c = OracleConfig()
+        self.L.svpf_ref_read_config(self.s, C.byref(c))
+        return c
+
+    def apply_config(self, cfg: OracleConfig):
+        self.L.svpf_ref_apply_config(self.s, C.byref(cfg))
+
+    def initialize(self, params: OracleParams, init_normals):
+        z = np.ascontiguousarray(init_normals, np.float32)
+        return self.L.svpf_ref_initialize(self.s, C.byref(params), _fptr(z))
+
+    def get_state(self):
+        ctl = OracleCtl()
+        h, hp, v, lw = (np.zeros(self.n) for _ in range(4))
+        rc = self.L.svpf_ref_get_state(self.s, C.byref(ctl), _dptr(h), _dptr(hp), _dptr(v), _dptr(lw))
+        assert rc == 0, rc
+        return ctl, h, hp, v, lw
+
+    def set_state(self, ctl, h, hp, v, lw):
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (h, hp, v, lw)]
+        rc = self.L.svpf_ref_set_state(self.s, C.byref(ctl), *[_dptr(a) for a in arrs])
+        assert rc == 0, rc
+
+    def step(self, y_t, y_prev, params, normals, uniforms):
+        nrm = np.ascontiguousarray(normals, np.float32)
+        uni = np.ascontiguousarray(uniforms, np.float32)
+        ll, vol, hm = C.c_float(), C.c_float(), C.c_float()
+        flags = self.L.svpf_ref_step(self.s, float(y_t), float(y_prev), C.byref(params),
+                                     _fptr(nrm), nrm.shape[0], _fptr(uni), uni.shape[0],
+                                     C.byref(ll), C.byref(vol), C.byref(hm))
+        return flags, ll.value, vol.value, hm.value

@@ -1,0 +1,763 @@
+/*
+ * svpf_oracle.cpp -- TEST INFRASTRUCTURE ONLY (the oracle).
+ *
+ * Plain CPU restatement of one SVPF tick of the reference, written for
+ * clarity, not speed: every stage is a direct O(N) or O(N^2) loop in index
+ * order.  R = double is the FP64 oracle; R = float is the FP32 CPU baseline.
+ * Each function cites the reference file:line whose behaviour it restates.
+ *
+ * Not linked into, imported by, or called from the product library.
+ */
+#include "svpf_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+/* ------------------------------------------------------------------------ */
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11, "Parallel random        */
+/* numbers: as easy as 1, 2, 3").  Written from the paper's round function.  */
+/* ------------------------------------------------------------------------ */
+struct Block { uint32_t v[4]; };
+
+Block philox(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)M0 * c0;
+        uint64_t p1 = (uint64_t)M1 * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0;
+        uint32_t n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+        k0 += W0; k1 += W1;
+    }
+    return Block{{c0, c1, c2, c3}};
+}
+
+/* Project RNG convention (also implemented, independently, on the GPU):
+ * key  = (seed_lo, seed_hi + 0x9E3779B9 * filter)
+ * ctr  = (particle, draw index, tick_lo, stream) with stream 0 = normals,
+ *        1 = uniforms, 2 = initial draw.
+ * normal  = sqrt(-2 ln u1) cos(2 pi u2), u1 = (x0>>8 + 1) 2^-24, u2 = (x1>>8) 2^-24
+ * uniform = (x0>>8 + 1) 2^-24  in (0, 1]                                      */
+struct PhiloxKey { uint32_t k0, k1; };
+PhiloxKey make_key(uint64_t seed, int filter) {
+    return PhiloxKey{(uint32_t)seed, (uint32_t)(seed >> 32) + 0x9E3779B9u * (uint32_t)filter};
+}
+template <typename R>
+R philox_normal(PhiloxKey k, uint32_t particle, uint32_t draw, uint32_t tick, uint32_t stream) {
+    Block b = philox(k.k0, k.k1, particle, draw, tick, stream);
+    R u1 = (R)((b.v[0] >> 8) + 1u) * (R)(1.0 / 16777216.0);
+    R u2 = (R)(b.v[1] >> 8) * (R)(1.0 / 16777216.0);
+    return std::sqrt((R)-2 * std::log(u1)) * std::cos((R)(2.0 * kPi) * u2);
+}
+template <typename R>
+R philox_uniform(PhiloxKey k, uint32_t particle, uint32_t draw, uint32_t tick, uint32_t stream) {
+    Block b = philox(k.k0, k.k1, particle, draw, tick, stream);
+    return (R)((b.v[0] >> 8) + 1u) * (R)(1.0 / 16777216.0);
+}
+
+/* Noise source with one normal counter and one uniform counter per tick.  The
+ * draw order per particle matches the reference's curand call order:
+ * predict normal(s) then predict uniform (svpf_opt_kernels.cu:187-193), one
+ * normal per Stein transport (:594 etc.), rejuvenation uniform then normal
+ * (:1261-1265). */
+template <typename R>
+struct Noise {
+    const oracle_noise* src;
+    PhiloxKey key;
+    int n;
+    int bad = 0;
+    Noise(const oracle_noise* s, int n_) : src(s), n(n_) {
+        key = make_key(s->seed, s->filter_id);
+    }
+    R normal(int i, int k) {
+        if (src->mode == 0) {
+            if (k >= src->n_normal_slots) { bad = 1; return 0; }
+            return (R)src->normals[(size_t)k * n + i];
+        }
+        return philox_normal<R>(key, (uint32_t)i, (uint32_t)k, (uint32_t)src->tick, 0u);
+    }
+    R uniform(int i, int k) {
+        if (src->mode == 0) {
+            if (k >= src->n_uniform_slots) { bad = 1; return 1; }
+            return (R)src->uniforms[(size_t)k * n + i];
+        }
+        return philox_uniform<R>(key, (uint32_t)i, (uint32_t)k, (uint32_t)src->tick, 1u);
+    }
+};
+
+template <typename R> R clampv(R x, R lo, R hi) { return std::min(std::max(x, lo), hi); }
+/* clamp_logvol, svpf_opt_kernels.cu:20-22 */
+template <typename R> R clamp_h(R h) { return clampv<R>(h, (R)-15, (R)5); }
+/* safe_exp, svpf_opt_kernels.cu:24-26 */
+template <typename R> R safe_exp(R x) { return std::exp(std::min(x, (R)20)); }
+
+/* Student-t state noise, svpf_opt_kernels.cu:31-53.  Returns draws used. */
+template <typename R>
+R student_t_noise(Noise<R>& nz, int i, int& kn, R nu_state) {
+    if (nu_state > (R)30) return nz.normal(i, kn++);
+    R z = nz.normal(i, kn++);
+    int nu_int = std::max((int)(nu_state + (R)0.5), 3);
+    R chi2 = 0;
+    for (int m = 0; m < nu_int; ++m) { R u = nz.normal(i, kn++); chi2 += u * u; }
+    return z * std::sqrt((R)nu_int / (chi2 + (R)1e-8));
+}
+
+template <typename R>
+struct Tick {
+    const oracle_config& c;
+    const oracle_params& p;
+    oracle_ctl& s;
+    int n;
+    std::vector<R> h, hp, v, lw, g, curv, precond, ksd_part;
+    R y_t, y_prev;
+
+    Tick(const oracle_config& c_, const oracle_params& p_, oracle_ctl& s_, int n_)
+        : c(c_), p(p_), s(s_), n(n_) {}
+
+    /* Student-t normaliser, svpf_optimized_graph.cu:951-953 */
+    R student_t_const() const {
+        R nu = (R)c.nu;
+        return std::lgamma((nu + 1) / 2) - std::lgamma(nu / 2) - (R)0.5 * std::log((R)kPi * nu);
+    }
+    /* student_t_implied_offset is fixed when the filter is created
+     * (svpf_optimized_graph.cu:127-138) and read from the state afterwards. */
+    R implied_offset() const { return (R)c.student_t_implied_offset; }
+
+    /* EKF guide update, include/svpf_kernels.cuh:509-541 (FP64 here). */
+    void ekf(R mu, R rho, R sigma_z, R offset) {
+        double m = s.guide_mean, P = s.guide_var;
+        if (!s.guide_initialized) {
+            m = (double)mu;
+            P = (double)sigma_z * (double)sigma_z / (1.0 - (double)rho * (double)rho);
+            s.guide_initialized = 1;
+        }
+        double m_pred = (double)mu + (double)rho * (m - (double)mu);
+        double P_pred = (double)rho * (double)rho * P + (double)sigma_z * (double)sigma_z;
+        double log_y2 = std::log((double)y_t * (double)y_t + 1e-8);
+        double Rn = 4.93 + 2.0;
+        double S = P_pred + Rn;
+        double K = P_pred / (S + 1e-8);
+        double innov = log_y2 - (m_pred - (double)offset);
+        s.guide_mean = m_pred + K * innov;
+        s.guide_var = (1.0 - K) * P_pred;
+        s.guide_K = K;
+    }
+
+    /* svpf_fused_bandwidth_kernel, svpf_opt_kernels.cu:1159-1235 */
+    void bandwidth() {
+        R sum = 0, sum2 = 0, mn = (R)1e10, mx = (R)-1e10;
+        for (int i = 0; i < n; ++i) {
+            sum += h[i]; sum2 += h[i] * h[i];
+            mn = std::min(mn, h[i]); mx = std::max(mx, h[i]);
+        }
+        R mean = sum / (R)n;
+        R var = sum2 / (R)n - mean * mean;
+        R spread = mx - mn;
+        R bw2_new = std::max((R)2 * var / std::log((R)n + 1), (R)1e-6);
+        R bw2_prev = (R)s.bw_sq;
+        R bw2 = bw2_prev > 0 ? (R)0.3 * bw2_new + (R)0.7 * bw2_prev : bw2_new;
+        R a = std::fabs(y_t);
+        R ema = (R)s.return_ema, rv = (R)s.return_var;
+        ema = ema > 0 ? (R)0.05 * a + (R)0.95 * ema : a;
+        rv = rv > 0 ? (R)0.05 * a * a + (R)0.95 * rv : a * a;
+        s.return_ema = (float)ema;
+        s.return_var = (float)rv;
+        R ratio = a / std::max(ema, (R)1e-8);
+        R spread_f = std::min(spread * (R)0.5, (R)2);
+        R comb = std::max(ratio, spread_f);
+        R scale = clampv<R>((R)1 - (R)0.25 * std::min(comb - 1, (R)2), (R)0.5, (R)1);
+        bw2 *= scale;
+        R bw = clampv<R>(std::sqrt(bw2), (R)0.01, (R)2);
+        s.bw_sq = (float)bw2;
+        s.bw = (float)bw;
+    }
+
+    /* svpf_fused_gradient_kernel, svpf_opt_kernels.cu:354-521 */
+    void gradient(R beta, R rho, R sigma_z, R mu, R stc) {
+        R lev_num = (R)p.gamma * y_prev;
+        std::vector<R> mu_k(n);
+        for (int k = 0; k < n; ++k) {
+            R volk = std::exp(hp[k] * (R)0.5);
+            mu_k[k] = mu + rho * (hp[k] - mu) + lev_num / (volk + (R)1e-8);
+        }
+        R s2 = sigma_z * sigma_z;
+        R nu = (R)c.nu;
+        for (int j = 0; j < n; ++j) {
+            R hj = h[j];
+            R grad_prior, hess_prior;
+            if (c.use_student_t_state) {
+                /* :406-447 */
+                R nus = (R)c.nu_state, nus2 = nus * s2, np1 = nus + 1;
+                R lmax = (R)-1e10;
+                for (int k = 0; k < n; ++k) {
+                    R d = hj - mu_k[k];
+                    lmax = std::max(lmax, -(R)0.5 * np1 * std::log(1 + d * d / nus2));
+                }
+                R sr = 0, wg = 0, wh = 0;
+                for (int k = 0; k < n; ++k) {
+                    R d = hj - mu_k[k], d2 = d * d, den = nus2 + d2;
+                    R r = std::exp(-(R)0.5 * np1 * std::log(1 + d2 / nus2) - lmax);
+                    sr += r;
+                    wg -= r * np1 * d / den;
+                    wh += r * (-np1 * (nus2 - d2) / (den * den));
+                }
+                grad_prior = wg / (sr + (R)1e-8);
+                hess_prior = wh / (sr + (R)1e-8);
+            } else {
+                /* :449-473 */
+                R inv2 = (R)0.5 / s2, inv = (R)1 / s2;
+                R lmax = (R)-1e10;
+                for (int k = 0; k < n; ++k) {
+                    R d = hj - mu_k[k];
+                    lmax = std::max(lmax, -d * d * inv2);
+                }
+                R sr = 0, wg = 0;
+                for (int k = 0; k < n; ++k) {
+                    R d = hj - mu_k[k];
+                    R r = std::exp(-d * d * inv2 - lmax);
+                    sr += r;
+                    wg -= r * d * inv;
+                }
+                grad_prior = wg / (sr + (R)1e-8);
+                hess_prior = -inv;
+            }
+            /* likelihood, :475-499 */
+            R vol = safe_exp(hj);
+            R y2 = y_t * y_t;
+            R A = y2 / (vol + (R)1e-8) / nu;
+            R opA = 1 + A;
+            if (c.use_fan_mode) lw[j] = 0;
+            else lw[j] = stc - (R)0.5 * hj - (nu + 1) * (R)0.5 * std::log1p(std::max(A, (R)-0.999));
+            R glik;
+            if (c.use_exact_gradient) glik = (R)-0.5 + (R)0.5 * (nu + 1) * A / opA - (R)c.lik_offset;
+            else glik = (std::log(y2 + (R)1e-10) - hj + (R)c.lik_offset) / (R)1.4;
+            /* combine, :504-507 */
+            R eb = c.use_fan_mode ? (R)1 : beta;
+            R gg = clampv<R>(grad_prior + eb * glik, (R)-10, (R)10);
+            g[j] = gg;
+            /* curvature, :510-520 */
+            if (c.use_newton) {
+                R hl = (R)-0.5 * (nu + 1) * A / (opA * opA);
+                R cv = clampv<R>(-(hl + hess_prior), (R)0.1, (R)100);
+                curv[j] = cv;
+                precond[j] = (R)0.7 * gg / cv;
+            }
+        }
+    }
+
+    /* Stein operator phi_i plus the optional per-row KSD sum.  Variants:
+     * vanilla :527-599 / :618-709, Newton :742-906, full Newton :912-1103. */
+    R phi_row(int i, R bw, bool want_ksd, R& ksd_row) {
+        R inv_bw2 = 1 / (bw * bw);
+        R sign = c.stein_repulsive_sign == 1 ? (R)1 : (R)-1;
+        bool newton = c.use_newton != 0, full = newton && c.use_full_newton;
+        const std::vector<R>& score = (newton && !full) ? precond : g;
+        R hi = h[i], si = score[i];
+        R ks = 0, gk = 0, hw = 0, kn = 0, ksd = 0;
+        for (int j = 0; j < n; ++j) {
+            R d = hi - h[j];
+            R dist2 = d * d * inv_bw2;
+            R K = 1 / (1 + dist2);
+            R K2 = K * K;
+            ks += K * score[j];
+            R rep = sign * 2 * d * inv_bw2 * K2;
+            if (newton && !full) rep /= curv[j];
+            gk += rep;
+            if (full) {
+                hw += curv[j] * K + 2 * inv_bw2 * K2 * std::fabs(3 * dist2 - 1);
+                kn += K;
+            }
+            if (want_ksd) {
+                R gxk = -2 * d * inv_bw2 * K2;
+                R hxy = 2 * inv_bw2 * K2 * (4 * dist2 * K - 1);
+                ksd += K * si * score[j] + si * (-gxk) + score[j] * gxk + hxy;
+            }
+        }
+        ksd_row = ksd;
+        R phi = (ks + gk) / (R)n;
+        if (full) {
+            R H = clampv<R>(hw / std::max(kn, (R)1e-6), (R)0.1, (R)100);
+            phi = phi / H * (R)0.7;
+        }
+        return phi;
+    }
+
+    /* Transport: RMSProp + drift + SVLD diffusion + clamp (Jacobi: all rows
+     * read the pre-iteration h), e.g. svpf_opt_kernels.cu:1078-1102. */
+    R transport(R eps_step, R bf, R temp, bool want_ksd, Noise<R>& nz, int kn) {
+        R bw = (R)s.bw;
+        std::vector<R> hn(n);
+        R ksd_sum = 0;
+        for (int i = 0; i < n; ++i) {
+            R kr = 0;
+            R phi = phi_row(i, bw, want_ksd, kr);
+            ksd_sum += kr;
+            R rr = (R)c.rmsprop_rho;
+            R vn = rr * v[i] + (1 - rr) * phi * phi;
+            v[i] = vn;
+            R es = eps_step * bf;
+            R drift = es * phi / std::sqrt(vn + (R)c.rmsprop_eps);
+            R diff = 0;
+            if (temp > (R)1e-6) diff = std::sqrt(2 * es * temp) * nz.normal(i, kn);
+            hn[i] = clamp_h(h[i] + drift + diff);
+        }
+        h.swap(hn);
+        return ksd_sum;
+    }
+
+    /* Heun (use_heun), svpf_optimized_graph.cu:1147-1232 with kernels
+     * svpf_opt_kernels.cu:1293-1566. */
+    R heun(R beta, R bf, R temp, R eps_step, bool last, Noise<R>& nz, int kn,
+           R rho, R sz, R mu, R stc) {
+        std::vector<R> h0 = h;
+        gradient(beta, rho, sz, mu, stc);
+        R bw = (R)s.bw, dummy;
+        bool full = c.use_newton && c.use_full_newton;
+        auto op = [&](int i) -> R {
+            /* svpf_stein_operator[_full_newton]_kernel: raw score, no Newton
+             * (non-full) variant. */
+            R inv_bw2 = 1 / (bw * bw);
+            R sign = c.stein_repulsive_sign == 1 ? (R)1 : (R)-1;
+            R ks = 0, gk = 0, hw = 0, kn2 = 0;
+            for (int j = 0; j < n; ++j) {
+                R d = h[i] - h[j];
+                R dist2 = d * d * inv_bw2;
+                R K = 1 / (1 + dist2), K2 = K * K;
+                if (full) { hw += curv[j] * K + 2 * inv_bw2 * K2 * std::fabs(3 * dist2 - 1); kn2 += K; }
+                ks += K * g[j];
+                gk += sign * 2 * d * inv_bw2 * K2;
+            }
+            R phi = (ks + gk) / (R)n;
+            if (full) {
+                R H = clampv<R>(hw / std::max(kn2, (R)1e-6), (R)0.1, (R)100);
+                phi = phi / H * (R)0.7;
+            }
+            return phi;
+        };
+        (void)dummy;
+        std::vector<R> phi0(n), phi1(n);
+        for (int i = 0; i < n; ++i) phi0[i] = op(i);
+        R es = eps_step * bf;
+        for (int i = 0; i < n; ++i)
+            h[i] = clamp_h(h0[i] + es * phi0[i] / std::sqrt(v[i] + (R)c.rmsprop_eps));
+        std::vector<R> g0 = g;  /* grad at h0 kept for the KSD below */
+        gradient(beta, rho, sz, mu, stc);
+        for (int i = 0; i < n; ++i) phi1[i] = op(i);
+        R ksd_sum = 0;
+        if (last) {
+            /* svpf_heun_corrector_ksd_kernel uses h_orig with the grad buffer,
+             * which at this point holds the gradient at the predicted h. */
+            R inv_bw2 = 1 / (bw * bw);
+            for (int i = 0; i < n; ++i) {
+                R si = g[i], acc = 0;
+                for (int j = 0; j < n; ++j) {
+                    R d = h0[i] - h0[j];
+                    R dist2 = d * d * inv_bw2;
+                    R K = 1 / (1 + dist2), K2 = K * K;
+                    R gxk = -2 * d * inv_bw2 * K2;
+                    R hxy = 2 * inv_bw2 * K2 * (4 * dist2 * K - 1);
+                    acc += K * si * g[j] + si * (-gxk) + g[j] * gxk + hxy;
+                }
+                ksd_sum += acc;
+            }
+        }
+        for (int i = 0; i < n; ++i) {
+            R pa = (R)0.5 * (phi0[i] + phi1[i]);
+            R rr = (R)c.rmsprop_rho;
+            R vn = rr * v[i] + (1 - rr) * pa * pa;
+            v[i] = vn;
+            R diff = 0;
+            if (temp > (R)1e-6) diff = std::sqrt(2 * es * temp) * nz.normal(i, kn);
+            h[i] = clamp_h(h0[i] + es * pa / std::sqrt(vn + (R)c.rmsprop_eps) + diff);
+        }
+        (void)g0;
+        return ksd_sum;
+    }
+
+    /* Adaptive beta, svpf_optimized_graph.cu:1066-1092 */
+    static R adaptive_beta(R ksd_prev, int ai, int na) {
+        if (ai == na - 1) return 1;
+        R b;
+        if (ksd_prev > (R)0.5) b = (R)0.3;
+        else if (ksd_prev < (R)0.05) b = (R)0.8;
+        else b = (R)0.3 + ((R)0.5 - ksd_prev) / (R)0.45 * (R)0.5;
+        b *= (R)0.5 + (R)0.5 * ((R)(ai + 1) / (R)na);
+        return clampv<R>(b, (R)0.1, (R)1);
+    }
+
+    /* Smoother, svpf_optimized_graph.cu:658-737 */
+    R smooth(R hm, R hvar) {
+        if (!c.use_smoothing) return hm;
+        int k = std::min(std::max(c.smooth_lag, 1), ORACLE_SMOOTH_MAX_LAG);
+        int head = s.smooth_head;
+        s.smooth_h_mean[head] = (float)hm;
+        s.smooth_h_var[head] = (float)hvar;
+        s.smooth_y[head] = (float)y_t;
+        s.smooth_head = (head + 1) % k;
+        if (s.timestep >= k) {
+            R rho = (R)p.rho;
+            R mu = c.use_adaptive_mu ? (R)s.mu_state : (R)p.mu;
+            R q = (R)p.sigma_z * (R)p.sigma_z;
+            for (int lag = 1; lag < k; ++lag) {
+                int ic = (s.smooth_head - lag - 1 + k) % k;
+                int inx = (s.smooth_head - lag + k) % k;
+                R hc = s.smooth_h_mean[ic], hn = s.smooth_h_mean[inx], vc = s.smooth_h_var[ic];
+                R pv = rho * rho * vc + q;
+                R J = rho * vc / (pv + (R)1e-8);
+                s.smooth_h_mean[ic] = (float)(hc + J * (hn - (mu + rho * (hc - mu))));
+                s.smooth_h_var[ic] = (float)(vc * (1 - J * rho));
+            }
+        }
+        /* svpf_get_smoothed_output :720-737 (k not re-floored at 1 there) */
+        int k2 = std::min(c.smooth_lag, ORACLE_SMOOTH_MAX_LAG);
+        if (k2 < 1 || s.timestep < k2) return hm;
+        int ol = c.smooth_output_lag;
+        if (ol <= 0) return hm;
+        if (ol >= k2) ol = k2 - 1;
+        int idx = (s.smooth_head - ol - 1 + k2) % k2;
+        return (R)s.smooth_h_mean[idx];
+    }
+
+    int run(R yt, R yp, Noise<R>& nz, oracle_out* out) {
+        y_t = yt; y_prev = yp;
+        const int t = s.timestep;
+        /* effective parameters, svpf_optimized_graph.cu:933-948 */
+        R mu_eff = c.use_adaptive_mu ? (R)s.mu_state : (R)p.mu;
+        R sz_eff = (R)p.sigma_z;
+        if (c.use_adaptive_sigma && t > 0) {
+            R ve = std::max((R)s.vol_prev, (R)1e-4);
+            R z = std::fabs(y_t) / ve;
+            R boost = 1;
+            if (z > (R)c.sigma_boost_threshold) {
+                R sev = std::min((z - (R)c.sigma_boost_threshold) / 3, (R)1);
+                boost = 1 + ((R)c.sigma_boost_max - 1) * sev;
+            }
+            sz_eff = (R)p.sigma_z * boost;
+            s.sigma_z_effective = (float)sz_eff;
+        }
+        R stc = student_t_const();
+        R off = implied_offset();
+        R rho_up = c.use_asymmetric_rho ? (R)c.rho_up : (R)p.rho;
+        R rho_dn = c.use_asymmetric_rho ? (R)c.rho_down : (R)p.rho;
+        R drho = c.use_local_params ? (R)c.delta_rho : 0;
+        R dsig = c.use_local_params ? (R)c.delta_sigma : 0;
+
+        int kn = 0, ku = 0;
+        /* predict, svpf_opt_kernels.cu:125-276 */
+        {
+            R hbar = (R)s.h_mean_prev;
+            for (int i = 0; i < n; ++i) {
+                R hi = h[i], hpi = hp[i];
+                hp[i] = hi;
+                int kk = 0;
+                R noise = c.use_student_t_state ? student_t_noise<R>(nz, i, kk, (R)c.nu_state)
+                                                : nz.normal(i, kk++);
+                if (i == 0) kn = kk;
+                R lev = (R)p.gamma * y_prev / (safe_exp(hi / 2) + (R)1e-8);
+                if (c.use_guided || c.use_mim) {
+                    R dev = hi - hbar;
+                    R rho_adj = drho * std::tanh(dev);
+                    R sscale = 1 + dsig * std::fabs(dev);
+                    R sel = nz.uniform(i, 0);
+                    R scale = sel < (R)c.mim_jump_prob ? (R)c.mim_jump_scale : (R)1;
+                    R br = hi > hpi ? rho_up : rho_dn;
+                    R rho = clampv<R>(br + rho_adj, (R)0, (R)0.999);
+                    R sl = sz_eff * sscale;
+                    R mprior = mu_eff + rho * (hi - mu_eff) + lev;
+                    if (c.use_guided) {
+                        R ly2 = std::log(y_t * y_t + (R)1e-10);
+                        R mimp = std::max(ly2 + off, (R)-5);
+                        R z = (mimp - mprior) / (R)2.5;
+                        R act = z > (R)c.guided_innovation_threshold
+                                    ? std::tanh(z - (R)c.guided_innovation_threshold) : (R)0;
+                        R ga = (R)c.guided_alpha_base + ((R)c.guided_alpha_shock - (R)c.guided_alpha_base) * act;
+                        mprior = (1 - ga) * mprior + ga * mimp;
+                    }
+                    h[i] = clamp_h(mprior + sl * scale * noise);
+                } else {
+                    h[i] = clamp_h(mu_eff + (R)p.rho * (hi - mu_eff) + sz_eff * noise + lev);
+                }
+            }
+            if (c.use_guided || c.use_mim) ku = 1;
+        }
+
+        /* guide, svpf_optimized_graph.cu:1006-1039 */
+        R gs = (R)c.guide_strength_base;
+        if (c.use_guide && c.use_adaptive_guide && t > 0) {
+            R ve = std::max((R)s.vol_prev, (R)1e-4);
+            R z = std::fabs(y_t) / ve;
+            R ih = std::log(y_t * y_t + (R)1e-8) + off;
+            R he = std::log(ve * ve + (R)1e-8);
+            if (ih - he > 0 && z > (R)c.guide_innovation_threshold) {
+                R sev = std::min((z - (R)c.guide_innovation_threshold) / 3, (R)1);
+                gs = (R)c.guide_strength_base + ((R)c.guide_strength_max - (R)c.guide_strength_base) * sev;
+            }
+        }
+        if (c.use_guide) {
+            ekf(mu_eff, (R)p.rho, (R)p.sigma_z, off);
+            R gm = (R)s.guide_mean;
+            if (c.use_guide_preserving) {
+                R cm = (R)s.h_mean_prev;
+                R nm = (1 - gs) * cm + gs * gm;
+                for (int i = 0; i < n; ++i) h[i] = clamp_h(nm + (h[i] - cm));
+            } else {
+                for (int i = 0; i < n; ++i) h[i] = clamp_h(h[i] + gs * (gm - h[i]));
+            }
+        }
+
+        bandwidth();
+
+        /* Stein budget / beta schedule, svpf_optimized_graph.cu:1057-1138 */
+        int na = c.use_annealing ? std::max(c.n_anneal_steps, 1) : 1;
+        R eps_step = (R)0.1 * (c.use_guide ? (R)0.5 : (R)1);
+        int budget;
+        if (t < 10) budget = c.stein_max_steps;
+        else {
+            /* a discrete decision: evaluated in float exactly as the host does */
+            float kn01 = (s.ksd_prev - 0.05f) / (0.50f - 0.05f);
+            kn01 = std::min(std::max(kn01, 0.0f), 1.0f);
+            budget = c.stein_min_steps + (int)(kn01 * (float)(c.stein_max_steps - c.stein_min_steps));
+        }
+        if (budget < 0) budget = 0;
+        int total = 0;
+        for (int ai = 0; ai < na; ++ai) {
+            R beta;
+            if (!c.use_annealing) beta = 1;
+            else if (c.use_adaptive_beta) beta = adaptive_beta((R)s.ksd_prev, ai, na);
+            else { static const double sch[3] = {0.3, 0.65, 1.0}; beta = (R)sch[ai % 3]; }
+            R bf = std::sqrt(beta);
+            R temp = c.use_svld ? (R)c.temperature : (R)0;
+            int si = budget / na;
+            if (ai == na - 1) si = budget - si * (na - 1);
+            for (int st = 0; st < si; ++st) {
+                ++total;
+                bool last = (ai == na - 1) && (st == si - 1);
+                R ksd_sum;
+                if (c.use_heun) {
+                    ksd_sum = heun(beta, bf, temp, eps_step, last, nz, kn, (R)p.rho, sz_eff, mu_eff, stc);
+                } else {
+                    gradient(beta, (R)p.rho, sz_eff, mu_eff, stc);
+                    ksd_sum = transport(eps_step, bf, temp, last, nz, kn);
+                }
+                if (temp > (R)1e-6) ++kn;
+                if (last) {
+                    R k2 = ksd_sum / ((R)n * (R)n);
+                    s.ksd_last = (float)std::sqrt(std::max(k2, (R)0));
+                }
+            }
+        }
+        s.stein_steps_used = total;
+
+        /* rejuvenation, svpf_optimized_graph.cu:1328-1341 + kernel :1248-1275 */
+        int fired = 0;
+        if (c.use_rejuvenation && c.use_guide && t > 10 && (R)s.ksd_prev > (R)c.rejuv_ksd_threshold) {
+            fired = 1;
+            R gstd = std::sqrt(std::max((R)s.guide_var, (R)1e-6));
+            R gm = (R)s.guide_mean;
+            R b = (R)c.rejuv_blend;
+            for (int i = 0; i < n; ++i) {
+                R u = nz.uniform(i, ku);
+                if (u < (R)c.rejuv_prob) {
+                    R z = nz.normal(i, kn);
+                    h[i] = clamp_h((1 - b) * h[i] + b * (gm + gstd * z));
+                }
+            }
+        }
+
+        /* outputs, svpf_opt_kernels.cu:1109-1153 */
+        R mx = (R)-1e10;
+        for (int i = 0; i < n; ++i) mx = std::max(mx, lw[i]);
+        R se = 0, sv = 0, sh = 0;
+        for (int i = 0; i < n; ++i) {
+            se += std::exp(lw[i] - mx);
+            sv += safe_exp(h[i] * (R)0.5);
+            sh += h[i];
+        }
+        R ll = mx + std::log(std::max(se / (R)n, (R)1e-10));
+        R vol = sv / (R)n;
+        R hm = sh / (R)n;
+        s.h_mean_prev = (float)hm;
+
+        /* host tail, svpf_optimized_graph.cu:1361-1388 */
+        R bwl = (R)s.bw;
+        R hm_out = smooth(hm, bwl * bwl);
+        s.vol_prev = (float)vol;
+        s.ksd_prev = s.ksd_last;
+        if (c.use_adaptive_mu && t > 10) {
+            /* svpf_adaptive_mu_update :619-642 */
+            R mp = (R)s.mu_state, Pp = (R)s.mu_var + (R)c.mu_process_var;
+            R Rm = (R)c.mu_obs_var_scale * bwl * bwl;
+            R K = Pp / (Pp + Rm + (R)1e-8);
+            s.mu_state = (float)clampv<R>(mp + K * (hm - mp), (R)c.mu_min, (R)c.mu_max);
+            s.mu_var = (float)((1 - K) * Pp);
+        }
+        s.loglik_sum += (double)ll;
+        s.timestep = t + 1;
+
+        out->loglik = (float)ll;
+        out->vol = (float)vol;
+        out->h_mean = (float)hm_out;
+        out->h_mean_raw = (float)hm;
+        out->bw = s.bw;
+        out->ksd = s.ksd_last;
+        out->steps_used = total;
+        out->rejuv_fired = fired;
+        return nz.bad ? -3 : 0;
+    }
+};
+
+template <typename R>
+int tick_impl(const oracle_config* cfg, const oracle_params* p, oracle_ctl* ctl, int n,
+              double* h, double* hp, double* v, double* lw, float yt, float yp,
+              const oracle_noise* noise, oracle_out* out) {
+    Tick<R> tk(*cfg, *p, *ctl, n);
+    tk.h.assign(h, h + n); tk.hp.assign(hp, hp + n); tk.v.assign(v, v + n);
+    tk.lw.assign(lw, lw + n);
+    tk.g.assign(n, 0); tk.curv.assign(n, 1); tk.precond.assign(n, 0);
+    Noise<R> nz(noise, n);
+    int rc = tk.run((R)yt, (R)yp, nz, out);
+    for (int i = 0; i < n; ++i) { h[i] = tk.h[i]; hp[i] = tk.hp[i]; v[i] = tk.v[i]; lw[i] = tk.lw[i]; }
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+void svpf_oracle_philox(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1,
+                        uint32_t c2, uint32_t c3, uint32_t* out) {
+    Block b = philox(k0, k1, c0, c1, c2, c3);
+    for (int i = 0; i < 4; ++i) out[i] = b.v[i];
+}
+
+/* Defaults of svpf_create, svpf_optimized_graph.cu:116-283. */
+void svpf_oracle_config_defaults(oracle_config* c, int n_stein_steps, float nu) {
+    std::memset(c, 0, sizeof(*c));
+    c->n_stein_steps = n_stein_steps;
+    c->nu = nu;
+    {
+        /* svpf_optimized_graph.cu:127-138, evaluated in float like svpf_create */
+        const float psi_half = -1.9635100260214235f;
+        float nh = nu / 2.0f, psi;
+        if (nh >= 1.0f) psi = std::log(nh) - 1.0f / (2.0f * nh) - 1.0f / (12.0f * nh * nh);
+        else psi = -0.5772156649f - 1.0f / nh;
+        c->student_t_implied_offset = -(std::log(nu) + psi_half - psi);
+    }
+    c->lik_offset = 0.45f;
+    c->use_exact_gradient = 0;
+    c->use_svld = 1; c->use_annealing = 1; c->use_adaptive_beta = 1; c->n_anneal_steps = 3;
+    c->temperature = 1.0f; c->rmsprop_rho = 0.9f; c->rmsprop_eps = 1e-6f;
+    c->use_mim = 1; c->mim_jump_prob = 0.05f; c->mim_jump_scale = 5.0f;
+    c->use_asymmetric_rho = 1; c->rho_up = 0.98f; c->rho_down = 0.93f;
+    c->use_guide = 1; c->use_guide_preserving = 1; c->guide_strength = 0.05f;
+    c->use_adaptive_guide = 0; c->guide_strength_base = 0.05f; c->guide_strength_max = 0.30f;
+    c->guide_innovation_threshold = 1.0f;
+    c->use_rejuvenation = 1; c->rejuv_ksd_threshold = 0.30f; c->rejuv_prob = 0.30f; c->rejuv_blend = 0.30f;
+    c->use_newton = 0; c->use_full_newton = 0;
+    c->use_guided = 0; c->guided_alpha_base = 0.0f; c->guided_alpha_shock = 0.5f;
+    c->guided_innovation_threshold = 1.5f;
+    c->use_local_params = 0; c->delta_rho = 0.02f; c->delta_sigma = 0.1f;
+    c->use_adaptive_mu = 0; c->mu_process_var = 0.001f; c->mu_obs_var_scale = 10.0f;
+    c->mu_min = -6.0f; c->mu_max = -1.0f;
+    c->use_adaptive_sigma = 0; c->sigma_boost_threshold = 1.0f; c->sigma_boost_max = 3.0f;
+    c->stein_repulsive_sign = 0; c->use_fan_mode = 0;
+    c->stein_min_steps = 4; c->stein_max_steps = 12; c->ksd_improvement_threshold = 0.05f;
+    c->use_student_t_state = 0; c->nu_state = 5.0f;
+    c->use_smoothing = 0; c->smooth_lag = 3; c->smooth_output_lag = 1;
+    c->use_heun = 0;
+}
+
+void svpf_oracle_ctl_defaults(oracle_ctl* s) {
+    std::memset(s, 0, sizeof(*s));
+    s->ksd_prev = 1e10f;
+    s->ksd_last = 0.0f;
+    s->vol_prev = 0.05f;
+    s->h_mean_prev = -3.5f;   /* svpf_optimized_graph.cu:492-494 */
+    s->bw_sq = 0.0f;          /* :483-484 */
+    s->return_ema = 0.0f;     /* :158-165 */
+    s->return_var = 0.0f;
+    s->sigma_z_effective = 0.10f;
+    s->mu_state = -3.5f;
+    s->mu_var = 1.0f;
+    for (int i = 0; i < ORACLE_SMOOTH_MAX_LAG; ++i) s->smooth_h_var[i] = 1.0f;
+}
+
+int svpf_oracle_initialize(oracle_config* cfg, const oracle_params* p, oracle_ctl* s, int n,
+                           double* h, double* hp, double* v, const float* init_normals,
+                           uint64_t seed, int filter_id) {
+    if (n <= 0) return -1;
+    s->timestep = 0;
+    s->y_prev = 0.0f;
+    cfg->nu_state = std::max(cfg->nu_state, 2.5f);
+    float rho = p->rho, sz = p->sigma_z;
+    float base_var = (sz * sz) / (1.0f - rho * rho + 1e-6f);
+    float var = cfg->use_student_t_state ? cfg->nu_state / (cfg->nu_state - 2.0f) * base_var : base_var;
+    double sd = std::sqrt((double)var);
+    PhiloxKey key = make_key(seed, filter_id);
+    for (int i = 0; i < n; ++i) {
+        double z = init_normals ? (double)init_normals[i]
+                                : philox_normal<double>(key, (uint32_t)i, 0u, 0u, 2u);
+        double hv = std::min(std::max((double)p->mu + sd * z, -15.0), 5.0);
+        h[i] = hv; hp[i] = hv; v[i] = 0.0;
+    }
+    s->guide_initialized = 0;
+    s->guide_mean = p->mu;
+    s->guide_var = var;
+    if (cfg->use_adaptive_mu) { s->mu_state = p->mu; s->mu_var = 1.0f; }
+    if (cfg->use_adaptive_sigma) s->sigma_z_effective = p->sigma_z;
+    s->ksd_prev = 1e10f;
+    s->stein_steps_used = cfg->n_stein_steps;
+    return 0;
+}
+
+int svpf_oracle_tick(const oracle_config* cfg, const oracle_params* p, oracle_ctl* ctl, int n,
+                     double* h, double* hp, double* v, double* lw, float yt, float yp,
+                     const oracle_noise* noise, oracle_out* out, int precision) {
+    if (n <= 0 || !cfg || !p || !ctl || !noise || !out) return -1;
+    if (precision == 0) return tick_impl<double>(cfg, p, ctl, n, h, hp, v, lw, yt, yp, noise, out);
+    return tick_impl<float>(cfg, p, ctl, n, h, hp, v, lw, yt, yp, noise, out);
+}
+
+int svpf_oracle_batch_tick_f32(int nf, const oracle_config* cfgs, const oracle_params* ps,
+                               oracle_ctl* ctls, const int* ns, int n_max,
+                               float* h, float* hp, float* v, float* lw,
+                               const float* yt, const float* yp, uint64_t seed, uint64_t tick,
+                               int n_threads, oracle_out* outs) {
+    int bad = 0;
+#ifdef _OPENMP
+    if (n_threads > 0) omp_set_num_threads(n_threads);
+#pragma omp parallel for schedule(dynamic, 1) reduction(| : bad)
+#endif
+    for (int f = 0; f < nf; ++f) {
+        int n = ns[f];
+        size_t off = (size_t)f * n_max;
+        Tick<float> tk(cfgs[f], ps[f], ctls[f], n);
+        tk.h.assign(h + off, h + off + n); tk.hp.assign(hp + off, hp + off + n);
+        tk.v.assign(v + off, v + off + n); tk.lw.assign(lw + off, lw + off + n);
+        tk.g.assign(n, 0); tk.curv.assign(n, 1); tk.precond.assign(n, 0);
+        oracle_noise nzs;
+        std::memset(&nzs, 0, sizeof(nzs));
+        nzs.mode = 1; nzs.seed = seed; nzs.tick = tick; nzs.filter_id = f;
+        Noise<float> nz(&nzs, n);
+        bad |= tk.run(yt[f], yp[f], nz, &outs[f]) != 0;
+        for (int i = 0; i < n; ++i) {
+            h[off + i] = tk.h[i]; hp[off + i] = tk.hp[i]; v[off + i] = tk.v[i]; lw[off + i] = tk.lw[i];
+        }
+    }
+    return bad ? -3 : 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,191 @@
+/*
+ * svpf_oracle.h -- TEST INFRASTRUCTURE ONLY (the oracle).
+ *
+ * CPU restatement of one Stein Variational Particle Filter tick as the
+ * reference computes it (src/svpf_optimized_graph.cu:915-1389 driving the
+ * kernels of src/svpf_opt_kernels.cu:125-1566 and the host EKF of
+ * include/svpf_kernels.cuh:509-541).  Only tests/, the smoke check and the
+ * CPU-baseline leg of bench.py may load it.  It is never part of the product
+ * path.
+ *
+ * The structs below are laid out field for field like the product's
+ * svpf_config_t / svpf_params_t / svpf_ctl_t so one ctypes definition can
+ * fill both, but they are declared here independently.
+ */
+#ifndef SVPF_ORACLE_H
+#define SVPF_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORACLE_SMOOTH_MAX_LAG 8
+
+/* Filter configuration: same names and defaults as the SVPFState fields of the
+ * reference (include/svpf.cuh:337-545, defaults svpf_optimized_graph.cu:116-283). */
+typedef struct {
+    int   n_stein_steps;
+    float nu;
+    float student_t_implied_offset;  /* fixed at create from nu (:127-138) */
+    float lik_offset;
+    int   use_exact_gradient;
+    int   use_svld;
+    int   use_annealing;
+    int   use_adaptive_beta;
+    int   n_anneal_steps;
+    float temperature;
+    float rmsprop_rho;
+    float rmsprop_eps;
+    int   use_mim;
+    float mim_jump_prob;
+    float mim_jump_scale;
+    int   use_local_params;
+    float delta_rho;
+    float delta_sigma;
+    int   use_asymmetric_rho;
+    float rho_up;
+    float rho_down;
+    int   use_newton;
+    int   use_full_newton;
+    int   use_guided;
+    float guided_alpha_base;
+    float guided_alpha_shock;
+    float guided_innovation_threshold;
+    int   use_rejuvenation;
+    float rejuv_ksd_threshold;
+    float rejuv_prob;
+    float rejuv_blend;
+    int   use_guide;
+    int   use_guide_preserving;
+    float guide_strength;
+    int   use_adaptive_guide;
+    float guide_strength_base;
+    float guide_strength_max;
+    float guide_innovation_threshold;
+    int   use_adaptive_mu;
+    float mu_process_var;
+    float mu_obs_var_scale;
+    float mu_min;
+    float mu_max;
+    int   use_adaptive_sigma;
+    float sigma_boost_threshold;
+    float sigma_boost_max;
+    int   stein_repulsive_sign;
+    int   use_fan_mode;
+    int   stein_min_steps;
+    int   stein_max_steps;
+    float ksd_improvement_threshold;
+    int   use_student_t_state;
+    float nu_state;
+    int   use_smoothing;
+    int   smooth_lag;
+    int   smooth_output_lag;
+    int   use_heun;
+} oracle_config;
+
+/* SVPFParams of the reference (include/svpf.cuh:257-262). */
+typedef struct {
+    float rho;
+    float sigma_z;
+    float mu;
+    float gamma;
+} oracle_params;
+
+/* Per-filter control state carried from tick to tick.  In the reference these
+ * live partly in host fields of SVPFState (timestep, ksd_prev, vol_prev,
+ * guide_*, mu_*, smooth_*) and partly in device scalars of the backend
+ * (d_h_mean_prev, d_bandwidth[_sq], d_return_ema/var, d_ksd). */
+typedef struct {
+    double guide_mean;
+    double guide_var;
+    double guide_K;
+    double loglik_sum;          /* FP64 running sum of per-tick log-likelihoods */
+    int    timestep;
+    int    guide_initialized;
+    int    stein_steps_used;
+    int    smooth_head;
+    float  ksd_prev;            /* host ksd_prev: drives budget/beta/rejuvenation */
+    float  ksd_last;            /* device d_ksd: last KSD actually computed */
+    float  vol_prev;
+    float  h_mean_prev;         /* device d_h_mean_prev (-3.5 on first use) */
+    float  bw;
+    float  bw_sq;
+    float  return_ema;
+    float  return_var;
+    float  sigma_z_effective;
+    float  mu_state;
+    float  mu_var;
+    float  y_prev;              /* used by svpf_step(): previous observation */
+    float  smooth_h_mean[ORACLE_SMOOTH_MAX_LAG];
+    float  smooth_h_var[ORACLE_SMOOTH_MAX_LAG];
+    float  smooth_y[ORACLE_SMOOTH_MAX_LAG];
+    int    status;
+    int    reserved;
+} oracle_ctl;
+
+typedef struct {
+    float loglik;
+    float vol;
+    float h_mean;        /* output h mean (smoothed when smoothing is on) */
+    float h_mean_raw;
+    float bw;
+    float ksd;
+    int   steps_used;
+    int   rejuv_fired;
+} oracle_out;
+
+/* Noise for one tick.  mode 0: tape; normals[k*n + i] is the k-th normal draw
+ * of particle i within the tick, uniforms likewise.  mode 1: the project's
+ * counter-based Philox4x32-10 keyed by (seed, filter) and counted by
+ * (particle, draw, tick). */
+typedef struct {
+    int          mode;
+    int          n_normal_slots;
+    int          n_uniform_slots;
+    int          filter_id;
+    const float* normals;
+    const float* uniforms;
+    uint64_t     seed;
+    uint64_t     tick;
+} oracle_noise;
+
+/* Run one tick.  Arrays are double on the interface; precision 0 computes in
+ * FP64, precision 1 computes in FP32 (the CPU baseline).  Returns 0 on
+ * success, a negative code on bad arguments or when the tape runs short. */
+int svpf_oracle_tick(const oracle_config* cfg, const oracle_params* p,
+                     oracle_ctl* ctl, int n,
+                     double* h, double* h_prev, double* v, double* log_w,
+                     float y_t, float y_prev, const oracle_noise* noise,
+                     oracle_out* out, int precision);
+
+/* FP32 batched baseline: filters are independent, OpenMP over filters.
+ * Arrays are float [n_filters][n_max]; per-filter n in ns[]. */
+int svpf_oracle_batch_tick_f32(int n_filters, const oracle_config* cfgs,
+                               const oracle_params* ps, oracle_ctl* ctls,
+                               const int* ns, int n_max,
+                               float* h, float* h_prev, float* v, float* log_w,
+                               const float* y_t, const float* y_prev,
+                               uint64_t seed, uint64_t tick, int n_threads,
+                               oracle_out* outs);
+
+/* svpf_initialize (svpf_optimized_graph.cu:349-451): stationary draw, resets.
+ * init_normals[i] is particle i's draw (tape) or NULL for Philox mode. */
+int svpf_oracle_initialize(oracle_config* cfg, const oracle_params* p,
+                           oracle_ctl* ctl, int n, double* h, double* h_prev,
+                           double* v, const float* init_normals,
+                           uint64_t seed, int filter_id);
+
+/* Fresh control record as svpf_create + the lazy backend init leave it. */
+void svpf_oracle_ctl_defaults(oracle_ctl* ctl);
+void svpf_oracle_config_defaults(oracle_config* cfg, int n_stein_steps, float nu);
+
+/* Philox4x32-10 block (Salmon et al. 2011), for bit-exact checks of the GPU
+ * generator: out[0..3] for key (k0,k1) and counter (c0..c3). */
+void svpf_oracle_philox(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1,
+                        uint32_t c2, uint32_t c3, uint32_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,72 @@
+"""Parity cases: configuration overrides on top of the reference's svpf_create
+defaults (svpf_optimized_graph.cu:116-283), model parameters and sizes.
+
+Each case is run tick by tick on the reference's own CUDA step with a noise
+tape (make_golden.py, GPU) and stored as a fixture; the oracle and the product
+engine replay every tick from the stored pre-tick state with the same tape.
+"""
+
+# BASELINE configuration 1 mapped onto the reference knobs: N=512, at most 8
+# Newton-Stein iterations over 3 annealing stages, full Newton, SVLD, MIM,
+# asymmetric rho, preserving EKF guide, rejuvenation, Student-t nu = 30.
+PRODUCTION = dict(use_newton=1, use_full_newton=1, stein_min_steps=4, stein_max_steps=8,
+                  n_anneal_steps=3)
+
+# The pybind production defaults (py-torch/svpf_python.cpp:90-176).
+PYBIND = dict(lik_offset=0.345, use_asymmetric_rho=1, rho_up=0.98, rho_down=0.93, use_svld=1,
+              temperature=0.45, rmsprop_rho=0.9, rmsprop_eps=1e-6, use_annealing=1,
+              n_anneal_steps=5, use_mim=1, mim_jump_prob=0.25, mim_jump_scale=9.0,
+              use_adaptive_beta=1, use_rejuvenation=1, rejuv_ksd_threshold=0.05,
+              rejuv_prob=0.30, rejuv_blend=0.30, use_newton=1, use_full_newton=1,
+              use_exact_gradient=1, stein_min_steps=8, stein_max_steps=16,
+              use_guided=1, guided_alpha_base=0.0, guided_alpha_shock=0.40,
+              guided_innovation_threshold=1.5, use_guide=1, use_guide_preserving=1,
+              guide_strength=0.05, use_adaptive_guide=1, guide_strength_base=0.05,
+              guide_strength_max=0.30, guide_innovation_threshold=1.0, use_adaptive_mu=1,
+              mu_process_var=0.001, mu_obs_var_scale=11.0, mu_min=-4.0, mu_max=-1.0,
+              use_adaptive_sigma=1, sigma_boost_threshold=0.95, sigma_boost_max=3.2,
+              use_local_params=0, delta_rho=0.0, delta_sigma=0.0)
+
+CASES = {
+    "production_n512": dict(n=512, n_stein=8, nu=30.0, cfg=PRODUCTION,
+                            params=(0.97, 0.15, -1.0, 0.0), path=(-1.0, 0.97, 0.15), ticks=14),
+    "pybind_n256": dict(n=256, n_stein=8, nu=30.0, cfg=PYBIND,
+                        params=(0.97, 0.15, -3.5, -0.5), path=(-3.5, 0.97, 0.25), ticks=14),
+    "vanilla_paper_n300": dict(n=300, n_stein=6, nu=5.0,
+                               cfg=dict(use_newton=0, use_adaptive_beta=0, use_guide_preserving=0,
+                                        stein_repulsive_sign=1, stein_min_steps=3, stein_max_steps=7,
+                                        rejuv_ksd_threshold=0.05),
+                               params=(0.95, 0.2, -2.0, -0.2), path=(-2.0, 0.95, 0.2), ticks=14),
+    "newton_local_n256": dict(n=256, n_stein=8, nu=8.0,
+                              cfg=dict(use_newton=1, use_full_newton=0, use_local_params=1,
+                                       use_exact_gradient=1, lik_offset=0.27, stein_min_steps=4,
+                                       stein_max_steps=9, use_adaptive_sigma=1),
+                              params=(0.98, 0.12, -1.5, 0.0), path=(-1.5, 0.98, 0.12), ticks=14),
+    "student_t_state_n200": dict(n=200, n_stein=6, nu=6.0,
+                                 cfg=dict(use_student_t_state=1, nu_state=5.0, use_newton=1,
+                                          use_full_newton=1, stein_min_steps=4, stein_max_steps=6,
+                                          use_guided=1),
+                                 params=(0.96, 0.18, -1.0, 0.0), path=(-1.0, 0.96, 0.18), ticks=14),
+    "heun_n256": dict(n=256, n_stein=6, nu=30.0,
+                      cfg=dict(use_heun=1, use_newton=1, use_full_newton=1, stein_min_steps=3,
+                               stein_max_steps=6),
+                      params=(0.97, 0.15, -1.0, 0.0), path=(-1.0, 0.97, 0.15), ticks=14),
+    "fan_smooth_n128": dict(n=128, n_stein=5, nu=10.0,
+                            cfg=dict(use_fan_mode=1, stein_repulsive_sign=1, use_annealing=0,
+                                     use_smoothing=1, smooth_lag=4, smooth_output_lag=1,
+                                     use_adaptive_mu=1, mu_min=-3.0, mu_max=0.0,
+                                     stein_min_steps=2, stein_max_steps=5, use_guide=1),
+                            params=(0.97, 0.15, -1.0, 0.0), path=(-1.0, 0.97, 0.15), ticks=14),
+}
+
+TAPE_SEED = 20240601
+
+
+def normal_slots(case) -> int:
+    """Upper bound on normal draws per particle per tick for the case."""
+    cfg = case["cfg"]
+    max_steps = cfg.get("stein_max_steps", 12)
+    pred = 1
+    if cfg.get("use_student_t_state", 0) and cfg.get("nu_state", 5.0) <= 30.0:
+        pred = 1 + max(int(cfg.get("nu_state", 5.0) + 0.5), 3)
+    return pred + max_steps + 1

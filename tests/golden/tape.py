@@ -1,0 +1,74 @@
+"""Deterministic noise tapes and synthetic SV paths for parity tests.
+
+A tape for one tick holds ``normals[k, i]`` (the k-th normal draw of particle
+i within the tick) and ``uniforms[k, i]``.  Values come from splitmix64 on an
+integer counter (exact uint64 arithmetic, so identical on every machine) and a
+Box-Muller transform in float64 rounded to float32.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def splitmix64(x: np.ndarray) -> np.ndarray:
+    with np.errstate(over="ignore"):
+        z = x.astype(np.uint64) + _GOLDEN
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        return z ^ (z >> np.uint64(31))
+
+
+def _counters(seed: int, stream: int, tick: int, slots: int, n: int) -> np.ndarray:
+    k = np.arange(slots, dtype=np.uint64)[:, None]
+    i = np.arange(n, dtype=np.uint64)[None, :]
+    with np.errstate(over="ignore"):
+        base = np.uint64((seed * 1_000_003 + stream * 7_919 + tick) & 0xFFFFFFFFFFFF)
+        return (base << np.uint64(32)) ^ (k << np.uint64(16)) ^ i
+
+
+def _unit(z: np.ndarray) -> np.ndarray:
+    """(0, 1] with 24 bits, exactly representable in float32."""
+    return ((z >> np.uint64(40)).astype(np.float64) + 1.0) * (1.0 / 16777216.0)
+
+
+def tape_normals(seed: int, tick: int, slots: int, n: int) -> np.ndarray:
+    c = _counters(seed, 1, tick, slots, n)
+    u1 = _unit(splitmix64(c))
+    u2 = _unit(splitmix64(c ^ np.uint64(0x5555555555555555))) - (1.0 / 16777216.0)
+    z = np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2)
+    return z.astype(np.float32)
+
+
+def tape_uniforms(seed: int, tick: int, slots: int, n: int) -> np.ndarray:
+    c = _counters(seed, 2, tick, slots, n)
+    return _unit(splitmix64(c)).astype(np.float32)
+
+
+def tape(seed: int, tick: int, n: int, normal_slots: int, uniform_slots: int = 2):
+    return tape_normals(seed, tick, normal_slots, n), tape_uniforms(seed, tick, uniform_slots, n)
+
+
+def init_normals(seed: int, n: int) -> np.ndarray:
+    return tape_normals(seed, 10_000_000, 1, n)[0]
+
+
+def sv_path(T: int, mu: float, rho: float, sigma_z: float, seed: int):
+    """Synthetic 1-factor SV path h_t = mu + rho (h_{t-1} - mu) + sigma_z eps,
+    h_0 ~ stationary, y_t = exp(h_t / 2) eta_t with Gaussian eta."""
+    c = np.arange(3 * T + 3, dtype=np.uint64) + np.uint64(seed) * np.uint64(1 << 40)
+    u = _unit(splitmix64(c))
+    u2 = _unit(splitmix64(c ^ np.uint64(0x3333333333333333))) - (1.0 / 16777216.0)
+    g = np.sqrt(-2.0 * np.log(u)) * np.cos(2.0 * np.pi * u2)
+    h = np.empty(T)
+    y = np.empty(T)
+    hv = mu + sigma_z / np.sqrt(1.0 - rho * rho) * g[0]
+    for t in range(T):
+        hv = mu + rho * (hv - mu) + sigma_z * g[1 + 3 * t]
+        eta = g[2 + 3 * t]
+        h[t] = hv
+        y[t] = np.exp(hv / 2.0) * eta
+    return h, y.astype(np.float32)

@@ -1,0 +1,73 @@
+"""The C ABI: the library loads, exports every function include/svpf.h
+declares, and the ctypes mirrors have the C layouts.  No compute calls."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "svpf.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"static inline[^{]*\{[^}]*\}", "", text)
+    names = set()
+    for m in re.finditer(r"^\s*[A-Za-z_][\w\s\*]*?\b(svpf_\w+)\s*\(", text, flags=re.M):
+        names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_reference_entry_points():
+    names = set(declared_functions())
+    for ref in ("svpf_create", "svpf_destroy", "svpf_initialize", "svpf_step", "svpf_step_seeded",
+                "svpf_step_adaptive", "svpf_step_graph", "svpf_run_sequence", "svpf_run_sequence_device",
+                "svpf_get_particles", "svpf_get_stats", "svpf_get_ess", "svpf_graph_is_captured",
+                "svpf_graph_invalidate"):
+        assert ref in names
+
+
+def test_library_exports_every_declared_function(pkg):
+    lib = C.CDLL(pkg.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def _c_sizes():
+    src = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "svpf.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu\n", sizeof(svpf_config_t), sizeof(svpf_ctl_t), sizeof(svpf_out_t),
+         sizeof(SVPFParams), offsetof(svpf_ctl_t, status));
+  return 0;
+}'''
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "s.c")
+        open(c, "w").write(src)
+        exe = os.path.join(d, "s")
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include", c, "-o", exe],
+                       check=True)
+        return [int(x) for x in subprocess.run([exe], capture_output=True, text=True).stdout.split()]
+
+
+def test_ctypes_layouts_match_c(pkg, oracle_mod):
+    cfg, ctl, out, prm, status_off = _c_sizes()
+    assert C.sizeof(pkg.Config) == cfg == C.sizeof(oracle_mod.OracleConfig)
+    assert C.sizeof(pkg.Ctl) == ctl == C.sizeof(oracle_mod.OracleCtl)
+    assert C.sizeof(pkg.Out) == out == C.sizeof(oracle_mod.OracleOut)
+    assert C.sizeof(pkg.Params) == prm
+    assert pkg.Ctl.status.offset == status_off
+
+
+def test_config_fields_follow_header_order(pkg, oracle_mod):
+    text = open(HEADER).read()
+    block = text[text.index("#define SVPF_CONFIG_FIELDS"):text.index("#define SVPF_DECL_INT_")]
+    names = re.findall(r"X_(?:INT|FLOAT)\((\w+)\)", block)
+    assert names == [f for f, _ in pkg.CONFIG_FIELDS]
+    assert names == [f for f, _ in oracle_mod.CONFIG_FIELDS]

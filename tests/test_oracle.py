@@ -1,0 +1,112 @@
+"""Oracle checks that need no GPU: known-answer vectors for the RNG, FP32 vs
+FP64 agreement, and replay of the reference's own recorded ticks."""
+import glob
+import json
+import os
+
+import numpy as np
+import pytest
+
+import cases
+import tape
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+# Random123 known-answer vectors for Philox4x32-10: counter, key -> output.
+PHILOX_KAT = [
+    ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+    ((0xFFFFFFFF,) * 4, (0xFFFFFFFF, 0xFFFFFFFF), (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+    ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+     (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+]
+
+
+def test_philox_known_answers(oracle_mod):
+    for ctr, key, out in PHILOX_KAT:
+        assert oracle_mod.philox(key[0], key[1], *ctr) == list(out)
+
+
+def _oracle_filter(oracle_mod, case, precision):
+    cfg = oracle_mod.default_config(case["n_stein"], case["nu"])
+    for k, v in case["cfg"].items():
+        setattr(cfg, k, v)
+    f = oracle_mod.OracleFilter(case["n"], cfg, oracle_mod.OracleParams(*case["params"]), precision)
+    f.initialize(tape.init_normals(cases.TAPE_SEED, case["n"]))
+    return f
+
+
+@pytest.mark.parametrize("name", sorted(cases.CASES))
+def test_fp32_mirror_tracks_fp64(oracle_mod, name):
+    case = cases.CASES[name]
+    fs = [_oracle_filter(oracle_mod, case, p) for p in (0, 1)]
+    _, ys = tape.sv_path(8, *case["path"], seed=3)
+    yp = 0.0
+    for t in range(6):
+        nrm, uni = tape.tape(cases.TAPE_SEED, t, case["n"], cases.normal_slots(case), 2)
+        outs = [f.step(ys[t], yp, nrm, uni) for f in fs]
+        yp = float(ys[t])
+        assert outs[0].steps_used == outs[1].steps_used
+        assert abs(outs[0].loglik - outs[1].loglik) < 1e-3 * max(1, abs(outs[0].loglik))
+    d = np.max(np.abs(fs[0].h - fs[1].h))
+    assert d < 1e-3, d
+
+
+def _fixtures():
+    return sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def test_fixtures_present():
+    names = {os.path.basename(p)[:-4] for p in _fixtures()}
+    assert set(cases.CASES) <= names, f"missing golden fixtures: {set(cases.CASES) - names}"
+
+
+def load_fixture(path):
+    z = np.load(path, allow_pickle=False)
+    return dict(config=json.loads(str(z["config"])), params=z["params"], n=int(z["n"]), ys=z["ys"],
+                normal_slots=int(z["normal_slots"]), tape_seed=int(z["tape_seed"]), h=z["h"], hp=z["hp"],
+                v=z["v"], lw=z["lw"], ctl=json.loads(str(z["ctl"])), outs=z["outs"])
+
+
+def rel_err(a, b, floor=1.0):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor)))
+
+
+# Tolerance of per-tick parity with state re-sync (BASELINE: 1e-4 relative).
+TOL = 1e-4
+
+
+@pytest.mark.parametrize("path", _fixtures(), ids=lambda p: os.path.basename(p)[:-4])
+def test_oracle_replays_reference_ticks(oracle_mod, path):
+    """Pin the oracle: from every recorded pre-tick state of the reference's own
+    CUDA step, one oracle tick with the same tape lands on the recorded
+    post-tick state (h, h_prev, RMSProp v, log-weights) and outputs."""
+    fx = load_fixture(path)
+    n = fx["n"]
+    cfg = oracle_mod.config_from_dict(fx["config"])
+    params = oracle_mod.OracleParams(*[float(x) for x in fx["params"]])
+    T = fx["outs"].shape[0]
+    y_prev = 0.0
+    for t in range(T):
+        f = oracle_mod.OracleFilter(n, cfg, params, precision=0)
+        f.ctl = oracle_mod.ctl_from_dict(fx["ctl"][t])
+        f.h, f.h_prev, f.v, f.log_w = (fx[k][t].astype(np.float64) for k in ("h", "hp", "v", "lw"))
+        nrm, uni = tape.tape(fx["tape_seed"], t, n, fx["normal_slots"], 2)
+        out = f.step(fx["ys"][t], y_prev, nrm, uni)
+        y_prev = float(fx["ys"][t])
+        post = fx["ctl"][t + 1]
+        assert out.steps_used == post["stein_steps_used"], (t, out.steps_used, post["stein_steps_used"])
+        assert rel_err(f.h, fx["h"][t + 1]) < TOL, (t, rel_err(f.h, fx["h"][t + 1]))
+        assert rel_err(f.h_prev, fx["hp"][t + 1]) < TOL
+        assert rel_err(f.v, fx["v"][t + 1], floor=1e-3) < TOL * 10, (t, rel_err(f.v, fx["v"][t + 1], 1e-3))
+        assert rel_err(f.log_w, fx["lw"][t + 1]) < TOL, (t, rel_err(f.log_w, fx["lw"][t + 1]))
+        ll, vol, hm = fx["outs"][t]
+        assert abs(out.loglik - ll) < TOL * max(1, abs(ll)), (t, out.loglik, ll)
+        assert abs(out.vol - vol) < TOL * max(1, abs(vol))
+        assert abs(out.h_mean - hm) < TOL * max(1, abs(hm)), (t, out.h_mean, hm)
+        for k in ("ksd_prev", "bw", "bw_sq", "return_ema", "return_var", "h_mean_prev", "vol_prev", "mu_state"):
+            a, b = getattr(f.ctl, k), post[k]
+            assert abs(a - b) <= TOL * max(1.0, abs(b)), (t, k, a, b)
+        assert abs(f.ctl.guide_mean - post["guide_mean"]) < TOL * max(1, abs(post["guide_mean"]))
+        assert abs(f.ctl.guide_var - post["guide_var"]) < TOL * max(1, abs(post["guide_var"]))
