@@ -1,0 +1,415 @@
+"""Benchmark of the batched SVPF tick on B200.
+
+Workload (the batched configuration): 4096 independent filters, each with its
+own theta (rho ~ U[0.90, 0.995], sigma_z ~ U[0.05, 0.4], mu ~ U[-2, 0],
+Student-t nu ~ U[4, 30]) and its own particle count drawn from
+{256, 512, 1024, 2048, 4096}; production configuration (full Newton, at most 8
+Stein iterations over 3 annealing stages, SVLD, MIM, EKF guide,
+rejuvenation).  A step is one tick of every filter: one persistent kernel
+launch (CUDA-graph replayed).  Observations are seeded synthetic SV paths.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line.  Under torchrun every rank runs its own 4096 filters
+(weak scaling, no per-tick exchange); rank 0 prints the line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_CHOICES = (256, 512, 1024, 2048, 4096)
+MAX_STEPS = 8
+METRIC = "filter-ticks/s batched vs plain step on 1 B200 at matched RMSE; p50/p99 µs/tick"
+
+
+def make_workload(F: int, seed: int):
+    rng = np.random.default_rng(seed)
+    ns = rng.choice(N_CHOICES, size=F).astype(np.int32)
+    rho = rng.uniform(0.90, 0.995, F)
+    sz = rng.uniform(0.05, 0.4, F)
+    mu = rng.uniform(-2.0, 0.0, F)
+    nu = rng.uniform(4.0, 30.0, F)
+    return ns, rho, sz, mu, nu
+
+
+def sv_paths(T: int, rho, sz, mu, nu, seed: int):
+    """Observations [T, F]: h_t = mu + rho (h_{t-1} - mu) + sz eps, y = e^{h/2} eta,
+    eta Student-t(nu) per filter (each filter's own nu)."""
+    rng = np.random.default_rng(seed + 7)
+    F = rho.shape[0]
+    h = mu + sz / np.sqrt(1 - rho ** 2) * rng.standard_normal(F)
+    ys = np.empty((T, F), np.float32)
+    for t in range(T):
+        h = mu + rho * (h - mu) + sz * rng.standard_normal(F)
+        eta = rng.standard_t(nu)
+        ys[t] = np.exp(h / 2) * eta
+    return ys
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in getattr(self, "out", "").splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                rows.append((float(p[1]), float(p[2]), p[5], p[6], p[7], p[8]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            for name, val in zip(names, r[2:]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def read_ncu_traffic():
+    """DRAM bytes per full-size batch launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "batch_tick_kernel_ncu.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_full_launch:"):
+            try:
+                return float(line.split(":")[1])
+            except ValueError:
+                return None
+    return None
+
+
+def oracle_cpu_rate(F_sample: int, ns, rho, sz, mu, nu, ys, n_threads: int, reps: int = 1):
+    """Filter-ticks/s of the oracle's FP32 mirror (OpenMP over filters) on a
+    bounded sample of the same workload: one tick of the first F_sample
+    filters, repeated ``reps`` times."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # test infrastructure, used here only as the CPU baseline
+
+    L = oracle.lib()
+    Fs = int(F_sample)
+    cfgs = (oracle.OracleConfig * Fs)()
+    prms = (oracle.OracleParams * Fs)()
+    ctls = (oracle.OracleCtl * Fs)()
+    outs = (oracle.OracleOut * Fs)()
+    n_max = int(ns[:Fs].max())
+    h = np.zeros((Fs, n_max), np.float32)
+    hp, v, lw = np.zeros_like(h), np.zeros_like(h), np.zeros_like(h)
+    for f in range(Fs):
+        c = oracle.default_config(MAX_STEPS, float(nu[f]))
+        c.use_newton, c.use_full_newton, c.stein_min_steps, c.stein_max_steps, c.n_anneal_steps = 1, 1, 4, MAX_STEPS, 3
+        cfgs[f] = c
+        prms[f] = oracle.OracleParams(float(rho[f]), float(sz[f]), float(mu[f]), 0.0)
+        ctls[f] = oracle.default_ctl()
+        hh, hpp, vv = (np.zeros(int(ns[f])) for _ in range(3))
+        L.svpf_oracle_initialize(C.byref(cfgs[f]), C.byref(prms[f]), C.byref(ctls[f]), int(ns[f]),
+                                 hh.ctypes.data_as(C.POINTER(C.c_double)), hpp.ctypes.data_as(C.POINTER(C.c_double)),
+                                 vv.ctypes.data_as(C.POINTER(C.c_double)), None, 1, f)
+        h[f, :ns[f]] = hh
+        hp[f, :ns[f]] = hpp
+    nsa = np.ascontiguousarray(ns[:Fs], np.int32)
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))  # noqa: E731
+    t0 = time.perf_counter()
+    for r in range(reps):
+        yt = np.ascontiguousarray(ys[r % ys.shape[0], :Fs])
+        yp = np.ascontiguousarray(ys[(r - 1) % ys.shape[0], :Fs]) if r else np.zeros(Fs, np.float32)
+        rc = L.svpf_oracle_batch_tick_f32(Fs, cfgs, prms, ctls, nsa.ctypes.data_as(C.POINTER(C.c_int)), n_max,
+                                          fp(h), fp(hp), fp(v), fp(lw), fp(yt), fp(yp), 1, r, n_threads, outs)
+        if rc != 0:
+            raise RuntimeError(f"oracle batch tick rc={rc}")
+    dt = time.perf_counter() - t0
+    return Fs * reps / dt, dt
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args, rank: int, world: int):
+    """Reference arm: the reference has no CPU implementation of the step, so
+    the CPU restatement (oracle FP32 mirror, OpenMP over filters, all host
+    threads) is timed on a bounded sample of the same workload."""
+    if rank != 0:
+        return
+    F = args.filters
+    ns, rho, sz, mu, nu = make_workload(F, seed=0)
+    ys = sv_paths(args.warmup + args.steps + 1, rho, sz, mu, nu, seed=0)
+    threads = cpu_threads()
+    sample = max(2 * threads, 32)
+    # warm-up: one small rep
+    oracle_cpu_rate(min(sample, 16), ns, rho, sz, mu, nu, ys, threads, reps=1)
+    rate, dt = oracle_cpu_rate(sample, ns, rho, sz, mu, nu, ys, threads, reps=max(1, args.steps))
+    line = {
+        "metric": METRIC, "value": rate, "unit": "filter-ticks/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * dt / max(1, args.steps), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "impl": "reference",
+        "config": workload_config(F),
+        "cpu_baseline": {"value": rate, "unit": "filter-ticks/s", "cores": threads, "kind": "port",
+                         "sample": f"{sample} filters of the workload x {max(1, args.steps)} ticks per run "
+                                   f"(the reference has no CPU step; oracle FP32 mirror, OpenMP)"},
+        "e2e": {"value": rate, "unit": "filter-ticks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(F: int):
+    return {"workload": f"batched SVPF tick: {F} filters per GPU, own theta, N ~ U{{256,512,1024,2048,4096}}, "
+                        f"production config (full Newton, <= {MAX_STEPS} Stein iterations, 3 stages)",
+            "filters_per_gpu": F, "particles": list(N_CHOICES), "stein_max_steps": MAX_STEPS,
+            "l2": "flushed between timed steps (256 MiB write)", "parallelism": "filters sharded per GPU"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--filters", type=int, default=4096)
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--latency-ticks", type=int, default=400)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    import __graft_entry__ as ge
+    pkg = ge.load_package()
+
+    F = args.filters
+    ns, rho, sz, mu, nu = make_workload(F, seed=rank)
+    T = args.warmup + args.steps + 2
+    ys = sv_paths(T, rho, sz, mu, nu, seed=rank)
+    tiles = {}
+    if not args.no_autotune:
+        tiles = pkg.autotune(sorted(set(ns.tolist())), ticks=2)
+    cfgs = [pkg.production_config(float(nu[f]), MAX_STEPS) for f in range(F)]
+    prms = [pkg.Params(float(rho[f]), float(sz[f]), float(mu[f]), 0.0) for f in range(F)]
+    stream = torch.cuda.Stream()
+    batch = pkg.Batch(ns, cfgs, prms, stream=stream.cuda_stream)
+    batch.initialize(seed=1000 + rank)
+
+    d_ys = torch.from_numpy(ys).to("cuda")
+    d_yt = torch.empty(F, dtype=torch.float32, device="cuda")
+    d_yp = torch.zeros(F, dtype=torch.float32, device="cuda")
+    d_out = torch.empty((F, 8), dtype=torch.float32, device="cuda")   # svpf_out_t is 8 x 4 bytes
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def device_step(t):
+        with torch.cuda.stream(stream):
+            d_yt.copy_(d_ys[t], non_blocking=True)
+            if t > 0:
+                d_yp.copy_(d_ys[t - 1], non_blocking=True)
+        batch.graph_launch(d_yt.data_ptr(), d_yp.data_ptr(), d_out.data_ptr())
+
+    for t in range(args.warmup):
+        device_step(t)
+    torch.cuda.synchronize()
+    launches0 = batch.kernel_launches
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    pairs = []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = ev[k]
+            e0.record(stream)
+            device_step(args.warmup + k)
+            e1.record(stream)
+            e1.synchronize()
+            steps = d_out.view(torch.int32)[:, 6].to(torch.float64)   # svpf_out_t.steps_used
+            n2 = torch.from_numpy(ns.astype(np.float64)).to("cuda") ** 2
+            pairs.append(float((steps * n2).sum()))
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = batch.kernel_launches - launches0
+    step_ms = [ev[k][0].elapsed_time(ev[k][1]) for k in range(args.steps)]
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        tt = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    value = world * F * args.steps / (total_ms / 1e3)
+
+    # ---- end to end through the C ABI with host buffers (pinned staging inside)
+    e2e_steps = max(3, min(args.steps, 6))
+    host_y = ys
+    batch.step(host_y[0], np.zeros(F, np.float32))   # warm
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        batch.step(host_y[(k + 1) % T], host_y[k % T])
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e_s = float(te.item())
+    e2e_value = world * F * e2e_steps / e2e_s
+
+    # ---- end-of-run exchange: per-filter log-likelihood sums, gathered on rank 0
+    ctl = batch.ctl()
+    ll_sum = torch.tensor([c.loglik_sum for c in ctl], dtype=torch.float64, device="cuda")
+    if world > 1:
+        gathered = [torch.empty_like(ll_sum) for _ in range(world)]
+        dist.all_gather(gathered, ll_sum)
+    status_bad = sum(1 for c in ctl if c.status != 0)
+
+    # ---- single-filter latency (configuration 1: N=512) and the plain-step loop
+    lat = {}
+    plain = {}
+    if rank == 0:
+        f1 = pkg.SVPF(512, MAX_STEPS, 30.0)
+        f1.configure(**pkg.production_config(30.0, MAX_STEPS).to_dict())
+        f1.initialize(0.97, 0.15, -1.0, 0.0, seed=0)
+        yl = sv_paths(args.latency_ticks + 20, np.array([0.97]), np.array([0.15]), np.array([-1.0]),
+                      np.array([1e6]), seed=5)[:, 0]
+        us = []
+        yprev = 0.0
+        lib = pkg.lib()
+        p = C.byref(f1.params)
+        for t in range(args.latency_ticks + 20):
+            t0 = time.perf_counter()
+            lib.svpf_step_graph(f1._s, float(yl[t]), yprev, p, None, None, None)
+            dt = time.perf_counter() - t0
+            yprev = float(yl[t])
+            if t >= 20:
+                us.append(dt * 1e6)
+        us.sort()
+        lat = {"n": 512, "p50_us": us[len(us) // 2], "p99_us": us[int(len(us) * 0.99)],
+               "mean_us": float(np.mean(us)), "ticks": len(us), "timing": "host wall clock per blocking call"}
+        f1.close()
+        # plain step looped over a sample of the batch's filters (one tick each)
+        sample = 64
+        filt = []
+        for f in range(sample):
+            s = pkg.SVPF(int(ns[f]), MAX_STEPS, float(nu[f]))
+            s.configure(**cfgs[f].to_dict())
+            s.initialize(float(rho[f]), float(sz[f]), float(mu[f]), 0.0, seed=f)
+            filt.append(s)
+        for s in filt:   # warm (t = 0 tick)
+            lib.svpf_step_graph(s._s, float(ys[0, 0]), 0.0, C.byref(s.params), None, None, None)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for f, s in enumerate(filt):
+            lib.svpf_step_graph(s._s, float(ys[1, f]), float(ys[0, f]), C.byref(s.params), None, None, None)
+        dtp = time.perf_counter() - t0
+        plain = {"value": sample / dtp, "unit": "filter-ticks/s", "sample": f"{sample} filters of the workload, "
+                 "one blocking svpf_step_graph call each"}
+        for s in filt:
+            s.close()
+
+    # ---- roofline: pair-interactions per launch / mean launch time
+    props = torch.cuda.get_device_properties(local)
+    sms = props.multi_processor_count
+    clk = clk.summary()
+    sm_mhz = clk["sm_mhz"] or 1965.0
+    mean_pairs = float(np.mean(pairs))
+    mean_s = (sum(step_ms) / len(step_ms)) / 1e3
+    achieved = mean_pairs / mean_s / 1e9
+    # per pair-iteration: 15 FP32-pipe and 2 MUFU instructions (one mixture-prior
+    # pair + one full-Newton transport pair); MUFU issues 16/clk/SM, FP32 128/clk/SM
+    peak = sms * sm_mhz * 1e6 * min(128.0 / 15.0, 16.0 / 2.0) / 1e9
+    traffic = read_ncu_traffic()
+
+    cpu = {}
+    if rank == 0:
+        threads = cpu_threads()
+        sample = max(2 * threads, 32)
+        rate, dt = oracle_cpu_rate(sample, ns, rho, sz, mu, nu, ys, threads, reps=1)
+        cpu = {"value": rate, "unit": "filter-ticks/s", "cores": threads, "kind": "port",
+               "sample": f"one tick of {sample} filters of the workload ({dt:.1f} s); oracle FP32 mirror, OpenMP"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "filter-ticks/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": dict(workload_config(F), tiles={str(k): list(v) for k, v in tiles.items()}),
+            "e2e": {"value": e2e_value, "unit": "filter-ticks/s", "h2d_bytes_per_step": 2 * F * 4,
+                    "d2h_bytes_per_step": F * 32, "timing": "host wall clock around svpf_batch_step"},
+            "gpu_launches": launches,
+            "roofline": {"bound": "fp32+mufu", "achieved": achieved, "peak": peak, "unit": "Gpair/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "note": "pair = one (i,j) Stein iteration: mixture-prior pair + transport pair; peak = "
+                                 f"{sms} SMs x {sm_mhz:.0f} MHz (measured) x min(128/15 FP32, 16/2 MUFU)"},
+            "single_filter_latency": lat,
+            "plain_step_loop": plain,
+            "cpu_baseline": cpu,
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+            "status_errors": status_bad,
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -54,6 +54,7 @@ struct svpf_batch {
     size_t smem = 0;
     int grid = 0;
     int launches = 0;
+    int heun = 0;
     // graph
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -105,6 +106,7 @@ BatchArgs make_args(svpf_batch* b, const float* d_yt, const float* d_yp, svpf_ou
     a.slots_n = b->slots_n;
     a.slots_u = b->slots_u;
     a.tape_stride = b->n_max;
+    a.heun = b->heun;
     return a;
 }
 
@@ -144,8 +146,11 @@ svpf_batch_t* svpf_batch_create(int F, const int* ns, const svpf_config_t* cfgs,
         if (ns[f] < 1 || ns[f] > SVPF_MAX_PARTICLES) return nullptr;
         n_max = std::max(n_max, ns[f]);
     }
-    if (tick_smem_bytes(n_max, 1) > max_dyn_smem()) return nullptr;
+    int heun = 0;
+    for (int f = 0; f < F; ++f) heun |= cfgs[f].use_heun != 0;
+    if (tick_smem_bytes(n_max, 1, heun != 0) > max_dyn_smem()) return nullptr;
     svpf_batch* b = new svpf_batch();
+    b->heun = heun;
     b->F = F;
     b->n_max = n_max;
     b->ns.assign(ns, ns + F);
@@ -190,7 +195,7 @@ svpf_batch_t* svpf_batch_create(int F, const int* ns, const svpf_config_t* cfgs,
          cudaMemset(b->d_lw, 0, b->total * sizeof(float)) == cudaSuccess;
     ok = ok && upload_tiles(b) == SVPF_OK;
     if (ok) {
-        b->smem = tick_smem_bytes(n_max, 1);
+        b->smem = tick_smem_bytes(n_max, 1, heun != 0);
         b->grid = batch_grid(b->smem);
         ok = b->grid > 0;
     }
@@ -403,7 +408,7 @@ int svpf_autotune(const int* ns, int count, int ticks) {
     for (int k = 0; k < count; ++k) {
         const int n = ns[k];
         if (n < 1 || n > SVPF_MAX_PARTICLES) return SVPF_ERR_INVALID_ARG;
-        const size_t smem = tick_smem_bytes(n, 1);
+        const size_t smem = tick_smem_bytes(n, 1, false);
         if (smem > max_dyn_smem()) return SVPF_ERR_INVALID_ARG;
         const int grid = batch_grid(smem);
         if (grid < 1) return SVPF_ERR_CUDA;

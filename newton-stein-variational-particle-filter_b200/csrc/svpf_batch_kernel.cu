@@ -36,7 +36,7 @@ __global__ void __launch_bounds__(kThreads, 2) batch_tick_kernel(const __grid_co
         __syncthreads();
         const int n = a.n[f];
         const long long off = a.off[f];
-        const Smem sm = carve(smem, n, 1, 0);
+        const Smem sm = carve(smem, n, 1, 0, a.heun != 0);
         const FilterIO io{a.h + off, a.hp + off, a.v + off, a.lw + off, n};
         const Noise nz{philox_key(a.seed, f), (uint32_t)ctl.timestep, a.tape_n, a.tape_u,
                        a.slots_n, a.slots_u, a.tape_stride, &pl.flag};

@@ -381,16 +381,17 @@ __host__ __device__ inline int pow2_at_least(int n) {
 }
 __host__ __device__ inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
-// Floats of dynamic shared memory for N particles on a team of C CTAs.
-__host__ __device__ inline int smem_floats(int n, int C) {
+// Floats of dynamic shared memory for N particles on a team of C CTAs; the two
+// Heun operator buffers are present only when `heun`.
+__host__ __device__ inline int smem_floats(int n, int C, bool heun) {
     const int np = round_up(n, 64);
     const int p2 = pow2_at_least(n);
     const int m_len = round_up(p2 > np ? p2 : np, 64);
     const int L = round_up((n + C - 1) / C, 4);
-    return 2 * np + np + np + m_len + 3 * L;
+    return 2 * np + np + np + m_len + (heun ? 3 : 1) * L;
 }
 
-__device__ inline Smem carve(float* base, int n, int C, int rank) {
+__device__ inline Smem carve(float* base, int n, int C, int rank, bool heun) {
     Smem s;
     const int np = round_up(n, 64);
     s.n = n;
@@ -405,8 +406,8 @@ __device__ inline Smem carve(float* base, int n, int C, int rank) {
     const int L = (n + C - 1) / C;
     const int Lp = round_up(L, 4);
     s.v = s.mu + s.m_len;
-    s.phi0 = s.v + Lp;
-    s.phi1 = s.phi0 + Lp;
+    s.phi0 = heun ? s.v + Lp : nullptr;
+    s.phi1 = heun ? s.phi0 + Lp : nullptr;
     s.row0 = min(rank * L, n);
     s.row1 = min(s.row0 + L, n);
     return s;

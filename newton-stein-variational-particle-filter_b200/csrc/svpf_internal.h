@@ -55,6 +55,7 @@ struct BatchArgs {
     const float* tape_n;
     const float* tape_u;
     int slots_n, slots_u, tape_stride;
+    int heun;              // any filter of the batch uses Heun (shared-memory layout)
 };
 
 struct InitArgs {
@@ -73,7 +74,7 @@ struct InitArgs {
 };
 
 // Dynamic shared-memory bytes of a tick kernel for n particles on C CTAs.
-size_t tick_smem_bytes(int n, int C);
+size_t tick_smem_bytes(int n, int C, bool heun);
 // Largest dynamic shared memory a CTA may use on this device.
 size_t max_dyn_smem();
 

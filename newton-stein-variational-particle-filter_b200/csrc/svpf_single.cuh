@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(kThreads) single_tick_kernel(const __grid_cons
     copy_words(&cfg, &a.cfg);
     copy_words(&prm, &a.prm);
     __syncthreads();
-    const Smem sm = carve(smem, a.n, team.size, team.rank);
+    const Smem sm = carve(smem, a.n, team.size, team.rank, a.cfg.use_heun != 0);
     const Noise nz{philox_key(a.seed, 0), (uint32_t)ctl.timestep, a.tape_n, a.tape_u,
                    a.slots_n, a.slots_u, a.n, &pl.flag};
     const FilterIO io{a.h, a.hp, a.v, a.lw, a.n};
@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(kThreads) single_tick_kernel(const __grid_cons
 
 template <int R, int S>
 static cudaError_t launch_single_t(const SingleArgs& a, int C, cudaStream_t s) {
-    const size_t smem = tick_smem_bytes(a.n, C);
+    const size_t smem = tick_smem_bytes(a.n, C, a.cfg.use_heun != 0);
     auto kern = single_tick_kernel<R, S>;
     static bool configured[kMaxCluster + 1] = {};
     cudaError_t e;

@@ -1,0 +1,95 @@
+"""Free-running comparison with the reference's own CUDA step (unmodified
+build, its own cuRAND noise) on seeded synthetic SV paths: filtered log-vol
+RMSE must agree within 2% (independent particle noise on both sides, so the
+check is statistical).  Latency of both steps is recorded alongside."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import cases
+import tape
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _ref_stock():
+    import oracle
+    return oracle, oracle.RefLib("stock")
+
+
+def run_reference(oracle, reflib, cfg_dict, params, ys, n, n_stein, nu):
+    import ctypes as C
+    f = oracle.RefFilter(reflib, n, n_stein, nu)
+    f.apply_config(oracle.config_from_dict(cfg_dict))
+    p = oracle.OracleParams(*params)
+    f.L.svpf_ref_initialize(f.s, C.byref(p), tape.init_normals(1, n).ctypes.data_as(C.POINTER(C.c_float)))
+    T = ys.shape[0]
+    lat = np.zeros(T, np.float32)
+    hm = np.zeros(T, np.float32)
+    # the harness times each svpf_step_graph call with CUDA events (like test/profile_svpf.cu)
+    f.L.svpf_ref_time_steps(f.s, ys.ctypes.data_as(C.POINTER(C.c_float)), T, C.byref(p),
+                            lat.ctypes.data_as(C.POINTER(C.c_float)))
+    f.close()
+    # second pass for the outputs (timing run discards them)
+    f = oracle.RefFilter(reflib, n, n_stein, nu)
+    f.apply_config(oracle.config_from_dict(cfg_dict))
+    f.L.svpf_ref_initialize(f.s, C.byref(p), tape.init_normals(1, n).ctypes.data_as(C.POINTER(C.c_float)))
+    yp = 0.0
+    for t in range(T):
+        _, _, _, hm[t] = f.step(ys[t], yp, p, np.zeros((1, n), np.float32), np.ones((1, n), np.float32))
+        yp = float(ys[t])
+    f.close()
+    return hm, lat
+
+
+def run_engine(pkg, cfg_dict, params, ys, n, n_stein, nu, seed):
+    import time
+    f = pkg.SVPF(n, n_stein, nu)
+    f.configure(**cfg_dict)
+    f.initialize(*params, seed=seed)
+    T = ys.shape[0]
+    hm = np.zeros(T, np.float32)
+    lat = np.zeros(T, np.float32)
+    yp = 0.0
+    for t in range(T):
+        t0 = time.perf_counter()
+        rc, out = f.step_raw(ys[t], yp)
+        lat[t] = (time.perf_counter() - t0) * 1e6
+        assert rc == 0
+        hm[t] = out.h_mean
+        yp = float(ys[t])
+    f.close()
+    return hm, lat
+
+
+@pytest.mark.parametrize("n", [512, 1024])
+def test_rmse_matches_reference_cuda_step(pkg, n):
+    oracle, reflib = _ref_stock()
+    nu = 30.0
+    cfg = pkg.production_config(nu, 8).to_dict()
+    params = (0.97, 0.15, -1.0, 0.0)
+    res = {"n": n, "paths": []}
+    r_ours, r_ref = [], []
+    for seed in (0, 1, 2):
+        h_true, ys = tape.sv_path(2500, -1.0, 0.97, 0.15, seed=100 + seed)
+        hm_ref, lat_ref = run_reference(oracle, reflib, cfg, params, ys, n, 8, nu)
+        hm_ours, lat_ours = run_engine(pkg, cfg, params, ys, n, 8, nu, seed)
+        w = 100
+        r_ref.append(float(np.sqrt(np.mean((hm_ref[w:] - h_true[w:]) ** 2))))
+        r_ours.append(float(np.sqrt(np.mean((hm_ours[w:] - h_true[w:]) ** 2))))
+        res["paths"].append({"seed": seed, "rmse_ref": r_ref[-1], "rmse_ours": r_ours[-1],
+                             "ref_p50_us": float(np.percentile(lat_ref[w:], 50)),
+                             "ref_p99_us": float(np.percentile(lat_ref[w:], 99)),
+                             "ours_p50_us": float(np.percentile(lat_ours[w:], 50)),
+                             "ours_p99_us": float(np.percentile(lat_ours[w:], 99))})
+    res["rmse_ref"] = float(np.mean(r_ref))
+    res["rmse_ours"] = float(np.mean(r_ours))
+    out_dir = os.path.join(ROOT, "gpurun_out")
+    os.makedirs(out_dir, exist_ok=True)
+    with open(os.path.join(out_dir, f"reference_compare_n{n}.json"), "w") as fh:
+        json.dump(res, fh, indent=1)
+    assert abs(res["rmse_ours"] - res["rmse_ref"]) <= 0.02 * res["rmse_ref"], res
