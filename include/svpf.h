@@ -373,6 +373,32 @@ int svpf_batch_set_noise_tape(svpf_batch_t* b, const float* normals, int n_norma
  * -1 when no choice was made. */
 int svpf_batch_tile_of(const svpf_batch_t* b, int n, int* rows_per_thread, int* col_split);
 
+/* One tick of a batch whose buffers the caller owns, with no allocation of any
+ * kind.  No counterpart in the reference: it serves callers that cannot call
+ * cudaMalloc (a host application that owns all device memory in a fixed arena,
+ * a plugin inside another framework's memory manager, a latency-critical loop
+ * that must not take the device synchronisation an allocation may cause).
+ * Every buffer is a device pointer the caller allocated: particle counts d_n,
+ * packed-array offsets d_off (16-float aligned, as the batch layout), per-filter
+ * configuration, parameters and control records (updated in place), the packed
+ * particle arrays (updated in place), this tick's observations and, optionally,
+ * the outputs.  The kernel's scratch (work counter, work order, tile per
+ * filter) is a fixed array inside the library, resident on every GPU that
+ * loads it until the process exits; at most SVPF_NOALLOC_MAX_FILTERS filters
+ * per call, larger batches are rejected with SVPF_ERR_INVALID_ARG.  The first
+ * call on a device looks up that array's device address (make it before any
+ * stream capture).  All calls share the one array and each call rewrites what
+ * it uses; calls that overlap on the GPU race, so issue them in one stream or
+ * order them.  Asynchronous on `stream`. */
+#define SVPF_NOALLOC_MAX_FILTERS   16384
+int svpf_batch_tick_noalloc(int n_filters, const int* d_n, const long long* d_off,
+                            const svpf_config_t* d_cfg, const SVPFParams* d_params,
+                            svpf_ctl_t* d_ctl, float* d_h, float* d_h_prev, float* d_v,
+                            float* d_log_w, const float* d_y_t, const float* d_y_prev,
+                            svpf_out_t* d_out, int n_max, int any_heun,
+                            unsigned long long seed, cudaStream_t stream);
+int svpf_noalloc_max_filters(void);
+
 /* Autotuner: time each compiled tile shape on a synthetic filter of each
  * particle count in ns[] and keep the fastest per size for this process. */
 int svpf_autotune(const int* ns, int count, int ticks);

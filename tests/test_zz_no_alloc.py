@@ -1,0 +1,106 @@
+"""The allocation-free batch tick, checked against the regular batch entry point.
+
+svpf_batch_tick_noalloc exists for callers that cannot call cudaMalloc (an
+application that owns all device memory in a fixed arena, a plugin inside
+another framework's memory manager, a latency-critical loop that must not take
+an allocation's implicit synchronisation): they pass every buffer, and the
+kernel's scratch is a fixed array inside the library.  Here the same filters,
+from the same state, are stepped twice in a row through both entry points
+(svpf_batch_step_device on a regular batch, and svpf_batch_tick_noalloc on
+caller-owned torch buffers); outputs and particles must agree within the
+parity tolerance of the other GPU tests (1e-4 relative).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from test_oracle import TOL, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _bind(lib):
+    vp = C.c_void_p
+    lib.svpf_batch_tick_noalloc.restype = C.c_int
+    lib.svpf_batch_tick_noalloc.argtypes = [C.c_int] + [vp] * 12 + [C.c_int, C.c_int, C.c_ulonglong, vp]
+    lib.svpf_noalloc_max_filters.restype = C.c_int
+    return lib
+
+
+def _dev_bytes(torch, ctypes_array):
+    raw = C.string_at(C.addressof(ctypes_array), C.sizeof(ctypes_array))
+    return torch.frombuffer(bytearray(raw), dtype=torch.uint8).cuda()
+
+
+def test_noalloc_tick_matches_batch_entry_point(pkg):
+    import torch
+
+    lib = _bind(pkg.lib())
+    ns = [256, 512, 300, 1024, 2048, 64, 4096, 700]
+    F = len(ns)
+    n_max = max(ns)
+    nus = np.linspace(5.0, 30.0, F)
+    cfgs = (pkg.Config * F)(*[pkg.production_config(float(nus[f]), 8) for f in range(F)])
+    prms = (pkg.Params * F)(*[pkg.Params(0.9 + 0.01 * f, 0.1 + 0.03 * f, -1.5 + 0.1 * f, 0.0) for f in range(F)])
+    seed = 11
+
+    # regular batch: the existing entry point
+    batch = pkg.Batch(ns, list(cfgs), list(prms))
+    batch.initialize(seed=seed)
+
+    # caller-owned buffers for the allocation-free entry point, same state
+    offs = np.zeros(F, np.int64)
+    acc = 0
+    for f, n in enumerate(ns):
+        offs[f] = acc
+        acc += (n + 15) // 16 * 16
+    h0 = np.zeros(acc, np.float32)
+    for f, n in enumerate(ns):
+        h0[offs[f]:offs[f] + n] = batch.get_particles(f)
+    d_n = torch.tensor(ns, dtype=torch.int32, device="cuda")
+    d_off = torch.from_numpy(offs).cuda()
+    d_cfg = _dev_bytes(torch, cfgs)
+    d_prm = _dev_bytes(torch, prms)
+    d_ctl = _dev_bytes(torch, batch.ctl())
+    d_h = torch.from_numpy(h0.copy()).cuda()
+    d_hp = torch.from_numpy(h0.copy()).cuda()
+    d_v = torch.zeros(acc, dtype=torch.float32, device="cuda")
+    d_lw = torch.zeros(acc, dtype=torch.float32, device="cuda")
+    d_out_a = torch.zeros((F, 8), dtype=torch.float32, device="cuda")
+    d_out_b = torch.zeros((F, 8), dtype=torch.float32, device="cuda")
+
+    ys = np.array([[0.31, -0.8, 0.05, 1.9, -0.4, 0.2, -0.07, 0.6],
+                   [-0.2, 0.5, -1.1, 0.3, 0.9, -0.6, 0.12, -0.3]], np.float32)
+    y_prev = np.zeros(F, np.float32)
+    for t in range(2):   # two calls in a row
+        d_yt = torch.from_numpy(ys[t]).cuda()
+        d_yp = torch.from_numpy(y_prev).cuda()
+        torch.cuda.synchronize()
+        batch.step_device(d_yt.data_ptr(), d_yp.data_ptr(), d_out_a.data_ptr())
+        batch.sync()
+        rc = lib.svpf_batch_tick_noalloc(F, d_n.data_ptr(), d_off.data_ptr(), d_cfg.data_ptr(), d_prm.data_ptr(),
+                                         d_ctl.data_ptr(), d_h.data_ptr(), d_hp.data_ptr(), d_v.data_ptr(),
+                                         d_lw.data_ptr(), d_yt.data_ptr(), d_yp.data_ptr(), d_out_b.data_ptr(),
+                                         n_max, 0, seed, None)
+        assert rc == 0, rc
+        torch.cuda.synchronize()
+        out_a = d_out_a.cpu().numpy()
+        out_b = d_out_b.cpu().numpy()
+        steps_a = out_a.view(np.int32)[:, 6]
+        steps_b = out_b.view(np.int32)[:, 6]
+        assert np.array_equal(steps_a, steps_b), (t, steps_a, steps_b)
+        for col in (0, 1, 2):   # loglik, vol, h_mean
+            assert rel_err(out_b[:, col], out_a[:, col]) < TOL, (t, col, out_a[:, col], out_b[:, col])
+        h_b = d_h.cpu().numpy()
+        for f, n in enumerate(ns):
+            assert rel_err(h_b[offs[f]:offs[f] + n], batch.get_particles(f)) < TOL, (t, f)
+        y_prev = ys[t]
+    batch.close()
+
+
+def test_noalloc_rejects_oversized_batches(pkg):
+    lib = _bind(pkg.lib())
+    too_many = lib.svpf_noalloc_max_filters() + 1
+    rc = lib.svpf_batch_tick_noalloc(too_many, *([None] * 12), 256, 0, 0, None)
+    assert rc == 1   # SVPF_ERR_INVALID_ARG, before any device work
