@@ -131,6 +131,9 @@ struct Plan {
     float eps_step, temp;
     float y_t, y_prev;
     float bw, inv_bw, inv_bw2;
+    float center;          // transport coordinates: hs = (h - center) / bw during the Stein loop
+    float mu_center;       // prior coordinates: (h - mu_center) * prior_scale, in log2 units
+    float prior_scale;     // sqrt(log2(e) / (2 sigma^2))
     float beta[SVPF_MAX_ANNEAL_STEPS];
     int budget, na, si_base;
     int rejuv;
@@ -335,15 +338,17 @@ __device__ inline void bitonic_sort(float* m, int P) {
 // Largest log-responsibility of row value x: attained at the nearest prior
 // mean, found by binary search in the sorted means (the reference scans all N,
 // svpf_opt_kernels.cu:453-459; the value is the same).
-__device__ __forceinline__ float nearest_lmax_gauss(const float* m, int n, float x, float inv2) {
+// Scaled Gaussian prior: the smallest squared distance from x to the sorted,
+// scaled prior means (its negative is the row maximum of the exponent).
+__device__ __forceinline__ float nearest_d2(const float* m, int n, float x) {
     int lo = 0, hi = n;
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
         if (m[mid] < x) lo = mid + 1; else hi = mid;
     }
-    float best = -1e10f;
-    if (lo < n) { const float d = x - m[lo]; best = fmaxf(best, -d * d * inv2); }
-    if (lo > 0) { const float d = x - m[lo - 1]; best = fmaxf(best, -d * d * inv2); }
+    float best = 3.0e38f;
+    if (lo < n) { const float d = x - m[lo]; best = fminf(best, d * d); }
+    if (lo > 0) { const float d = x - m[lo - 1]; best = fminf(best, d * d); }
     return best;
 }
 __device__ __forceinline__ float nearest_lmax_student(const float* m, int n, float x, float inv_nus2,
@@ -423,6 +428,11 @@ __device__ inline Smem carve(float* base, int n, int C, int rank, bool heun) {
 template <int R, int S, bool STUDENT>
 __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_config_t& cfg,
                           float beta, float* __restrict__ lw_out, const Team& team) {
+    // Positions arrive in transport coordinates hs = (h - center) / bw.  The
+    // Gaussian prior runs in scaled prior coordinates x = (h - mu_center) * sc
+    // with sc^2 = log2(e) / (2 sigma^2), where the log-responsibility in base 2
+    // is -(x - m)^2 and the sorted means m are stored scaled the same way; the
+    // pair then costs one FADD, one FFMA, one ex2 and two accumulations.
     constexpr int G = kThreads / S;
     const int grp = threadIdx.x / S, q = threadIdx.x % S;
     const float* __restrict__ hc = sm.h[cur];
@@ -430,30 +440,30 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
     const int nloc = sm.row1 - sm.row0;
     const int nv = round_up(sm.n, 4 * S);
     const float s2 = pl.sz_eff * pl.sz_eff;
-    const float inv2 = 0.5f / s2, inv_s2 = 1.0f / s2;
+    const float inv_s2 = 1.0f / s2;
+    const float sc = pl.prior_scale;
     const float nu = cfg.nu;
     // Student-t prior constants (:406-447)
     const float nus2 = cfg.nu_state * s2, inv_nus2 = 1.0f / nus2, np1 = cfg.nu_state + 1.0f;
     const float half_np1 = 0.5f * np1;
 
     for (int base = 0; base < nloc; base += G * R) {
-        float hj[R], lmax[R], sr[R], wg[R], wh[R];
+        float hj[R], xj[R], lm[R], sr[R], wg[R], wh[R];
         int jl[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             jl[r] = base + r * G + grp;
             const int j = sm.row0 + min(jl[r], nloc - 1);
-            hj[r] = hc[j];
-            lmax[r] = STUDENT ? nearest_lmax_student(mu, sm.n, hj[r], inv_nus2, half_np1)
-                              : nearest_lmax_gauss(mu, sm.n, hj[r], inv2);
+            hj[r] = fmaf(hc[j], pl.bw, pl.center);
+            if (STUDENT) {
+                xj[r] = hj[r];
+                lm[r] = nearest_lmax_student(mu, sm.n, hj[r], inv_nus2, half_np1);
+            } else {
+                xj[r] = (hj[r] - pl.mu_center) * sc;
+                lm[r] = nearest_d2(mu, sm.n, xj[r]);
+            }
             sr[r] = 0.0f; wg[r] = 0.0f; wh[r] = 0.0f;
         }
-        // exponent in base 2: r = 2^((-d^2 c - lmax) log2 e)
-        const float c2 = -inv2 * kLog2e;
-        float l2[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) l2[r] = -lmax[r] * kLog2e;
-
         for (int cb = q * 4; cb < nv; cb += 4 * S) {
             const float4 m4 = *reinterpret_cast<const float4*>(mu + cb);
             const float mm[4] = {m4.x, m4.y, m4.z, m4.w};
@@ -461,16 +471,16 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
             for (int e = 0; e < 4; ++e) {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    const float d = hj[r] - mm[e];
+                    const float d = xj[r] - mm[e];
                     if (!STUDENT) {
-                        const float w = ex2_approx(fmaf(d * d, c2, l2[r]));
+                        const float w = ex2_approx(fmaf(-d, d, lm[r]));
                         sr[r] += w;
                         wg[r] = fmaf(w, d, wg[r]);
                     } else {
                         const float d2 = d * d;
                         const float den = nus2 + d2;
                         const float lr = -half_np1 * kLn2 * lg2_approx(fmaf(d2, inv_nus2, 1.0f));
-                        const float w = ex2_approx((lr - lmax[r]) * kLog2e);
+                        const float w = ex2_approx((lr - lm[r]) * kLog2e);
                         const float iden = rcp_approx(den);
                         sr[r] += w;
                         wg[r] = fmaf(w * d, iden, wg[r]);
@@ -497,7 +507,7 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
                 const float h = hj[r];
                 float gp, hp;
                 if (!STUDENT) {
-                    gp = -wg[r] * inv_s2 / (sr[r] + 1e-8f);
+                    gp = -(wg[r] / sc) * inv_s2 / (sr[r] + 1e-8f);
                     hp = -inv_s2;
                 } else {
                     gp = -np1 * wg[r] / (sr[r] + 1e-8f);
@@ -542,6 +552,7 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
 // 2 d/bw^2 K^2 (sign by stein_repulsive_sign), Newton scaling, optional KSD
 // row sum, RMSProp, drift, SVLD diffusion, clamp.  KIND 0 vanilla, 1 Newton
 // (precondition per column), 2 full Newton (kernel-weighted Hessian per row).
+// Positions are read and written in transport coordinates hs = (h - center)/bw.
 // Returns this thread's KSD row sums.
 // ---------------------------------------------------------------------------
 enum { kTransport = 0, kPhiOnly = 1, kKsdOnly = 2 };
@@ -588,27 +599,31 @@ __device__ float transport_pass(const Smem& sm, int cur, const Plan& pl, const s
             const float cc[4] = {c4.x, c4.y, c4.z, c4.w};
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-                // columns past n hold h = kHPad, g = c = 0: their terms vanish
+                // positions are in transport coordinates, so u = (h_i - h_j) / bw
+                // is one FADD; columns past n hold a far pad whose terms vanish
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    const float d = hi[r] - hh[e];
-                    const float u = d * inv_bw;
+                    const float u = hi[r] - hh[e];
                     const float base_ = fmaf(u, u, 1.0f);
                     const float K = rcp_approx(base_);
                     const float K2 = K * K;
                     kg[r] = fmaf(K, gg[e], kg[r]);
-                    const float dk2 = d * K2;
-                    if (KIND == 1) gk[r] = fmaf(dk2, cc[e], gk[r]);
-                    else gk[r] += dk2;
+                    if (KIND == 1 || KSD) {
+                        const float uk2 = u * K2;
+                        if (KIND == 1) gk[r] = fmaf(uk2, cc[e], gk[r]);
+                        else gk[r] += uk2;
+                        if (KSD) {
+                            if (KIND == 1) gkr[r] += uk2;
+                            gdk[r] = fmaf(gg[e], uk2, gdk[r]);
+                            hs[r] = fmaf(K2, fmaf(-4.0f, K, 3.0f), hs[r]);   // 4 (d/bw)^2 K - 1 = 3 - 4K
+                        }
+                    } else {
+                        gk[r] = fmaf(u, K2, gk[r]);
+                    }
                     if (KIND == 2) {
                         ks[r] += K;
                         kc[r] = fmaf(K, cc[e], kc[r]);
-                        nk[r] = fmaf(K2, fabsf(fmaf(3.0f, base_, -4.0f)), nk[r]);   // |3 d^2/bw^2 - 1|
-                    }
-                    if (KSD) {
-                        if (KIND == 1) gkr[r] += dk2;
-                        gdk[r] = fmaf(gg[e], dk2, gdk[r]);
-                        hs[r] = fmaf(K2, fmaf(-4.0f, K, 3.0f), hs[r]);           // 4 (d^2/bw^2) K - 1 = 3 - 4K
+                        nk[r] = fmaf(K2, fabsf(fmaf(3.0f, base_, -4.0f)), nk[r]);   // |3 (d/bw)^2 - 1|
                     }
                 }
             }
@@ -636,7 +651,8 @@ __device__ float transport_pass(const Smem& sm, int cur, const Plan& pl, const s
             for (int r = 0; r < R; ++r) {
                 if (il[r] >= nloc) continue;
                 const int i = sm.row0 + il[r];
-                float phi = (kg[r] + sign * 2.0f * inv_bw2 * gk[r]) * inv_n;
+                // sums over u = d / bw carry one factor bw: 2 d K^2 / bw^2 = 2 u K^2 / bw
+                float phi = (kg[r] + sign * 2.0f * inv_bw * gk[r]) * inv_n;
                 if (KIND == 2) {
                     float H = (kc[r] + 2.0f * inv_bw2 * nk[r]) / fmaxf(ks[r], 1e-6f);
                     H = clampf(H, 0.1f, 100.0f);
@@ -644,7 +660,7 @@ __device__ float transport_pass(const Smem& sm, int cur, const Plan& pl, const s
                 }
                 if (KSD) {
                     const float gsum = (KIND == 1) ? gkr[r] : gk[r];
-                    ksd_thread += si[r] * kg[r] + 2.0f * inv_bw2 * (si[r] * gsum - gdk[r] + hs[r]);
+                    ksd_thread += si[r] * kg[r] + 2.0f * inv_bw * (si[r] * gsum - gdk[r]) + 2.0f * inv_bw2 * hs[r];
                 }
                 const int li = i - sm.row0;
                 if (MODE == kPhiOnly) { phi_out[li] = phi; continue; }
@@ -654,8 +670,9 @@ __device__ float transport_pass(const Smem& sm, int cur, const Plan& pl, const s
                 const float drift = es * phi * rsqrtf(vn + cfg.rmsprop_eps);
                 float diff = 0.0f;
                 if (pl.temp > 1e-6f) diff = sqrtf(2.0f * es * pl.temp) * nz.normal(i, kn);
-                const float h_new = clamp_h(hi[r] + drift + diff);
-                for (int rk = 0; rk < team.size; ++rk) team.at(hn, rk)[i] = h_new;
+                const float h_new = clamp_h(fmaf(hi[r], pl.bw, pl.center) + drift + diff);
+                const float hs_new = (h_new - pl.center) * inv_bw;
+                for (int rk = 0; rk < team.size; ++rk) team.at(hn, rk)[i] = hs_new;
             }
         }
     }

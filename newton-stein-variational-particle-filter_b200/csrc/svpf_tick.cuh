@@ -162,9 +162,21 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
         pl.bw = bw;
         pl.inv_bw = 1.0f / bw;
         pl.inv_bw2 = 1.0f / (bw * bw);
+        pl.center = mean;
+        pl.mu_center = pl.mu_eff;
+        pl.prior_scale = sqrtf(kLog2e * 0.5f / (pl.sz_eff * pl.sz_eff));
     }
     // ---- sort prior means once per tick (used for the per-row maximum)
     bitonic_sort(sm.mu, sm.p2);
+    // ---- Stein-loop coordinates: positions (h - center) / bw, Gaussian prior
+    //      means (mu - mu_center) * prior_scale (order preserving)
+    const bool student = cfg.use_student_t_state != 0;
+    if (pl.budget > 0) {
+        for (int i = tid; i < n; i += kThreads) {
+            sm.h[0][i] = (sm.h[0][i] - pl.center) * pl.inv_bw;
+            if (!student) sm.mu[i] = (sm.mu[i] - pl.mu_center) * pl.prior_scale;
+        }
+    }
     // ---- own rows' RMSProp state
     for (int li = tid; li < sm.row1 - sm.row0; li += kThreads) sm.v[li] = io.v[sm.row0 + li];
     team.sync();   // every member has read io.h / io.h_prev; smem ready
@@ -172,7 +184,6 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
     // ---- annealed Stein loop (svpf_optimized_graph.cu:1120-1317)
     int cur = 0;
     int kn = pl.kn_pred;
-    const bool student = cfg.use_student_t_state != 0;
     const int budget = pl.budget;
     for (int it = 0; it < budget; ++it) {
         const int ai = stage_of(pl, it);
@@ -197,8 +208,10 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
             __syncthreads();
             for (int li = tid; li < nloc; li += kThreads) {
                 const int i = sm.row0 + li;
-                const float hpred = clamp_h(sm.h[cur][i] + es * sm.phi0[li] * rsqrtf(sm.v[li] + cfg.rmsprop_eps));
-                for (int rk = 0; rk < team.size; ++rk) team.at(sm.h[cur ^ 1], rk)[i] = hpred;
+                const float h0 = fmaf(sm.h[cur][i], pl.bw, pl.center);
+                const float hpred = clamp_h(h0 + es * sm.phi0[li] * rsqrtf(sm.v[li] + cfg.rmsprop_eps));
+                const float hs = (hpred - pl.center) * pl.inv_bw;
+                for (int rk = 0; rk < team.size; ++rk) team.at(sm.h[cur ^ 1], rk)[i] = hs;
             }
             team.sync();
             grad_dispatch<R, S>(student, sm, cur ^ 1, pl, cfg, beta, io.lw, team);
@@ -217,8 +230,10 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
                 sm.v[li] = vn;
                 float diff = 0.0f;
                 if (pl.temp > 1e-6f) diff = sqrtf(2.0f * es * pl.temp) * nz.normal(i, kn);
-                const float hn = clamp_h(sm.h[cur][i] + es * pa * rsqrtf(vn + cfg.rmsprop_eps) + diff);
-                for (int rk = 0; rk < team.size; ++rk) team.at(sm.h[cur ^ 1], rk)[i] = hn;
+                const float h0 = fmaf(sm.h[cur][i], pl.bw, pl.center);
+                const float hn = clamp_h(h0 + es * pa * rsqrtf(vn + cfg.rmsprop_eps) + diff);
+                const float hs = (hn - pl.center) * pl.inv_bw;
+                for (int rk = 0; rk < team.size; ++rk) team.at(sm.h[cur ^ 1], rk)[i] = hs;
             }
             team.sync();
             cur ^= 1;
@@ -240,8 +255,13 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
         ctl.stein_steps_used = budget;
     }
 
-    // ---- partial rejuvenation (svpf_opt_kernels.cu:1248-1275)
+    // ---- back to log-volatility coordinates
     float* hf = sm.h[cur];
+    if (budget > 0) {
+        for (int i = tid; i < n; i += kThreads) hf[i] = fmaf(hf[i], pl.bw, pl.center);
+        __syncthreads();
+    }
+    // ---- partial rejuvenation (svpf_opt_kernels.cu:1248-1275)
     if (pl.rejuv) {
         const int ku = pl.uses_uniform_predict;
         const float b = cfg.rejuv_blend;
