@@ -128,7 +128,7 @@ void drop_graph(svpf_batch* b) {
 int upload_tiles(svpf_batch* b) {
     for (int f = 0; f < b->F; ++f) {
         const int t = tuned_batch_tile(b->ns[f]);
-        b->tiles[f] = (uint8_t)(t >= kBatchTileLo ? t : default_batch_tile(b->ns[f]));
+        b->tiles[f] = (uint8_t)(t >= kBatchTileLo && t <= kBatchTileHi ? t : default_batch_tile(b->ns[f]));
     }
     return cudaMemcpy(b->d_tile, b->tiles.data(), b->F, cudaMemcpyHostToDevice) == cudaSuccess ? SVPF_OK
                                                                                               : SVPF_ERR_CUDA;
@@ -440,7 +440,7 @@ int svpf_autotune(const int* ns, int count, int ticks) {
         cudaEventCreate(&e1);
         float best = 1e30f;
         int best_t = default_batch_tile(n);
-        for (int t = kBatchTileLo; t < kNumTiles; ++t) {
+        for (int t = kBatchTileLo; t <= kBatchTileHi; ++t) {
             std::fill(b->tiles.begin(), b->tiles.end(), (uint8_t)t);
             cudaMemcpy(b->d_tile, b->tiles.data(), F, cudaMemcpyHostToDevice);
             enqueue_tick(b, d_y, d_y + F, nullptr);   // warm
@@ -466,7 +466,7 @@ int svpf_autotune(const int* ns, int count, int ticks) {
 
 int svpf_tile_choice(int n, int* R, int* S) {
     int t = tuned_batch_tile(n);
-    if (t < kBatchTileLo) t = default_batch_tile(n);
+    if (t < kBatchTileLo || t > kBatchTileHi) t = default_batch_tile(n);
     if (R) *R = kTiles[t].R;
     if (S) *S = kTiles[t].S;
     return SVPF_OK;

@@ -46,8 +46,7 @@ __global__ void __launch_bounds__(kThreads, 2) batch_tick_kernel(const __grid_co
             case 2: run_tick<1, 2>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
             case 3: run_tick<1, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
             case 4: run_tick<2, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
-            case 5: run_tick<4, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
-            default: run_tick<8, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
+            default: run_tick<4, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
         }
         __syncthreads();
         copy_words(&a.ctl[f], &ctl);

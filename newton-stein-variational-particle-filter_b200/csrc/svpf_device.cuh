@@ -54,6 +54,44 @@ __device__ __forceinline__ float lg2_approx(float x) {
     asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
+// Packed FP32x2 arithmetic (sm_100): one issue slot for two FP32 results.
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// 2^-q for q >= 0 on the FMA pipe, two lanes at once.  Range reduction: t =
+// 1.5 * 2^23 - q rounds -q to the nearest integer n, which lands in the low
+// mantissa bits of t; 2^n is then added straight into the exponent field of
+// p(f), f = -q - n in [-1/2, 1/2] (exponent-field construction as in
+// Schraudolph, "A fast, compact approximation of the exponential function",
+// Neural Computation 1999).  p is a degree-5 polynomial for 2^f fitted for
+// this file by relative-error least squares on Chebyshev nodes (max relative
+// error 2.1e-7 in FP32), evaluated here in g = -f with alternating-sign
+// coefficients.  q is capped at 125, so results are never denormal; such
+// weights (< 3e-38) are negligible in every sum they enter.
+__device__ __forceinline__ float2 exp2_neg_fma2(float2 q) {
+    q.x = fminf(q.x, 125.0f);
+    q.y = fminf(q.y, 125.0f);
+    const float2 t = fma2(q, f2(-1.0f), f2(12582912.0f));
+    const float2 g = add2(q, add2(t, f2(-12582912.0f)));
+    float2 p = f2(-1.327646663e-03f);
+    p = fma2(p, g, f2(9.675540961e-03f));
+    p = fma2(p, g, f2(-5.550713465e-02f));
+    p = fma2(p, g, f2(2.402212024e-01f));
+    p = fma2(p, g, f2(-6.931469440e-01f));
+    p = fma2(p, g, f2(1.000000119e+00f));
+    return make_float2(__int_as_float(__float_as_int(p.x) + (__float_as_int(t.x) << 23)),
+                       __int_as_float(__float_as_int(p.y) + (__float_as_int(t.y) << 23)));
+}
+
+// Which packed exponentials (column pair hf of a chunk, row r) of the mixture
+// loop run on the FMA pipe: 3 of 16 with 8 rows per thread, 1 of 8 with 4.
+template <int R>
+__host__ __device__ constexpr bool exp_on_fma(int hf, int r) {
+    return R >= 4 && ((hf + 2 * r) % 5) == 4;
+}
+
 constexpr float kLog2e = 1.4426950408889634f;
 constexpr float kLn2 = 0.6931471805599453f;
 
@@ -464,6 +502,43 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
             }
             sr[r] = 0.0f; wg[r] = 0.0f; wh[r] = 0.0f;
         }
+        if (!STUDENT) {
+            // two columns per packed op; a few exponentials per chunk go to the
+            // FMA pipe so that MUFU and FMA pipes finish together
+            float2 x2[R], nl2[R], sr2[R], wg2[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                x2[r] = f2(xj[r]);
+                nl2[r] = f2(-lm[r]);
+                sr2[r] = f2(0.0f);
+                wg2[r] = f2(0.0f);
+            }
+            for (int cb = q * 4; cb < nv; cb += 4 * S) {
+                const float4 m4 = *reinterpret_cast<const float4*>(mu + cb);
+                const float2 mm[2] = {make_float2(m4.x, m4.y), make_float2(m4.z, m4.w)};
+#pragma unroll
+                for (int hf = 0; hf < 2; ++hf) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const float2 d = fma2(mm[hf], f2(-1.0f), x2[r]);   // x - m
+                        const float2 qq = fma2(d, d, nl2[r]);                // (x - m)^2 - min >= 0
+                        float2 w;
+                        if (exp_on_fma<R>(hf, r)) {
+                            w = exp2_neg_fma2(qq);
+                        } else {
+                            w = make_float2(ex2_approx(-qq.x), ex2_approx(-qq.y));
+                        }
+                        sr2[r] = add2(sr2[r], w);
+                        wg2[r] = fma2(w, d, wg2[r]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                sr[r] = sr2[r].x + sr2[r].y;
+                wg[r] = wg2[r].x + wg2[r].y;
+            }
+        } else {
         for (int cb = q * 4; cb < nv; cb += 4 * S) {
             const float4 m4 = *reinterpret_cast<const float4*>(mu + cb);
             const float mm[4] = {m4.x, m4.y, m4.z, m4.w};
@@ -472,22 +547,17 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const float d = xj[r] - mm[e];
-                    if (!STUDENT) {
-                        const float w = ex2_approx(fmaf(-d, d, lm[r]));
-                        sr[r] += w;
-                        wg[r] = fmaf(w, d, wg[r]);
-                    } else {
-                        const float d2 = d * d;
-                        const float den = nus2 + d2;
-                        const float lr = -half_np1 * kLn2 * lg2_approx(fmaf(d2, inv_nus2, 1.0f));
-                        const float w = ex2_approx((lr - lm[r]) * kLog2e);
-                        const float iden = rcp_approx(den);
-                        sr[r] += w;
-                        wg[r] = fmaf(w * d, iden, wg[r]);
-                        wh[r] = fmaf(w * (nus2 - d2), iden * iden, wh[r]);
-                    }
+                    const float d2 = d * d;
+                    const float den = nus2 + d2;
+                    const float lr = -half_np1 * kLn2 * lg2_approx(fmaf(d2, inv_nus2, 1.0f));
+                    const float w = ex2_approx((lr - lm[r]) * kLog2e);
+                    const float iden = rcp_approx(den);
+                    sr[r] += w;
+                    wg[r] = fmaf(w * d, iden, wg[r]);
+                    wh[r] = fmaf(w * (nus2 - d2), iden * iden, wh[r]);
                 }
             }
+        }
         }
         // combine the S column slices
 #pragma unroll
@@ -587,45 +657,68 @@ __device__ float transport_pass(const Smem& sm, int cur, const Plan& pl, const s
             const int i = sm.row0 + min(il[r], nloc - 1);
             hi[r] = hc[i];
             si[r] = gs[i];
-            ks[r] = kg[r] = gk[r] = kc[r] = nk[r] = gkr[r] = gdk[r] = hs[r] = 0.0f;
         }
-        for (int cb = q * 4; cb < nv; cb += 4 * S) {
-            const float4 h4 = *reinterpret_cast<const float4*>(hc + cb);
-            const float4 g4 = *reinterpret_cast<const float4*>(gs + cb);
-            float4 c4 = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (KIND != 0) c4 = *reinterpret_cast<const float4*>(cs + cb);
-            const float hh[4] = {h4.x, h4.y, h4.z, h4.w};
-            const float gg[4] = {g4.x, g4.y, g4.z, g4.w};
-            const float cc[4] = {c4.x, c4.y, c4.z, c4.w};
+        {
+            // two columns per packed op: u = (h_i - h_j) / bw is one FFMA2 in
+            // transport coordinates; columns past n hold a far pad whose terms
+            // vanish.  Row sums are kept as two partial lanes and folded after.
+            float2 hi2[R], ks2[R], kg2[R], gk2[R], kc2[R], gkr2[R], gdk2[R], hs2[R];
+            float nks[R];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                // positions are in transport coordinates, so u = (h_i - h_j) / bw
-                // is one FADD; columns past n hold a far pad whose terms vanish
+            for (int r = 0; r < R; ++r) {
+                hi2[r] = f2(hi[r]);
+                ks2[r] = kg2[r] = gk2[r] = kc2[r] = gkr2[r] = gdk2[r] = hs2[r] = f2(0.0f);
+                nks[r] = 0.0f;
+            }
+            for (int cb = q * 4; cb < nv; cb += 4 * S) {
+                const float4 h4 = *reinterpret_cast<const float4*>(hc + cb);
+                const float4 g4 = *reinterpret_cast<const float4*>(gs + cb);
+                float4 c4 = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (KIND != 0) c4 = *reinterpret_cast<const float4*>(cs + cb);
+                const float2 hh[2] = {make_float2(h4.x, h4.y), make_float2(h4.z, h4.w)};
+                const float2 gg[2] = {make_float2(g4.x, g4.y), make_float2(g4.z, g4.w)};
+                const float2 cc[2] = {make_float2(c4.x, c4.y), make_float2(c4.z, c4.w)};
 #pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const float u = hi[r] - hh[e];
-                    const float base_ = fmaf(u, u, 1.0f);
-                    const float K = rcp_approx(base_);
-                    const float K2 = K * K;
-                    kg[r] = fmaf(K, gg[e], kg[r]);
-                    if (KIND == 1 || KSD) {
-                        const float uk2 = u * K2;
-                        if (KIND == 1) gk[r] = fmaf(uk2, cc[e], gk[r]);
-                        else gk[r] += uk2;
-                        if (KSD) {
-                            if (KIND == 1) gkr[r] += uk2;
-                            gdk[r] = fmaf(gg[e], uk2, gdk[r]);
-                            hs[r] = fmaf(K2, fmaf(-4.0f, K, 3.0f), hs[r]);   // 4 (d/bw)^2 K - 1 = 3 - 4K
+                for (int hf = 0; hf < 2; ++hf) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const float2 u = fma2(hh[hf], f2(-1.0f), hi2[r]);
+                        const float2 b2 = fma2(u, u, f2(1.0f));
+                        const float2 K = make_float2(rcp_approx(b2.x), rcp_approx(b2.y));
+                        const float2 K2 = mul2(K, K);
+                        kg2[r] = fma2(K, gg[hf], kg2[r]);
+                        if (KIND == 1 || KSD) {
+                            const float2 uk2 = mul2(u, K2);
+                            if (KIND == 1) gk2[r] = fma2(uk2, cc[hf], gk2[r]);
+                            else gk2[r] = add2(gk2[r], uk2);
+                            if (KSD) {
+                                if (KIND == 1) gkr2[r] = add2(gkr2[r], uk2);
+                                gdk2[r] = fma2(gg[hf], uk2, gdk2[r]);
+                                hs2[r] = fma2(K2, fma2(K, f2(-4.0f), f2(3.0f)), hs2[r]);   // 4 (d/bw)^2 K - 1 = 3 - 4K
+                            }
+                        } else {
+                            gk2[r] = fma2(u, K2, gk2[r]);
                         }
-                    } else {
-                        gk[r] = fmaf(u, K2, gk[r]);
-                    }
-                    if (KIND == 2) {
-                        ks[r] += K;
-                        kc[r] = fmaf(K, cc[e], kc[r]);
-                        nk[r] = fmaf(K2, fabsf(fmaf(3.0f, base_, -4.0f)), nk[r]);   // |3 (d/bw)^2 - 1|
+                        if (KIND == 2) {
+                            ks2[r] = add2(ks2[r], K);
+                            kc2[r] = fma2(K, cc[hf], kc2[r]);
+                            const float2 w = fma2(b2, f2(3.0f), f2(-4.0f));             // 3 (d/bw)^2 - 1
+                            nks[r] = fmaf(K2.x, fabsf(w.x), nks[r]);
+                            nks[r] = fmaf(K2.y, fabsf(w.y), nks[r]);
+                        }
                     }
                 }
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                ks[r] = ks2[r].x + ks2[r].y;
+                kg[r] = kg2[r].x + kg2[r].y;
+                gk[r] = gk2[r].x + gk2[r].y;
+                kc[r] = kc2[r].x + kc2[r].y;
+                nk[r] = nks[r];
+                gkr[r] = gkr2[r].x + gkr2[r].y;
+                gdk[r] = gdk2[r].x + gdk2[r].y;
+                hs[r] = hs2[r].x + hs2[r].y;
             }
         }
 #pragma unroll

@@ -38,9 +38,9 @@ __device__ int tile_for(int n) {
                                  kTiles[2].R * (kThreads / kTiles[2].S), kTiles[3].R * (kThreads / kTiles[3].S),
                                  kTiles[4].R * (kThreads / kTiles[4].S), kTiles[5].R * (kThreads / kTiles[5].S),
                                  kTiles[6].R * (kThreads / kTiles[6].S)};
-    for (int t = kBatchTileLo; t < kNumTiles; ++t)
+    for (int t = kBatchTileLo; t <= kBatchTileHi; ++t)
         if (rows[t] >= n) return t;
-    return kNumTiles - 1;
+    return kBatchTileHi;
 }
 
 __device__ int bucket_of(int n) {
