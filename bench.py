@@ -237,6 +237,9 @@ def main():
 
     import __graft_entry__ as ge
     pkg = ge.load_package()
+    import importlib
+    shard = importlib.import_module("svpf_b200.shard")
+    dev = torch.device("cuda", local)
 
     F = args.filters
     ns, rho, sz, mu, nu = make_workload(F, seed=rank)
@@ -290,34 +293,30 @@ def main():
         dist.barrier()
     launches = batch.kernel_launches - launches0
     step_ms = [ev[k][0].elapsed_time(ev[k][1]) for k in range(args.steps)]
-    total_ms = float(sum(step_ms))
-    if world > 1:
-        tt = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    total_ms = shard.max_over_ranks(float(sum(step_ms)), dev)
     value = world * F * args.steps / (total_ms / 1e3)
 
-    # ---- end to end through the C ABI with host buffers (pinned staging inside)
-    e2e_steps = max(3, min(args.steps, 6))
-    host_y = ys
-    batch.step(host_y[0], np.zeros(F, np.float32))   # warm
+    # ---- end to end through the C ABI with host buffers: a second batch with the
+    #      same seed replays exactly the timed ticks (same states, same budgets)
+    batch_e2e = pkg.Batch(ns, cfgs, prms, stream=stream.cuda_stream)
+    batch_e2e.initialize(seed=1000 + rank)
+    zeros = np.zeros(F, np.float32)
+    for t in range(args.warmup):
+        batch_e2e.step(ys[t], ys[t - 1] if t else zeros)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for k in range(e2e_steps):
-        batch.step(host_y[(k + 1) % T], host_y[k % T])
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e_s = float(te.item())
-    e2e_value = world * F * e2e_steps / e2e_s
+    e2e_s = 0.0
+    for k in range(args.steps):
+        t = args.warmup + k
+        t0 = time.perf_counter()
+        batch_e2e.step(ys[t], ys[t - 1])
+        e2e_s += time.perf_counter() - t0
+    e2e_s = shard.max_over_ranks(e2e_s, dev)
+    e2e_value = world * F * args.steps / e2e_s
+    batch_e2e.close()
 
-    # ---- end-of-run exchange: per-filter log-likelihood sums, gathered on rank 0
+    # ---- end-of-run exchange: per-filter FP64 log-likelihood sums of every rank
     ctl = batch.ctl()
-    ll_sum = torch.tensor([c.loglik_sum for c in ctl], dtype=torch.float64, device="cuda")
-    if world > 1:
-        gathered = [torch.empty_like(ll_sum) for _ in range(world)]
-        dist.all_gather(gathered, ll_sum)
+    ll_all = shard.gather_by_filter(np.arange(F) + rank * F, [c.loglik_sum for c in ctl], world * F, dev)
     status_bad = sum(1 for c in ctl if c.status != 0)
 
     # ---- single-filter latency (configuration 1: N=512) and the plain-step loop
@@ -372,9 +371,11 @@ def main():
     mean_pairs = float(np.mean(pairs))
     mean_s = (sum(step_ms) / len(step_ms)) / 1e3
     achieved = mean_pairs / mean_s / 1e9
-    # per pair-iteration: 15 FP32-pipe and 2 MUFU instructions (one mixture-prior
-    # pair + one full-Newton transport pair); MUFU issues 16/clk/SM, FP32 128/clk/SM
-    peak = sms * sm_mhz * 1e6 * min(128.0 / 15.0, 16.0 / 2.0) / 1e9
+    # per pair-iteration (one mixture-prior pair + one full-Newton transport pair):
+    # 2 MUFU evaluations (ex2, rcp) at 16/clk/SM and 13 FP32 operations at
+    # 128/clk/SM -> the MUFU bounds it at 8 pair-iterations per clock per SM
+    PAIRS_PER_CLK = min(16.0 / 2.0, 128.0 / 13.0)
+    peak = sms * sm_mhz * 1e6 * PAIRS_PER_CLK / 1e9
     traffic = read_ncu_traffic()
 
     cpu = {}
@@ -392,17 +393,21 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
             "config": dict(workload_config(F), tiles={str(k): list(v) for k, v in tiles.items()}),
             "e2e": {"value": e2e_value, "unit": "filter-ticks/s", "h2d_bytes_per_step": 2 * F * 4,
-                    "d2h_bytes_per_step": F * 32, "timing": "host wall clock around svpf_batch_step"},
+                    "d2h_bytes_per_step": F * 32,
+                    "timing": "host wall clock around each svpf_batch_step call (host y in, host outputs back), "
+                              "same ticks as the device-timed steps"},
             "gpu_launches": launches,
             "roofline": {"bound": "fp32+mufu", "achieved": achieved, "peak": peak, "unit": "Gpair/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "note": "pair = one (i,j) Stein iteration: mixture-prior pair + transport pair; peak = "
-                                 f"{sms} SMs x {sm_mhz:.0f} MHz (measured) x min(128/15 FP32, 16/2 MUFU)"},
+                                 f"{sms} SMs x {sm_mhz:.0f} MHz (measured) x 8 pair/clk/SM (2 MUFU evaluations per "
+                                 "pair at 16/clk/SM; 13 FP32 ops at 128/clk/SM)"},
             "single_filter_latency": lat,
             "plain_step_loop": plain,
             "cpu_baseline": cpu,
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
             "status_errors": status_bad,
+            "loglik_sum_all_ranks": float(np.nansum(ll_all)),
         }
         print(json.dumps(line), flush=True)
     batch.close()

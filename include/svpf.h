@@ -407,9 +407,7 @@ int svpf_tile_choice(int n, int* rows_per_thread, int* col_split);
 /* Library facts. */
 const char* svpf_build_info(void);
 int svpf_debug_philox(uint32_t k0, uint32_t k1, const uint32_t* ctr4, uint32_t* out4, int count);
-/* The engine's FMA-pipe 2^x next to the hardware ex2.approx, evaluated on the
- * device for x[0..count) <= 0 (host arrays), for accuracy checks. */
-int svpf_debug_exp2(const float* x, float* poly_out, float* mufu_out, int count);
+
 
 #ifdef __cplusplus
 }

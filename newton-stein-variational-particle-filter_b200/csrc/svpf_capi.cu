@@ -586,19 +586,6 @@ int svpf_debug_philox(uint32_t k0, uint32_t k1, const uint32_t* ctr4, uint32_t* 
     return e == cudaSuccess ? SVPF_OK : SVPF_ERR_CUDA;
 }
 
-int svpf_debug_exp2(const float* x, float* poly, float* mufu, int count) {
-    if (count <= 0 || !x || !poly || !mufu) return SVPF_ERR_INVALID_ARG;
-    float* d = nullptr;
-    const size_t b = (size_t)count * sizeof(float);
-    if (cudaMalloc(&d, 3 * b) != cudaSuccess) return SVPF_ERR_CUDA;
-    cudaError_t e = cudaMemcpy(d, x, b, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = debug_exp2(d, d + count, d + 2 * count, count);
-    if (e == cudaSuccess) e = cudaMemcpy(poly, d + count, b, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(mufu, d + 2 * count, b, cudaMemcpyDeviceToHost);
-    cudaFree(d);
-    return e == cudaSuccess ? SVPF_OK : SVPF_ERR_CUDA;
-}
-
 const char* svpf_build_info(void) {
     return "svpf_b200: sm_100a; single-filter tick = 1 cluster launch (<=16 CTAs, DSMEM); "
            "batch tick = 1 persistent launch; particles resident in shared memory";

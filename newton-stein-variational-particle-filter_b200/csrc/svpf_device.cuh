@@ -60,38 +60,6 @@ __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
-// 2^-q for q >= 0 on the FMA pipe, two lanes at once.  Range reduction: t =
-// 1.5 * 2^23 - q rounds -q to the nearest integer n, which lands in the low
-// mantissa bits of t; 2^n is then added straight into the exponent field of
-// p(f), f = -q - n in [-1/2, 1/2] (exponent-field construction as in
-// Schraudolph, "A fast, compact approximation of the exponential function",
-// Neural Computation 1999).  p is a degree-5 polynomial for 2^f fitted for
-// this file by relative-error least squares on Chebyshev nodes (max relative
-// error 2.1e-7 in FP32), evaluated here in g = -f with alternating-sign
-// coefficients.  q is capped at 125, so results are never denormal; such
-// weights (< 3e-38) are negligible in every sum they enter.
-__device__ __forceinline__ float2 exp2_neg_fma2(float2 q) {
-    q.x = fminf(q.x, 125.0f);
-    q.y = fminf(q.y, 125.0f);
-    const float2 t = fma2(q, f2(-1.0f), f2(12582912.0f));
-    const float2 g = add2(q, add2(t, f2(-12582912.0f)));
-    float2 p = f2(-1.327646663e-03f);
-    p = fma2(p, g, f2(9.675540961e-03f));
-    p = fma2(p, g, f2(-5.550713465e-02f));
-    p = fma2(p, g, f2(2.402212024e-01f));
-    p = fma2(p, g, f2(-6.931469440e-01f));
-    p = fma2(p, g, f2(1.000000119e+00f));
-    return make_float2(__int_as_float(__float_as_int(p.x) + (__float_as_int(t.x) << 23)),
-                       __int_as_float(__float_as_int(p.y) + (__float_as_int(t.y) << 23)));
-}
-
-// Which packed exponentials (column pair hf of a chunk, row r) of the mixture
-// loop run on the FMA pipe: 3 of 16 with 8 rows per thread, 1 of 8 with 4.
-template <int R>
-__host__ __device__ constexpr bool exp_on_fma(int hf, int r) {
-    return R >= 4 && ((hf + 2 * r) % 5) == 4;
-}
-
 constexpr float kLog2e = 1.4426950408889634f;
 constexpr float kLn2 = 0.6931471805599453f;
 
@@ -503,8 +471,7 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
             sr[r] = 0.0f; wg[r] = 0.0f; wh[r] = 0.0f;
         }
         if (!STUDENT) {
-            // two columns per packed op; a few exponentials per chunk go to the
-            // FMA pipe so that MUFU and FMA pipes finish together
+            // two columns per packed op: 3 issue slots and 2 ex2 per column pair
             float2 x2[R], nl2[R], sr2[R], wg2[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -522,12 +489,7 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
                     for (int r = 0; r < R; ++r) {
                         const float2 d = fma2(mm[hf], f2(-1.0f), x2[r]);   // x - m
                         const float2 qq = fma2(d, d, nl2[r]);                // (x - m)^2 - min >= 0
-                        float2 w;
-                        if (exp_on_fma<R>(hf, r)) {
-                            w = exp2_neg_fma2(qq);
-                        } else {
-                            w = make_float2(ex2_approx(-qq.x), ex2_approx(-qq.y));
-                        }
+                        const float2 w = make_float2(ex2_approx(-qq.x), ex2_approx(-qq.y));
                         sr2[r] = add2(sr2[r], w);
                         wg2[r] = fma2(w, d, wg2[r]);
                     }

@@ -94,7 +94,6 @@ cudaError_t launch_single_large(const SingleArgs& a, int C, int tile, cudaStream
 cudaError_t launch_batch(const BatchArgs& a, size_t smem_bytes, int grid, cudaStream_t s);
 cudaError_t launch_init(const InitArgs& a, cudaStream_t s);
 int batch_grid(size_t smem_bytes);
-cudaError_t debug_exp2(const float* d_x, float* d_poly, float* d_mufu, int n);
 cudaError_t debug_philox(uint32_t k0, uint32_t k1, const uint32_t* d_ctr, uint32_t* d_out, int count);
 
 // Process-wide tuner table: tile chosen for a particle count (-1 = none yet).

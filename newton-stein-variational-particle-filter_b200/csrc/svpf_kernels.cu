@@ -44,20 +44,6 @@ __global__ void philox_kernel(uint32_t k0, uint32_t k1, const uint32_t* ctr, uin
     out[4 * i] = r.x; out[4 * i + 1] = r.y; out[4 * i + 2] = r.z; out[4 * i + 3] = r.w;
 }
 
-// The FMA-pipe 2^x (x <= 0) next to the hardware ex2.approx, for accuracy tests.
-__global__ void exp2_check_kernel(const float* x, float* poly, float* mufu, int n) {
-    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-    if (i >= n) return;
-    const float a = x[i], b = (i + 1 < n) ? x[i + 1] : 0.0f;
-    const float2 p = exp2_neg_fma2(make_float2(-a, -b));
-    poly[i] = p.x;
-    mufu[i] = ex2_approx(a);
-    if (i + 1 < n) {
-        poly[i + 1] = p.y;
-        mufu[i + 1] = ex2_approx(b);
-    }
-}
-
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -106,12 +92,6 @@ cudaError_t launch_single(const SingleArgs& a, int C, int tile, cudaStream_t s) 
 cudaError_t launch_init(const InitArgs& a, cudaStream_t s) {
     if (a.F < 1) return cudaErrorInvalidValue;
     init_kernel<<<a.F, kThreads, 0, s>>>(a);
-    return cudaGetLastError();
-}
-
-cudaError_t debug_exp2(const float* d_x, float* d_poly, float* d_mufu, int n) {
-    if (n <= 0) return cudaSuccess;
-    exp2_check_kernel<<<(n / 2 + 256) / 256, 256>>>(d_x, d_poly, d_mufu, n);
     return cudaGetLastError();
 }
 

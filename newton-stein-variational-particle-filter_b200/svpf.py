@@ -138,7 +138,6 @@ def lib() -> C.CDLL:
         "svpf_tile_choice": (_I, [_I, C.POINTER(_I), C.POINTER(_I)]),
         "svpf_build_info": (C.c_char_p, []),
         "svpf_debug_philox": (_I, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), _I]),
-        "svpf_debug_exp2": (_I, [_FP, _FP, _FP, _I]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -528,16 +527,6 @@ def philox(k0: int, k1: int, counters: np.ndarray) -> np.ndarray:
     if rc != SVPF_OK:
         raise RuntimeError(f"philox failed: {ERRORS.get(rc, rc)}")
     return out
-
-
-def exp2_check(x):
-    """(FMA-pipe 2^x, hardware ex2.approx) evaluated on the GPU for x <= 0."""
-    xs = _f32(x)
-    poly, mufu = np.empty_like(xs), np.empty_like(xs)
-    rc = lib().svpf_debug_exp2(_fp(xs), _fp(poly), _fp(mufu), xs.shape[0])
-    if rc != SVPF_OK:
-        raise RuntimeError(f"exp2 check failed: {ERRORS.get(rc, rc)}")
-    return poly, mufu
 
 
 def build_info() -> str:

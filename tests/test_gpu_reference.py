@@ -93,3 +93,68 @@ def test_rmse_matches_reference_cuda_step(pkg, n):
     with open(os.path.join(out_dir, f"reference_compare_n{n}.json"), "w") as fh:
         json.dump(res, fh, indent=1)
     assert abs(res["rmse_ours"] - res["rmse_ref"]) <= 0.02 * res["rmse_ref"], res
+
+
+def test_reference_plain_step_loop_on_batched_workload(pkg):
+    """The reference's svpf_step_graph looped over a sample of the batched
+    workload (own theta and N per filter, production configuration), the way
+    test/profile_svpf.cu:687-790 loops instruments; the engine's own plain
+    step over the same filters beside it.  Rates go to gpurun_out."""
+    import ctypes as C
+    import sys
+    import time
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    oracle, reflib = _ref_stock()
+    F = 32
+    ns, rho, sz, mu, nu = bench.make_workload(4096, 0)
+    ys = bench.sv_paths(6, rho, sz, mu, nu, 0)
+    refs, ours = [], []
+    for f in range(F):
+        cfg = pkg.production_config(float(nu[f]), bench.MAX_STEPS).to_dict()
+        r = oracle.RefFilter(reflib, int(ns[f]), bench.MAX_STEPS, float(nu[f]))
+        r.apply_config(oracle.config_from_dict(cfg))
+        p = oracle.OracleParams(float(rho[f]), float(sz[f]), float(mu[f]), 0.0)
+        r.L.svpf_ref_initialize(r.s, C.byref(p), tape.init_normals(f, int(ns[f])).ctypes.data_as(C.POINTER(C.c_float)))
+        refs.append((r, p))
+        o = pkg.SVPF(int(ns[f]), bench.MAX_STEPS, float(nu[f]))
+        o.configure(**cfg)
+        o.initialize(float(rho[f]), float(sz[f]), float(mu[f]), 0.0, seed=f)
+        ours.append(o)
+    dummy_n = np.zeros((1, 1), np.float32)
+
+    def ref_tick(t):
+        for f, (r, p) in enumerate(refs):
+            ll, vol, hm = C.c_float(), C.c_float(), C.c_float()
+            r.L.svpf_step_graph(r.s, C.c_float(float(ys[t, f])), C.c_float(float(ys[t - 1, f]) if t else 0.0),
+                                C.byref(p), C.byref(ll), C.byref(vol), C.byref(hm))
+
+    def our_tick(t):
+        for f, o in enumerate(ours):
+            o.step_raw(float(ys[t, f]), float(ys[t - 1, f]) if t else 0.0)
+
+    reflib.L.svpf_step_graph.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p]
+    ref_tick(0)
+    our_tick(0)
+    t0 = time.perf_counter()
+    for t in range(1, 5):
+        ref_tick(t)
+    ref_rate = F * 4 / (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    for t in range(1, 5):
+        our_tick(t)
+    our_rate = F * 4 / (time.perf_counter() - t0)
+    for r, _ in refs:
+        r.close()
+    for o in ours:
+        o.close()
+    out = {"filters": F, "ticks": 4, "reference_plain_loop_filter_ticks_per_s": ref_rate,
+           "engine_plain_loop_filter_ticks_per_s": our_rate,
+           "sample": "first 32 filters of the batched workload (bench.make_workload seed 0)"}
+    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+    with open(os.path.join(ROOT, "gpurun_out", "reference_plain_loop.json"), "w") as fh:
+        json.dump(out, fh, indent=1)
+    assert ref_rate > 0 and our_rate > 0
