@@ -95,7 +95,10 @@ typedef struct {
     X_INT(stein_repulsive_sign) X_INT(use_fan_mode) X_INT(stein_min_steps)    \
     X_INT(stein_max_steps) X_FLOAT(ksd_improvement_threshold)                 \
     X_INT(use_student_t_state) X_FLOAT(nu_state) X_INT(use_smoothing)         \
-    X_INT(smooth_lag) X_INT(smooth_output_lag) X_INT(use_heun)
+    X_INT(smooth_lag) X_INT(smooth_output_lag) X_INT(use_heun)                \
+    X_INT(use_two_factor) X_FLOAT(rho_fast) X_FLOAT(sigma_fast)               \
+    X_FLOAT(rho_slow) X_FLOAT(sigma_slow) X_FLOAT(bw_floor_fast)              \
+    X_FLOAT(bw_floor_slow)
 
 #define SVPF_DECL_INT_(f) int f;
 #define SVPF_DECL_FLOAT_(f) float f;
@@ -110,10 +113,15 @@ typedef struct {
     double guide_var;         /* EKF posterior variance (FP64 recursion) */
     double guide_K;
     double loglik_sum;        /* FP64 sum of per-tick log-likelihoods */
+    double guide_mean_fast;   /* two-factor EKF (innovation split), FP64 */
+    double guide_mean_slow;
+    double guide_var_fast;
+    double guide_var_slow;
     int    timestep;
     int    guide_initialized;
     int    stein_steps_used;
     int    smooth_head;
+    int    guide_2f_initialized;
     float  ksd_prev;          /* KSD of the previous tick: budget, beta, rejuvenation */
     float  ksd_last;          /* last KSD computed */
     float  vol_prev;
@@ -126,6 +134,8 @@ typedef struct {
     float  mu_state;
     float  mu_var;
     float  y_prev;
+    float  h_fast_mean;       /* two-factor: factor means of the previous tick */
+    float  h_slow_mean;
     float  smooth_h_mean[SVPF_SMOOTH_MAX_LAG];
     float  smooth_h_var[SVPF_SMOOTH_MAX_LAG];
     float  smooth_y[SVPF_SMOOTH_MAX_LAG];
@@ -235,7 +245,20 @@ typedef struct {
     int   use_persistent_kernel;   /* accepted, no effect: every tick is one launch */
     int   persistent_kernel_supported;
     int   use_heun;
-    int   use_two_factor;          /* not supported by this engine: step reports SVPF_ERR_UNSUPPORTED */
+
+    /* two-factor volatility h = mu + h_fast + h_slow (include/svpf.cuh:533-544) */
+    int   use_two_factor;
+    float rho_fast;
+    float sigma_fast;
+    float rho_slow;
+    float sigma_slow;
+    float bw_floor_fast;
+    float bw_floor_slow;
+    float guide_mean_fast;
+    float guide_mean_slow;
+    float guide_var_fast;
+    float guide_var_slow;
+    int   guide_2f_initialized;
 
     void* impl;                    /* engine-private state */
 } SVPFState;
@@ -322,6 +345,13 @@ int svpf_get_state(const SVPFState* state, svpf_ctl_t* ctl, float* h, float* h_p
 int svpf_set_state(SVPFState* state, const svpf_ctl_t* ctl, const float* h,
                    const float* h_prev, const float* v, const float* log_w);
 
+/* Two-factor particle arrays [n] each (any pointer may be NULL). */
+int svpf_get_state_2f(const SVPFState* state, float* h_fast, float* h_slow, float* h_fast_prev,
+                      float* h_slow_prev, float* v_fast, float* v_slow);
+int svpf_set_state_2f(SVPFState* state, const float* h_fast, const float* h_slow,
+                      const float* h_fast_prev, const float* h_slow_prev, const float* v_fast,
+                      const float* v_slow);
+
 /* Test hook: drive the next ticks' noise from a host tape instead of Philox.
  * normals[k*n + i] is the k-th normal of particle i within a tick; uniforms
  * likewise.  Pass NULL to return to Philox.  The tape is copied. */
@@ -366,6 +396,7 @@ int svpf_batch_sync(svpf_batch_t* b);
 int svpf_batch_n_filters(const svpf_batch_t* b);
 int svpf_batch_kernel_launches(const svpf_batch_t* b);  /* launches issued so far */
 int svpf_batch_get_ctl(const svpf_batch_t* b, svpf_ctl_t* ctl_host);          /* [n_filters] */
+/* h_out receives n values, or 2n (fast then slow) for a two-factor filter. */
 int svpf_batch_get_particles(const svpf_batch_t* b, int filter, float* h_out);
 int svpf_batch_set_noise_tape(svpf_batch_t* b, const float* normals, int n_normal_slots,
                               const float* uniforms, int n_uniform_slots);   /* same tape for all, [k][n_max] */

@@ -2,11 +2,13 @@
 // per tick.
 //
 // HBM layout: the particle arrays of all filters are packed back to back
-// (filter f at offset off[f], n[f] floats, offsets rounded to 16 floats), one
-// packed array each for h, h_prev, v and log_w.  Per-filter configuration,
-// parameters and control records are arrays of structs.  The kernel takes
-// filters from a work counter in decreasing order of cost (n^2 times the
-// Stein budget bound), so the largest ticks start first.
+// (filter f at offset off[f], n[f] floats -- 2 n[f] for a two-factor filter,
+// fast then slow -- offsets rounded to 16 floats), one packed array each for
+// h, h_prev, v and log_w.  Per-filter configuration, parameters and control
+// records are arrays of structs.  Single-factor and two-factor filters run in
+// two persistent kernels, one after the other on the batch's stream; each
+// takes its filters from a work counter in decreasing order of cost (n^2 times
+// the Stein budget bound), so the largest ticks start first.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -21,7 +23,10 @@ using namespace svpf;
 
 struct svpf_batch {
     int F = 0;
+    int F1 = 0, F2 = 0;          // single-factor / two-factor filters
     int n_max = 0;
+    int n_max1 = 0, n_max2 = 0;
+    std::vector<uint8_t> tf;     // two-factor flag per filter
     long long total = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -51,8 +56,8 @@ struct svpf_batch {
     float* tape_u = nullptr;
     int slots_n = 0, slots_u = 0;
     unsigned long long seed = 0;
-    size_t smem = 0;
-    int grid = 0;
+    size_t smem = 0, smem2 = 0;
+    int grid = 0, grid2 = 0;
     int launches = 0;
     int heun = 0;
     // graph
@@ -84,7 +89,7 @@ void ctl_fresh(svpf_ctl_t* c) {
 BatchArgs make_args(svpf_batch* b, const float* d_yt, const float* d_yp, svpf_out_t* d_out) {
     BatchArgs a;
     std::memset(&a, 0, sizeof(a));
-    a.F = b->F;
+    a.F = b->F1;
     a.order = b->d_order;
     a.queue = b->d_queue;
     a.n = b->d_n;
@@ -110,11 +115,22 @@ BatchArgs make_args(svpf_batch* b, const float* d_yt, const float* d_yp, svpf_ou
     return a;
 }
 
+int kernels_per_tick(const svpf_batch* b) { return (b->F1 > 0 ? 1 : 0) + (b->F2 > 0 ? 1 : 0); }
+
 int enqueue_tick(svpf_batch* b, const float* d_yt, const float* d_yp, svpf_out_t* d_out) {
-    if (cudaMemsetAsync(b->d_queue, 0, sizeof(int), b->stream) != cudaSuccess) return SVPF_ERR_CUDA;
-    const BatchArgs a = make_args(b, d_yt, d_yp, d_out);
-    if (launch_batch(a, b->smem, b->grid, b->stream) != cudaSuccess) return SVPF_ERR_CUDA;
-    ++b->launches;
+    if (cudaMemsetAsync(b->d_queue, 0, 2 * sizeof(int), b->stream) != cudaSuccess) return SVPF_ERR_CUDA;
+    BatchArgs a = make_args(b, d_yt, d_yp, d_out);
+    if (b->F1 > 0) {
+        if (launch_batch(a, b->smem, b->grid, b->stream) != cudaSuccess) return SVPF_ERR_CUDA;
+        ++b->launches;
+    }
+    if (b->F2 > 0) {
+        a.F = b->F2;
+        a.order = b->d_order + b->F1;
+        a.queue = b->d_queue + 1;
+        if (launch_batch_2f(a, b->smem2, b->grid2, b->stream) != cudaSuccess) return SVPF_ERR_CUDA;
+        ++b->launches;
+    }
     return SVPF_OK;
 }
 
@@ -141,18 +157,31 @@ extern "C" {
 svpf_batch_t* svpf_batch_create(int F, const int* ns, const svpf_config_t* cfgs, const SVPFParams* prms,
                                 cudaStream_t stream) {
     if (F < 1 || !ns || !cfgs || !prms) return nullptr;
-    int n_max = 0;
+    int n_max = 0, n_max1 = 0, n_max2 = 0, F1 = 0, heun = 0;
     for (int f = 0; f < F; ++f) {
         if (ns[f] < 1 || ns[f] > SVPF_MAX_PARTICLES) return nullptr;
         n_max = std::max(n_max, ns[f]);
+        if (cfgs[f].use_two_factor) {
+            if (cfgs[f].n_stein_steps < 1) return nullptr;
+            n_max2 = std::max(n_max2, ns[f]);
+        } else {
+            n_max1 = std::max(n_max1, ns[f]);
+            heun |= cfgs[f].use_heun != 0;
+            ++F1;
+        }
     }
-    int heun = 0;
-    for (int f = 0; f < F; ++f) heun |= cfgs[f].use_heun != 0;
-    if (tick_smem_bytes(n_max, 1, heun != 0) > max_dyn_smem()) return nullptr;
+    if (F1 > 0 && tick_smem_bytes(n_max1, 1, heun != 0) > max_dyn_smem()) return nullptr;
+    if (F1 < F && tick_smem_bytes_2f(n_max2, 1) > max_dyn_smem()) return nullptr;
     svpf_batch* b = new svpf_batch();
     b->heun = heun;
     b->F = F;
+    b->F1 = F1;
+    b->F2 = F - F1;
     b->n_max = n_max;
+    b->n_max1 = n_max1;
+    b->n_max2 = n_max2;
+    b->tf.resize(F);
+    for (int f = 0; f < F; ++f) b->tf[f] = cfgs[f].use_two_factor ? 1 : 0;
     b->ns.assign(ns, ns + F);
     b->cfgs.assign(cfgs, cfgs + F);
     b->prms.assign(prms, prms + F);
@@ -161,7 +190,7 @@ svpf_batch_t* svpf_batch_create(int F, const int* ns, const svpf_config_t* cfgs,
     long long off = 0;
     for (int f = 0; f < F; ++f) {
         b->offs[f] = off;
-        off += (ns[f] + 15) / 16 * 16;
+        off += ((b->tf[f] ? 2 : 1) * ns[f] + 15) / 16 * 16;
     }
     b->total = off;
     if (stream) {
@@ -170,18 +199,26 @@ svpf_batch_t* svpf_batch_create(int F, const int* ns, const svpf_config_t* cfgs,
         cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
         b->own_stream = true;
     }
-    // work order: largest expected cost first
+    // work order: single-factor filters then two-factor filters, each
+    // largest expected cost first
+    auto cost = [&](int f) {
+        const svpf_config_t& c = cfgs[f];
+        if (c.use_two_factor) {
+            const int na = c.use_annealing ? c.n_anneal_steps : 1;
+            return 2.0 * ns[f] * ns[f] * std::max(na * c.n_stein_steps, 1);
+        }
+        return (double)ns[f] * ns[f] * std::max(c.stein_max_steps, 1);
+    };
     std::vector<int> order(F);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
-        const double ca = (double)ns[a] * ns[a] * std::max(cfgs[a].stein_max_steps, 1);
-        const double cc = (double)ns[c] * ns[c] * std::max(cfgs[c].stein_max_steps, 1);
-        return ca > cc;
+        if (b->tf[a] != b->tf[c]) return b->tf[a] < b->tf[c];
+        return cost(a) > cost(c);
     });
     std::vector<svpf_ctl_t> ctl(F);
     for (auto& c : ctl) ctl_fresh(&c);
     bool ok = dalloc(&b->d_n, F) && dalloc(&b->d_off, F) && dalloc(&b->d_tile, F) && dalloc(&b->d_order, F) &&
-              dalloc(&b->d_queue, 1) && dalloc(&b->d_cfg, F) && dalloc(&b->d_prm, F) && dalloc(&b->d_ctl, F) &&
+              dalloc(&b->d_queue, 2) && dalloc(&b->d_cfg, F) && dalloc(&b->d_prm, F) && dalloc(&b->d_ctl, F) &&
               dalloc(&b->d_h, b->total) && dalloc(&b->d_hp, b->total) && dalloc(&b->d_v, b->total) &&
               dalloc(&b->d_lw, b->total) && dalloc(&b->d_y, 2 * (size_t)F) && dalloc(&b->d_out, F);
     ok = ok && cudaHostAlloc(&b->h_stage, 2 * (size_t)F * sizeof(float), cudaHostAllocDefault) == cudaSuccess &&
@@ -194,10 +231,15 @@ svpf_batch_t* svpf_batch_create(int F, const int* ns, const svpf_config_t* cfgs,
          cudaMemcpy(b->d_ctl, ctl.data(), F * sizeof(svpf_ctl_t), cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemset(b->d_lw, 0, b->total * sizeof(float)) == cudaSuccess;
     ok = ok && upload_tiles(b) == SVPF_OK;
-    if (ok) {
-        b->smem = tick_smem_bytes(n_max, 1, heun != 0);
+    if (ok && b->F1 > 0) {
+        b->smem = tick_smem_bytes(n_max1, 1, heun != 0);
         b->grid = batch_grid(b->smem);
         ok = b->grid > 0;
+    }
+    if (ok && b->F2 > 0) {
+        b->smem2 = tick_smem_bytes_2f(n_max2, 1);
+        b->grid2 = batch_grid_2f(b->smem2);
+        ok = b->grid2 > 0;
     }
     if (!ok) {
         svpf_batch_destroy(b);
@@ -236,7 +278,8 @@ void svpf_batch_destroy(svpf_batch_t* b) {
 int svpf_batch_initialize(svpf_batch_t* b, unsigned long long seed) {
     if (!b) return SVPF_ERR_INVALID_ARG;
     b->seed = seed;
-    std::vector<float> mu(b->F), sd(b->F);
+    if (b->F2 > 0 && b->tape_n && b->slots_n < 3) return SVPF_ERR_TAPE_SHORT;
+    std::vector<float> mu(b->F), sd(b->F), sdf(b->F, 0.0f), sds(b->F, 0.0f);
     std::vector<svpf_ctl_t> ctl(b->F);
     if (cudaMemcpy(ctl.data(), b->d_ctl, b->F * sizeof(svpf_ctl_t), cudaMemcpyDeviceToHost) != cudaSuccess)
         return SVPF_ERR_CUDA;
@@ -263,11 +306,34 @@ int svpf_batch_initialize(svpf_batch_t* b, unsigned long long seed) {
         s.stein_steps_used = c.n_stein_steps;
         s.loglik_sum = 0.0;
         s.status = SVPF_OK;
+        if (c.use_two_factor) {
+            // svpf_optimized_graph.cu:414-447; the factor means of the previous
+            // tick (the guide's reference point) are kept, as the reference does
+            sdf[f] = c.sigma_fast / std::sqrt(1.0f - c.rho_fast * c.rho_fast + 1e-8f);
+            sds[f] = c.sigma_slow / std::sqrt(1.0f - c.rho_slow * c.rho_slow + 1e-8f);
+            s.guide_2f_initialized = 0;
+            s.guide_mean_fast = 0.0;
+            s.guide_mean_slow = 0.0;
+            s.guide_var_fast = c.sigma_fast * c.sigma_fast / (1.0f - c.rho_fast * c.rho_fast + 1e-6f);
+            s.guide_var_slow = c.sigma_slow * c.sigma_slow / (1.0f - c.rho_slow * c.rho_slow + 1e-6f);
+        }
     }
-    float *d_mu = nullptr, *d_sd = nullptr;
-    if (!dalloc(&d_mu, b->F) || !dalloc(&d_sd, b->F)) return SVPF_ERR_CUDA;
+    float *d_mu = nullptr, *d_sd = nullptr, *d_sdf = nullptr, *d_sds = nullptr;
+    uint8_t* d_tf = nullptr;
+    if (!dalloc(&d_mu, b->F) || !dalloc(&d_sd, b->F) || !dalloc(&d_sdf, b->F) || !dalloc(&d_sds, b->F) ||
+        !dalloc(&d_tf, b->F)) {
+        cudaFree(d_mu);
+        cudaFree(d_sd);
+        cudaFree(d_sdf);
+        cudaFree(d_sds);
+        cudaFree(d_tf);
+        return SVPF_ERR_CUDA;
+    }
     cudaMemcpy(d_mu, mu.data(), b->F * sizeof(float), cudaMemcpyHostToDevice);
     cudaMemcpy(d_sd, sd.data(), b->F * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_sdf, sdf.data(), b->F * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_sds, sds.data(), b->F * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_tf, b->tf.data(), b->F, cudaMemcpyHostToDevice);
     cudaMemcpy(b->d_cfg, b->cfgs.data(), b->F * sizeof(svpf_config_t), cudaMemcpyHostToDevice);
     cudaMemcpy(b->d_ctl, ctl.data(), b->F * sizeof(svpf_ctl_t), cudaMemcpyHostToDevice);
     InitArgs a;
@@ -281,11 +347,18 @@ int svpf_batch_initialize(svpf_batch_t* b, unsigned long long seed) {
     a.mu = d_mu;
     a.sd = d_sd;
     a.seed = seed;
-    a.tape0 = b->tape_n;   // test tape: slot 0 holds the initial normals
+    a.tape0 = b->tape_n;   // test tape: slot 0 (and 1, 2 for two factors) hold the initial normals
+    a.tape_stride = b->n_max;
+    a.tf = d_tf;
+    a.sdf = d_sdf;
+    a.sds = d_sds;
     cudaError_t e = launch_init(a, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     cudaFree(d_mu);
     cudaFree(d_sd);
+    cudaFree(d_sdf);
+    cudaFree(d_sds);
+    cudaFree(d_tf);
     return e == cudaSuccess ? SVPF_OK : SVPF_ERR_CUDA;
 }
 
@@ -324,7 +397,7 @@ int svpf_batch_graph_launch(svpf_batch_t* b, const float* d_yt, const float* d_y
         if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return SVPF_ERR_CUDA;
         const int launches = b->launches;
         const int rc = enqueue_tick(b, d_yt, d_yp, d_out);
-        b->launches = launches;
+        b->launches = launches;   // counted per replay below
         cudaGraph_t g = nullptr;
         const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
         if (rc != SVPF_OK || e != cudaSuccess) {
@@ -341,7 +414,7 @@ int svpf_batch_graph_launch(svpf_batch_t* b, const float* d_yt, const float* d_y
         b->g_out = d_out;
     }
     if (cudaGraphLaunch(b->gexec, b->stream) != cudaSuccess) return SVPF_ERR_CUDA;
-    ++b->launches;
+    b->launches += kernels_per_tick(b);
     return SVPF_OK;
 }
 
@@ -363,7 +436,8 @@ int svpf_batch_get_ctl(const svpf_batch_t* b, svpf_ctl_t* ctl) {
 int svpf_batch_get_particles(const svpf_batch_t* b, int f, float* h_out) {
     if (!b || !h_out || f < 0 || f >= b->F) return SVPF_ERR_INVALID_ARG;
     cudaStreamSynchronize(b->stream);
-    return cudaMemcpy(h_out, b->d_h + b->offs[f], b->ns[f] * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess
+    const size_t len = (size_t)(b->tf[f] ? 2 : 1) * b->ns[f];
+    return cudaMemcpy(h_out, b->d_h + b->offs[f], len * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess
                ? SVPF_OK : SVPF_ERR_CUDA;
 }
 

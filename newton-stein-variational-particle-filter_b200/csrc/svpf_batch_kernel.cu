@@ -3,6 +3,7 @@
 // each filter's whole tick in shared memory.  No CTA ever waits on another.
 #include "svpf_internal.h"
 #include "svpf_tick.cuh"
+#include "svpf_tick2f.cuh"
 
 namespace svpf {
 
@@ -34,6 +35,10 @@ __global__ void __launch_bounds__(kThreads, 2) batch_tick_kernel(const __grid_co
         copy_words(&prm, &a.prm[f]);
         copy_words(&ctl, &a.ctl[f]);
         __syncthreads();
+        if (cfg.use_two_factor) {   // two-factor filters run in batch_tick_2f_kernel
+            if (threadIdx.x == 0) a.ctl[f].status = SVPF_ERR_UNSUPPORTED;
+            continue;
+        }
         const int n = a.n[f];
         const long long off = a.off[f];
         const Smem sm = carve(smem, n, 1, 0, a.heun != 0);
@@ -53,6 +58,67 @@ __global__ void __launch_bounds__(kThreads, 2) batch_tick_kernel(const __grid_co
         if (a.out != nullptr) copy_words(&a.out[f], &out);
         __syncthreads();
     }
+}
+
+// Two-factor filters (their particle segments hold [fast (n); slow (n)]).
+__global__ void __launch_bounds__(kThreads, 2) batch_tick_2f_kernel(const __grid_constant__ BatchArgs a) {
+    extern __shared__ __align__(16) float smem[];
+    __shared__ Plan pl;
+    __shared__ svpf_ctl_t ctl;
+    __shared__ svpf_config_t cfg;
+    __shared__ SVPFParams prm;
+    __shared__ svpf_out_t out;
+    __shared__ int s_next;
+    const Team team{0, 1};
+    for (;;) {
+        if (threadIdx.x == 0) s_next = atomicAdd(a.queue, 1);
+        __syncthreads();
+        const int w = s_next;
+        if (w >= a.F) break;
+        const int f = a.order[w];
+        copy_words(&cfg, &a.cfg[f]);
+        copy_words(&prm, &a.prm[f]);
+        copy_words(&ctl, &a.ctl[f]);
+        __syncthreads();
+        const int n = a.n[f];
+        const long long off = a.off[f];
+        const Smem2 sm = carve_2f(smem, n, 1, 0);
+        const FilterIO io{a.h + off, a.hp + off, a.v + off, a.lw + off, n};
+        const Noise nz{philox_key(a.seed, f), (uint32_t)ctl.timestep, a.tape_n, a.tape_u,
+                       a.slots_n, a.slots_u, a.tape_stride, &pl.flag};
+        const float yt = a.y_t[f], yp = a.y_prev[f];
+        switch (a.tile[f]) {
+            case 1: run_tick_2f<1, 4>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
+            case 2: run_tick_2f<1, 2>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
+            case 3: run_tick_2f<1, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
+            case 4: run_tick_2f<2, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
+            default: run_tick_2f<4, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
+        }
+        __syncthreads();
+        copy_words(&a.ctl[f], &ctl);
+        if (a.out != nullptr) copy_words(&a.out[f], &out);
+        __syncthreads();
+    }
+}
+
+int batch_grid_2f(size_t smem_bytes) {
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(batch_tick_2f_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn_smem());
+        configured = true;
+    }
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_tick_2f_kernel, kThreads, smem_bytes);
+    if (per_sm < 1) return 0;
+    return sms * per_sm;
+}
+
+cudaError_t launch_batch_2f(const BatchArgs& a, size_t smem_bytes, int grid, cudaStream_t s) {
+    if (grid < 1) return cudaErrorInvalidConfiguration;
+    batch_tick_2f_kernel<<<grid, kThreads, smem_bytes, s>>>(a);
+    return cudaGetLastError();
 }
 
 int batch_grid(size_t smem_bytes) {

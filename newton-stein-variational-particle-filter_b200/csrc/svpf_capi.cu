@@ -101,7 +101,19 @@ void set_defaults(SVPFState* s, int n_stein_steps, float nu) {
     s->ksd_prev = 1e10f;
     s->stein_steps_used = n_stein_steps;
     s->use_heun = 0;
+    // two-factor (:257-271)
     s->use_two_factor = 0;
+    s->rho_fast = 0.90f;
+    s->sigma_fast = 0.15f;
+    s->rho_slow = 0.99f;
+    s->sigma_slow = 0.05f;
+    s->bw_floor_fast = 0.01f;
+    s->bw_floor_slow = 0.05f;
+    s->guide_mean_fast = 0.0f;
+    s->guide_mean_slow = 0.0f;
+    s->guide_var_fast = 0.0f;
+    s->guide_var_slow = 0.0f;
+    s->guide_2f_initialized = 0;
     s->use_smoothing = 0;
     s->smooth_lag = 3;
     s->smooth_output_lag = 1;
@@ -128,6 +140,9 @@ struct Impl {
     int slots_n = 0, slots_u = 0;
     size_t cap_n = 0, cap_u = 0;
     bool tape_on = false;
+    float* h2 = nullptr;              // two-factor particles [fast (n); slow (n)]
+    float* hp2 = nullptr;
+    float* v2 = nullptr;
     unsigned long long seed = 0;
     int cluster = 0;                  // 0 = automatic
     int tile = -1;
@@ -154,6 +169,11 @@ void ctl_gather(const SVPFState* s, const Impl* im, svpf_ctl_t* c) {
     c->mu_state = s->mu_state;
     c->mu_var = s->mu_var;
     c->y_prev = s->y_prev;
+    if ((float)c->guide_mean_fast != s->guide_mean_fast) c->guide_mean_fast = s->guide_mean_fast;
+    if ((float)c->guide_mean_slow != s->guide_mean_slow) c->guide_mean_slow = s->guide_mean_slow;
+    if ((float)c->guide_var_fast != s->guide_var_fast) c->guide_var_fast = s->guide_var_fast;
+    if ((float)c->guide_var_slow != s->guide_var_slow) c->guide_var_slow = s->guide_var_slow;
+    c->guide_2f_initialized = s->guide_2f_initialized;
     for (int i = 0; i < SVPF_SMOOTH_MAX_LAG; ++i) {
         c->smooth_h_mean[i] = s->smooth_h_mean[i];
         c->smooth_h_var[i] = s->smooth_h_var[i];
@@ -175,6 +195,11 @@ void ctl_scatter(const svpf_ctl_t* c, SVPFState* s, Impl* im) {
     s->sigma_z_effective = c->sigma_z_effective;
     s->mu_state = c->mu_state;
     s->mu_var = c->mu_var;
+    s->guide_mean_fast = (float)c->guide_mean_fast;
+    s->guide_mean_slow = (float)c->guide_mean_slow;
+    s->guide_var_fast = (float)c->guide_var_fast;
+    s->guide_var_slow = (float)c->guide_var_slow;
+    s->guide_2f_initialized = c->guide_2f_initialized;
     for (int i = 0; i < SVPF_SMOOTH_MAX_LAG; ++i) {
         s->smooth_h_mean[i] = c->smooth_h_mean[i];
         s->smooth_h_var[i] = c->smooth_h_var[i];
@@ -216,6 +241,14 @@ int pick_cluster(const SVPFState* s, const Impl* im) {
     return C;
 }
 
+// Two-factor: the smallest cluster at least the default whose shared memory
+// fits (every member holds both factors' positions); 0 if none does.
+int pick_cluster_2f(const SVPFState* s, const Impl* im) {
+    int C = im->cluster > 0 ? im->cluster : default_cluster(s->n_particles);
+    while (C <= 16 && tick_smem_bytes_2f(s->n_particles, C) > max_dyn_smem()) C <<= 1;   // 16: largest cluster
+    return C <= 16 ? C : 0;
+}
+
 void step_impl(SVPFState* s, float y_t, float y_prev, const SVPFParams* params,
                unsigned long long seed, float* ll, float* vol, float* hm) {
     Impl* im = impl_of(s);
@@ -223,8 +256,9 @@ void step_impl(SVPFState* s, float y_t, float y_prev, const SVPFParams* params,
         if (s) set_err(s, SVPF_ERR_INVALID_ARG);
         return;
     }
-    if (s->use_two_factor) {
-        set_err(s, SVPF_ERR_UNSUPPORTED);
+    const bool tf = s->use_two_factor != 0;
+    if (tf && s->n_stein_steps < 1) {
+        set_err(s, SVPF_ERR_INVALID_ARG);
         return;
     }
     SingleArgs a;
@@ -234,9 +268,9 @@ void step_impl(SVPFState* s, float y_t, float y_prev, const SVPFParams* params,
     ctl_gather(s, im, &a.ctl);
     a.y_t = y_t;
     a.y_prev = y_prev;
-    a.h = s->h;
-    a.hp = s->h_prev;
-    a.v = s->d_grad_v;
+    a.h = tf ? im->h2 : s->h;
+    a.hp = tf ? im->hp2 : s->h_prev;
+    a.v = tf ? im->v2 : s->d_grad_v;
     a.lw = s->log_weights;
     a.n = s->n_particles;
     a.seed = seed;
@@ -248,9 +282,13 @@ void step_impl(SVPFState* s, float y_t, float y_prev, const SVPFParams* params,
     }
     a.ctl_out = im->dev_res_ctl;
     a.out = im->dev_res_out;
-    const int C = pick_cluster(s, im);
+    const int C = tf ? pick_cluster_2f(s, im) : pick_cluster(s, im);
+    if (C < 1) {
+        set_err(s, SVPF_ERR_UNSUPPORTED);
+        return;
+    }
     const int tile = im->tile >= 0 ? im->tile : default_single_tile(s->n_particles, C);
-    cudaError_t e = launch_single(a, C, tile, s->stream);
+    cudaError_t e = tf ? launch_single_2f(a, C, tile, s->stream) : launch_single(a, C, tile, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) {
         set_err(s, SVPF_ERR_CUDA);
@@ -285,13 +323,17 @@ SVPFState* svpf_create(int n_particles, int n_stein_steps, float nu, cudaStream_
     const size_t bytes = (size_t)n_particles * sizeof(float);
     bool ok = cudaMalloc(&s->h, bytes) == cudaSuccess && cudaMalloc(&s->h_prev, bytes) == cudaSuccess &&
               cudaMalloc(&s->log_weights, bytes) == cudaSuccess && cudaMalloc(&s->d_grad_v, bytes) == cudaSuccess;
+    ok = ok && cudaMalloc(&im->h2, 2 * bytes) == cudaSuccess && cudaMalloc(&im->hp2, 2 * bytes) == cudaSuccess &&
+         cudaMalloc(&im->v2, 2 * bytes) == cudaSuccess;
     ok = ok && cudaHostAlloc(&im->res_ctl, sizeof(svpf_ctl_t), cudaHostAllocMapped) == cudaSuccess &&
          cudaHostAlloc(&im->res_out, sizeof(svpf_out_t), cudaHostAllocMapped) == cudaSuccess;
     ok = ok && cudaHostGetDevicePointer((void**)&im->dev_res_ctl, im->res_ctl, 0) == cudaSuccess &&
          cudaHostGetDevicePointer((void**)&im->dev_res_out, im->res_out, 0) == cudaSuccess;
     if (ok) {
         ok = cudaMemset(s->h, 0, bytes) == cudaSuccess && cudaMemset(s->h_prev, 0, bytes) == cudaSuccess &&
-             cudaMemset(s->log_weights, 0, bytes) == cudaSuccess && cudaMemset(s->d_grad_v, 0, bytes) == cudaSuccess;
+             cudaMemset(s->log_weights, 0, bytes) == cudaSuccess && cudaMemset(s->d_grad_v, 0, bytes) == cudaSuccess &&
+             cudaMemset(im->h2, 0, 2 * bytes) == cudaSuccess && cudaMemset(im->hp2, 0, 2 * bytes) == cudaSuccess &&
+             cudaMemset(im->v2, 0, 2 * bytes) == cudaSuccess;
     }
     if (!ok) {
         svpf_destroy(s);
@@ -314,6 +356,9 @@ void svpf_destroy(SVPFState* s) {
         if (im->res_out) cudaFreeHost(im->res_out);
         if (im->tape_n) cudaFree(im->tape_n);
         if (im->tape_u) cudaFree(im->tape_u);
+        cudaFree(im->h2);
+        cudaFree(im->hp2);
+        cudaFree(im->v2);
         delete im;
     }
     std::free(s);
@@ -343,8 +388,34 @@ void svpf_initialize(SVPFState* s, const SVPFParams* p, unsigned long long seed)
     a.sd0 = sqrtf(var);
     a.seed = seed;
     a.tape0 = im->tape_on ? im->tape_n : nullptr;
+    a.tape_stride = s->n_particles;
+    const bool tf = s->use_two_factor != 0;
+    if (tf && im->tape_on && im->slots_n < 3) {
+        set_err(s, SVPF_ERR_TAPE_SHORT);
+        return;
+    }
+    if (tf) {
+        // svpf_optimized_graph.cu:414-447
+        a.tf0 = 1;
+        a.sdf0 = s->sigma_fast / sqrtf(1.0f - s->rho_fast * s->rho_fast + 1e-8f);
+        a.sds0 = s->sigma_slow / sqrtf(1.0f - s->rho_slow * s->rho_slow + 1e-8f);
+        a.h2 = im->h2;
+        a.hp2 = im->hp2;
+        a.v2 = im->v2;
+    }
     cudaError_t e = launch_init(a, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (tf) {
+        s->guide_2f_initialized = 0;
+        s->guide_mean_fast = 0.0f;
+        s->guide_mean_slow = 0.0f;
+        s->guide_var_fast = s->sigma_fast * s->sigma_fast / (1.0f - s->rho_fast * s->rho_fast + 1e-6f);
+        s->guide_var_slow = s->sigma_slow * s->sigma_slow / (1.0f - s->rho_slow * s->rho_slow + 1e-6f);
+        im->cache.guide_mean_fast = s->guide_mean_fast;
+        im->cache.guide_mean_slow = s->guide_mean_slow;
+        im->cache.guide_var_fast = s->guide_var_fast;
+        im->cache.guide_var_slow = s->guide_var_slow;
+    }
     s->guide_initialized = 0;
     s->guide_mean = p->mu;
     s->guide_var = var;
@@ -530,6 +601,30 @@ int svpf_set_state(SVPFState* s, const svpf_ctl_t* ctl, const float* h, const fl
     if (hp && cudaMemcpy(s->h_prev, hp, b, cudaMemcpyHostToDevice) != cudaSuccess) return SVPF_ERR_CUDA;
     if (v && cudaMemcpy(s->d_grad_v, v, b, cudaMemcpyHostToDevice) != cudaSuccess) return SVPF_ERR_CUDA;
     if (lw && cudaMemcpy(s->log_weights, lw, b, cudaMemcpyHostToDevice) != cudaSuccess) return SVPF_ERR_CUDA;
+    return SVPF_OK;
+}
+
+int svpf_get_state_2f(const SVPFState* s, float* hf, float* hs, float* hfp, float* hsp, float* vf, float* vs) {
+    const Impl* im = impl_of(s);
+    if (!s || !im) return SVPF_ERR_INVALID_ARG;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    const size_t n = (size_t)s->n_particles, b = n * sizeof(float);
+    const float* src[6] = {im->h2, im->h2 + n, im->hp2, im->hp2 + n, im->v2, im->v2 + n};
+    float* dst[6] = {hf, hs, hfp, hsp, vf, vs};
+    for (int k = 0; k < 6; ++k)
+        if (dst[k] && cudaMemcpy(dst[k], src[k], b, cudaMemcpyDeviceToHost) != cudaSuccess) return SVPF_ERR_CUDA;
+    return SVPF_OK;
+}
+
+int svpf_set_state_2f(SVPFState* s, const float* hf, const float* hs, const float* hfp, const float* hsp,
+                      const float* vf, const float* vs) {
+    Impl* im = impl_of(s);
+    if (!s || !im) return SVPF_ERR_INVALID_ARG;
+    const size_t n = (size_t)s->n_particles, b = n * sizeof(float);
+    float* dst[6] = {im->h2, im->h2 + n, im->hp2, im->hp2 + n, im->v2, im->v2 + n};
+    const float* src[6] = {hf, hs, hfp, hsp, vf, vs};
+    for (int k = 0; k < 6; ++k)
+        if (src[k] && cudaMemcpy(dst[k], src[k], b, cudaMemcpyHostToDevice) != cudaSuccess) return SVPF_ERR_CUDA;
     return SVPF_OK;
 }
 

@@ -25,6 +25,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "svpf.h"
 
 namespace svpf {
@@ -34,6 +36,8 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr float kMuPad = 1e18f;   // sorted-prior pad: exp weight is exactly 0, products stay finite
 constexpr float kHPad = 1e15f;    // particle pad column: K ~ 1e-34, K^2 flushes to 0, no inf/NaN
+constexpr float kHPadRaw = 1e12f; // the same in log-volatility units: |u| <= 1e12 / bw stays far below
+                                  // sqrt(FLT_MAX) for any bandwidth the floors allow
 constexpr int kMaxCluster = 16;
 
 // ---------------------------------------------------------------------------
@@ -125,6 +129,14 @@ struct Noise {
     }
 };
 
+// Transport coordinates and step of one factor of the two-factor tick (the
+// single-factor tick keeps the same fields in its Plan).
+struct FactorPlan {
+    float eps_step, temp;
+    float bw, inv_bw, inv_bw2;
+    float center;
+};
+
 // ---------------------------------------------------------------------------
 // Tick plan: every scalar decision of a tick, made by one thread before the
 // particle phases (the reference makes them on the host between launches,
@@ -148,6 +160,9 @@ struct Plan {
     int transport;         // 0 vanilla, 1 Newton, 2 full Newton
     int fan;
     int flag;              // tape overrun etc.
+    FactorPlan fac[2];     // two-factor: fast, slow
+    float fmean[2];        // two-factor: factor means of the previous tick (guide)
+    float gmean2[2];       // two-factor: EKF guide means
     float red[4][kWarps];  // block reduction scratch
     float ksd_slot[kMaxCluster];
 };
@@ -402,6 +417,45 @@ __host__ __device__ inline int smem_floats(int n, int C, bool heun) {
     return 2 * np + np + np + m_len + (heun ? 3 : 1) * L;
 }
 
+// Two-factor tick: per factor x[2][np] (transport coordinates, double
+// buffered), g[np], prev[np] (positions at tick start), v[L] of own rows.
+__host__ __device__ inline int smem_floats_2f(int n, int C) {
+    const int np = round_up(n, 64);
+    const int L = round_up((n + C - 1) / C, 4);
+    return 2 * (4 * np + L);
+}
+
+struct Smem2 {
+    Smem f[2];          // per-factor views for transport_pass (c, mu unused)
+    float* prev[2];     // positions at tick start, all n
+};
+
+__device__ inline Smem2 carve_2f(float* base, int n, int C, int rank) {
+    Smem2 s;
+    const int np = round_up(n, 64);
+    const int L = (n + C - 1) / C;
+    const int Lp = round_up(L, 4);
+    for (int k = 0; k < 2; ++k) {
+        float* b = base + k * (4 * np + Lp);
+        Smem& f = s.f[k];
+        f.h[0] = b;
+        f.h[1] = b + np;
+        f.g = b + 2 * np;
+        s.prev[k] = b + 3 * np;
+        f.v = b + 4 * np;
+        f.c = nullptr;
+        f.mu = nullptr;
+        f.phi0 = f.phi1 = nullptr;
+        f.n = n;
+        f.np = np;
+        f.m_len = 0;
+        f.p2 = 0;
+        f.row0 = min(rank * L, n);
+        f.row1 = min(f.row0 + L, n);
+    }
+    return s;
+}
+
 __device__ inline Smem carve(float* base, int n, int C, int rank, bool heun) {
     Smem s;
     const int np = round_up(n, 64);
@@ -589,10 +643,15 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
 // ---------------------------------------------------------------------------
 enum { kTransport = 0, kPhiOnly = 1, kKsdOnly = 2 };
 
-template <int R, int S, int KIND, bool KSD, int MODE = kTransport>
-__device__ float transport_pass(const Smem& sm, int cur, const Plan& pl, const svpf_config_t& cfg,
+// P is Plan (single factor: positions stored in transport coordinates
+// (h - center) / bw) or FactorPlan (one factor of the two-factor tick:
+// positions stored in log-volatility units, scaled inside the pair FMA as
+// u = h_i / bw - h_j / bw, so the stiff per-factor priors read exact positions).
+template <int R, int S, int KIND, bool KSD, int MODE = kTransport, class P = Plan>
+__device__ float transport_pass(const Smem& sm, int cur, const P& pl, const svpf_config_t& cfg,
                                 float bf, const Noise& nz, int kn, const Team& team,
                                 float* __restrict__ phi_out = nullptr) {
+    constexpr bool RAW = std::is_same<P, FactorPlan>::value;
     constexpr int G = kThreads / S;
     const int grp = threadIdx.x / S, q = threadIdx.x % S;
     const float* __restrict__ hc = sm.h[cur];
@@ -626,9 +685,10 @@ __device__ float transport_pass(const Smem& sm, int cur, const Plan& pl, const s
             // vanish.  Row sums are kept as two partial lanes and folded after.
             float2 hi2[R], ks2[R], kg2[R], gk2[R], kc2[R], gkr2[R], gdk2[R], hs2[R];
             float nks[R];
+            const float2 colscale = f2(RAW ? -inv_bw : -1.0f);
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                hi2[r] = f2(hi[r]);
+                hi2[r] = f2(RAW ? hi[r] * inv_bw : hi[r]);
                 ks2[r] = kg2[r] = gk2[r] = kc2[r] = gkr2[r] = gdk2[r] = hs2[r] = f2(0.0f);
                 nks[r] = 0.0f;
             }
@@ -644,7 +704,7 @@ __device__ float transport_pass(const Smem& sm, int cur, const Plan& pl, const s
                 for (int hf = 0; hf < 2; ++hf) {
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
-                        const float2 u = fma2(hh[hf], f2(-1.0f), hi2[r]);
+                        const float2 u = fma2(hh[hf], colscale, hi2[r]);
                         const float2 b2 = fma2(u, u, f2(1.0f));
                         const float2 K = make_float2(rcp_approx(b2.x), rcp_approx(b2.y));
                         const float2 K2 = mul2(K, K);
@@ -725,8 +785,8 @@ __device__ float transport_pass(const Smem& sm, int cur, const Plan& pl, const s
                 const float drift = es * phi * rsqrtf(vn + cfg.rmsprop_eps);
                 float diff = 0.0f;
                 if (pl.temp > 1e-6f) diff = sqrtf(2.0f * es * pl.temp) * nz.normal(i, kn);
-                const float h_new = clamp_h(fmaf(hi[r], pl.bw, pl.center) + drift + diff);
-                const float hs_new = (h_new - pl.center) * inv_bw;
+                const float h_new = clamp_h((RAW ? hi[r] : fmaf(hi[r], pl.bw, pl.center)) + drift + diff);
+                const float hs_new = RAW ? h_new : (h_new - pl.center) * inv_bw;
                 for (int rk = 0; rk < team.size; ++rk) team.at(hn, rk)[i] = hs_new;
             }
         }

@@ -73,11 +73,24 @@ struct InitArgs {
     const float* sd;        // per filter [F] or nullptr (sd0)
     float mu0, sd0;
     unsigned long long seed;
-    const float* tape0;     // optional [n] initial normals (single filter)
+    const float* tape0;     // optional initial normals [slots][tape_stride]: slot 0 the
+                            // single-factor draw, slots 1 and 2 the fast and slow draws
+    int tape_stride;
+    // two-factor filters (svpf_init_two_factor_kernel, svpf_two_factor.cu:29-48)
+    const uint8_t* tf;      // per filter [F] or nullptr (tf0)
+    int tf0;
+    const float* sdf;       // stationary sd of the fast / slow factor, per filter or sdf0/sds0
+    const float* sds;
+    float sdf0, sds0;
+    float* h2;              // single filter: separate [2n] arrays for the factors; batch:
+    float* hp2;             // nullptr (the filter's own segment holds [fast; slow])
+    float* v2;
 };
 
-// Dynamic shared-memory bytes of a tick kernel for n particles on C CTAs.
+// Dynamic shared-memory bytes of a tick kernel for n particles on C CTAs
+// (single-factor, and two-factor).
 size_t tick_smem_bytes(int n, int C, bool heun);
+size_t tick_smem_bytes_2f(int n, int C);
 // Largest dynamic shared memory a CTA may use on this device.
 size_t max_dyn_smem();
 
@@ -91,9 +104,12 @@ int default_cluster(int n);
 cudaError_t launch_single(const SingleArgs& a, int C, int tile, cudaStream_t s);
 cudaError_t launch_single_small(const SingleArgs& a, int C, int tile, cudaStream_t s);
 cudaError_t launch_single_large(const SingleArgs& a, int C, int tile, cudaStream_t s);
+cudaError_t launch_single_2f(const SingleArgs& a, int C, int tile, cudaStream_t s);
 cudaError_t launch_batch(const BatchArgs& a, size_t smem_bytes, int grid, cudaStream_t s);
+cudaError_t launch_batch_2f(const BatchArgs& a, size_t smem_bytes, int grid, cudaStream_t s);
 cudaError_t launch_init(const InitArgs& a, cudaStream_t s);
 int batch_grid(size_t smem_bytes);
+int batch_grid_2f(size_t smem_bytes);
 cudaError_t debug_philox(uint32_t k0, uint32_t k1, const uint32_t* d_ctr, uint32_t* d_out, int count);
 
 // Process-wide tuner table: tile chosen for a particle count (-1 = none yet).

@@ -21,19 +21,37 @@ __global__ void init_kernel(const InitArgs a) {
     const long long off = a.off ? a.off[f] : 0;
     const float mu = a.mu ? a.mu[f] : a.mu0;
     const float sd = a.sd ? a.sd[f] : a.sd0;
+    const bool tf = a.tf ? a.tf[f] != 0 : a.tf0 != 0;
     const uint2 key = philox_key(a.seed, f);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        float z;
-        if (a.tape0 != nullptr) {
-            z = a.tape0[i];
-        } else {
-            const uint4 r = philox10(key, make_uint4((uint32_t)i, 0u, 0u, 2u));
-            z = normal_from_bits(r.x, r.y);
+    auto draw = [&](int i, int slot) {
+        if (a.tape0 != nullptr) return a.tape0[(size_t)slot * a.tape_stride + i];
+        const uint4 r = philox10(key, make_uint4((uint32_t)i, (uint32_t)slot, 0u, 2u));
+        return normal_from_bits(r.x, r.y);
+    };
+    if (!tf || a.h2 != nullptr) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const float h = clamp_h(mu + sd * draw(i, 0));
+            a.h[off + i] = h;
+            a.hp[off + i] = h;
+            a.v[off + i] = 0.0f;
         }
-        const float h = clamp_h(mu + sd * z);
-        a.h[off + i] = h;
-        a.hp[off + i] = h;
-        a.v[off + i] = 0.0f;
+    }
+    if (tf) {
+        const float sdf = a.sdf ? a.sdf[f] : a.sdf0;
+        const float sds = a.sds ? a.sds[f] : a.sds0;
+        float* H = a.h2 ? a.h2 : a.h + off;
+        float* HP = a.h2 ? a.hp2 : a.hp + off;
+        float* V = a.h2 ? a.v2 : a.v + off;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const float hf = clamp_h(sdf * draw(i, 1));
+            const float hs = clamp_h(sds * draw(i, 2));
+            H[i] = hf;
+            H[n + i] = hs;
+            HP[i] = hf;
+            HP[n + i] = hs;
+            V[i] = 0.0f;
+            V[n + i] = 0.0f;
+        }
     }
 }
 
@@ -48,6 +66,7 @@ __global__ void philox_kernel(uint32_t k0, uint32_t k1, const uint32_t* ctr, uin
 // host side
 // ---------------------------------------------------------------------------
 size_t tick_smem_bytes(int n, int C, bool heun) { return (size_t)smem_floats(n, C, heun) * sizeof(float); }
+size_t tick_smem_bytes_2f(int n, int C) { return (size_t)smem_floats_2f(n, C) * sizeof(float); }
 
 size_t max_dyn_smem() {
     static size_t cached = 0;

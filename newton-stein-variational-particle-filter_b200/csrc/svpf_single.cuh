@@ -5,6 +5,7 @@
 
 #include "svpf_internal.h"
 #include "svpf_tick.cuh"
+#include "svpf_tick2f.cuh"
 
 namespace svpf {
 
@@ -45,10 +46,39 @@ __global__ void __launch_bounds__(kThreads) single_tick_kernel(const __grid_cons
     }
 }
 
+// Two-factor tick: a.h / a.hp / a.v hold [fast (n); slow (n)].
 template <int R, int S>
+__global__ void __launch_bounds__(kThreads) single_tick_2f_kernel(const __grid_constant__ SingleArgs a) {
+    extern __shared__ __align__(16) float smem[];
+    __shared__ Plan pl;
+    __shared__ svpf_ctl_t ctl;
+    __shared__ svpf_config_t cfg;
+    __shared__ SVPFParams prm;
+    __shared__ svpf_out_t out;
+    cg::cluster_group cl = cg::this_cluster();
+    const Team team{(int)cl.block_rank(), (int)cl.num_blocks()};
+    copy_words(&ctl, &a.ctl);
+    copy_words(&cfg, &a.cfg);
+    copy_words(&prm, &a.prm);
+    __syncthreads();
+    const Smem2 sm = carve_2f(smem, a.n, team.size, team.rank);
+    const Noise nz{philox_key(a.seed, 0), (uint32_t)ctl.timestep, a.tape_n, a.tape_u,
+                   a.slots_n, a.slots_u, a.n, &pl.flag};
+    const FilterIO io{a.h, a.hp, a.v, a.lw, a.n};
+    run_tick_2f<R, S>(cfg, prm, ctl, a.y_t, a.y_prev, io, nz, sm, pl, team, out);
+    if (team.rank == 0) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            *a.ctl_out = ctl;
+            *a.out = out;
+        }
+    }
+}
+
+template <int R, int S, bool TWO_FACTOR = false>
 static cudaError_t launch_single_t(const SingleArgs& a, int C, cudaStream_t s) {
-    const size_t smem = tick_smem_bytes(a.n, C, a.cfg.use_heun != 0);
-    auto kern = single_tick_kernel<R, S>;
+    const size_t smem = TWO_FACTOR ? tick_smem_bytes_2f(a.n, C) : tick_smem_bytes(a.n, C, a.cfg.use_heun != 0);
+    auto kern = TWO_FACTOR ? single_tick_2f_kernel<R, S> : single_tick_kernel<R, S>;
     static bool configured[kMaxCluster + 1] = {};
     cudaError_t e;
     if (!configured[0]) {

@@ -43,7 +43,8 @@ CONFIG_FIELDS = [
     ("sigma_boost_max", _F), ("stein_repulsive_sign", _I), ("use_fan_mode", _I),
     ("stein_min_steps", _I), ("stein_max_steps", _I), ("ksd_improvement_threshold", _F),
     ("use_student_t_state", _I), ("nu_state", _F), ("use_smoothing", _I), ("smooth_lag", _I),
-    ("smooth_output_lag", _I), ("use_heun", _I),
+    ("smooth_output_lag", _I), ("use_heun", _I), ("use_two_factor", _I), ("rho_fast", _F),
+    ("sigma_fast", _F), ("rho_slow", _F), ("sigma_slow", _F), ("bw_floor_fast", _F), ("bw_floor_slow", _F),
 ]
 
 
@@ -71,11 +72,14 @@ class Ctl(C.Structure):
     """svpf_ctl_t: per-filter control record."""
     _fields_ = [
         ("guide_mean", C.c_double), ("guide_var", C.c_double), ("guide_K", C.c_double),
-        ("loglik_sum", C.c_double), ("timestep", _I), ("guide_initialized", _I),
-        ("stein_steps_used", _I), ("smooth_head", _I), ("ksd_prev", _F), ("ksd_last", _F),
+        ("loglik_sum", C.c_double), ("guide_mean_fast", C.c_double), ("guide_mean_slow", C.c_double),
+        ("guide_var_fast", C.c_double), ("guide_var_slow", C.c_double), ("timestep", _I),
+        ("guide_initialized", _I), ("stein_steps_used", _I), ("smooth_head", _I),
+        ("guide_2f_initialized", _I), ("ksd_prev", _F), ("ksd_last", _F),
         ("vol_prev", _F), ("h_mean_prev", _F), ("bw", _F), ("bw_sq", _F), ("return_ema", _F),
         ("return_var", _F), ("sigma_z_effective", _F), ("mu_state", _F), ("mu_var", _F),
-        ("y_prev", _F), ("smooth_h_mean", _F * SMOOTH_MAX_LAG), ("smooth_h_var", _F * SMOOTH_MAX_LAG),
+        ("y_prev", _F), ("h_fast_mean", _F), ("h_slow_mean", _F),
+        ("smooth_h_mean", _F * SMOOTH_MAX_LAG), ("smooth_h_var", _F * SMOOTH_MAX_LAG),
         ("smooth_y", _F * SMOOTH_MAX_LAG), ("status", _I), ("reserved", _I),
     ]
 
@@ -118,6 +122,8 @@ def lib() -> C.CDLL:
         "svpf_set_config": (None, [vp, C.POINTER(Config)]),
         "svpf_get_state": (_I, [vp, C.POINTER(Ctl), _FP, _FP, _FP, _FP]),
         "svpf_set_state": (_I, [vp, C.POINTER(Ctl), _FP, _FP, _FP, _FP]),
+        "svpf_get_state_2f": (_I, [vp, _FP, _FP, _FP, _FP, _FP, _FP]),
+        "svpf_set_state_2f": (_I, [vp, _FP, _FP, _FP, _FP, _FP, _FP]),
         "svpf_set_noise_tape": (_I, [vp, _FP, _I, _FP, _I]),
         "svpf_get_last_output": (_I, [vp, C.POINTER(Out)]),
         "svpf_set_cluster_size": (_I, [vp, _I]),
@@ -403,8 +409,23 @@ class SVPF:
         return ctl, h, hp, v, lw
 
     def set_state(self, ctl: Ctl, h, hp, v, lw):
-        arrs = [_f32(a) for a in (h, hp, v, lw)]
-        self._check(lib().svpf_set_state(self._s, C.byref(ctl), *[_fp(a) for a in arrs]))
+        """Restore the control record and the arrays; an array given as None is left as it is."""
+        arrs = [None if a is None else _f32(a) for a in (h, hp, v, lw)]
+        self._check(lib().svpf_set_state(self._s, C.byref(ctl), *[None if a is None else _fp(a) for a in arrs]))
+
+    def get_state_2f(self):
+        """Two-factor particle arrays, each [2n] as (fast, slow) concatenated:
+        positions, previous positions, RMSProp moments."""
+        n = self._n
+        bufs = [np.empty(n, np.float32) for _ in range(6)]
+        self._check(lib().svpf_get_state_2f(self._s, *[_fp(b) for b in bufs]))
+        return (np.concatenate(bufs[0:2]), np.concatenate(bufs[2:4]), np.concatenate(bufs[4:6]))
+
+    def set_state_2f(self, h, hp, v):
+        n = self._n
+        arrs = [_f32(a) for a in (h, hp, v)]
+        parts = [np.ascontiguousarray(a[k * n:(k + 1) * n]) for a in arrs for k in range(2)]
+        self._check(lib().svpf_set_state_2f(self._s, *[_fp(a) for a in parts]))
 
     def set_noise_tape(self, normals=None, uniforms=None):
         if normals is None:
@@ -487,7 +508,9 @@ class Batch:
         return arr
 
     def get_particles(self, f: int) -> np.ndarray:
-        out = np.empty(int(self._ns[f]), np.float32)
+        """Positions of filter f: [n], or [2n] (fast then slow) for two factors."""
+        m = 2 if self._cfgs[f].use_two_factor else 1
+        out = np.empty(m * int(self._ns[f]), np.float32)
         self._check(lib().svpf_batch_get_particles(self._b, int(f), _fp(out)))
         return out
 

@@ -43,6 +43,8 @@ CONFIG_FIELDS = [
     ("stein_max_steps", C.c_int), ("ksd_improvement_threshold", C.c_float),
     ("use_student_t_state", C.c_int), ("nu_state", C.c_float), ("use_smoothing", C.c_int),
     ("smooth_lag", C.c_int), ("smooth_output_lag", C.c_int), ("use_heun", C.c_int),
+    ("use_two_factor", C.c_int), ("rho_fast", C.c_float), ("sigma_fast", C.c_float), ("rho_slow", C.c_float),
+    ("sigma_slow", C.c_float), ("bw_floor_fast", C.c_float), ("bw_floor_slow", C.c_float),
 ]
 
 
@@ -57,12 +59,14 @@ class OracleParams(C.Structure):
 class OracleCtl(C.Structure):
     _fields_ = [
         ("guide_mean", C.c_double), ("guide_var", C.c_double), ("guide_K", C.c_double),
-        ("loglik_sum", C.c_double), ("timestep", C.c_int), ("guide_initialized", C.c_int),
-        ("stein_steps_used", C.c_int), ("smooth_head", C.c_int), ("ksd_prev", C.c_float),
+        ("loglik_sum", C.c_double), ("guide_mean_fast", C.c_double), ("guide_mean_slow", C.c_double),
+        ("guide_var_fast", C.c_double), ("guide_var_slow", C.c_double), ("timestep", C.c_int),
+        ("guide_initialized", C.c_int), ("stein_steps_used", C.c_int), ("smooth_head", C.c_int),
+        ("guide_2f_initialized", C.c_int), ("ksd_prev", C.c_float),
         ("ksd_last", C.c_float), ("vol_prev", C.c_float), ("h_mean_prev", C.c_float),
         ("bw", C.c_float), ("bw_sq", C.c_float), ("return_ema", C.c_float),
         ("return_var", C.c_float), ("sigma_z_effective", C.c_float), ("mu_state", C.c_float),
-        ("mu_var", C.c_float), ("y_prev", C.c_float),
+        ("mu_var", C.c_float), ("y_prev", C.c_float), ("h_fast_mean", C.c_float), ("h_slow_mean", C.c_float),
         ("smooth_h_mean", C.c_float * SMOOTH_MAX_LAG), ("smooth_h_var", C.c_float * SMOOTH_MAX_LAG),
         ("smooth_y", C.c_float * SMOOTH_MAX_LAG), ("status", C.c_int), ("reserved", C.c_int),
     ]
@@ -108,9 +112,11 @@ def config_to_dict(c) -> dict:
 
 
 def config_from_dict(d: dict, cls=None):
+    """Fields missing from d (records written before they existed) stay 0."""
     c = (cls or OracleConfig)()
     for f, _ in CONFIG_FIELDS:
-        setattr(c, f, d[f])
+        if f in d:
+            setattr(c, f, d[f])
     return c
 
 
@@ -186,9 +192,10 @@ class OracleFilter:
         self.cfg = cfg
         self.params = params
         self.ctl = default_ctl()
-        self.h = np.zeros(n)
-        self.h_prev = np.zeros(n)
-        self.v = np.zeros(n)
+        m = 2 * n if cfg.use_two_factor else n   # two factors: [fast; slow]
+        self.h = np.zeros(m)
+        self.h_prev = np.zeros(m)
+        self.v = np.zeros(m)
         self.log_w = np.zeros(n)
         self.precision = precision
 
@@ -285,7 +292,9 @@ class RefFilter:
 
     def get_state(self):
         ctl = OracleCtl()
-        h, hp, v, lw = (np.zeros(self.n) for _ in range(4))
+        m = 2 * self.n if self.read_config().use_two_factor else self.n
+        h, hp, v = (np.zeros(m) for _ in range(3))
+        lw = np.zeros(self.n)
         rc = self.L.svpf_ref_get_state(self.s, C.byref(ctl), _dptr(h), _dptr(hp), _dptr(v), _dptr(lw))
         assert rc == 0, rc
         return ctl, h, hp, v, lw

@@ -104,6 +104,8 @@ SVPFState* svpf_ref_create(int n, int n_stein, float nu) {
     cudaMemset(s->log_weights, 0, n * sizeof(float));
     cudaMemset(s->opt_backend.d_ksd, 0, sizeof(float));
     cudaMemset(s->opt_backend.d_bandwidth, 0, sizeof(float));
+    cudaMemset(s->opt_backend.d_h_fast_mean, 0, sizeof(float));
+    cudaMemset(s->opt_backend.d_h_slow_mean, 0, sizeof(float));
     cudaDeviceSynchronize();
     svpf_ref_tape_flags_take();
     return s;
@@ -126,7 +128,8 @@ void svpf_ref_destroy(SVPFState* s) { svpf_destroy(s); }
     X(sigma_boost_threshold) X(sigma_boost_max) X(stein_repulsive_sign)               \
     X(use_fan_mode) X(stein_min_steps) X(stein_max_steps)                             \
     X(ksd_improvement_threshold) X(use_student_t_state) X(nu_state) X(use_smoothing)  \
-    X(smooth_lag) X(smooth_output_lag) X(use_heun)
+    X(smooth_lag) X(smooth_output_lag) X(use_heun) X(use_two_factor) X(rho_fast)       \
+    X(sigma_fast) X(rho_slow) X(sigma_slow) X(bw_floor_fast) X(bw_floor_slow)
 
 void svpf_ref_apply_config(SVPFState* s, const oracle_config* c) {
 #define X(f) s->f = c->f;
@@ -140,15 +143,18 @@ void svpf_ref_read_config(const SVPFState* s, oracle_config* c) {
 #undef X
 }
 
+/* init_normals holds one draw per particle, three ([3][n]) with two factors. */
 int svpf_ref_initialize(SVPFState* s, const oracle_params* p, const float* init_normals) {
     int n = s->n_particles;
     float one = 1.0f;
-    if (svpf_ref_tape_set(init_normals, 1, &one, 0, n)) return -1;
+    if (svpf_ref_tape_set(init_normals, s->use_two_factor ? 3 : 1, &one, 0, n)) return -1;
     SVPFParams sp = {p->rho, p->sigma_z, p->mu, p->gamma};
     svpf_initialize(s, &sp, 0ull);
     return svpf_ref_tape_flags_take();
 }
 
+/* With two factors h, hp and v hold [fast (n); slow (n)] and map onto the
+ * backend's d_h_fast/d_h_slow, *_prev and d_grad_v_* buffers. */
 int svpf_ref_set_state(SVPFState* s, const oracle_ctl* c, const double* h, const double* hp,
                        const double* v, const double* lw) {
     int n = s->n_particles;
@@ -159,13 +165,26 @@ int svpf_ref_set_state(SVPFState* s, const oracle_ctl* c, const double* h, const
         for (int i = 0; i < n; ++i) buf[i] = (float)src[i];
         return check(cudaMemcpy(dst, buf.data(), n * sizeof(float), cudaMemcpyHostToDevice), "put");
     };
-    if (put(s->h, h) || put(s->h_prev, hp) || put(s->d_grad_v, v) || put(s->log_weights, lw)) return -1;
+    if (s->use_two_factor) {
+        if (put(o->d_h_fast, h) || put(o->d_h_slow, h + n) || put(o->d_h_fast_prev, hp) ||
+            put(o->d_h_slow_prev, hp + n) || put(o->d_grad_v_fast, v) || put(o->d_grad_v_slow, v + n) ||
+            put(s->log_weights, lw))
+            return -1;
+        s->guide_mean_fast = (float)c->guide_mean_fast;
+        s->guide_mean_slow = (float)c->guide_mean_slow;
+        s->guide_var_fast = (float)c->guide_var_fast;
+        s->guide_var_slow = (float)c->guide_var_slow;
+        s->guide_2f_initialized = c->guide_2f_initialized;
+    } else if (put(s->h, h) || put(s->h_prev, hp) || put(s->d_grad_v, v) || put(s->log_weights, lw)) {
+        return -1;
+    }
     auto put1 = [&](float* dst, float val) {
         return check(cudaMemcpy(dst, &val, sizeof(float), cudaMemcpyHostToDevice), "put1");
     };
     if (put1(o->d_h_mean_prev, c->h_mean_prev) || put1(o->d_bandwidth, c->bw) ||
         put1(o->d_bandwidth_sq, c->bw_sq) || put1(s->d_return_ema, c->return_ema) ||
-        put1(s->d_return_var, c->return_var) || put1(o->d_ksd, c->ksd_last))
+        put1(s->d_return_var, c->return_var) || put1(o->d_ksd, c->ksd_last) ||
+        put1(o->d_h_fast_mean, c->h_fast_mean) || put1(o->d_h_slow_mean, c->h_slow_mean))
         return -1;
     s->timestep = c->timestep;
     s->guide_initialized = c->guide_initialized;
@@ -198,13 +217,26 @@ int svpf_ref_get_state(SVPFState* s, oracle_ctl* c, double* h, double* hp, doubl
         for (int i = 0; i < n; ++i) dst[i] = buf[i];
         return 0;
     };
-    if (get(h, s->h) || get(hp, s->h_prev) || get(v, s->d_grad_v) || get(lw, s->log_weights)) return -1;
+    if (s->use_two_factor) {
+        if (get(h, o->d_h_fast) || get(h + n, o->d_h_slow) || get(hp, o->d_h_fast_prev) ||
+            get(hp + n, o->d_h_slow_prev) || get(v, o->d_grad_v_fast) || get(v + n, o->d_grad_v_slow) ||
+            get(lw, s->log_weights))
+            return -1;
+        c->guide_mean_fast = s->guide_mean_fast;
+        c->guide_mean_slow = s->guide_mean_slow;
+        c->guide_var_fast = s->guide_var_fast;
+        c->guide_var_slow = s->guide_var_slow;
+        c->guide_2f_initialized = s->guide_2f_initialized;
+    } else if (get(h, s->h) || get(hp, s->h_prev) || get(v, s->d_grad_v) || get(lw, s->log_weights)) {
+        return -1;
+    }
     auto get1 = [&](float* dst, const float* src) {
         return check(cudaMemcpy(dst, src, sizeof(float), cudaMemcpyDeviceToHost), "get1");
     };
     if (get1(&c->h_mean_prev, o->d_h_mean_prev) || get1(&c->bw, o->d_bandwidth) ||
         get1(&c->bw_sq, o->d_bandwidth_sq) || get1(&c->return_ema, s->d_return_ema) ||
-        get1(&c->return_var, s->d_return_var) || get1(&c->ksd_last, o->d_ksd))
+        get1(&c->return_var, s->d_return_var) || get1(&c->ksd_last, o->d_ksd) ||
+        get1(&c->h_fast_mean, o->d_h_fast_mean) || get1(&c->h_slow_mean, o->d_h_slow_mean))
         return -1;
     c->timestep = s->timestep;
     c->guide_initialized = s->guide_initialized;

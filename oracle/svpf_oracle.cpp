@@ -431,6 +431,151 @@ struct Tick {
         return (R)s.smooth_h_mean[idx];
     }
 
+    /* Two-factor tick: svpf_step_two_factor, svpf_optimized_graph.cu:744-897,
+     * kernels src/svpf_two_factor.cu, host EKF include/svpf_two_factor.cuh:245-300.
+     * h/hp/v hold [fast (n) ; slow (n)]. */
+    int run2f(R yt, R yp, Noise<R>& nz, oracle_out* out) {
+        y_t = yt; y_prev = yp;
+        const R rf = (R)c.rho_fast, sf = (R)c.sigma_fast, rs = (R)c.rho_slow, ss = (R)c.sigma_slow;
+        const R mu = (R)p.mu, nu = (R)c.nu;
+        /* predict, svpf_two_factor.cu:55-90 */
+        for (int i = 0; i < n; ++i) {
+            R hf = h[i], hs = h[n + i];
+            hp[i] = hf; hp[n + i] = hs;
+            R zf = nz.normal(i, 0), zs = nz.normal(i, 1);
+            if (c.use_mim) {
+                R u = nz.uniform(i, 0);
+                if (u < (R)c.mim_jump_prob) zf *= (R)c.mim_jump_scale;
+            }
+            h[i] = clamp_h(rf * hf + sf * zf);
+            h[n + i] = clamp_h(rs * hs + ss * zs);
+        }
+        /* EKF with innovation split (FP64 here) + guide, :781-807 */
+        if (c.use_guide) {
+            double gmf = s.guide_mean_fast, gms = s.guide_mean_slow, gvf = s.guide_var_fast, gvs = s.guide_var_slow;
+            if (!s.guide_2f_initialized) {
+                gmf = 0.0; gms = 0.0;
+                gvf = (double)sf * sf / (1.0 - (double)rf * rf);
+                gvs = (double)ss * ss / (1.0 - (double)rs * rs);
+                s.guide_2f_initialized = 1;
+            }
+            const double pf = (double)rf * gmf, ps = (double)rs * gms;
+            const double Pf = (double)rf * rf * gvf + (double)sf * sf;
+            const double Ps = (double)rs * rs * gvs + (double)ss * ss;
+            const double implied = std::log((double)y_t * y_t + 1e-8) + (double)c.student_t_implied_offset;
+            const double innov = implied - ((double)mu + pf + ps);
+            const double S = Pf + Ps + (4.93 + 2.0);
+            const double Kf = Pf / (S + 1e-8), Ks = Ps / (S + 1e-8);
+            s.guide_mean_fast = pf + Kf * innov;
+            s.guide_mean_slow = ps + Ks * innov;
+            s.guide_var_fast = std::max((1.0 - Kf) * Pf, 1e-6);
+            s.guide_var_slow = std::max((1.0 - Ks) * Ps, 1e-6);
+            const R g = (R)c.guide_strength;
+            const R cmf = (R)s.h_fast_mean, cms = (R)s.h_slow_mean;
+            const R gf = (R)s.guide_mean_fast, gsl = (R)s.guide_mean_slow;
+            for (int i = 0; i < n; ++i) {
+                if (c.use_guide_preserving) {
+                    h[i] = clamp_h(((1 - g) * cmf + g * gf) + (h[i] - cmf));
+                    h[n + i] = clamp_h(((1 - g) * cms + g * gsl) + (h[n + i] - cms));
+                } else {
+                    h[i] = clamp_h((1 - g) * h[i] + g * gf);
+                    h[n + i] = clamp_h((1 - g) * h[n + i] + g * gsl);
+                }
+            }
+        }
+        /* Silverman bandwidth per factor, svpf_two_factor.cu:256-318 */
+        R bw2[2];
+        for (int k = 0; k < 2; ++k) {
+            R sum = 0, sum2 = 0;
+            for (int i = 0; i < n; ++i) { R x = h[k * n + i]; sum += x; sum2 += x * x; }
+            R mean = sum / (R)n, var = sum2 / (R)n - mean * mean;
+            R sd = std::sqrt(std::max(var, (R)1e-8));
+            R bw = (R)1.06 * sd * std::pow((R)n, (R)-0.2);
+            bw2[k] = std::max(bw, k == 0 ? (R)c.bw_floor_fast : (R)c.bw_floor_slow);
+        }
+        /* Stein loop: n_stein_steps per stage, beta = (a+1)/na, step 0.5/n_stein */
+        const int na = c.use_annealing ? c.n_anneal_steps : 1;   /* 0 stages: no Stein step */
+        const R base_step = (R)0.5 / (R)c.n_stein_steps;
+        const R stc = student_t_const();
+        const R sign = c.stein_repulsive_sign == 1 ? (R)1 : (R)-1;
+        std::vector<R> gfa(n), gsa(n), hn(2 * n);
+        int kn = 2;
+        for (int a = 0; a < na; ++a) {
+            const R beta = (R)(a + 1) / (R)na;
+            const R temp = c.use_svld ? (R)c.temperature : (R)0;
+            for (int st = 0; st < c.n_stein_steps; ++st) {
+                /* gradient, svpf_two_factor.cu:166-243 */
+                const R sf2 = sf * sf + (R)1e-8, ss2 = ss * ss + (R)1e-8;
+                const R wf = sf2 / (sf2 + ss2), ws = 1 - wf;
+                for (int i = 0; i < n; ++i) {
+                    const R hf = h[i], hs = h[n + i];
+                    const R hc = mu + hf + hs;
+                    const R y2 = y_t * y_t;
+                    const R ratio = y2 / (nu * std::exp(hc) + (R)1e-8);
+                    lw[i] = stc - (R)0.5 * hc - (R)0.5 * (nu + 1) * std::log(1 + ratio);
+                    R lg;
+                    if (c.use_exact_gradient) lg = (R)-0.5 + (R)0.5 * (nu + 1) * ratio / (1 + ratio + (R)1e-8);
+                    else lg = (R)0.5 * (std::log(y2 + (R)1e-8) - hc);
+                    gfa[i] = -(hf - rf * hp[i]) / sf2 + beta * wf * lg;
+                    gsa[i] = -(hs - rs * hp[n + i]) / ss2 + beta * ws * lg;
+                }
+                /* two vanilla transports, svpf_opt_kernels.cu:527-599 (fast, then slow) */
+                for (int k = 0; k < 2; ++k) {
+                    const R* hh = &h[k * n];
+                    const std::vector<R>& gg = k == 0 ? gfa : gsa;
+                    const R inv_bw2 = 1 / (bw2[k] * bw2[k]);
+                    for (int i = 0; i < n; ++i) {
+                        R ks = 0, gk = 0;
+                        for (int j = 0; j < n; ++j) {
+                            const R d = hh[i] - hh[j];
+                            const R K = 1 / (1 + d * d * inv_bw2);
+                            ks += K * gg[j];
+                            gk += sign * 2 * d * inv_bw2 * K * K;
+                        }
+                        const R phi = (ks + gk) / (R)n;
+                        const R rr = (R)c.rmsprop_rho;
+                        R& vv = v[k * n + i];
+                        vv = rr * vv + (1 - rr) * phi * phi;
+                        const R es = base_step * beta;
+                        R diff = 0;
+                        if (temp > (R)1e-6) diff = std::sqrt(2 * es * temp) * nz.normal(i, kn + k);
+                        hn[k * n + i] = clamp_h(hh[i] + es * phi / std::sqrt(vv + (R)c.rmsprop_eps) + diff);
+                    }
+                }
+                for (int i = 0; i < 2 * n; ++i) h[i] = hn[i];
+                if (temp > (R)1e-6) kn += 2;
+            }
+        }
+        /* outputs, svpf_two_factor.cu:368-470 */
+        R mx = (R)-1e30, sfm = 0, ssm = 0, svol = 0;
+        for (int i = 0; i < n; ++i) {
+            mx = std::max(mx, lw[i]);
+            sfm += h[i]; ssm += h[n + i];
+            svol += std::exp((R)0.5 * (mu + h[i] + h[n + i]));
+        }
+        R se = 0;
+        for (int i = 0; i < n; ++i) se += std::exp(lw[i] - mx);
+        const R ll = mx + std::log(std::max(se / (R)n, (R)1e-10));
+        const R mf = sfm / (R)n, ms = ssm / (R)n;
+        const R hm = mu + mf + ms, vol = svol / (R)n;
+        s.h_fast_mean = (float)mf;
+        s.h_slow_mean = (float)ms;
+        s.h_mean_prev = (float)hm;
+        s.vol_prev = (float)vol;
+        s.loglik_sum += (double)ll;
+        s.timestep += 1;
+        out->loglik = (float)ll;
+        out->vol = (float)vol;
+        out->h_mean = (float)hm;
+        out->h_mean_raw = (float)hm;
+        /* the single-factor bandwidth, KSD and step counter are left as they were */
+        out->bw = (float)bw2[0];
+        out->ksd = s.ksd_last;
+        out->steps_used = std::max(na, 0) * c.n_stein_steps;
+        out->rejuv_fired = 0;
+        return nz.bad ? -3 : 0;
+    }
+
     int run(R yt, R yp, Noise<R>& nz, oracle_out* out) {
         y_t = yt; y_prev = yp;
         const int t = s.timestep;
@@ -624,12 +769,14 @@ int tick_impl(const oracle_config* cfg, const oracle_params* p, oracle_ctl* ctl,
               double* h, double* hp, double* v, double* lw, float yt, float yp,
               const oracle_noise* noise, oracle_out* out) {
     Tick<R> tk(*cfg, *p, *ctl, n);
-    tk.h.assign(h, h + n); tk.hp.assign(hp, hp + n); tk.v.assign(v, v + n);
+    const int m = cfg->use_two_factor ? 2 * n : n;   /* two-factor: [fast; slow] */
+    tk.h.assign(h, h + m); tk.hp.assign(hp, hp + m); tk.v.assign(v, v + m);
     tk.lw.assign(lw, lw + n);
     tk.g.assign(n, 0); tk.curv.assign(n, 1); tk.precond.assign(n, 0);
     Noise<R> nz(noise, n);
-    int rc = tk.run((R)yt, (R)yp, nz, out);
-    for (int i = 0; i < n; ++i) { h[i] = tk.h[i]; hp[i] = tk.hp[i]; v[i] = tk.v[i]; lw[i] = tk.lw[i]; }
+    int rc = cfg->use_two_factor ? tk.run2f((R)yt, (R)yp, nz, out) : tk.run((R)yt, (R)yp, nz, out);
+    for (int i = 0; i < m; ++i) { h[i] = tk.h[i]; hp[i] = tk.hp[i]; v[i] = tk.v[i]; }
+    for (int i = 0; i < n; ++i) lw[i] = tk.lw[i];
     return rc;
 }
 
@@ -678,6 +825,9 @@ void svpf_oracle_config_defaults(oracle_config* c, int n_stein_steps, float nu) 
     c->use_student_t_state = 0; c->nu_state = 5.0f;
     c->use_smoothing = 0; c->smooth_lag = 3; c->smooth_output_lag = 1;
     c->use_heun = 0;
+    c->use_two_factor = 0;   /* :257-266 */
+    c->rho_fast = 0.90f; c->sigma_fast = 0.15f; c->rho_slow = 0.99f; c->sigma_slow = 0.05f;
+    c->bw_floor_fast = 0.01f; c->bw_floor_slow = 0.05f;
 }
 
 void svpf_oracle_ctl_defaults(oracle_ctl* s) {
@@ -716,6 +866,28 @@ int svpf_oracle_initialize(oracle_config* cfg, const oracle_params* p, oracle_ct
     s->guide_initialized = 0;
     s->guide_mean = p->mu;
     s->guide_var = var;
+    if (cfg->use_two_factor) {
+        /* svpf_optimized_graph.cu:414-447, svpf_init_two_factor_kernel (svpf_two_factor.cu:29-48):
+         * draws 1 (fast) and 2 (slow) after the single-factor draw 0; h/hp/v are [fast; slow] */
+        const float rf = cfg->rho_fast, sf = cfg->sigma_fast, rs = cfg->rho_slow, ss = cfg->sigma_slow;
+        const double sdf = sf / std::sqrt((double)(1.0f - rf * rf + 1e-8f));
+        const double sds = ss / std::sqrt((double)(1.0f - rs * rs + 1e-8f));
+        for (int i = 0; i < n; ++i) {
+            double zf = init_normals ? (double)init_normals[(size_t)n + i]
+                                     : philox_normal<double>(key, (uint32_t)i, 1u, 0u, 2u);
+            double zs = init_normals ? (double)init_normals[2 * (size_t)n + i]
+                                     : philox_normal<double>(key, (uint32_t)i, 2u, 0u, 2u);
+            h[i] = std::min(std::max(sdf * zf, -15.0), 5.0);
+            h[n + i] = std::min(std::max(sds * zs, -15.0), 5.0);
+            hp[i] = h[i]; hp[n + i] = h[n + i];
+            v[i] = 0.0; v[n + i] = 0.0;
+        }
+        s->guide_2f_initialized = 0;
+        s->guide_mean_fast = 0.0;
+        s->guide_mean_slow = 0.0;
+        s->guide_var_fast = (double)(sf * sf / (1.0f - rf * rf + 1e-6f));
+        s->guide_var_slow = (double)(ss * ss / (1.0f - rs * rs + 1e-6f));
+    }
     if (cfg->use_adaptive_mu) { s->mu_state = p->mu; s->mu_var = 1.0f; }
     if (cfg->use_adaptive_sigma) s->sigma_z_effective = p->sigma_z;
     s->ksd_prev = 1e10f;

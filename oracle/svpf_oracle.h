@@ -82,6 +82,13 @@ typedef struct {
     int   smooth_lag;
     int   smooth_output_lag;
     int   use_heun;
+    int   use_two_factor;
+    float rho_fast;
+    float sigma_fast;
+    float rho_slow;
+    float sigma_slow;
+    float bw_floor_fast;
+    float bw_floor_slow;
 } oracle_config;
 
 /* SVPFParams of the reference (include/svpf.cuh:257-262). */
@@ -101,10 +108,15 @@ typedef struct {
     double guide_var;
     double guide_K;
     double loglik_sum;          /* FP64 running sum of per-tick log-likelihoods */
+    double guide_mean_fast;     /* two-factor EKF, svpf_two_factor.cuh:245-300 */
+    double guide_mean_slow;
+    double guide_var_fast;
+    double guide_var_slow;
     int    timestep;
     int    guide_initialized;
     int    stein_steps_used;
     int    smooth_head;
+    int    guide_2f_initialized;
     float  ksd_prev;            /* host ksd_prev: drives budget/beta/rejuvenation */
     float  ksd_last;            /* device d_ksd: last KSD actually computed */
     float  vol_prev;
@@ -117,6 +129,8 @@ typedef struct {
     float  mu_state;
     float  mu_var;
     float  y_prev;              /* used by svpf_step(): previous observation */
+    float  h_fast_mean;         /* device d_h_fast_mean / d_h_slow_mean */
+    float  h_slow_mean;
     float  smooth_h_mean[ORACLE_SMOOTH_MAX_LAG];
     float  smooth_h_var[ORACLE_SMOOTH_MAX_LAG];
     float  smooth_y[ORACLE_SMOOTH_MAX_LAG];
@@ -152,7 +166,9 @@ typedef struct {
 
 /* Run one tick.  Arrays are double on the interface; precision 0 computes in
  * FP64, precision 1 computes in FP32 (the CPU baseline).  Returns 0 on
- * success, a negative code on bad arguments or when the tape runs short. */
+ * success, a negative code on bad arguments or when the tape runs short.
+ * With use_two_factor, h / h_prev / v hold 2n values: the fast factor then
+ * the slow factor. */
 int svpf_oracle_tick(const oracle_config* cfg, const oracle_params* p,
                      oracle_ctl* ctl, int n,
                      double* h, double* h_prev, double* v, double* log_w,
@@ -170,7 +186,9 @@ int svpf_oracle_batch_tick_f32(int n_filters, const oracle_config* cfgs,
                                oracle_out* outs);
 
 /* svpf_initialize (svpf_optimized_graph.cu:349-451): stationary draw, resets.
- * init_normals[i] is particle i's draw (tape) or NULL for Philox mode. */
+ * init_normals[i] is particle i's draw (tape) or NULL for Philox mode; with
+ * use_two_factor the tape holds three draws per particle ([3][n]: the
+ * single-factor draw, then fast, then slow) and h/h_prev/v hold 2n values. */
 int svpf_oracle_initialize(oracle_config* cfg, const oracle_params* p,
                            oracle_ctl* ctl, int n, double* h, double* h_prev,
                            double* v, const float* init_normals,

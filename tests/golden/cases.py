@@ -5,6 +5,7 @@ Each case is run tick by tick on the reference's own CUDA step with a noise
 tape (make_golden.py, GPU) and stored as a fixture; the oracle and the product
 engine replay every tick from the stored pre-tick state with the same tape.
 """
+import tape
 
 # BASELINE configuration 1 mapped onto the reference knobs: N=512, at most 8
 # Newton-Stein iterations over 3 annealing stages, full Newton, SVLD, MIM,
@@ -59,12 +60,65 @@ CASES = {
                             params=(0.97, 0.15, -1.0, 0.0), path=(-1.0, 0.97, 0.15), ticks=14),
 }
 
+# Two-factor cases.  TWO_FACTOR_TEST is the reference's two-factor test setup
+# (test/test_two_factor.cu:199-280: the production single-factor knobs, then
+# guide strength 0.12 and the factor parameters of its "balanced" process).
+TWO_FACTOR_TEST = dict(use_two_factor=1, rho_fast=0.90, sigma_fast=0.15, rho_slow=0.99, sigma_slow=0.05,
+                       bw_floor_fast=0.01, bw_floor_slow=0.05, use_svld=1, use_annealing=1,
+                       n_anneal_steps=5, temperature=0.45, use_mim=1, mim_jump_prob=0.25,
+                       mim_jump_scale=9.0, use_guide=1, use_guide_preserving=1, guide_strength=0.12,
+                       use_exact_gradient=1, lik_offset=0.345)
+
+CASES.update({
+    "two_factor_n512": dict(n=512, n_stein=8, nu=7.0, cfg=TWO_FACTOR_TEST,
+                            params=(0.99, 0.05, -3.5, 0.0), path=("2f", -3.5, 0.90, 0.15, 0.99, 0.05, 7.0),
+                            ticks=12),
+    # factor parameters of the reference test's "slow dominant" process.  (Its
+    # "fast dominant" process, sigma_slow = 0.02, makes the first tick after
+    # initialisation chaotic in FP32: with the RMSProp moments at zero the
+    # slow factor's stiff prior moves particles by several bandwidths per
+    # step, and the FP32 and FP64 oracles already differ by 2.7e-4 there.)
+    "two_factor_plain_n256": dict(n=256, n_stein=6, nu=30.0,
+                                  cfg=dict(use_two_factor=1, use_svld=0, use_mim=0, use_guide=0,
+                                           use_annealing=0, use_exact_gradient=0, stein_repulsive_sign=1,
+                                           rho_fast=0.95, sigma_fast=0.08, rho_slow=0.98, sigma_slow=0.12),
+                                  params=(0.98, 0.12, -3.5, 0.0),
+                                  path=("2f", -3.5, 0.95, 0.08, 0.98, 0.12, 0.0), ticks=12),
+    "two_factor_blend_n300": dict(n=300, n_stein=4, nu=5.0,
+                                  cfg=dict(use_two_factor=1, use_guide=1, use_guide_preserving=0,
+                                           guide_strength=0.2, n_anneal_steps=3, use_svld=1, temperature=0.6,
+                                           use_mim=1, rho_fast=0.92, sigma_fast=0.20, rho_slow=0.995,
+                                           sigma_slow=0.08, bw_floor_slow=0.1),
+                                  params=(0.995, 0.08, -3.0, 0.0),
+                                  path=("2f", -3.0, 0.92, 0.20, 0.995, 0.08, 5.0), ticks=12),
+})
+
 TAPE_SEED = 20240601
+
+
+def is_two_factor(case) -> bool:
+    return bool(case["cfg"].get("use_two_factor", 0))
+
+
+def init_slots(case) -> int:
+    """Initial draws per particle: the single-factor draw, plus fast and slow."""
+    return 3 if is_two_factor(case) else 1
+
+
+def observations(case, T: int, seed: int):
+    """(h, y) of the case's synthetic path, T ticks."""
+    path = case["path"]
+    if path[0] == "2f":
+        return tape.sv2_path(T, *path[1:6], seed=seed, nu_obs=path[6])
+    return tape.sv_path(T, *path, seed=seed)
 
 
 def normal_slots(case) -> int:
     """Upper bound on normal draws per particle per tick for the case."""
     cfg = case["cfg"]
+    if is_two_factor(case):
+        na = cfg.get("n_anneal_steps", 3) if cfg.get("use_annealing", 1) else 1
+        return 2 + 2 * na * case["n_stein"]
     max_steps = cfg.get("stein_max_steps", 12)
     pred = 1
     if cfg.get("use_student_t_state", 0) and cfg.get("nu_state", 5.0) <= 30.0:

@@ -5,7 +5,7 @@ in place with its curand draws routed to a noise tape, oracle/_ref/
 libsvpf_ref_tape.so) free-running for ``ticks`` ticks and records, per tick,
 the full filter state before and after the tick plus the step outputs.
 
-    python tests/golden/make_golden.py [out_dir]
+    python tests/golden/make_golden.py [out_dir [case ...]]
 
 The fixtures are committed under tests/golden/*.npz.
 """
@@ -36,12 +36,11 @@ def run_case(name, case, reflib):
         setattr(cfg, k, v)
     f.apply_config(cfg)
     params = oracle.OracleParams(*case["params"])
-    rc = f.initialize(params, tape.init_normals(cases.TAPE_SEED, n))
+    rc = f.initialize(params, tape.init_normals(cases.TAPE_SEED, n, cases.init_slots(case)))
     assert rc == 0, f"init tape flags {rc}"
     # nu_state is clamped by svpf_initialize; read the effective config back
     cfg = f.read_config()
-    mu, rho, sz = case["path"]
-    _, ys = tape.sv_path(case["ticks"] + 1, mu, rho, sz, seed=zlib.crc32(name.encode()) % 1000)
+    _, ys = cases.observations(case, case["ticks"] + 1, seed=zlib.crc32(name.encode()) % 1000)
     ns = cases.normal_slots(case)
     rec = {k: [] for k in ("h", "hp", "v", "lw")}
     ctls, outs = [], []
@@ -76,9 +75,12 @@ def run_case(name, case, reflib):
 
 def main():
     out_dir = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden")
+    only = set(sys.argv[2:])
     os.makedirs(out_dir, exist_ok=True)
     reflib = oracle.RefLib("tape")
     for name, case in cases.CASES.items():
+        if only and name not in only:
+            continue
         d = run_case(name, case, reflib)
         np.savez_compressed(os.path.join(out_dir, f"{name}.npz"), **d)
         print(f"{name}: ticks={case['ticks']} n={case['n']} loglik[0]={d['outs'][0, 0]:.5f} "

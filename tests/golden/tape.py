@@ -52,8 +52,11 @@ def tape(seed: int, tick: int, n: int, normal_slots: int, uniform_slots: int = 2
     return tape_normals(seed, tick, normal_slots, n), tape_uniforms(seed, tick, uniform_slots, n)
 
 
-def init_normals(seed: int, n: int) -> np.ndarray:
-    return tape_normals(seed, 10_000_000, 1, n)[0]
+def init_normals(seed: int, n: int, slots: int = 1) -> np.ndarray:
+    """Initial draws: [n] for one slot, else [slots, n] (slot 0 is the same
+    either way; a two-factor initialisation draws slots 0, 1 and 2)."""
+    z = tape_normals(seed, 10_000_000, slots, n)
+    return z[0] if slots == 1 else z
 
 
 def sv_path(T: int, mu: float, rho: float, sigma_z: float, seed: int):
@@ -71,4 +74,33 @@ def sv_path(T: int, mu: float, rho: float, sigma_z: float, seed: int):
         eta = g[2 + 3 * t]
         h[t] = hv
         y[t] = np.exp(hv / 2.0) * eta
+    return h, y.astype(np.float32)
+
+
+def sv2_path(T: int, mu: float, rho_fast: float, sigma_fast: float, rho_slow: float, sigma_slow: float,
+             seed: int, nu_obs: float = 0.0):
+    """Synthetic two-factor SV path h_t = mu + f_t + s_t with AR(1) factors
+    f_t = rho_f f_{t-1} + sigma_f eps, s_t = rho_s s_{t-1} + sigma_s eps', both
+    started from their stationary laws; y_t = exp(h_t / 2) eta_t with Gaussian
+    eta, or Student-t eta when nu_obs > 0 (chi-square from nu_obs squared
+    normals, nu_obs rounded)."""
+    k = int(round(nu_obs)) if nu_obs > 0 else 0
+    per = 3 + k
+    c = np.arange(per * T + 2, dtype=np.uint64) + np.uint64(seed) * np.uint64(1 << 40) + np.uint64(1 << 39)
+    u = _unit(splitmix64(c))
+    u2 = _unit(splitmix64(c ^ np.uint64(0x3333333333333333))) - (1.0 / 16777216.0)
+    g = np.sqrt(-2.0 * np.log(u)) * np.cos(2.0 * np.pi * u2)
+    f = sigma_fast / np.sqrt(1.0 - rho_fast * rho_fast) * g[0]
+    s = sigma_slow / np.sqrt(1.0 - rho_slow * rho_slow) * g[1]
+    h = np.empty(T)
+    y = np.empty(T)
+    for t in range(T):
+        b = 2 + per * t
+        f = rho_fast * f + sigma_fast * g[b]
+        s = rho_slow * s + sigma_slow * g[b + 1]
+        eta = g[b + 2]
+        if k:
+            eta = eta / np.sqrt(np.sum(g[b + 3:b + 3 + k] ** 2) / k)
+        h[t] = mu + f + s
+        y[t] = np.exp(h[t] / 2.0) * eta
     return h, y.astype(np.float32)

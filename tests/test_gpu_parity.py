@@ -7,7 +7,7 @@ import pytest
 
 import cases
 import tape
-from test_oracle import TOL, _fixtures, load_fixture, rel_err
+from test_oracle import TOL, TWO_FACTOR_SCALARS, _fixtures, load_fixture, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -43,18 +43,27 @@ def engine_for(pkg, n, n_stein, nu, cfg_dict, params, cluster=0):
 def test_engine_matches_reference_ticks(pkg, path, cluster):
     fx = load_fixture(path)
     n = fx["n"]
+    tf = bool(fx["config"].get("use_two_factor", 0))
     f = engine_for(pkg, n, fx["config"]["n_stein_steps"], fx["config"]["nu"], fx["config"], fx["params"], cluster)
     y_prev = 0.0
     for t in range(fx["outs"].shape[0]):
-        f.set_state(to_ctl(pkg, fx["ctl"][t]), fx["h"][t], fx["hp"][t], fx["v"][t], fx["lw"][t])
+        if tf:
+            # two factors: h, h_prev, v hold [fast; slow]; the log-weights are [n]
+            f.set_state(to_ctl(pkg, fx["ctl"][t]), None, None, None, fx["lw"][t])
+            f.set_state_2f(fx["h"][t], fx["hp"][t], fx["v"][t])
+        else:
+            f.set_state(to_ctl(pkg, fx["ctl"][t]), fx["h"][t], fx["hp"][t], fx["v"][t], fx["lw"][t])
         nrm, uni = tape.tape(fx["tape_seed"], t, n, fx["normal_slots"], 2)
         f.set_noise_tape(nrm, uni)
         rc, out = f.step_raw(fx["ys"][t], y_prev)
         y_prev = float(fx["ys"][t])
         assert rc == 0, (t, rc)
         ctl, h, hp, v, lw = f.get_state()
+        if tf:
+            h, hp, v = f.get_state_2f()
         post = fx["ctl"][t + 1]
-        assert out.steps_used == post["stein_steps_used"]
+        if not tf:
+            assert out.steps_used == post["stein_steps_used"]
         assert rel_err(h, fx["h"][t + 1]) < TOL, (t, rel_err(h, fx["h"][t + 1]))
         assert rel_err(hp, fx["hp"][t + 1]) < TOL
         assert rel_err(v, fx["v"][t + 1], floor=1e-3) < 10 * TOL, (t, rel_err(v, fx["v"][t + 1], 1e-3))
@@ -63,7 +72,7 @@ def test_engine_matches_reference_ticks(pkg, path, cluster):
         assert abs(out.loglik - ll) < TOL * max(1, abs(ll)), (t, out.loglik, ll)
         assert abs(out.vol - vol) < TOL * max(1, abs(vol)), (t, out.vol, vol)
         assert abs(out.h_mean - hm) < TOL * max(1, abs(hm)), (t, out.h_mean, hm)
-        for k in SCALARS:
+        for k in SCALARS + (TWO_FACTOR_SCALARS if tf else ()):
             a, b = getattr(ctl, k), post[k]
             assert abs(a - b) <= TOL * max(1.0, abs(b)), (t, k, a, b)
     f.close()

@@ -31,7 +31,7 @@ def _oracle_filter(oracle_mod, case, precision):
     for k, v in case["cfg"].items():
         setattr(cfg, k, v)
     f = oracle_mod.OracleFilter(case["n"], cfg, oracle_mod.OracleParams(*case["params"]), precision)
-    f.initialize(tape.init_normals(cases.TAPE_SEED, case["n"]))
+    f.initialize(tape.init_normals(cases.TAPE_SEED, case["n"], cases.init_slots(case)))
     return f
 
 
@@ -39,7 +39,7 @@ def _oracle_filter(oracle_mod, case, precision):
 def test_fp32_mirror_tracks_fp64(oracle_mod, name):
     case = cases.CASES[name]
     fs = [_oracle_filter(oracle_mod, case, p) for p in (0, 1)]
-    _, ys = tape.sv_path(8, *case["path"], seed=3)
+    _, ys = cases.observations(case, 8, seed=3)
     yp = 0.0
     for t in range(6):
         nrm, uni = tape.tape(cases.TAPE_SEED, t, case["n"], cases.normal_slots(case), 2)
@@ -96,7 +96,8 @@ def test_oracle_replays_reference_ticks(oracle_mod, path):
         out = f.step(fx["ys"][t], y_prev, nrm, uni)
         y_prev = float(fx["ys"][t])
         post = fx["ctl"][t + 1]
-        assert out.steps_used == post["stein_steps_used"], (t, out.steps_used, post["stein_steps_used"])
+        if not cfg.use_two_factor:   # the two-factor step leaves the step counter alone
+            assert out.steps_used == post["stein_steps_used"], (t, out.steps_used, post["stein_steps_used"])
         assert rel_err(f.h, fx["h"][t + 1]) < TOL, (t, rel_err(f.h, fx["h"][t + 1]))
         assert rel_err(f.h_prev, fx["hp"][t + 1]) < TOL
         assert rel_err(f.v, fx["v"][t + 1], floor=1e-3) < TOL * 10, (t, rel_err(f.v, fx["v"][t + 1], 1e-3))
@@ -110,3 +111,12 @@ def test_oracle_replays_reference_ticks(oracle_mod, path):
             assert abs(a - b) <= TOL * max(1.0, abs(b)), (t, k, a, b)
         assert abs(f.ctl.guide_mean - post["guide_mean"]) < TOL * max(1, abs(post["guide_mean"]))
         assert abs(f.ctl.guide_var - post["guide_var"]) < TOL * max(1, abs(post["guide_var"]))
+        if cfg.use_two_factor:
+            for k in TWO_FACTOR_SCALARS:
+                a, b = getattr(f.ctl, k), post[k]
+                assert abs(a - b) <= TOL * max(1.0, abs(b)), (t, k, a, b)
+
+
+# Two-factor control fields compared after every replayed tick.
+TWO_FACTOR_SCALARS = ("h_fast_mean", "h_slow_mean", "guide_mean_fast", "guide_mean_slow", "guide_var_fast",
+                      "guide_var_slow", "guide_2f_initialized", "timestep")
