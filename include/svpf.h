@@ -440,6 +440,37 @@ const char* svpf_build_info(void);
 int svpf_debug_philox(uint32_t k0, uint32_t k1, const uint32_t* ctr4, uint32_t* out4, int count);
 
 
+/* ---- gradients of the log-likelihood (adjoint) ---------------------------
+ * d(sum_t w_t loglik_t)/d(mu, rho, sigma_z, nu) of every filter of a batch
+ * over a run of T ticks that starts with svpf_initialize from theta, under
+ * common random numbers (the engine's counter-based noise keyed by seed and
+ * filter index).  Reverse mode: the forward keeps a checkpoint every
+ * `checkpoint_every` ticks, the backward recomputes one segment at a time.
+ * The configuration must be inside the differentiable set
+ * (svpf_grad_supported): single factor, plain or MIM predict with the
+ * model's rho (use_asymmetric_rho = use_local_params = use_guided = 0), EKF
+ * guide without adaptive strength, Gaussian prior, vanilla or full-Newton
+ * transport, fixed beta schedule (no adaptive beta), no rejuvenation, no
+ * adaptive mu / sigma, no Heun / fan mode. */
+typedef struct svpf_grad svpf_grad_t;
+
+int svpf_grad_supported(const svpf_config_t* cfg);
+svpf_grad_t* svpf_grad_create(int n_filters, const int* n_particles, const svpf_config_t* cfgs,
+                              int T_max, int checkpoint_every, cudaStream_t stream);
+void svpf_grad_destroy(svpf_grad_t* g);
+/* theta [F][4] = (mu, rho, sigma_z, nu); gamma [F] leverage or NULL; y [F][T].
+ * Outputs (host, may be NULL): loglik [F][T] (FP32), loglik_sum [F] (FP64). */
+int svpf_grad_forward(svpf_grad_t* g, const float* theta, const float* gamma, const float* y, int T,
+                      unsigned long long seed, float* loglik, double* loglik_sum);
+/* w [F][T]: weight of each tick's loglik (NULL = all ones); grad [F][4]. */
+int svpf_grad_backward(svpf_grad_t* g, const float* w, double* grad);
+/* Device-pointer variants, stream ordered, no host synchronisation; the
+ * device arrays given to the forward must stay valid until the backward. */
+int svpf_grad_forward_device(svpf_grad_t* g, const float* d_theta, const float* d_gamma,
+                             const float* d_y, int T, unsigned long long seed, float* d_loglik);
+int svpf_grad_backward_device(svpf_grad_t* g, const float* d_w, double* d_grad);
+int svpf_grad_checkpoint_every(const svpf_grad_t* g);
+
 #ifdef __cplusplus
 }
 #endif

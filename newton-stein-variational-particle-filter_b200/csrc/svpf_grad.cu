@@ -1,0 +1,1292 @@
+// svpf_grad.cu -- gradient of a run's log-likelihood, sum_t w_t loglik_t,
+// with respect to theta = (mu, rho, sigma_z, nu) of every filter of a batch,
+// under common random numbers (the project's counter-based Philox draws are
+// replayed exactly), by a hand-written reverse-mode adjoint of the tick.
+//
+// Forward: one CTA per filter runs the ticks of a segment of k ticks and
+// stores a checkpoint (state, particles, RMSProp moments) at the start of
+// every segment.  Backward, segment by segment from the last: the CTA
+// recomputes the segment from its checkpoint and keeps every tick's input
+// state, then walks the ticks in reverse; for each tick it recomputes the tick
+// once more while recording every Stein iterate and the per-row statistics
+// the adjoint needs, and then sweeps the Stein iterations backwards.
+//
+// Differentiable configuration (svpf_grad_supported): single factor; plain or
+// MIM predict with the model's rho (svpf_opt_kernels.cu:125-206); EKF guide,
+// preserving or blending, with the base strength (svpf_kernels.cuh:509-541,
+// svpf_optimized_graph.cu:1006-1039); Gaussian mixture prior and Student-t
+// likelihood (svpf_opt_kernels.cu:354-521); vanilla IMQ or full-Newton
+// transport with RMSProp and SVLD (:527-599, :912-1103); no rejuvenation and
+// no adaptive mu/sigma/guide.  Decisions that are piecewise constant in theta
+// (the KSD-driven Stein budget, adaptive beta, the MIM jump selection) are
+// taken as in the forward pass; clamps contribute their one-sided derivative.
+//
+// Adjoint of one Stein iteration (x = positions, u = (x_i - x_j)/bw,
+// K = 1/(1+u^2), a_i = dL/dphi_raw_i / n, s = repulsion sign):
+//   phi_raw_i = (1/n) sum_j [K g_j + 2 s u K^2 / bw]
+//   dx_i += (1/bw) [a_i (-2 S1 + 2 s S2/bw) - 2 g_i C1 - 2 s C2/bw]
+//     S1 = sum_j g_j u K^2, S2 = sum_j K^2 (4K-3), C1 = sum_j a_j u K^2,
+//     C2 = sum_j a_j K^2 (4K-3)   (d(uK^2)/du = K^2 (4K-3); column terms
+//     written as row sums with u_ji = -u_ij)
+//   dg_i = sum_j a_j K,  dbw += a_i (1/bw) [2 Q1 - 2 s Q2/bw],
+//     Q1 = sum_j g_j u^2 K^2, Q2 = sum_j u K^2 (4K-2)
+// and for full Newton H_i = hw_i/kn_i, hw_i = sum_j [c_j K + 2K^2 |3u^2-1|/bw^2],
+// kn_i = sum_j K, the analogous row and column sums of their derivatives.
+// Gaussian mixture score gp(x) = -E_w[d]/s2, d_k = x - mu_k, w = softmax(-d^2/2s2):
+//   dgp/dx = -1/s2 + Var_w(d)/s2^2
+//   dgp/ds2 = E[d]/s2^2 - (E[d^3] - E[d] E[d^2]) / (2 s2^3)
+//   dgp/dmu_k = (w_k/s2) [1 - d_k (d_k - E[d]) / s2]   (a column pass)
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <vector>
+
+#include "svpf.h"
+#include "svpf_device.cuh"
+#include "svpf_internal.h"
+
+namespace svpf {
+namespace grad {
+
+constexpr int kRecFixed = 4;       // XS, HPR, HGR, MUK
+constexpr int kRecPerIt = 14;      // X V GPRE AL LMAX Z DBAR VARD SKEW PHIR HR HW KN XR
+enum { XS = 0, HPR = 1, HGR = 2, MUK = 3 };
+enum { IX = 0, IV, IGPRE, IAL, ILMAX, IZ, IDBAR, IVARD, ISKEW, IPHIR, IHR, IHW, IKN, IXR };
+
+struct GState {
+    double m, P;                   // EKF guide mean / variance
+    float bw_sq, h_mean_prev, return_ema, return_var, ksd_prev;
+    int guide_init, timestep, pad;
+};
+
+struct GAdj {
+    double m, P, bw_sq, h_mean;    // adjoints of the scalar state
+    double th[4];                  // accumulated d/d(mu, rho, sigma_z, nu)
+};
+
+struct GArgs {
+    int F, T, k, np, bmax;
+    const int* n;
+    const svpf_config_t* cfg;
+    const float* theta;            // [F][4]
+    const float* gamma;            // [F] or nullptr
+    const float* y;                // [F][T]
+    const float* w;                // [F][T] or nullptr (all ones)
+    float* loglik;                 // [F][T] or nullptr
+    double* ll_sum;                // [F]
+    unsigned long long seed;
+    // per filter
+    float* fx;                     // [F][np] forward positions
+    float* fv;                     // [F][np]
+    GState* fs;                    // [F]
+    float* ck;                     // [F][nseg][2 np] checkpoints (x, v)
+    GState* cks;                   // [F][nseg]
+    float* ax;                     // [F][np] adjoint of positions
+    float* av;                     // [F][np]
+    GAdj* as;                      // [F]
+    // per CTA
+    float* seg;                    // [grid][k][2 np] tick inputs of the segment
+    GState* segs;                  // [grid][k]
+    float* rec;                    // [grid][rec_floats] per-tick record
+    size_t rec_floats;
+    int nseg;
+    int* status;                   // [F]
+};
+
+__host__ __device__ inline size_t rec_floats_for(int np, int bmax) {
+    return (size_t)np * (kRecFixed + kRecPerIt * bmax + 2);
+}
+
+// psi(x), x > 0: shift to x >= 8 with psi(x) = psi(x+1) - 1/x, then the
+// asymptotic series (Abramowitz & Stegun 6.3.18).
+__device__ inline double digamma_d(double x) {
+    double acc = 0.0;
+    while (x < 8.0) { acc -= 1.0 / x; x += 1.0; }
+    const double r = 1.0 / x, r2 = r * r;
+    return acc + log(x) - 0.5 * r -
+           r2 * (1.0 / 12 - r2 * (1.0 / 120 - r2 * (1.0 / 252 - r2 * (1.0 / 240 - r2 * (1.0 / 132)))));
+}
+
+// ---- block reductions over kThreads threads ----------------------------------
+template <int K>
+__device__ __forceinline__ void reduce_sum(float (&v)[K], float (*scr)[kWarps]) {
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        v[q] = warp_sum(v[q]);
+        if (lane == 0) scr[q][wp] = v[q];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        float a = 0.0f;
+        for (int i = 0; i < kWarps; ++i) a += scr[q][i];
+        v[q] = a;
+    }
+    __syncthreads();
+}
+__device__ __forceinline__ float reduce_max(float v, float (*scr)[kWarps]) {
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    v = warp_max(v);
+    if (lane == 0) scr[0][wp] = v;
+    __syncthreads();
+    float a = scr[0][0];
+    for (int i = 1; i < kWarps; ++i) a = fmaxf(a, scr[0][i]);
+    __syncthreads();
+    return a;
+}
+// (value, index) minimum / maximum; ties go to the smaller index
+__device__ __forceinline__ void reduce_argminmax(float& mn, int& imn, float& mx, int& imx, float (*scr)[kWarps],
+                                                 int* iscr) {
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float m2 = __shfl_xor_sync(0xffffffffu, mn, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, imn, o);
+        if (m2 < mn || (m2 == mn && i2 < imn)) { mn = m2; imn = i2; }
+        const float x2 = __shfl_xor_sync(0xffffffffu, mx, o);
+        const int j2 = __shfl_xor_sync(0xffffffffu, imx, o);
+        if (x2 > mx || (x2 == mx && j2 < imx)) { mx = x2; imx = j2; }
+    }
+    if (lane == 0) {
+        scr[0][wp] = mn; iscr[wp] = imn;
+        scr[1][wp] = mx; iscr[kWarps + wp] = imx;
+    }
+    __syncthreads();
+    mn = scr[0][0]; imn = iscr[0]; mx = scr[1][0]; imx = iscr[kWarps];
+    for (int i = 1; i < kWarps; ++i) {
+        if (scr[0][i] < mn || (scr[0][i] == mn && iscr[i] < imn)) { mn = scr[0][i]; imn = iscr[i]; }
+        if (scr[1][i] > mx || (scr[1][i] == mx && iscr[kWarps + i] < imx)) { mx = scr[1][i]; imx = iscr[kWarps + i]; }
+    }
+    __syncthreads();
+}
+
+// Per-tick scalars shared by the forward and the backward of one tick.
+struct TickScalars {
+    float mu, rho, sz, nu, gamma, s2;
+    float y_t, y_prev, stc, off, gs, cm, gm;
+    double m_in, P_in, m_pred, P_pred, K;
+    int init_here;
+    float mean, var, mn, mx;
+    int imn, imx;
+    float bw2_new_raw, bw2_prev, pre, ratio, spread_f, comb, scale_raw, bw2, bw, ib;
+    int budget, na;
+    float es[64], beta[64];
+    float mxl, se;
+    float ksd_last;
+};
+
+struct Shared {
+    float red[8][kWarps];
+    int ired[2 * kWarps];
+    TickScalars ts;
+    GState st;
+    int flag;
+    double acc[8];
+};
+
+// Stage of Stein iteration `it` (budget split as the reference host loop).
+__device__ inline int stage_of_it(int it, int budget, int na) {
+    const int si = budget / na;
+    if (si == 0) return na - 1;
+    const int a = it / si;
+    return a < na - 1 ? a : na - 1;
+}
+
+// One tick of one filter (CTA-wide).  x, v: positions and RMSProp moments
+// (smem, updated in place); work: 6 np floats of smem scratch.  rec: per-tick
+// record for the backward, or nullptr.  Returns loglik on every thread.
+__device__ float fwd_tick(const svpf_config_t& c, int n, int np, float* x, float* v, float* work, Shared& sh,
+                          const Noise& nz, float y_t, float y_prev, float* rec, int bmax) {
+    const int tid = threadIdx.x;
+    TickScalars& ts = sh.ts;
+    GState& st = sh.st;
+    float* xn = work;                 // next positions
+    float* g = work + np;             // transport score (clamped)
+    float* curv = work + 2 * np;      // full-Newton curvature
+    float* lw = work + 3 * np;        // log-weights of the last gradient pass
+    float* muk = work + 4 * np;       // prior means
+    const bool full = c.use_newton && c.use_full_newton;
+    if (tid == 0) {
+        ts.y_t = y_t;
+        ts.y_prev = y_prev;
+        ts.s2 = ts.sz * ts.sz;
+        ts.stc = lgammaf((ts.nu + 1.0f) * 0.5f) - lgammaf(ts.nu * 0.5f) - 0.5f * logf(3.14159265358979f * ts.nu);
+        ts.off = c.student_t_implied_offset;
+        ts.gs = c.guide_strength_base;
+        ts.cm = st.h_mean_prev;
+        // EKF guide in FP64 (svpf_kernels.cuh:509-541)
+        if (c.use_guide) {
+            const double mu = ts.mu, rho = ts.rho, sz = ts.sz;
+            ts.init_here = st.guide_init ? 0 : 1;
+            double m = st.m, P = st.P;
+            if (!st.guide_init) {
+                m = mu;
+                P = sz * sz / (1.0 - rho * rho);
+                st.guide_init = 1;
+            }
+            ts.m_in = m;
+            ts.P_in = P;
+            ts.m_pred = mu + rho * (m - mu);
+            ts.P_pred = rho * rho * P + sz * sz;
+            ts.K = ts.P_pred / (ts.P_pred + 6.93 + 1e-8);
+            const double ly2 = log((double)y_t * (double)y_t + 1e-8);
+            st.m = ts.m_pred + ts.K * (ly2 - (ts.m_pred - (double)ts.off));
+            st.P = (1.0 - ts.K) * ts.P_pred;
+            ts.gm = (float)st.m;
+        }
+    }
+    __syncthreads();
+    // ---- predict and prior means (svpf_opt_kernels.cu:125-206, 384-392), guide
+    {
+        const float lev_num = ts.gamma * y_prev;
+        const float rc = fminf(fmaxf(ts.rho, 0.0f), 0.999f);
+        for (int i = tid; i < n; i += kThreads) {
+            const float xi = x[i];
+            const float z = nz.normal(i, 0);
+            const float lev = lev_num / (expf(fminf(xi * 0.5f, 20.0f)) + 1e-8f);
+            muk[i] = ts.mu + ts.rho * (xi - ts.mu) + lev_num / (expf(xi * 0.5f) + 1e-8f);
+            float hpr;
+            if (c.use_mim) {
+                const float sel = nz.uniform(i, 0);
+                const float scale = sel < c.mim_jump_prob ? c.mim_jump_scale : 1.0f;
+                hpr = ts.mu + rc * (xi - ts.mu) + lev + ts.sz * (scale * z);
+            } else {
+                hpr = ts.mu + ts.rho * (xi - ts.mu) + ts.sz * z + lev;
+            }
+            const float hp = clamp_h(hpr);
+            float hgr = hp;
+            if (c.use_guide) {
+                if (c.use_guide_preserving) {
+                    const float nm = (1.0f - ts.gs) * ts.cm + ts.gs * ts.gm;
+                    hgr = nm + (hp - ts.cm);
+                } else {
+                    hgr = hp + ts.gs * (ts.gm - hp);
+                }
+            }
+            if (rec) {
+                rec[XS * np + i] = xi;
+                rec[HPR * np + i] = hpr;
+                rec[HGR * np + i] = hgr;
+                rec[MUK * np + i] = muk[i];
+            }
+            xn[i] = c.use_guide ? clamp_h(hgr) : hp;
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += kThreads) x[i] = xn[i];
+    // ---- bandwidth (svpf_opt_kernels.cu:1159-1235)
+    {
+        float s[2] = {0.0f, 0.0f};
+        float mn = 1e10f, mx = -1e10f;
+        int imn = 0, imx = 0;
+        for (int i = tid; i < n; i += kThreads) {
+            const float xi = xn[i];
+            s[0] += xi;
+            s[1] += xi * xi;
+            if (xi < mn) { mn = xi; imn = i; }
+            if (xi > mx) { mx = xi; imx = i; }
+        }
+        reduce_sum<2>(s, sh.red);
+        reduce_argminmax(mn, imn, mx, imx, sh.red, sh.ired);
+        if (tid == 0) {
+            const float inv_n = 1.0f / (float)n;
+            ts.mean = s[0] * inv_n;
+            ts.var = s[1] * inv_n - ts.mean * ts.mean;
+            ts.mn = mn; ts.mx = mx; ts.imn = imn; ts.imx = imx;
+            ts.bw2_new_raw = 2.0f * ts.var / logf((float)n + 1.0f);
+            const float bw2_new = fmaxf(ts.bw2_new_raw, 1e-6f);
+            ts.bw2_prev = st.bw_sq;
+            ts.pre = st.bw_sq > 0.0f ? 0.3f * bw2_new + 0.7f * st.bw_sq : bw2_new;
+            const float a = fabsf(y_t);
+            float ema = st.return_ema, rv = st.return_var;
+            ema = ema > 0.0f ? 0.05f * a + 0.95f * ema : a;
+            rv = rv > 0.0f ? 0.05f * a * a + 0.95f * rv : a * a;
+            st.return_ema = ema;
+            st.return_var = rv;
+            ts.ratio = a / fmaxf(ema, 1e-8f);
+            ts.spread_f = fminf((mx - mn) * 0.5f, 2.0f);
+            ts.comb = fmaxf(ts.ratio, ts.spread_f);
+            ts.scale_raw = 1.0f - 0.25f * fminf(ts.comb - 1.0f, 2.0f);
+            ts.bw2 = ts.pre * clampf(ts.scale_raw, 0.5f, 1.0f);
+            ts.bw = clampf(sqrtf(ts.bw2), 0.01f, 2.0f);
+            ts.ib = 1.0f / ts.bw;
+            st.bw_sq = ts.bw2;
+            // Stein budget and beta schedule (svpf_optimized_graph.cu:1057-1138)
+            const int na = c.use_annealing ? max(min(c.n_anneal_steps, SVPF_MAX_ANNEAL_STEPS), 1) : 1;
+            int budget;
+            if (st.timestep < 10) {
+                budget = c.stein_max_steps;
+            } else {
+                float kn01 = (st.ksd_prev - 0.05f) / (0.50f - 0.05f);
+                kn01 = fminf(fmaxf(kn01, 0.0f), 1.0f);
+                budget = c.stein_min_steps + (int)(kn01 * (float)(c.stein_max_steps - c.stein_min_steps));
+            }
+            budget = max(min(budget, bmax), 0);
+            ts.budget = budget;
+            ts.na = na;
+            const float eps_step = SVPF_STEIN_STEP_SIZE * (c.use_guide ? 0.5f : 1.0f);
+            for (int it = 0; it < budget; ++it) {
+                const int ai = stage_of_it(it, budget, na);
+                float beta;
+                if (!c.use_annealing) beta = 1.0f;
+                else if (c.use_adaptive_beta) beta = adaptive_beta(st.ksd_prev, ai, na);
+                else beta = (ai % 3 == 0) ? 0.30f : (ai % 3 == 1) ? 0.65f : 1.0f;
+                ts.beta[it] = beta;
+                ts.es[it] = eps_step * sqrtf(beta);
+            }
+        }
+        __syncthreads();
+    }
+    // ---- Stein loop
+    const float sign = c.stein_repulsive_sign == 1 ? 1.0f : -1.0f;
+    const float temp = c.use_svld ? c.temperature : 0.0f;
+    const float y2 = y_t * y_t;
+    const float inv2 = 0.5f / ts.s2, inv = 1.0f / ts.s2;
+    const float ib = ts.ib, ib2 = ib * ib;
+    const float inv_n = 1.0f / (float)n;
+    const int budget = ts.budget;
+    int kn = 1;
+    float ksd_acc = 0.0f;
+    for (int it = 0; it < budget; ++it) {
+        const float beta = ts.beta[it];
+        const bool last = it == budget - 1;
+        float* R = rec ? rec + (size_t)np * (kRecFixed + kRecPerIt * it) : nullptr;
+        // gradient pass (svpf_opt_kernels.cu:354-521)
+        for (int j = tid; j < n; j += kThreads) {
+            const float xj = x[j];
+            float lmax = -1e10f;
+            for (int k = 0; k < n; ++k) {
+                const float d = xj - muk[k];
+                lmax = fmaxf(lmax, -d * d * inv2);
+            }
+            float sr = 0.0f, wg = 0.0f, m2 = 0.0f, m3 = 0.0f;
+            for (int k = 0; k < n; ++k) {
+                const float d = xj - muk[k];
+                const float r = expf(-d * d * inv2 - lmax);
+                sr += r;
+                wg -= r * d * inv;
+                if (R) {
+                    const float rd2 = r * d * d;
+                    m2 += rd2;
+                    m3 += rd2 * d;
+                }
+            }
+            const float gp = wg / (sr + 1e-8f);
+            const float A = y2 / (expf(fminf(xj, 20.0f)) + 1e-8f) / ts.nu;
+            const float opA = 1.0f + A;
+            lw[j] = ts.stc - 0.5f * xj - (ts.nu + 1.0f) * 0.5f * log1pf(fmaxf(A, -0.999f));
+            float glik;
+            if (c.use_exact_gradient) glik = -0.5f + 0.5f * (ts.nu + 1.0f) * A / opA - c.lik_offset;
+            else glik = (logf(y2 + 1e-10f) - xj + c.lik_offset) / 1.4f;
+            const float gpre = gp + beta * glik;
+            g[j] = clampf(gpre, -10.0f, 10.0f);
+            if (full) {
+                const float hl = -0.5f * (ts.nu + 1.0f) * A / (opA * opA);
+                curv[j] = clampf(-(hl - inv), 0.1f, 100.0f);
+            }
+            if (R) {
+                const float dbar = -gp * ts.s2;              // E_w[d]
+                const float e2 = m2 / sr, e3 = m3 / sr;
+                R[IX * np + j] = xj;
+                R[IV * np + j] = v[j];
+                R[IGPRE * np + j] = gpre;
+                R[IAL * np + j] = A;
+                R[ILMAX * np + j] = lmax;
+                R[IZ * np + j] = sr;
+                R[IDBAR * np + j] = dbar;
+                R[IVARD * np + j] = e2 - dbar * dbar;
+                R[ISKEW * np + j] = e3 - dbar * e2;
+            }
+        }
+        __syncthreads();
+        // transport (vanilla :527-599 or full Newton :912-1103), Jacobi
+        const float es = ts.es[it];
+        for (int i = tid; i < n; i += kThreads) {
+            const float xi = x[i], gi = g[i];
+            float ks = 0.0f, gk = 0.0f, hw = 0.0f, kk = 0.0f, kq = 0.0f;
+            for (int j = 0; j < n; ++j) {
+                const float u = (xi - x[j]) * ib;
+                const float K = 1.0f / (1.0f + u * u);
+                const float K2 = K * K;
+                ks += K * g[j];
+                gk += u * K2;
+                if (full) {
+                    hw += curv[j] * K + 2.0f * ib2 * K2 * fabsf(3.0f * u * u - 1.0f);
+                    kk += K;
+                }
+                if (last) {
+                    const float gxk = -2.0f * u * ib * K2;
+                    const float hxy = 2.0f * ib2 * K2 * (4.0f * u * u * K - 1.0f);
+                    kq += K * gi * g[j] + gi * (-gxk) + g[j] * gxk + hxy;
+                }
+            }
+            const float phir = (ks + sign * 2.0f * ib * gk) * inv_n;
+            float phi = phir, hr = 0.0f;
+            if (full) {
+                hr = hw / fmaxf(kk, 1e-6f);
+                phi = phir / clampf(hr, 0.1f, 100.0f) * 0.7f;
+            }
+            ksd_acc += kq;
+            const float rr = c.rmsprop_rho;
+            const float vn = rr * v[i] + (1.0f - rr) * phi * phi;
+            float diff = 0.0f;
+            if (temp > 1e-6f) diff = sqrtf(2.0f * es * temp) * nz.normal(i, kn);
+            const float xr = xi + es * phi * rsqrtf(vn + c.rmsprop_eps) + diff;
+            xn[i] = clamp_h(xr);
+            v[i] = vn;
+            if (R) {
+                R[IPHIR * np + i] = phir;
+                R[IHR * np + i] = hr;
+                R[IHW * np + i] = hw;
+                R[IKN * np + i] = kk;
+                R[IXR * np + i] = xr;
+            }
+        }
+        __syncthreads();
+        for (int i = tid; i < n; i += kThreads) x[i] = xn[i];
+        __syncthreads();
+        if (temp > 1e-6f) ++kn;
+    }
+    // ---- outputs (svpf_opt_kernels.cu:1109-1153)
+    float mxl = -1e10f;
+    for (int i = tid; i < n; i += kThreads) mxl = fmaxf(mxl, lw[i]);
+    mxl = reduce_max(mxl, sh.red);
+    float s[3] = {0.0f, 0.0f, ksd_acc};
+    for (int i = tid; i < n; i += kThreads) {
+        s[0] += expf(lw[i] - mxl);
+        s[1] += x[i];
+    }
+    reduce_sum<3>(s, sh.red);
+    if (rec) {
+        float* RB = rec + (size_t)np * (kRecFixed + kRecPerIt * bmax);
+        for (int i = tid; i < n; i += kThreads) {
+            RB[i] = x[i];
+            RB[np + i] = v[i];
+        }
+    }
+    const float ll = mxl + logf(fmaxf(s[0] * inv_n, 1e-10f));
+    if (tid == 0) {
+        ts.mxl = mxl;
+        ts.se = s[0];
+        st.h_mean_prev = s[1] * inv_n;
+        if (budget > 0) {
+            const float k2 = s[2] / ((float)n * (float)n);
+            st.ksd_prev = sqrtf(fmaxf(k2, 0.0f));
+        }
+        st.timestep += 1;
+    }
+    __syncthreads();
+    return ll;
+}
+
+// Backward of one recorded tick.  xb, vb: adjoints of the tick's output
+// positions / moments on entry, of its input positions / moments on exit.
+// sa: adjoints of the scalar state (in: outputs of this tick; out: inputs).
+__device__ void bwd_tick(const svpf_config_t& c, int n, int np, float* xb, float* vb, float* work,
+                         Shared& sh, GAdj& sa, const Noise& nz, const float* rec, int bmax, float wt) {
+    const int tid = threadIdx.x;
+    const TickScalars& ts = sh.ts;
+    float* xs = work;                 // x^(it)
+    float* g = work + np;             // clamped score
+    float* a = work + 2 * np;         // dL/dphi_raw / n
+    float* cv = work + 3 * np;        // curvature
+    float* hwb = work + 4 * np;       // dL/dhw
+    float* knb = work + 5 * np;       // dL/dkn
+    float* coef = work + 6 * np;      // mixture column coefficients
+    float* lmx = work + 7 * np;
+    float* dbr = work + 8 * np;
+    float* mub = work + 9 * np;       // dL/dmu_k accumulated over iterations
+    float* lwb = work + 10 * np;      // dL/dlw of the last gradient pass
+    const bool full = c.use_newton && c.use_full_newton;
+    const float sign = c.stein_repulsive_sign == 1 ? 1.0f : -1.0f;
+    const float s2 = ts.s2, inv = 1.0f / s2;
+    const float nu = ts.nu;
+    const float ib = ts.ib, ib2 = ib * ib;
+    const float inv_n = 1.0f / (float)n;
+    const float rr = c.rmsprop_rho;
+    const int budget = ts.budget;
+    // thread-local partial sums of theta adjoints: mu, rho, sigma_z, nu, s2, bw
+    float pmu = 0.0f, prho = 0.0f, psz = 0.0f, pnu = 0.0f, ps2 = 0.0f, pbw = 0.0f;
+
+    // output mean -> next tick's guide reference
+    const float hmb = (float)sa.h_mean * inv_n;
+    for (int i = tid; i < n; i += kThreads) {
+        xb[i] += hmb;
+        mub[i] = 0.0f;
+        lwb[i] = 0.0f;
+    }
+    // loglik = mxl + log(se/n): dL/dlw_i = w_t exp(lw_i - mxl) / se
+    if (budget > 0 && ts.se * inv_n > 1e-10f) {
+        const float* R = rec + (size_t)np * (kRecFixed + kRecPerIt * (budget - 1));
+        for (int i = tid; i < n; i += kThreads) {
+            const float xi = R[IX * np + i], A = R[IAL * np + i];
+            const float lwi = ts.stc - 0.5f * xi - (nu + 1.0f) * 0.5f * log1pf(fmaxf(A, -0.999f));
+            lwb[i] = wt * expf(lwi - ts.mxl) / ts.se;
+        }
+    }
+    __syncthreads();
+
+    for (int it = budget - 1; it >= 0; --it) {
+        const float* R = rec + (size_t)np * (kRecFixed + kRecPerIt * it);
+        const float beta = ts.beta[it], es = ts.es[it];
+        // (a) elementwise: clamp, drift, RMSProp
+        for (int i = tid; i < n; i += kThreads) {
+            const float xr = R[IXR * np + i];
+            const float xi = R[IX * np + i];
+            const float vin = R[IV * np + i];
+            const float phir = R[IPHIR * np + i];
+            xs[i] = xi;
+            const float gp = R[IGPRE * np + i];
+            g[i] = clampf(gp, -10.0f, 10.0f);
+            float Hc = 1.0f, phi = phir;
+            if (full) {
+                Hc = clampf(R[IHR * np + i], 0.1f, 100.0f);
+                phi = phir / Hc * 0.7f;
+                const float A = R[IAL * np + i];
+                const float opA = 1.0f + A;
+                const float hl = -0.5f * (nu + 1.0f) * A / (opA * opA);
+                cv[i] = clampf(-(hl - inv), 0.1f, 100.0f);
+            }
+            const float vn = rr * vin + (1.0f - rr) * phi * phi;
+            const float r = rsqrtf(vn + c.rmsprop_eps);
+            const float cc = (xr >= SVPF_H_MIN && xr <= SVPF_H_MAX) ? xb[i] : 0.0f;
+            const float vbt = vb[i] + cc * es * phi * (-0.5f) * r * r * r;
+            const float phib = cc * es * r + vbt * 2.0f * (1.0f - rr) * phi;
+            vb[i] = vbt * rr;
+            xb[i] = cc;
+            float pr = phib;
+            if (full) {
+                pr = phib * 0.7f / Hc;
+                const float hr = R[IHR * np + i];
+                const float Hb = (hr >= 0.1f && hr <= 100.0f) ? -phib * 0.7f * phir / (Hc * Hc) : 0.0f;
+                const float kk = R[IKN * np + i], hw = R[IHW * np + i];
+                const float kkc = fmaxf(kk, 1e-6f);
+                hwb[i] = Hb / kkc;
+                knb[i] = kk > 1e-6f ? -Hb * hw / (kkc * kkc) : 0.0f;
+            }
+            a[i] = pr * inv_n;
+        }
+        __syncthreads();
+        // (b) transport adjoint: one pass of row sums (row and column terms)
+        for (int i = tid; i < n; i += kThreads) {
+            const float xi = xs[i], gi = g[i], ai = a[i];
+            float S1 = 0.f, S2 = 0.f, C1 = 0.f, C2 = 0.f, C3 = 0.f, Q1 = 0.f, Q2 = 0.f;
+            float R1 = 0.f, R2 = 0.f, R3 = 0.f, D1 = 0.f, D2 = 0.f, D3 = 0.f, E1 = 0.f, W1 = 0.f, W2 = 0.f, W3 = 0.f,
+                  W4 = 0.f;
+            for (int j = 0; j < n; ++j) {
+                const float u = (xi - xs[j]) * ib;
+                const float K = 1.0f / (1.0f + u * u);
+                const float K2 = K * K;
+                const float uK2 = u * K2;
+                const float t43 = K2 * (4.0f * K - 3.0f);
+                const float aj = a[j], gj = g[j];
+                S1 += gj * uK2;
+                S2 += t43;
+                C1 += aj * uK2;
+                C2 += aj * t43;
+                C3 += aj * K;
+                Q1 += gj * u * uK2;
+                Q2 += uK2 * (4.0f * K - 2.0f);
+                if (full) {
+                    const float w = 3.0f * u * u - 1.0f;
+                    const float aw = fabsf(w);
+                    const float sg = w > 0.0f ? 1.0f : (w < 0.0f ? -1.0f : 0.0f);
+                    const float f6 = uK2 * (6.0f * sg - 4.0f * K * aw);
+                    const float cj = cv[j], hbj = hwb[j], kbj = knb[j];
+                    R1 += cj * uK2;
+                    R2 += f6;
+                    R3 += uK2;
+                    D1 += hbj * uK2;
+                    D2 += hbj * f6;
+                    D3 += kbj * uK2;
+                    E1 += hbj * K;
+                    W1 += cj * u * uK2;
+                    W2 += u * f6;
+                    W3 += K2 * aw;
+                    W4 += u * uK2;
+                }
+            }
+            float dx = ib * (ai * (-2.0f * S1 + 2.0f * sign * ib * S2) - 2.0f * gi * C1 - 2.0f * sign * ib * C2);
+            pbw += ai * ib * (2.0f * Q1 - 2.0f * sign * ib * Q2);
+            float gb = C3;
+            if (full) {
+                const float hb = hwb[i], kb = knb[i];
+                dx += ib * (hb * (-2.0f * R1 + 2.0f * ib2 * R2) - 2.0f * kb * R3);
+                dx += ib * (-2.0f * cv[i] * D1 + 2.0f * ib2 * D2 - 2.0f * D3);
+                pbw += hb * (ib * (2.0f * W1 - 2.0f * ib2 * W2) - 4.0f * ib2 * ib * W3) + kb * 2.0f * ib * W4;
+                // curvature adjoint E1 -> A and s2 (clamp [0.1, 100])
+                const float A = R[IAL * np + i];
+                const float opA = 1.0f + A;
+                const float craw = 0.5f * (nu + 1.0f) * A / (opA * opA) + inv;
+                if (craw >= 0.1f && craw <= 100.0f) {
+                    // curv = 0.5 (nu+1) A / (1+A)^2 + 1/s2
+                    const float dcdA = 0.5f * (nu + 1.0f) * (1.0f - A) / (opA * opA * opA);
+                    const float dAdx = (xi < 20.0f) ? -A * expf(xi) / (expf(xi) + 1e-8f) : 0.0f;
+                    dx += E1 * dcdA * dAdx;
+                    pnu += E1 * (0.5f * A / (opA * opA) + dcdA * (-A / nu));
+                    ps2 += E1 * (-inv * inv);
+                }
+            }
+            xb[i] += dx;
+            // (c) gradient adjoint, O(N) part (g = clamp(gp + beta glik))
+            const float gpre = R[IGPRE * np + i];
+            const float gpb = (gpre >= -10.0f && gpre <= 10.0f) ? gb : 0.0f;
+            const float A = R[IAL * np + i];
+            const float opA = 1.0f + A;
+            const float ex = expf(fminf(xi, 20.0f));
+            const float dAdx = (xi < 20.0f) ? -A * ex / (ex + 1e-8f) : 0.0f;
+            const float dAdnu = -A / nu;
+            const float dbar = R[IDBAR * np + i], vard = R[IVARD * np + i], skew = R[ISKEW * np + i];
+            float dgdx = -inv + vard * inv * inv;
+            float dgdnu = 0.0f;
+            if (c.use_exact_gradient) {
+                const float dglA = 0.5f * (nu + 1.0f) / (opA * opA);
+                dgdx += beta * dglA * dAdx;
+                dgdnu = beta * (0.5f * A / opA + dglA * dAdnu);
+            } else {
+                dgdx += beta * (-1.0f / 1.4f);
+            }
+            float dxx = gpb * dgdx;
+            pnu += gpb * dgdnu;
+            ps2 += gpb * (dbar * inv * inv - skew * 0.5f * inv * inv * inv);
+            if (it == budget - 1) {
+                const float lb = lwb[i];
+                const float dlwdA = -(nu + 1.0f) * 0.5f / opA;
+                dxx += lb * (-0.5f + dlwdA * dAdx);
+                pnu += lb * (-0.5f * log1pf(A) + dlwdA * dAdnu);
+            }
+            xb[i] += dxx;
+            coef[i] = gpb * inv / R[IZ * np + i];
+            lmx[i] = R[ILMAX * np + i];
+            dbr[i] = dbar;
+        }
+        __syncthreads();
+        // (d) mixture column pass: dL/dmu_k
+        {
+            const float* MU = rec + (size_t)np * MUK;
+            const float inv2 = 0.5f * inv;
+            for (int k = tid; k < n; k += kThreads) {
+                const float mk = MU[k];
+                float acc = 0.0f;
+                for (int j = 0; j < n; ++j) {
+                    const float d = xs[j] - mk;
+                    const float r = expf(-d * d * inv2 - lmx[j]);
+                    acc += coef[j] * r * (1.0f - d * (d - dbr[j]) * inv);
+                }
+                mub[k] += acc;
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---- stc(nu) enters every log-weight: dL/dnu += stc'(nu) * sum lwb
+    // ---- bandwidth adjoint (needs the total dL/dbw)
+    {
+        float s[2] = {pbw, 0.0f};
+        for (int i = tid; i < n; i += kThreads) s[1] += lwb[i];
+        reduce_sum<2>(s, sh.red);
+        if (tid == 0) {
+            TickScalars& t = sh.ts;
+            const double dstc = 0.5 * digamma_d(0.5 * ((double)nu + 1.0)) - 0.5 * digamma_d(0.5 * (double)nu) -
+                                0.5 / (double)nu;
+            sh.acc[3] = dstc * (double)s[1];
+            const float bwb = s[0];
+            const float sq = sqrtf(t.bw2);
+            float bw2b = (sq >= 0.01f && sq <= 2.0f) ? bwb * 0.5f / sq : 0.0f;
+            bw2b += (float)sa.bw_sq;
+            const float sc = clampf(t.scale_raw, 0.5f, 1.0f);
+            const float scb = bw2b * t.pre;
+            const float preb = bw2b * sc;
+            float spb = 0.0f;
+            if (t.scale_raw >= 0.5f && t.scale_raw <= 1.0f && t.comb - 1.0f <= 2.0f) {
+                const float combb = -0.25f * scb;
+                if (t.spread_f > t.ratio && (t.mx - t.mn) * 0.5f <= 2.0f) spb = 0.5f * combb;
+            }
+            const float bnb = t.bw2_prev > 0.0f ? 0.3f * preb : preb;
+            sa.bw_sq = t.bw2_prev > 0.0f ? 0.7 * (double)preb : 0.0;
+            const float varb = t.bw2_new_raw >= 1e-6f ? bnb * 2.0f / logf((float)n + 1.0f) : 0.0f;
+            // broadcast through the scratch
+            sh.red[0][0] = varb;
+            sh.red[0][1] = spb;
+        }
+        __syncthreads();
+        const float varb = sh.red[0][0], spb = sh.red[0][1];
+        const float* X0 = rec + (size_t)np * (kRecFixed + 0);   // x^(0) = X of iteration 0
+        for (int i = tid; i < n; i += kThreads) {
+            float x0;
+            if (budget > 0) x0 = X0[IX * np + i];
+            else x0 = rec[(size_t)np * (kRecFixed + kRecPerIt * bmax) + i];
+            xb[i] += varb * 2.0f * (x0 - ts.mean) * inv_n;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            xb[ts.imx] += spb;
+            xb[ts.imn] -= spb;
+        }
+        __syncthreads();
+    }
+    // ---- guide adjoint, predict adjoint, prior-mean adjoint
+    {
+        const float rc = fminf(fmaxf(ts.rho, 0.0f), 0.999f);
+        const bool rin = ts.rho >= 0.0f && ts.rho <= 0.999f;
+        const float lev_num = ts.gamma * ts.y_prev;
+        float sc[1] = {0.0f};
+        for (int i = tid; i < n; i += kThreads) {
+            float hpb;
+            if (c.use_guide) {
+                const float hgr = rec[HGR * np + i];
+                const float cg = (hgr >= SVPF_H_MIN && hgr <= SVPF_H_MAX) ? xb[i] : 0.0f;
+                sc[0] += cg;
+                hpb = c.use_guide_preserving ? cg : (1.0f - ts.gs) * cg;
+            } else {
+                hpb = xb[i];
+            }
+            const float hpr = rec[HPR * np + i];
+            const float cp = (hpr >= SVPF_H_MIN && hpr <= SVPF_H_MAX) ? hpb : 0.0f;
+            const float xi = rec[XS * np + i];
+            const float z = nz.normal(i, 0);
+            const float e1 = expf(fminf(xi * 0.5f, 20.0f));
+            const float levd = (xi * 0.5f < 20.0f) ? -lev_num * 0.5f * e1 / ((e1 + 1e-8f) * (e1 + 1e-8f)) : 0.0f;
+            const float e2 = expf(xi * 0.5f);
+            const float mkd = -lev_num * 0.5f * e2 / ((e2 + 1e-8f) * (e2 + 1e-8f));
+            const float mb = mub[i];
+            float dxin;
+            if (c.use_mim) {
+                const float sel = nz.uniform(i, 0);
+                const float scale = sel < c.mim_jump_prob ? c.mim_jump_scale : 1.0f;
+                dxin = cp * (rc + levd);
+                pmu += cp * (1.0f - rc);
+                if (rin) prho += cp * (xi - ts.mu);
+                psz += cp * scale * z;
+            } else {
+                dxin = cp * (ts.rho + levd);
+                pmu += cp * (1.0f - ts.rho);
+                prho += cp * (xi - ts.mu);
+                psz += cp * z;
+            }
+            dxin += mb * (ts.rho + mkd);
+            pmu += mb * (1.0f - ts.rho);
+            prho += mb * (xi - ts.mu);
+            xb[i] = dxin;
+        }
+        reduce_sum<1>(sc, sh.red);
+        float s[6] = {pmu, prho, psz, pnu, ps2, 0.0f};
+        reduce_sum<6>(s, sh.red);
+        if (tid == 0) {
+            const double mu = ts.mu, rho = ts.rho, sz = ts.sz;
+            double dmu = s[0], drho = s[1], dsz = s[2], dnu = (double)s[3] + sh.acc[3];
+            dsz += (double)s[4] * 2.0 * sz;
+            double cmb = 0.0;
+            if (c.use_guide) {
+                const double gmb = (double)ts.gs * (double)sc[0];
+                cmb = c.use_guide_preserving ? -(double)ts.gs * (double)sc[0] : 0.0;
+                // EKF adjoint (FP64)
+                const double mpb0 = sa.m + gmb;
+                const double Pb = sa.P;
+                const double ly2 = log((double)ts.y_t * (double)ts.y_t + 1e-8);
+                const double Kb = mpb0 * (ly2 + (double)ts.off - ts.m_pred) - Pb * ts.P_pred;
+                const double mpb = mpb0 * (1.0 - ts.K);
+                const double den = ts.P_pred + 6.93 + 1e-8;
+                const double Ppb = Pb * (1.0 - ts.K) + Kb * (6.93 + 1e-8) / (den * den);
+                dmu += mpb * (1.0 - rho);
+                drho += mpb * (ts.m_in - mu) + Ppb * 2.0 * rho * ts.P_in;
+                dsz += Ppb * 2.0 * sz;
+                double mb = mpb * rho, Pbi = Ppb * rho * rho;
+                if (ts.init_here) {
+                    dmu += mb;
+                    const double q = 1.0 - rho * rho;
+                    dsz += Pbi * 2.0 * sz / q;
+                    drho += Pbi * sz * sz * 2.0 * rho / (q * q);
+                    mb = 0.0;
+                    Pbi = 0.0;
+                }
+                sa.m = mb;
+                sa.P = Pbi;
+            }
+            sa.h_mean = cmb;
+            sa.th[0] += dmu;
+            sa.th[1] += drho;
+            sa.th[2] += dsz;
+            sa.th[3] += dnu;
+        }
+        __syncthreads();
+    }
+}
+
+__device__ inline Noise make_noise(unsigned long long seed, int f, int tick, int n, int* flag) {
+    return Noise{philox_key(seed, f), (uint32_t)tick, nullptr, nullptr, 0, 0, n, flag};
+}
+
+__device__ inline void load_theta(const GArgs& a, int f, TickScalars& ts) {
+    ts.mu = a.theta[4 * f + 0];
+    ts.rho = a.theta[4 * f + 1];
+    ts.sz = a.theta[4 * f + 2];
+    ts.nu = a.theta[4 * f + 3];
+    ts.gamma = a.gamma ? a.gamma[f] : 0.0f;
+}
+
+// svpf_initialize (svpf_optimized_graph.cu:349-451), single factor, Philox draw 0 of stream 2.
+__device__ void init_filter(const GArgs& a, int f, int n, float* x, float* v, Shared& sh) {
+    const TickScalars& ts = sh.ts;
+    const float var = ts.sz * ts.sz / (1.0f - ts.rho * ts.rho + 1e-6f);
+    const float sd = sqrtf(var);
+    const uint2 key = philox_key(a.seed, f);
+    for (int i = threadIdx.x; i < n; i += kThreads) {
+        const uint4 r = philox10(key, make_uint4((uint32_t)i, 0u, 0u, 2u));
+        const float z = normal_from_bits(r.x, r.y);
+        x[i] = clamp_h(ts.mu + sd * z);
+        v[i] = 0.0f;
+    }
+    if (threadIdx.x == 0) {
+        GState& s = sh.st;
+        s.m = ts.mu;
+        s.P = var;
+        s.bw_sq = 0.0f;
+        s.h_mean_prev = -3.5f;   // :492-494
+        s.return_ema = 0.0f;
+        s.return_var = 0.0f;
+        s.ksd_prev = 1e10f;
+        s.guide_init = 0;
+        s.timestep = 0;
+        s.pad = 0;
+    }
+    __syncthreads();
+}
+
+// adjoint of the initialisation: h_i = clamp(mu + sd z_i), sd^2 = sz^2/(1 - rho^2 + 1e-6)
+__device__ void init_adjoint(const GArgs& a, int f, int n, const float* xb, Shared& sh, GAdj& sa) {
+    const TickScalars& ts = sh.ts;
+    const float q = 1.0f - ts.rho * ts.rho + 1e-6f;
+    const float var = ts.sz * ts.sz / q;
+    const float sd = sqrtf(var);
+    const uint2 key = philox_key(a.seed, f);
+    float s[2] = {0.0f, 0.0f};
+    for (int i = threadIdx.x; i < n; i += kThreads) {
+        const uint4 r = philox10(key, make_uint4((uint32_t)i, 0u, 0u, 2u));
+        const float z = normal_from_bits(r.x, r.y);
+        const float hr = ts.mu + sd * z;
+        if (hr >= SVPF_H_MIN && hr <= SVPF_H_MAX) {
+            s[0] += xb[i];
+            s[1] += xb[i] * z;
+        }
+    }
+    reduce_sum<2>(s, sh.red);
+    if (threadIdx.x == 0) {
+        const double varb = (double)s[1] / (2.0 * sd);
+        sa.th[0] += s[0];
+        sa.th[2] += varb * 2.0 * ts.sz / q;
+        sa.th[1] += varb * (double)ts.sz * ts.sz * 2.0 * ts.rho / ((double)q * q);
+    }
+    __syncthreads();
+}
+
+__device__ inline void copy_state_to(GState* dst, const GState& src) {
+    if (threadIdx.x == 0) *dst = src;
+}
+
+// Forward over ticks [t0, t1) for every filter; checkpoint at segment starts.
+__global__ void __launch_bounds__(kThreads) grad_forward_kernel(const GArgs a, int t0, int t1) {
+    extern __shared__ __align__(16) float smem[];
+    __shared__ Shared sh;
+    __shared__ svpf_config_t cfg;
+    const int np = a.np;
+    float* x = smem;
+    float* v = smem + np;
+    float* work = smem + 2 * np;
+    for (int f = blockIdx.x; f < a.F; f += gridDim.x) {
+        if (threadIdx.x == 0) {
+            cfg = a.cfg[f];
+            sh.flag = 0;
+            load_theta(a, f, sh.ts);
+        }
+        __syncthreads();
+        const int n = a.n[f];
+        if (t0 == 0) {
+            init_filter(a, f, n, x, v, sh);
+            if (threadIdx.x == 0) a.ll_sum[f] = 0.0;
+        } else {
+            for (int i = threadIdx.x; i < n; i += kThreads) {
+                x[i] = a.fx[(size_t)f * np + i];
+                v[i] = a.fv[(size_t)f * np + i];
+            }
+            if (threadIdx.x == 0) sh.st = a.fs[f];
+            __syncthreads();
+        }
+        for (int t = t0; t < t1; ++t) {
+            if (t % a.k == 0) {
+                const int sg = t / a.k;
+                float* ck = a.ck + ((size_t)f * a.nseg + sg) * 2 * np;
+                for (int i = threadIdx.x; i < n; i += kThreads) {
+                    ck[i] = x[i];
+                    ck[np + i] = v[i];
+                }
+                copy_state_to(&a.cks[(size_t)f * a.nseg + sg], sh.st);
+            }
+            const float yt = a.y[(size_t)f * a.T + t];
+            const float yp = t > 0 ? a.y[(size_t)f * a.T + t - 1] : 0.0f;
+            const Noise nz = make_noise(a.seed, f, sh.st.timestep, n, &sh.flag);
+            __syncthreads();
+            const float ll = fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, nullptr, a.bmax);
+            if (threadIdx.x == 0) {
+                if (a.loglik) a.loglik[(size_t)f * a.T + t] = ll;
+                a.ll_sum[f] += (double)ll;
+            }
+        }
+        for (int i = threadIdx.x; i < n; i += kThreads) {
+            a.fx[(size_t)f * np + i] = x[i];
+            a.fv[(size_t)f * np + i] = v[i];
+        }
+        if (threadIdx.x == 0) {
+            a.fs[f] = sh.st;
+            if (sh.flag) a.status[f] = sh.flag;
+        }
+        __syncthreads();
+    }
+}
+
+// Backward over segment sg for every filter.
+__global__ void __launch_bounds__(kThreads) grad_backward_kernel(const GArgs a, int sg) {
+    extern __shared__ __align__(16) float smem[];
+    __shared__ Shared sh;
+    __shared__ svpf_config_t cfg;
+    __shared__ GAdj sa;
+    const int np = a.np;
+    float* x = smem;
+    float* v = smem + np;
+    float* xb = smem + 2 * np;
+    float* vb = smem + 3 * np;
+    float* work = smem + 4 * np;
+    float* seg = a.seg + (size_t)blockIdx.x * a.k * 2 * np;
+    GState* segs = a.segs + (size_t)blockIdx.x * a.k;
+    float* rec = a.rec + (size_t)blockIdx.x * a.rec_floats;
+    const int t0 = sg * a.k;
+    const int t1 = min(a.T, t0 + a.k);
+    for (int f = blockIdx.x; f < a.F; f += gridDim.x) {
+        const int n = a.n[f];
+        if (threadIdx.x == 0) {
+            cfg = a.cfg[f];
+            sh.flag = 0;
+            load_theta(a, f, sh.ts);
+            sh.st = a.cks[(size_t)f * a.nseg + sg];
+            sa = a.as[f];
+        }
+        __syncthreads();
+        const float* ck = a.ck + ((size_t)f * a.nseg + sg) * 2 * np;
+        for (int i = threadIdx.x; i < n; i += kThreads) {
+            x[i] = ck[i];
+            v[i] = ck[np + i];
+            xb[i] = a.ax[(size_t)f * np + i];
+            vb[i] = a.av[(size_t)f * np + i];
+        }
+        __syncthreads();
+        // recompute the segment, keeping every tick's input state
+        for (int t = t0; t < t1; ++t) {
+            float* sx = seg + (size_t)(t - t0) * 2 * np;
+            for (int i = threadIdx.x; i < n; i += kThreads) {
+                sx[i] = x[i];
+                sx[np + i] = v[i];
+            }
+            copy_state_to(&segs[t - t0], sh.st);
+            const float yt = a.y[(size_t)f * a.T + t];
+            const float yp = t > 0 ? a.y[(size_t)f * a.T + t - 1] : 0.0f;
+            const Noise nz = make_noise(a.seed, f, sh.st.timestep, n, &sh.flag);
+            __syncthreads();
+            fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, nullptr, a.bmax);
+        }
+        // reverse over the segment's ticks
+        for (int t = t1 - 1; t >= t0; --t) {
+            const float* sx = seg + (size_t)(t - t0) * 2 * np;
+            for (int i = threadIdx.x; i < n; i += kThreads) {
+                x[i] = sx[i];
+                v[i] = sx[np + i];
+            }
+            if (threadIdx.x == 0) {
+                sh.st = segs[t - t0];
+                load_theta(a, f, sh.ts);
+            }
+            const float yt = a.y[(size_t)f * a.T + t];
+            const float yp = t > 0 ? a.y[(size_t)f * a.T + t - 1] : 0.0f;
+            __syncthreads();
+            const Noise nz = make_noise(a.seed, f, sh.st.timestep, n, &sh.flag);
+            fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, rec, a.bmax);
+            const float wt = a.w ? a.w[(size_t)f * a.T + t] : 1.0f;
+            bwd_tick(cfg, n, np, xb, vb, work, sh, sa, nz, rec, a.bmax, wt);
+        }
+        if (t0 == 0) init_adjoint(a, f, n, xb, sh, sa);
+        for (int i = threadIdx.x; i < n; i += kThreads) {
+            a.ax[(size_t)f * np + i] = xb[i];
+            a.av[(size_t)f * np + i] = vb[i];
+        }
+        if (threadIdx.x == 0) {
+            a.as[f] = sa;
+            if (sh.flag) a.status[f] = sh.flag;
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace grad
+}  // namespace svpf
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+using namespace svpf;
+using namespace svpf::grad;
+
+struct svpf_grad {
+    int F = 0, n_max = 0, np = 0, T_max = 0, k = 64, nseg = 0, bmax = 1, grid = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    size_t smem = 0, rec_floats = 0;
+    std::vector<int> ns;
+    std::vector<svpf_config_t> cfgs;
+    int T = 0;
+    unsigned long long seed = 0;
+    bool forward_done = false;
+    // device
+    int* d_n = nullptr;
+    svpf_config_t* d_cfg = nullptr;
+    float* d_theta = nullptr;
+    float* d_gamma = nullptr;
+    float* d_y = nullptr;
+    float* d_w = nullptr;
+    float* d_loglik = nullptr;
+    double* d_llsum = nullptr;
+    float* d_fx = nullptr;
+    float* d_fv = nullptr;
+    GState* d_fs = nullptr;
+    float* d_ck = nullptr;
+    GState* d_cks = nullptr;
+    float* d_ax = nullptr;
+    float* d_av = nullptr;
+    GAdj* d_as = nullptr;
+    float* d_seg = nullptr;
+    GState* d_segs = nullptr;
+    float* d_rec = nullptr;
+    int* d_status = nullptr;
+    const float* u_theta = nullptr;   // the arrays the last forward used
+    const float* u_gamma = nullptr;
+    const float* u_y = nullptr;
+};
+
+namespace {
+
+template <class T>
+bool galloc(T** p, size_t count) {
+    return cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T)) == cudaSuccess;
+}
+
+GArgs make_gargs(const svpf_grad* g, const float* theta, const float* gamma, const float* y, const float* w,
+                 float* loglik) {
+    GArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.F = g->F;
+    a.T = g->T;
+    a.k = g->k;
+    a.np = g->np;
+    a.bmax = g->bmax;
+    a.n = g->d_n;
+    a.cfg = g->d_cfg;
+    a.theta = theta;
+    a.gamma = gamma;
+    a.y = y;
+    a.w = w;
+    a.loglik = loglik;
+    a.ll_sum = g->d_llsum;
+    a.seed = g->seed;
+    a.fx = g->d_fx;
+    a.fv = g->d_fv;
+    a.fs = g->d_fs;
+    a.ck = g->d_ck;
+    a.cks = g->d_cks;
+    a.ax = g->d_ax;
+    a.av = g->d_av;
+    a.as = g->d_as;
+    a.seg = g->d_seg;
+    a.segs = g->d_segs;
+    a.rec = g->d_rec;
+    a.rec_floats = g->rec_floats;
+    a.nseg = g->nseg;
+    a.status = g->d_status;
+    return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+int svpf_grad_supported(const svpf_config_t* c) {
+    if (!c) return 0;
+    if (c->use_two_factor || c->use_heun || c->use_student_t_state || c->use_fan_mode) return 0;
+    if (c->use_adaptive_mu || c->use_adaptive_sigma || c->use_adaptive_guide) return 0;
+    if (c->use_asymmetric_rho || c->use_local_params || c->use_guided || c->use_rejuvenation) return 0;
+    if (c->use_newton && !c->use_full_newton) return 0;
+    // adaptive beta is a continuous function of the previous tick's KSD, which
+    // the adjoint does not differentiate
+    if (c->use_annealing && c->use_adaptive_beta) return 0;
+    return 1;
+}
+
+svpf_grad_t* svpf_grad_create(int F, const int* ns, const svpf_config_t* cfgs, int T_max, int k,
+                              cudaStream_t stream) {
+    if (F < 1 || !ns || !cfgs || T_max < 1 || k < 1) return nullptr;
+    int n_max = 0, bmax = 1;
+    for (int f = 0; f < F; ++f) {
+        if (ns[f] < 1 || ns[f] > SVPF_MAX_PARTICLES || !svpf_grad_supported(&cfgs[f])) return nullptr;
+        n_max = std::max(n_max, ns[f]);
+        bmax = std::max(bmax, std::max(cfgs[f].stein_max_steps, cfgs[f].stein_min_steps));
+    }
+    if (bmax > 64) return nullptr;
+    svpf_grad* g = new svpf_grad();
+    g->F = F;
+    g->n_max = n_max;
+    g->np = round_up(n_max, 64);
+    g->T_max = T_max;
+    g->k = k;
+    g->nseg = (T_max + k - 1) / k;
+    g->bmax = bmax;
+    g->ns.assign(ns, ns + F);
+    g->cfgs.assign(cfgs, cfgs + F);
+    if (stream) {
+        g->stream = stream;
+    } else {
+        cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+        g->own_stream = true;
+    }
+    const size_t np = (size_t)g->np;
+    g->smem = (size_t)(4 + 11) * np * sizeof(float);
+    int dev = 0, optin = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t static_bytes = sizeof(Shared) + sizeof(svpf_config_t) + sizeof(GAdj) + 64;
+    if (g->smem + static_bytes > (size_t)optin) {
+        delete g;
+        return nullptr;
+    }
+    cudaFuncSetAttribute(grad_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g->smem);
+    cudaFuncSetAttribute(grad_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g->smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grad_backward_kernel, kThreads, g->smem);
+    g->grid = std::min(F, std::max(1, per_sm) * sms);
+    g->rec_floats = rec_floats_for(g->np, bmax);
+    const size_t G = (size_t)g->grid;
+    bool ok = galloc(&g->d_n, F) && galloc(&g->d_cfg, F) && galloc(&g->d_theta, 4 * (size_t)F) &&
+              galloc(&g->d_gamma, F) && galloc(&g->d_y, (size_t)F * T_max) && galloc(&g->d_w, (size_t)F * T_max) &&
+              galloc(&g->d_loglik, (size_t)F * T_max) && galloc(&g->d_llsum, F) && galloc(&g->d_fx, F * np) &&
+              galloc(&g->d_fv, F * np) && galloc(&g->d_fs, F) && galloc(&g->d_ck, F * g->nseg * 2 * np) &&
+              galloc(&g->d_cks, (size_t)F * g->nseg) && galloc(&g->d_ax, F * np) && galloc(&g->d_av, F * np) &&
+              galloc(&g->d_as, F) && galloc(&g->d_seg, G * k * 2 * np) && galloc(&g->d_segs, G * k) &&
+              galloc(&g->d_rec, G * g->rec_floats) && galloc(&g->d_status, F);
+    ok = ok && cudaMemcpy(g->d_n, ns, F * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(g->d_cfg, cfgs, F * sizeof(svpf_config_t), cudaMemcpyHostToDevice) == cudaSuccess;
+    if (!ok) {
+        svpf_grad_destroy(g);
+        return nullptr;
+    }
+    return g;
+}
+
+void svpf_grad_destroy(svpf_grad_t* g) {
+    if (!g) return;
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    void* ptrs[] = {g->d_n, g->d_cfg, g->d_theta, g->d_gamma, g->d_y, g->d_w, g->d_loglik, g->d_llsum,
+                    g->d_fx, g->d_fv, g->d_fs, g->d_ck, g->d_cks, g->d_ax, g->d_av, g->d_as, g->d_seg,
+                    g->d_segs, g->d_rec, g->d_status};
+    for (void* p : ptrs) cudaFree(p);
+    if (g->own_stream) cudaStreamDestroy(g->stream);
+    delete g;
+}
+
+int svpf_grad_forward_device(svpf_grad_t* g, const float* d_theta, const float* d_gamma, const float* d_y, int T,
+                             unsigned long long seed, float* d_loglik) {
+    if (!g || !d_theta || !d_y || T < 1 || T > g->T_max) return SVPF_ERR_INVALID_ARG;
+    g->T = T;
+    g->seed = seed;
+    g->u_theta = d_theta;
+    g->u_gamma = d_gamma;
+    g->u_y = d_y;
+    if (cudaMemsetAsync(g->d_status, 0, g->F * sizeof(int), g->stream) != cudaSuccess) return SVPF_ERR_CUDA;
+    const GArgs a = make_gargs(g, d_theta, d_gamma, d_y, nullptr, d_loglik ? d_loglik : g->d_loglik);
+    for (int t0 = 0; t0 < T; t0 += g->k) {
+        grad_forward_kernel<<<g->grid, kThreads, g->smem, g->stream>>>(a, t0, std::min(T, t0 + g->k));
+        if (cudaGetLastError() != cudaSuccess) return SVPF_ERR_CUDA;
+    }
+    g->forward_done = true;
+    return SVPF_OK;
+}
+
+int svpf_grad_backward_device(svpf_grad_t* g, const float* d_w, double* d_grad) {
+    if (!g || !g->forward_done) return SVPF_ERR_NOT_INITIALIZED;
+    if (cudaMemsetAsync(g->d_ax, 0, (size_t)g->F * g->np * sizeof(float), g->stream) != cudaSuccess ||
+        cudaMemsetAsync(g->d_av, 0, (size_t)g->F * g->np * sizeof(float), g->stream) != cudaSuccess ||
+        cudaMemsetAsync(g->d_as, 0, (size_t)g->F * sizeof(GAdj), g->stream) != cudaSuccess)
+        return SVPF_ERR_CUDA;
+    const GArgs a = make_gargs(g, g->u_theta, g->u_gamma, g->u_y, d_w, nullptr);
+    const int nseg = (g->T + g->k - 1) / g->k;
+    for (int sg = nseg - 1; sg >= 0; --sg) {
+        grad_backward_kernel<<<g->grid, kThreads, g->smem, g->stream>>>(a, sg);
+        if (cudaGetLastError() != cudaSuccess) return SVPF_ERR_CUDA;
+    }
+    if (d_grad) {
+        // gather th[4] of every filter (strided copy)
+        if (cudaMemcpy2DAsync(d_grad, 4 * sizeof(double), reinterpret_cast<const char*>(g->d_as) + offsetof(GAdj, th),
+                              sizeof(GAdj), 4 * sizeof(double), g->F, cudaMemcpyDeviceToDevice,
+                              g->stream) != cudaSuccess)
+            return SVPF_ERR_CUDA;
+    }
+    return SVPF_OK;
+}
+
+int svpf_grad_forward(svpf_grad_t* g, const float* theta, const float* gamma, const float* y, int T,
+                      unsigned long long seed, float* loglik, double* loglik_sum) {
+    if (!g || !theta || !y || T < 1 || T > g->T_max) return SVPF_ERR_INVALID_ARG;
+    const size_t F = (size_t)g->F;
+    if (cudaMemcpyAsync(g->d_theta, theta, 4 * F * sizeof(float), cudaMemcpyHostToDevice, g->stream) != cudaSuccess)
+        return SVPF_ERR_CUDA;
+    if (gamma && cudaMemcpyAsync(g->d_gamma, gamma, F * sizeof(float), cudaMemcpyHostToDevice, g->stream) != cudaSuccess)
+        return SVPF_ERR_CUDA;
+    // y: [F][T] from the host, packed with row stride T
+    if (cudaMemcpyAsync(g->d_y, y, F * T * sizeof(float), cudaMemcpyHostToDevice, g->stream) != cudaSuccess)
+        return SVPF_ERR_CUDA;
+    int rc = svpf_grad_forward_device(g, g->d_theta, gamma ? g->d_gamma : nullptr, g->d_y, T, seed, g->d_loglik);
+    if (rc != SVPF_OK) return rc;
+    if (loglik && cudaMemcpyAsync(loglik, g->d_loglik, F * T * sizeof(float), cudaMemcpyDeviceToHost, g->stream) != cudaSuccess)
+        return SVPF_ERR_CUDA;
+    if (loglik_sum && cudaMemcpyAsync(loglik_sum, g->d_llsum, F * sizeof(double), cudaMemcpyDeviceToHost, g->stream) != cudaSuccess)
+        return SVPF_ERR_CUDA;
+    if (cudaStreamSynchronize(g->stream) != cudaSuccess) return SVPF_ERR_CUDA;
+    std::vector<int> st(F);
+    cudaMemcpy(st.data(), g->d_status, F * sizeof(int), cudaMemcpyDeviceToHost);
+    for (int s : st)
+        if (s) return s;
+    return SVPF_OK;
+}
+
+int svpf_grad_backward(svpf_grad_t* g, const float* w, double* grad) {
+    if (!g || !grad) return SVPF_ERR_INVALID_ARG;
+    if (!g->forward_done) return SVPF_ERR_NOT_INITIALIZED;
+    const size_t F = (size_t)g->F;
+    const float* dw = nullptr;
+    if (w) {
+        if (cudaMemcpyAsync(g->d_w, w, F * g->T * sizeof(float), cudaMemcpyHostToDevice, g->stream) != cudaSuccess)
+            return SVPF_ERR_CUDA;
+        dw = g->d_w;
+    }
+    double* d_grad = nullptr;
+    if (!galloc(&d_grad, 4 * F)) return SVPF_ERR_CUDA;
+    int rc = svpf_grad_backward_device(g, dw, d_grad);
+    if (rc == SVPF_OK &&
+        cudaMemcpyAsync(grad, d_grad, 4 * F * sizeof(double), cudaMemcpyDeviceToHost, g->stream) != cudaSuccess)
+        rc = SVPF_ERR_CUDA;
+    if (rc == SVPF_OK && cudaStreamSynchronize(g->stream) != cudaSuccess) rc = SVPF_ERR_CUDA;
+    cudaFree(d_grad);
+    return rc;
+}
+
+int svpf_grad_checkpoint_every(const svpf_grad_t* g) { return g ? g->k : 0; }
+
+}  // extern "C"

@@ -143,6 +143,14 @@ def lib() -> C.CDLL:
         "svpf_autotune": (_I, [C.POINTER(_I), _I, _I]),
         "svpf_tile_choice": (_I, [_I, C.POINTER(_I), C.POINTER(_I)]),
         "svpf_build_info": (C.c_char_p, []),
+        "svpf_grad_supported": (_I, [C.POINTER(Config)]),
+        "svpf_grad_create": (vp, [_I, C.POINTER(_I), C.POINTER(Config), _I, _I, vp]),
+        "svpf_grad_destroy": (None, [vp]),
+        "svpf_grad_forward": (_I, [vp, _FP, _FP, _FP, _I, C.c_ulonglong, _FP, C.POINTER(C.c_double)]),
+        "svpf_grad_backward": (_I, [vp, _FP, C.POINTER(C.c_double)]),
+        "svpf_grad_forward_device": (_I, [vp, vp, vp, vp, _I, C.c_ulonglong, vp]),
+        "svpf_grad_backward_device": (_I, [vp, vp, vp]),
+        "svpf_grad_checkpoint_every": (_I, [vp]),
         "svpf_debug_philox": (_I, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), _I]),
     }
     for name, (res, args) in sig.items():
@@ -526,6 +534,95 @@ class Batch:
         r, s = C.c_int(), C.c_int()
         lib().svpf_batch_tile_of(self._b, int(n), C.byref(r), C.byref(s))
         return r.value, s.value
+
+
+def grad_config(n_stein: int = 8, nu: float = 12.0, full_newton: bool = True, **kw) -> Config:
+    """The svpf_create defaults moved into the differentiable set: the model's
+    rho in predict (no asymmetric rho), no rejuvenation, fixed beta schedule
+    and a fixed Stein budget of n_stein iterations over 3 stages."""
+    c = default_config(n_stein, nu)
+    c.update(use_asymmetric_rho=0, use_rejuvenation=0, use_adaptive_beta=0, use_newton=int(full_newton),
+             use_full_newton=int(full_newton), stein_min_steps=n_stein, stein_max_steps=n_stein,
+             n_anneal_steps=3, use_exact_gradient=1)
+    c.update(**kw)
+    return c
+
+
+class Grad:
+    """Gradient engine: d(sum_t w_t loglik_t)/d(mu, rho, sigma_z, nu) for F
+    filters over a run of T ticks (svpf_grad_* in the C ABI).  Reverse mode
+    with a checkpoint every `checkpoint_every` ticks."""
+
+    def __init__(self, ns, configs, T_max: int, checkpoint_every: int = 64, stream=None):
+        ns = np.ascontiguousarray(ns, dtype=np.int32)
+        F = int(ns.shape[0])
+        if isinstance(configs, Config):
+            configs = [configs] * F
+        self._cfgs = (Config * F)(*configs)
+        self._ns = ns
+        self._g = lib().svpf_grad_create(F, ns.ctypes.data_as(C.POINTER(_I)), self._cfgs, int(T_max),
+                                         int(checkpoint_every), stream)
+        if not self._g:
+            raise RuntimeError("svpf_grad_create failed (configuration outside the differentiable set, "
+                               "sizes, or device)")
+        self.F = F
+        self.T_max = int(T_max)
+        self.T = 0
+        self.forward_id = 0
+
+    def close(self):
+        if getattr(self, "_g", None):
+            lib().svpf_grad_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def supported(cfg: Config) -> bool:
+        return bool(lib().svpf_grad_supported(C.byref(cfg)))
+
+    @property
+    def checkpoint_every(self) -> int:
+        return int(lib().svpf_grad_checkpoint_every(self._g))
+
+    def _check(self, rc):
+        if rc != SVPF_OK:
+            raise RuntimeError(f"svpf grad error {rc}: {ERRORS.get(rc, '?')}")
+
+    def forward(self, theta, y, gamma=None, seed: int = 0):
+        """theta [F,4] = (mu, rho, sigma_z, nu), y [F,T] (host arrays).
+        Returns (loglik [F,T] float32, loglik_sum [F] float64)."""
+        th = _f32(theta).reshape(self.F, 4)
+        yy = _f32(y).reshape(self.F, -1)
+        T = yy.shape[1]
+        gm = None if gamma is None else _f32(gamma)
+        ll = np.empty((self.F, T), np.float32)
+        ls = np.empty(self.F, np.float64)
+        self._check(lib().svpf_grad_forward(self._g, _fp(th), None if gm is None else _fp(gm), _fp(yy), T,
+                                            int(seed), _fp(ll), ls.ctypes.data_as(C.POINTER(C.c_double))))
+        self.T = T
+        self.forward_id += 1
+        return ll, ls
+
+    def backward(self, w=None) -> np.ndarray:
+        """Gradient [F,4] of sum_t w[f,t] loglik[f,t] (w None: all ones)."""
+        ww = None if w is None else _f32(w).reshape(self.F, self.T)
+        out = np.empty((self.F, 4), np.float64)
+        self._check(lib().svpf_grad_backward(self._g, None if ww is None else _fp(ww),
+                                             out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def forward_device(self, d_theta: int, d_gamma, d_y: int, T: int, seed: int, d_loglik: int):
+        self._check(lib().svpf_grad_forward_device(self._g, d_theta, d_gamma, d_y, int(T), int(seed), d_loglik))
+        self.T = int(T)
+        self.forward_id += 1
+
+    def backward_device(self, d_w, d_grad: int):
+        self._check(lib().svpf_grad_backward_device(self._g, d_w, d_grad))
 
 
 def autotune(ns, ticks: int = 2):

@@ -162,6 +162,13 @@ def lib():
             C.c_int, C.POINTER(OracleConfig), C.POINTER(OracleParams), C.POINTER(OracleCtl),
             C.POINTER(C.c_int), C.c_int] + [C.POINTER(C.c_float)] * 6 + [
             C.c_uint64, C.c_uint64, C.c_int, C.POINTER(OracleOut)]
+        L.svpf_oracle_grad_supported.restype = C.c_int
+        L.svpf_oracle_grad_supported.argtypes = [C.POINTER(OracleConfig)]
+        L.svpf_oracle_grad_run.restype = C.c_int
+        L.svpf_oracle_grad_run.argtypes = [C.POINTER(OracleConfig), C.c_int, C.c_int, C.POINTER(C.c_double),
+                                           C.c_double, C.POINTER(C.c_float), C.POINTER(C.c_double),
+                                           C.c_uint64, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                           C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -176,6 +183,49 @@ def default_ctl() -> OracleCtl:
     c = OracleCtl()
     lib().svpf_oracle_ctl_defaults(C.byref(c))
     return c
+
+
+def grad_supported(cfg: OracleConfig) -> bool:
+    return bool(lib().svpf_oracle_grad_supported(C.byref(cfg)))
+
+
+def grad_run(cfg: OracleConfig, n: int, theta, ys, gamma: float = 0.0, w=None, seed: int = 0,
+             filter_id: int = 0):
+    """FP64 forward-mode gradient oracle of one filter's run: initialisation
+    from theta = (mu, rho, sigma_z, nu), then len(ys) ticks (Philox noise keyed
+    by seed and filter_id).  Returns (loglik[T], grad[4] of sum_t w_t loglik_t,
+    final particles[n])."""
+    ys = np.ascontiguousarray(ys, np.float32)
+    T = int(ys.shape[0])
+    th = np.ascontiguousarray(theta, np.float64)
+    ll = np.zeros(T)
+    g = np.zeros(4)
+    hf = np.zeros(n)
+    wv = None if w is None else np.ascontiguousarray(w, np.float64)
+    rc = lib().svpf_oracle_grad_run(C.byref(cfg), n, T, _dptr(th), float(gamma), _fptr(ys),
+                                    _dptr(wv) if wv is not None else None, seed, filter_id,
+                                    _dptr(ll), _dptr(g), _dptr(hf))
+    if rc != 0:
+        raise RuntimeError(f"grad oracle rc={rc}")
+    return ll, g, hf
+
+
+def run_loglik(cfg: OracleConfig, n: int, theta, ys, gamma: float = 0.0, seed: int = 0, filter_id: int = 0,
+               precision: int = 0):
+    """The main oracle (OracleFilter) run the same way as grad_run: Philox
+    initialisation and noise, nu taken from theta.  Returns loglik[T]."""
+    c = OracleConfig.from_buffer_copy(cfg)
+    c.nu = float(theta[3])
+    p = OracleParams(float(theta[1]), float(theta[2]), float(theta[0]), float(gamma))
+    f = OracleFilter(n, c, p, precision)
+    f.initialize(None, seed=seed, filter_id=filter_id)
+    out = []
+    yp = 0.0
+    for t, y in enumerate(np.asarray(ys, np.float32)):
+        o = f.step(float(y), yp, seed=seed, tick=t, filter_id=filter_id)
+        out.append(o.loglik)
+        yp = float(y)
+    return np.array(out)
 
 
 def philox(k0, k1, c0, c1, c2, c3):

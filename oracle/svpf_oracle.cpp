@@ -782,6 +782,303 @@ int tick_impl(const oracle_config* cfg, const oracle_params* p, oracle_ctl* ctl,
 
 }  // namespace
 
+/* ======================================================================== */
+/* Gradient oracle: d(sum_t w_t loglik_t) / d(mu, rho, sigma_z, nu) of a     */
+/* whole run (initialisation included) under common random numbers, by       */
+/* forward-mode automatic differentiation in FP64 (a value plus four          */
+/* tangents carried through every operation).  It restates the single-factor  */
+/* tick for the differentiable configuration (see svpf_oracle_grad_supported) */
+/* with the same formulas and reference citations as Tick::run above, but     */
+/* keeps every quantity in FP64 (no float rounding of the stored bandwidth).  */
+/* Decisions that are piecewise constant in theta (the Stein budget, adaptive */
+/* beta, clamps, the MIM jump selection) are taken on the primal values.      */
+/* ======================================================================== */
+namespace {
+
+struct Dual {
+    double v;
+    double d[4];
+    Dual() : v(0), d{0, 0, 0, 0} {}
+    Dual(double x) : v(x), d{0, 0, 0, 0} {}  // NOLINT: implicit from constants
+    static Dual var(double x, int k) { Dual r(x); r.d[k] = 1; return r; }
+};
+inline Dual mk(double v, const Dual& a, double da) {   /* f(a) with f'(a) = da */
+    Dual r(v);
+    for (int k = 0; k < 4; ++k) r.d[k] = da * a.d[k];
+    return r;
+}
+inline Dual operator+(const Dual& a, const Dual& b) { Dual r(a.v + b.v); for (int k = 0; k < 4; ++k) r.d[k] = a.d[k] + b.d[k]; return r; }
+inline Dual operator-(const Dual& a, const Dual& b) { Dual r(a.v - b.v); for (int k = 0; k < 4; ++k) r.d[k] = a.d[k] - b.d[k]; return r; }
+inline Dual operator-(const Dual& a) { Dual r(-a.v); for (int k = 0; k < 4; ++k) r.d[k] = -a.d[k]; return r; }
+inline Dual operator*(const Dual& a, const Dual& b) { Dual r(a.v * b.v); for (int k = 0; k < 4; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k]; return r; }
+inline Dual operator/(const Dual& a, const Dual& b) {
+    Dual r(a.v / b.v);
+    for (int k = 0; k < 4; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) / b.v;
+    return r;
+}
+inline Dual& operator+=(Dual& a, const Dual& b) { a = a + b; return a; }
+inline Dual& operator-=(Dual& a, const Dual& b) { a = a - b; return a; }
+inline Dual& operator*=(Dual& a, const Dual& b) { a = a * b; return a; }
+inline bool operator<(const Dual& a, const Dual& b) { return a.v < b.v; }
+inline bool operator>(const Dual& a, const Dual& b) { return a.v > b.v; }
+inline double val(const Dual& a) { return a.v; }
+inline double val(double a) { return a; }
+
+/* psi(x), x > 0: recurrence psi(x) = psi(x+1) - 1/x up to x >= 8, then the
+ * asymptotic series (Abramowitz & Stegun 6.3.18). */
+double digamma(double x) {
+    double acc = 0;
+    while (x < 8) { acc -= 1 / x; x += 1; }
+    double r = 1 / x, r2 = r * r;
+    return acc + std::log(x) - 0.5 * r -
+           r2 * (1.0 / 12 - r2 * (1.0 / 120 - r2 * (1.0 / 252 - r2 * (1.0 / 240 - r2 * (1.0 / 132)))));
+}
+
+inline Dual dexp(const Dual& a) { double e = std::exp(a.v); return mk(e, a, e); }
+inline Dual dlog(const Dual& a) { return mk(std::log(a.v), a, 1 / a.v); }
+inline Dual dlog1p(const Dual& a) { return mk(std::log1p(a.v), a, 1 / (1 + a.v)); }
+inline Dual dsqrt(const Dual& a) { double s = std::sqrt(a.v); return mk(s, a, 0.5 / s); }
+inline Dual dlgamma(const Dual& a) { return mk(std::lgamma(a.v), a, digamma(a.v)); }
+inline Dual dmin(const Dual& a, const Dual& b) { return b.v < a.v ? b : a; }
+inline Dual dmax(const Dual& a, const Dual& b) { return b.v > a.v ? b : a; }
+inline Dual dclamp(const Dual& x, double lo, double hi) { return dmin(dmax(x, Dual(lo)), Dual(hi)); }
+inline Dual dclamp_h(const Dual& x) { return dclamp(x, -15, 5); }
+inline Dual dsafe_exp(const Dual& x) { return dexp(dmin(x, Dual(20))); }
+
+/* One filter of the differentiable configuration.  State carried between
+ * ticks that depends on theta is Dual; the return EMAs depend on y only. */
+struct GradFilter {
+    const oracle_config& c;
+    int n;
+    double gamma;
+    Dual mu, rho, sz, nu;            /* theta */
+    std::vector<Dual> h, v, lw, g, curv;
+    Dual bw_sq, h_mean_prev, gm, gP; /* bandwidth EMA, previous mean, EKF mean/variance */
+    int guide_initialized = 0, timestep = 0;
+    double return_ema = 0, return_var = 0, ksd_prev = 1e10;
+    Dual bw;
+
+    GradFilter(const oracle_config& c_, int n_, const double* theta, double gamma_)
+        : c(c_), n(n_), gamma(gamma_) {
+        mu = Dual::var(theta[0], 0);
+        rho = Dual::var(theta[1], 1);
+        sz = Dual::var(theta[2], 2);
+        nu = Dual::var(theta[3], 3);
+        h.assign(n, Dual()); v.assign(n, Dual()); lw.assign(n, Dual()); g.assign(n, Dual()); curv.assign(n, Dual(1));
+        bw_sq = Dual(0);
+        h_mean_prev = Dual(-3.5);   /* svpf_optimized_graph.cu:492-494 */
+    }
+
+    /* svpf_initialize, svpf_optimized_graph.cu:349-451 (single-factor part) */
+    void initialize(Noise<double>& nz_init, const float* init_normals, PhiloxKey key) {
+        Dual var = sz * sz / (Dual(1) - rho * rho + Dual(1e-6));
+        Dual sd = dsqrt(var);
+        for (int i = 0; i < n; ++i) {
+            double z = init_normals ? (double)init_normals[i] : philox_normal<double>(key, (uint32_t)i, 0u, 0u, 2u);
+            h[i] = dclamp_h(mu + sd * Dual(z));
+            v[i] = Dual(0);
+        }
+        (void)nz_init;
+        guide_initialized = 0;
+        gm = mu;
+        gP = var;
+        ksd_prev = 1e10;
+        timestep = 0;
+    }
+
+    Dual stc() const {   /* svpf_optimized_graph.cu:951-953 */
+        return dlgamma((nu + Dual(1)) * Dual(0.5)) - dlgamma(nu * Dual(0.5)) - Dual(0.5) * dlog(Dual(kPi) * nu);
+    }
+
+    /* one tick; returns loglik_t.  Citations as in Tick::run. */
+    Dual tick(double y_t, double y_prev, Noise<double>& nz) {
+        const int t = timestep;
+        const double off = c.student_t_implied_offset;
+        const Dual st = stc();
+        /* predict (:125-276) and prior means (:384-392) from tick-start positions */
+        std::vector<Dual> mu_k(n);
+        for (int i = 0; i < n; ++i) {
+            const Dual hi = h[i];
+            const double z = nz.normal(i, 0);
+            const Dual lev = Dual(gamma * y_prev) / (dsafe_exp(hi * Dual(0.5)) + Dual(1e-8));
+            mu_k[i] = mu + rho * (hi - mu) + Dual(gamma * y_prev) / (dexp(hi * Dual(0.5)) + Dual(1e-8));
+            if (c.use_mim) {
+                const double sel = nz.uniform(i, 0);
+                const double scale = sel < (double)c.mim_jump_prob ? (double)c.mim_jump_scale : 1.0;
+                const Dual r = dclamp(rho, 0, 0.999);
+                h[i] = dclamp_h(mu + r * (hi - mu) + lev + sz * Dual(scale * z));
+            } else {
+                h[i] = dclamp_h(mu + rho * (hi - mu) + sz * Dual(z) + lev);
+            }
+        }
+        /* EKF guide (svpf_kernels.cuh:509-541) and the preserving shift (:1006-1039) */
+        if (c.use_guide) {
+            if (!guide_initialized) {
+                gm = mu;
+                gP = sz * sz / (Dual(1) - rho * rho);
+                guide_initialized = 1;
+            }
+            const Dual m_pred = mu + rho * (gm - mu);
+            const Dual P_pred = rho * rho * gP + sz * sz;
+            const double log_y2 = std::log(y_t * y_t + 1e-8);
+            const Dual K = P_pred / (P_pred + Dual(4.93 + 2.0) + Dual(1e-8));
+            gm = m_pred + K * (Dual(log_y2) - (m_pred - Dual(off)));
+            gP = (Dual(1) - K) * P_pred;
+            const double gs = c.guide_strength_base;
+            if (c.use_guide_preserving) {
+                const Dual cm = h_mean_prev;
+                const Dual nm = Dual(1 - gs) * cm + Dual(gs) * gm;
+                for (int i = 0; i < n; ++i) h[i] = dclamp_h(nm + (h[i] - cm));
+            } else {
+                for (int i = 0; i < n; ++i) h[i] = dclamp_h(h[i] + Dual(gs) * (gm - h[i]));
+            }
+        }
+        /* bandwidth (:1159-1235) */
+        {
+            Dual sum(0), sum2(0), mn(1e10), mx(-1e10);
+            for (int i = 0; i < n; ++i) {
+                sum += h[i]; sum2 += h[i] * h[i];
+                mn = dmin(mn, h[i]); mx = dmax(mx, h[i]);
+            }
+            const Dual mean = sum / Dual(n);
+            const Dual var = sum2 / Dual(n) - mean * mean;
+            const Dual bw2_new = dmax(Dual(2) * var / Dual(std::log((double)n + 1)), Dual(1e-6));
+            Dual bw2 = bw_sq.v > 0 ? Dual(0.3) * bw2_new + Dual(0.7) * bw_sq : bw2_new;
+            const double a = std::fabs(y_t);
+            return_ema = return_ema > 0 ? 0.05 * a + 0.95 * return_ema : a;
+            return_var = return_var > 0 ? 0.05 * a * a + 0.95 * return_var : a * a;
+            const double ratio = a / std::max(return_ema, 1e-8);
+            const Dual spread_f = dmin((mx - mn) * Dual(0.5), Dual(2));
+            const Dual comb = dmax(Dual(ratio), spread_f);
+            const Dual scale = dclamp(Dual(1) - Dual(0.25) * dmin(comb - Dual(1), Dual(2)), 0.5, 1);
+            bw2 = bw2 * scale;
+            bw_sq = bw2;
+            bw = dclamp(dsqrt(bw2), 0.01, 2);
+        }
+        /* budget and beta schedule (:1057-1138) */
+        const int na = c.use_annealing ? std::max(c.n_anneal_steps, 1) : 1;
+        const double eps_step = 0.1 * (c.use_guide ? 0.5 : 1.0);
+        int budget;
+        if (t < 10) budget = c.stein_max_steps;
+        else {
+            float kn01 = ((float)ksd_prev - 0.05f) / (0.50f - 0.05f);
+            kn01 = std::min(std::max(kn01, 0.0f), 1.0f);
+            budget = c.stein_min_steps + (int)(kn01 * (float)(c.stein_max_steps - c.stein_min_steps));
+        }
+        if (budget < 0) budget = 0;
+        const bool full = c.use_newton && c.use_full_newton;
+        const double temp = c.use_svld ? c.temperature : 0.0;
+        int kn = 1;
+        double ksd_last = 0;
+        for (int ai = 0; ai < na; ++ai) {
+            double beta;
+            if (!c.use_annealing) beta = 1;
+            else if (c.use_adaptive_beta) beta = Tick<double>::adaptive_beta(ksd_prev, ai, na);
+            else { static const double sch[3] = {0.3, 0.65, 1.0}; beta = sch[ai % 3]; }
+            const double bf = std::sqrt(beta);
+            int si = budget / na;
+            if (ai == na - 1) si = budget - si * (na - 1);
+            for (int s = 0; s < si; ++s) {
+                const bool last = (ai == na - 1) && (s == si - 1);
+                gradient(beta, mu_k, st, y_t);
+                ksd_last = transport(eps_step * bf, temp, last, nz, kn, full, ksd_last);
+                if (temp > 1e-6) ++kn;
+            }
+        }
+        /* outputs (:1109-1153) */
+        Dual mxl(-1e10);
+        for (int i = 0; i < n; ++i) mxl = dmax(mxl, lw[i]);
+        Dual se(0), sh(0);
+        for (int i = 0; i < n; ++i) { se += dexp(lw[i] - mxl); sh += h[i]; }
+        const Dual ll = mxl + dlog(dmax(se / Dual(n), Dual(1e-10)));
+        h_mean_prev = sh / Dual(n);
+        ksd_prev = ksd_last;
+        timestep = t + 1;
+        return ll;
+    }
+
+    /* gradient pass, Gaussian mixture prior + Student-t likelihood (:354-521) */
+    void gradient(double beta, const std::vector<Dual>& mu_k, const Dual& st, double y_t) {
+        const Dual s2 = sz * sz;
+        const Dual inv2 = Dual(0.5) / s2, inv = Dual(1) / s2;
+        const double y2 = y_t * y_t;
+        for (int j = 0; j < n; ++j) {
+            const Dual hj = h[j];
+            Dual lmax(-1e10);
+            for (int k = 0; k < n; ++k) {
+                const Dual d = hj - mu_k[k];
+                lmax = dmax(lmax, -d * d * inv2);
+            }
+            Dual sr(0), wg(0);
+            for (int k = 0; k < n; ++k) {
+                const Dual d = hj - mu_k[k];
+                const Dual r = dexp(-d * d * inv2 - lmax);
+                sr += r;
+                wg -= r * d * inv;
+            }
+            const Dual gp = wg / (sr + Dual(1e-8));
+            const Dual A = Dual(y2) / (dsafe_exp(hj) + Dual(1e-8)) / nu;
+            const Dual opA = Dual(1) + A;
+            lw[j] = st - Dual(0.5) * hj - (nu + Dual(1)) * Dual(0.5) * dlog1p(dmax(A, Dual(-0.999)));
+            Dual glik;
+            if (c.use_exact_gradient) glik = Dual(-0.5) + Dual(0.5) * (nu + Dual(1)) * A / opA - Dual(c.lik_offset);
+            else glik = (Dual(std::log(y2 + 1e-10)) - hj + Dual(c.lik_offset)) / Dual(1.4);
+            g[j] = dclamp(gp + Dual(beta) * glik, -10, 10);
+            if (c.use_newton) {
+                const Dual hl = Dual(-0.5) * (nu + Dual(1)) * A / (opA * opA);
+                curv[j] = dclamp(-(hl - inv), 0.1, 100);
+            }
+        }
+    }
+
+    /* vanilla or full-Newton transport with RMSProp, SVLD and clamp (Jacobi) */
+    double transport(double es, double temp, bool want_ksd, Noise<double>& nz, int kn, bool full, double ksd_keep) {
+        const Dual inv_bw2 = Dual(1) / (bw * bw);
+        const double sign = c.stein_repulsive_sign == 1 ? 1.0 : -1.0;
+        std::vector<Dual> hn(n);
+        double ksd_sum = 0;
+        for (int i = 0; i < n; ++i) {
+            Dual ks(0), gk(0), hw(0), knn(0);
+            for (int j = 0; j < n; ++j) {
+                const Dual d = h[i] - h[j];
+                const Dual dist2 = d * d * inv_bw2;
+                const Dual K = Dual(1) / (Dual(1) + dist2);
+                const Dual K2 = K * K;
+                ks += K * g[j];
+                gk += Dual(sign * 2) * d * inv_bw2 * K2;
+                if (full) {
+                    const Dual w = Dual(3) * dist2 - Dual(1);
+                    hw += curv[j] * K + Dual(2) * inv_bw2 * K2 * (w.v < 0 ? -w : w);
+                    knn += K;
+                }
+                if (want_ksd) {
+                    const double dd = d.v, ib = inv_bw2.v, dd2 = dist2.v, k1 = K.v, k2 = K2.v;
+                    const double gxk = -2 * dd * ib * k2;
+                    const double hxy = 2 * ib * k2 * (4 * dd2 * k1 - 1);
+                    ksd_sum += k1 * g[i].v * g[j].v + g[i].v * (-gxk) + g[j].v * gxk + hxy;
+                }
+            }
+            Dual phi = (ks + gk) / Dual(n);
+            if (full) {
+                const Dual H = dclamp(hw / dmax(knn, Dual(1e-6)), 0.1, 100);
+                phi = phi / H * Dual(0.7);
+            }
+            const double rr = c.rmsprop_rho;
+            const Dual vn = Dual(rr) * v[i] + Dual(1 - rr) * phi * phi;
+            v[i] = vn;
+            const Dual drift = Dual(es) * phi / dsqrt(vn + Dual((double)c.rmsprop_eps));
+            double diff = 0;
+            if (temp > 1e-6) diff = std::sqrt(2 * es * temp) * nz.normal(i, kn);
+            hn[i] = dclamp_h(h[i] + drift + Dual(diff));
+        }
+        h.swap(hn);
+        if (!want_ksd) return ksd_keep;
+        return std::sqrt(std::max(ksd_sum / ((double)n * (double)n), 0.0));
+    }
+};
+
+}  // namespace
+
 extern "C" {
 
 void svpf_oracle_philox(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1,
@@ -930,6 +1227,64 @@ int svpf_oracle_batch_tick_f32(int nf, const oracle_config* cfgs, const oracle_p
         }
     }
     return bad ? -3 : 0;
+}
+
+}  // extern "C"
+
+/* ---- gradient oracle entry points ---------------------------------------- */
+extern "C" {
+
+/* 1 if the configuration is inside the differentiable set: single factor,
+ * plain or MIM predict with the model's rho, preserving or blending EKF guide
+ * with a fixed strength, Gaussian mixture prior, vanilla or full-Newton
+ * transport, fixed beta schedule, no rejuvenation, no adaptive mu / sigma /
+ * guide.  The Stein budget may follow the KSD: it is piecewise constant. */
+int svpf_oracle_grad_supported(const oracle_config* c) {
+    if (c->use_two_factor || c->use_heun || c->use_student_t_state || c->use_fan_mode) return 0;
+    if (c->use_adaptive_mu || c->use_adaptive_sigma || c->use_adaptive_guide) return 0;
+    if (c->use_asymmetric_rho || c->use_local_params || c->use_guided || c->use_rejuvenation) return 0;
+    if (c->use_newton && !c->use_full_newton) return 0;
+    /* adaptive beta is a continuous function of the previous tick's KSD, which
+     * the adjoint does not differentiate */
+    if (c->use_annealing && c->use_adaptive_beta) return 0;
+    return 1;
+}
+
+/* A whole run of one filter: initialisation from theta = (mu, rho, sigma_z,
+ * nu) with the project's Philox draws keyed by (seed, filter_id), then T ticks
+ * of ys (y_prev = 0 before the first).  Writes loglik[T] and
+ * grad[4] = d(sum_t w_t loglik_t)/d theta (w = NULL: all ones); h_final[n]
+ * optional.  Returns 0, or -2 for a configuration outside the
+ * differentiable set. */
+int svpf_oracle_grad_run(const oracle_config* cfg_in, int n, int T, const double* theta, double gamma,
+                         const float* ys, const double* w, uint64_t seed, int filter_id,
+                         double* loglik, double* grad, double* h_final) {
+    if (!svpf_oracle_grad_supported(cfg_in)) return -2;
+    if (n < 1 || T < 0) return -1;
+    oracle_config cfg = *cfg_in;
+    cfg.nu = (float)theta[3];
+    GradFilter f(cfg, n, theta, gamma);
+    oracle_noise nzs;
+    std::memset(&nzs, 0, sizeof(nzs));
+    nzs.mode = 1;
+    nzs.seed = seed;
+    nzs.filter_id = filter_id;
+    Noise<double> nz0(&nzs, n);
+    f.initialize(nz0, nullptr, make_key(seed, filter_id));
+    for (int k = 0; k < 4; ++k) grad[k] = 0;
+    double y_prev = 0;
+    for (int t = 0; t < T; ++t) {
+        nzs.tick = (uint64_t)t;
+        Noise<double> nz(&nzs, n);
+        const Dual ll = f.tick((double)ys[t], y_prev, nz);
+        y_prev = (double)ys[t];
+        if (loglik) loglik[t] = ll.v;
+        const double wt = w ? w[t] : 1.0;
+        for (int k = 0; k < 4; ++k) grad[k] += wt * ll.d[k];
+    }
+    if (h_final)
+        for (int i = 0; i < n; ++i) h_final[i] = f.h[i].v;
+    return 0;
 }
 
 }  // extern "C"

@@ -203,6 +203,13 @@ void svpf_oracle_config_defaults(oracle_config* cfg, int n_stein_steps, float nu
 void svpf_oracle_philox(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1,
                         uint32_t c2, uint32_t c3, uint32_t* out);
 
+
+/* ---- gradient oracle (forward-mode AD in FP64) ---------------------------- */
+int svpf_oracle_grad_supported(const oracle_config* cfg);
+int svpf_oracle_grad_run(const oracle_config* cfg, int n, int T, const double* theta, double gamma,
+                         const float* ys, const double* w, uint64_t seed, int filter_id,
+                         double* loglik, double* grad, double* h_final);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,185 @@
+"""The CUDA adjoint (svpf_grad_* through the C ABI) against the FP64
+forward-mode gradient oracle on the same Philox noise, checkpoint
+invariance, tick weights, central finite differences of the FP64 oracle at
+the step the benchmark quotes (1e-4), and the torch.autograd.Function.
+
+Tolerances: per-tick log-likelihoods 1e-5 relative; gradients 2e-4 relative
+(floor 1e-3) against the FP64 oracle, or four times the oracle's own
+sensitivity where that is larger: the FP64 gradient's relative change when
+theta moves by 1e-7 relative (FP32-sized input noise).  Most configurations
+have a sensitivity ~1e-5 and the measured agreement is ~1e-5; without SVLD
+noise and annealing the run is ill-conditioned (sensitivity 2e-3 .. 1e-2)."""
+import numpy as np
+import pytest
+
+import tape
+
+pytestmark = pytest.mark.gpu
+
+LL_TOL = 1e-5
+G_TOL = 2e-4
+
+
+def oracle_cfg(oracle_mod, cfg):
+    return oracle_mod.config_from_dict(cfg.to_dict())
+
+
+def thetas_for(F, seed=0):
+    rng = np.random.default_rng(seed)
+    return np.stack([rng.uniform(-2.0, 0.0, F), rng.uniform(0.90, 0.99, F), rng.uniform(0.08, 0.3, F),
+                     rng.uniform(5.0, 25.0, F)], axis=1).astype(np.float32)
+
+
+def paths_for(thetas, T, seed0=10):
+    return np.stack([tape.sv_path(T, float(th[0]), float(th[1]), float(th[2]), seed=seed0 + f)[1]
+                     for f, th in enumerate(thetas)])
+
+
+def check_against_oracle(pkg, oracle_mod, cfg, ns, T, k=64, seed=7, w=None, gamma=None):
+    F = len(ns)
+    th = thetas_for(F)
+    ys = paths_for(th, T)
+    g = pkg.Grad(ns, cfg, T_max=T, checkpoint_every=k)
+    ll, ls = g.forward(th, ys, gamma=gamma, seed=seed)
+    grad = g.backward(w)
+    g.close()
+    for f in range(F):
+        run = lambda t: oracle_mod.grad_run(oracle_cfg(oracle_mod, cfg), ns[f], t, ys[f],  # noqa: E731
+                                            gamma=0.0 if gamma is None else float(gamma[f]),
+                                            w=None if w is None else w[f].astype(np.float64), seed=seed,
+                                            filter_id=f)
+        base = th[f].astype(np.float64)
+        oll, og, _ = run(base)
+        assert np.max(np.abs(ll[f] - oll) / np.maximum(1, np.abs(oll))) < LL_TOL, f
+        assert abs(ls[f] - oll.sum()) < LL_TOL * max(1, abs(oll.sum())) * T
+        sens = 0.0
+        for trial in range(3):
+            pert = base * (1 + 1e-7 * np.random.default_rng(trial).standard_normal(4))
+            sens = max(sens, np.max(np.abs(run(pert)[1] - og) / np.maximum(np.abs(og), 1e-3)))
+        err = np.abs(grad[f] - og) / np.maximum(np.abs(og), 1e-3)
+        assert np.all(err < max(G_TOL, 4 * sens)), (f, ns[f], grad[f], og, err, sens)
+    return grad
+
+
+CFGS = {
+    "full_newton": dict(),
+    "vanilla": dict(full_newton=False),
+    "plain_predict_no_guide": dict(full_newton=False, use_mim=0, use_guide=0),
+    "blend_guide_approx_grad": dict(use_guide_preserving=0, use_exact_gradient=0),
+    "no_svld_no_annealing": dict(use_svld=0, use_annealing=0),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CFGS))
+def test_adjoint_matches_oracle_configs(pkg, oracle_mod, name):
+    kw = dict(CFGS[name])
+    full = kw.pop("full_newton", True)
+    cfg = pkg.grad_config(6, 12.0, full_newton=full, **kw)
+    check_against_oracle(pkg, oracle_mod, cfg, [64, 128, 200], T=12)
+
+
+@pytest.mark.parametrize("ns", [[1, 2, 31], [257, 33], [512], [1000]])
+def test_adjoint_matches_oracle_sizes(pkg, oracle_mod, ns):
+    cfg = pkg.grad_config(4, 12.0)
+    check_against_oracle(pkg, oracle_mod, cfg, ns, T=6)
+
+
+def test_leverage_and_weights(pkg, oracle_mod):
+    cfg = pkg.grad_config(4, 9.0)
+    rng = np.random.default_rng(3)
+    w = rng.standard_normal((2, 10)).astype(np.float32)
+    check_against_oracle(pkg, oracle_mod, cfg, [96, 160], T=10, w=w, gamma=np.array([-0.3, 0.2], np.float32))
+
+
+def test_checkpoint_interval_does_not_change_the_gradient(pkg):
+    """Recomputation from checkpoints is exact: every interval gives the
+    same bits."""
+    cfg = pkg.grad_config(4, 12.0)
+    ns = [128, 64, 300]
+    th = thetas_for(3, 1)
+    ys = paths_for(th, 40)
+    out = []
+    for k in (1, 3, 16, 64):
+        g = pkg.Grad(ns, cfg, T_max=40, checkpoint_every=k)
+        ll, _ = g.forward(th, ys, seed=11)
+        out.append((ll, g.backward()))
+        g.close()
+    for ll, gr in out[1:]:
+        assert np.array_equal(ll, out[0][0])
+        assert np.array_equal(gr, out[0][1])
+
+
+def test_weights_select_ticks(pkg):
+    """A one-hot weight on tick t gives the gradient of loglik_t alone, and
+    weights combine linearly."""
+    cfg = pkg.grad_config(4, 12.0)
+    ns = [128, 128]
+    th = thetas_for(2, 2)
+    T = 16
+    ys = paths_for(th, T)
+    g = pkg.Grad(ns, cfg, T_max=T, checkpoint_every=5)
+    g.forward(th, ys, seed=3)
+    full = g.backward()
+    parts = np.zeros_like(full)
+    for t0 in range(0, T, 4):
+        w = np.zeros((2, T), np.float32)
+        w[:, t0:t0 + 4] = 1.0
+        parts += g.backward(w)
+    g.close()
+    assert np.allclose(parts, full, rtol=1e-5, atol=1e-5)
+
+
+def test_adjoint_matches_fp64_central_differences(pkg, oracle_mod):
+    """Central finite differences of the FP64 oracle at step 1e-4 (vanilla
+    transport; 64 particles, 10 ticks) against the CUDA adjoint: 1e-3."""
+    cfg = pkg.grad_config(4, 12.0, full_newton=False)
+    th = thetas_for(1, 4)
+    ys = paths_for(th, 10)
+    g = pkg.Grad([64], cfg, T_max=10)
+    g.forward(th, ys, seed=5)
+    grad = g.backward()[0]
+    g.close()
+    oc = oracle_cfg(oracle_mod, cfg)
+    base = th[0].astype(np.float64)
+    for k in range(4):
+        h = 1e-4
+        tp, tm = base.copy(), base.copy()
+        tp[k] += h
+        tm[k] -= h
+        fd = (oracle_mod.grad_run(oc, 64, tp, ys[0], seed=5)[0].sum() -
+              oracle_mod.grad_run(oc, 64, tm, ys[0], seed=5)[0].sum()) / (2 * h)
+        assert abs(fd - grad[k]) <= 1e-3 * max(abs(grad[k]), 1e-2), (k, fd, grad[k])
+
+
+def test_unsupported_configuration_is_rejected(pkg):
+    cfg = pkg.grad_config(4, 12.0)
+    assert pkg.Grad.supported(cfg)
+    bad = pkg.default_config(4, 12.0)   # asymmetric rho and rejuvenation are on by default
+    assert not pkg.Grad.supported(bad)
+    with pytest.raises(RuntimeError):
+        pkg.Grad([64], bad, T_max=4)
+
+
+def test_torch_autograd_function(pkg):
+    torch = pytest.importorskip("torch")
+    from importlib import import_module
+    ag = import_module(pkg.__name__ + ".autograd")
+    cfg = pkg.grad_config(4, 12.0)
+    ns = [96, 128, 64]
+    th = thetas_for(3, 5)
+    T = 12
+    ys = paths_for(th, T)
+    eng = ag.GradEngine(ns, cfg, T_max=T, checkpoint_every=4)
+    theta = torch.tensor(th, device="cuda", requires_grad=True)
+    y = torch.tensor(ys, device="cuda")
+    ll = ag.svpf_loglik(theta, y, eng, seed=9)
+    w = torch.linspace(0.5, 1.5, T, device="cuda")
+    loss = (ll * w).sum()
+    loss.backward()
+    ref = pkg.Grad(ns, cfg, T_max=T, checkpoint_every=4)
+    ll2, _ = ref.forward(th, ys, seed=9)
+    g2 = ref.backward(np.broadcast_to(w.cpu().numpy(), (3, T)).copy())
+    ref.close()
+    assert np.array_equal(ll.detach().cpu().numpy(), ll2)
+    assert np.allclose(theta.grad.cpu().numpy(), g2, rtol=1e-6, atol=1e-6)
+    eng.close()
