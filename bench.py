@@ -200,6 +200,76 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+def gradient_workload(pkg, torch, F: int = 256, N: int = 512, T: int = 1000, k: int = 64):
+    """Differentiation workload: d(sum_t log p(y_t | y_1:t-1))/d(mu, rho,
+    sigma_z, nu) for F filters with N particles over T ticks (checkpoint every
+    k), paths generated at each filter's own theta with Student-t observation
+    noise.  Times the forward and the adjoint with CUDA events, and checks the
+    adjoint of four filters (T=200) against central differences of the FP32
+    forward at step 1e-4 relative (max(1, |theta|) * 1e-4; the run's
+    log-likelihood summed in FP64)."""
+    rng = np.random.default_rng(12)
+    th = np.stack([rng.uniform(-2.0, 0.0, F), rng.uniform(0.90, 0.995, F), rng.uniform(0.05, 0.4, F),
+                   rng.uniform(4.0, 30.0, F)], 1).astype(np.float32)
+    ys = sv_paths(T, th[:, 1].astype(np.float64), th[:, 2].astype(np.float64), th[:, 0].astype(np.float64),
+                  th[:, 3].astype(np.float64), seed=77).T.copy()
+    cfg = pkg.grad_config(MAX_STEPS, 12.0)
+    stream = torch.cuda.Stream()
+    g = pkg.Grad([N] * F, cfg, T_max=T, checkpoint_every=k, stream=stream.cuda_stream)
+    g.set_objective(g.PREDICTIVE)
+    d_th = torch.from_numpy(th).cuda()
+    d_y = torch.from_numpy(ys).cuda()
+    d_ll = torch.empty((F, T), dtype=torch.float32, device="cuda")
+    d_g = torch.empty((F, 4), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    g.forward_device(d_th.data_ptr(), None, d_y.data_ptr(), min(T, 64), 1, d_ll.data_ptr())   # warm-up
+    g.backward_device(None, d_g.data_ptr())
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(stream)
+    g.forward_device(d_th.data_ptr(), None, d_y.data_ptr(), T, 1, d_ll.data_ptr())
+    ev[1].record(stream)
+    g.backward_device(None, d_g.data_ptr())
+    ev[2].record(stream)
+    ev[2].synchronize()
+    fwd_ms, bwd_ms = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    grad = d_g.cpu().numpy()
+    g.close()
+    # central differences on a subset, step 1e-4 (float-rounded: the exact step used)
+    Fs, Ts = 4, 200
+    gs = pkg.Grad([N] * Fs, cfg, T_max=Ts, checkpoint_every=k)
+    gs.set_objective(gs.PREDICTIVE)
+    base = th[:Fs].copy()
+    gs.forward(base, ys[:Fs, :Ts], seed=1)
+    ad = gs.backward()
+    rel = np.zeros((Fs, 4))
+    for q in range(4):
+        tp, tm = base.copy(), base.copy()
+        h = 1e-4 * np.maximum(1.0, np.abs(base[:, q]))
+        tp[:, q] += h
+        tm[:, q] -= h
+        step = tp[:, q].astype(np.float64) - tm[:, q].astype(np.float64)
+        lp = gs.forward(tp, ys[:Fs, :Ts], seed=1)[1]
+        lm = gs.forward(tm, ys[:Fs, :Ts], seed=1)[1]
+        fd = (lp - lm) / step
+        rel[:, q] = np.abs(fd - ad[:, q]) / np.maximum(np.abs(ad[:, q]), 1e-2)
+    gs.close()
+    names = ("mu", "rho", "sigma_z", "nu")
+    return {
+        "workload": f"d sum_t log p(y_t|y_1:t-1) / d(mu, rho, sigma_z, nu): {F} filters, N={N}, T={T}, "
+                    f"checkpoint every {k} "
+                    "ticks, full Newton <= 8 Stein iterations, own theta per filter, Student-t paths",
+        "filter_ticks_per_s": F * T / ((fwd_ms + bwd_ms) / 1e3),
+        "forward_ms": fwd_ms, "backward_ms": bwd_ms, "backward_over_forward": bwd_ms / fwd_ms,
+        "grad_filter0": grad[0].tolist(),
+        "fd_check": {"step": "1e-4 * max(1, |theta|)", "filters": Fs, "ticks": Ts,
+                     "median_rel_err": {n: float(np.median(rel[:, q])) for q, n in enumerate(names)},
+                     "max_rel_err": {n: float(np.max(rel[:, q])) for q, n in enumerate(names)},
+                     "note": "FD of the FP32 forward; clamp kinks (score +-10, Newton curvature/Hessian, "
+                             "bandwidth) inside the step bias FD"},
+    }
+
+
 def workload_config(F: int):
     return {"workload": f"batched SVPF tick: {F} filters per GPU, own theta, N ~ U{{256,512,1024,2048,4096}}, "
                         f"production config (full Newton, <= {MAX_STEPS} Stein iterations, 3 stages)",
@@ -216,6 +286,7 @@ def main():
     ap.add_argument("--filters", type=int, default=4096)
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--latency-ticks", type=int, default=400)
+    ap.add_argument("--no-gradient", action="store_true", help="skip the differentiation workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -378,6 +449,10 @@ def main():
     peak = sms * sm_mhz * 1e6 * PAIRS_PER_CLK / 1e9
     traffic = read_ncu_traffic()
 
+    grad_line = {}
+    if rank == 0 and not args.no_gradient:
+        grad_line = gradient_workload(pkg, torch)
+
     cpu = {}
     if rank == 0:
         threads = cpu_threads()
@@ -404,6 +479,7 @@ def main():
                                  "pair at 16/clk/SM; 13 FP32 ops at 128/clk/SM)"},
             "single_filter_latency": lat,
             "plain_step_loop": plain,
+            "gradient": grad_line,
             "cpu_baseline": cpu,
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
             "status_errors": status_bad,

@@ -470,6 +470,14 @@ int svpf_grad_forward_device(svpf_grad_t* g, const float* d_theta, const float* 
                              const float* d_y, int T, unsigned long long seed, float* d_loglik);
 int svpf_grad_backward_device(svpf_grad_t* g, const float* d_w, double* d_grad);
 int svpf_grad_checkpoint_every(const svpf_grad_t* g);
+/* What the run's log-likelihood is made of (before the next forward):
+ * SVPF_GRAD_TICK_LOGLIK (default): each tick's loglik as svpf_step_graph
+ * reports it (log-mean-exp of the log-weights of the tick's last gradient
+ * pass, after the Stein moves); SVPF_GRAD_PREDICTIVE: log p(y_t | y_1:t-1)
+ * estimated at the predicted particles, before guide and Stein moves. */
+#define SVPF_GRAD_TICK_LOGLIK 0
+#define SVPF_GRAD_PREDICTIVE  1
+int svpf_grad_set_objective(svpf_grad_t* g, int objective);
 
 #ifdef __cplusplus
 }

@@ -92,6 +92,7 @@ struct GArgs {
     size_t rec_floats;
     int nseg;
     int* status;                   // [F]
+    int objective;                 // 0: the tick's log-likelihood, 1: predictive log p(y_t | y_1:t-1)
 };
 
 __host__ __device__ inline size_t rec_floats_for(int np, int bmax) {
@@ -174,6 +175,7 @@ struct TickScalars {
     int budget, na;
     float es[64], beta[64];
     float mxl, se;
+    float mxp, sep;                // predictive log-likelihood: max and sum of exp
     float ksd_last;
 };
 
@@ -198,7 +200,7 @@ __device__ inline int stage_of_it(int it, int budget, int na) {
 // (smem, updated in place); work: 6 np floats of smem scratch.  rec: per-tick
 // record for the backward, or nullptr.  Returns loglik on every thread.
 __device__ float fwd_tick(const svpf_config_t& c, int n, int np, float* x, float* v, float* work, Shared& sh,
-                          const Noise& nz, float y_t, float y_prev, float* rec, int bmax) {
+                          const Noise& nz, float y_t, float y_prev, float* rec, int bmax, int objective) {
     const int tid = threadIdx.x;
     TickScalars& ts = sh.ts;
     GState& st = sh.st;
@@ -272,10 +274,29 @@ __device__ float fwd_tick(const svpf_config_t& c, int n, int np, float* x, float
                 rec[MUK * np + i] = muk[i];
             }
             xn[i] = c.use_guide ? clamp_h(hgr) : hp;
+            if (objective == 1) {
+                // predictive: Student-t log density of y_t at the predicted particle
+                const float A = y_t * y_t / (expf(fminf(hp, 20.0f)) + 1e-8f) / ts.nu;
+                lw[i] = ts.stc - 0.5f * hp - (ts.nu + 1.0f) * 0.5f * log1pf(A);
+            }
         }
     }
     __syncthreads();
     for (int i = tid; i < n; i += kThreads) x[i] = xn[i];
+    float ll_pred = 0.0f;
+    if (objective == 1) {
+        float mp = -1e10f;
+        for (int i = tid; i < n; i += kThreads) mp = fmaxf(mp, lw[i]);
+        mp = reduce_max(mp, sh.red);
+        float sp[1] = {0.0f};
+        for (int i = tid; i < n; i += kThreads) sp[0] += expf(lw[i] - mp);
+        reduce_sum<1>(sp, sh.red);
+        ll_pred = mp + logf(fmaxf(sp[0] / (float)n, 1e-10f));
+        if (tid == 0) {
+            ts.mxp = mp;
+            ts.sep = sp[0];
+        }
+    }
     // ---- bandwidth (svpf_opt_kernels.cu:1159-1235)
     {
         float s[2] = {0.0f, 0.0f};
@@ -478,14 +499,15 @@ __device__ float fwd_tick(const svpf_config_t& c, int n, int np, float* x, float
         st.timestep += 1;
     }
     __syncthreads();
-    return ll;
+    return objective == 1 ? ll_pred : ll;
 }
 
 // Backward of one recorded tick.  xb, vb: adjoints of the tick's output
 // positions / moments on entry, of its input positions / moments on exit.
 // sa: adjoints of the scalar state (in: outputs of this tick; out: inputs).
 __device__ void bwd_tick(const svpf_config_t& c, int n, int np, float* xb, float* vb, float* work,
-                         Shared& sh, GAdj& sa, const Noise& nz, const float* rec, int bmax, float wt) {
+                         Shared& sh, GAdj& sa, const Noise& nz, const float* rec, int bmax, float wt,
+                         int objective) {
     const int tid = threadIdx.x;
     const TickScalars& ts = sh.ts;
     float* xs = work;                 // x^(it)
@@ -518,7 +540,7 @@ __device__ void bwd_tick(const svpf_config_t& c, int n, int np, float* xb, float
         lwb[i] = 0.0f;
     }
     // loglik = mxl + log(se/n): dL/dlw_i = w_t exp(lw_i - mxl) / se
-    if (budget > 0 && ts.se * inv_n > 1e-10f) {
+    if (objective == 0 && budget > 0 && ts.se * inv_n > 1e-10f) {
         const float* R = rec + (size_t)np * (kRecFixed + kRecPerIt * (budget - 1));
         for (int i = tid; i < n; i += kThreads) {
             const float xi = R[IX * np + i], A = R[IAL * np + i];
@@ -684,7 +706,9 @@ __device__ void bwd_tick(const svpf_config_t& c, int n, int np, float* xb, float
     // ---- stc(nu) enters every log-weight: dL/dnu += stc'(nu) * sum lwb
     // ---- bandwidth adjoint (needs the total dL/dbw)
     {
-        float s[2] = {pbw, 0.0f};
+        // predictive objective: its weights sum to one, so stc' enters once, times w_t
+        const bool pred_on = objective == 1 && ts.sep * inv_n > 1e-10f;
+        float s[2] = {pbw, (tid == 0 && pred_on) ? wt : 0.0f};
         for (int i = tid; i < n; i += kThreads) s[1] += lwb[i];
         reduce_sum<2>(s, sh.red);
         if (tid == 0) {
@@ -744,6 +768,18 @@ __device__ void bwd_tick(const svpf_config_t& c, int n, int np, float* xb, float
                 hpb = xb[i];
             }
             const float hpr = rec[HPR * np + i];
+            if (objective == 1 && ts.sep * inv_n > 1e-10f) {
+                // d/dhp and d/dnu of w_t log mean_i p(y_t | hp_i)
+                const float hp = clamp_h(hpr);
+                const float e = expf(fminf(hp, 20.0f));
+                const float A = ts.y_t * ts.y_t / (e + 1e-8f) / nu;
+                const float lp = ts.stc - 0.5f * hp - (nu + 1.0f) * 0.5f * log1pf(A);
+                const float pw = wt * expf(lp - ts.mxp) / ts.sep;
+                const float dlpdA = -(nu + 1.0f) * 0.5f / (1.0f + A);
+                const float dAdh = hp < 20.0f ? -A * e / (e + 1e-8f) : 0.0f;
+                hpb += pw * (-0.5f + dlpdA * dAdh);
+                pnu += pw * (-0.5f * log1pf(A) + dlpdA * (-A / nu));
+            }
             const float cp = (hpr >= SVPF_H_MIN && hpr <= SVPF_H_MAX) ? hpb : 0.0f;
             const float xi = rec[XS * np + i];
             const float z = nz.normal(i, 0);
@@ -928,7 +964,7 @@ __global__ void __launch_bounds__(kThreads) grad_forward_kernel(const GArgs a, i
             const float yp = t > 0 ? a.y[(size_t)f * a.T + t - 1] : 0.0f;
             const Noise nz = make_noise(a.seed, f, sh.st.timestep, n, &sh.flag);
             __syncthreads();
-            const float ll = fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, nullptr, a.bmax);
+            const float ll = fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, nullptr, a.bmax, a.objective);
             if (threadIdx.x == 0) {
                 if (a.loglik) a.loglik[(size_t)f * a.T + t] = ll;
                 a.ll_sum[f] += (double)ll;
@@ -993,7 +1029,7 @@ __global__ void __launch_bounds__(kThreads) grad_backward_kernel(const GArgs a, 
             const float yp = t > 0 ? a.y[(size_t)f * a.T + t - 1] : 0.0f;
             const Noise nz = make_noise(a.seed, f, sh.st.timestep, n, &sh.flag);
             __syncthreads();
-            fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, nullptr, a.bmax);
+            fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, nullptr, a.bmax, a.objective);
         }
         // reverse over the segment's ticks
         for (int t = t1 - 1; t >= t0; --t) {
@@ -1010,9 +1046,9 @@ __global__ void __launch_bounds__(kThreads) grad_backward_kernel(const GArgs a, 
             const float yp = t > 0 ? a.y[(size_t)f * a.T + t - 1] : 0.0f;
             __syncthreads();
             const Noise nz = make_noise(a.seed, f, sh.st.timestep, n, &sh.flag);
-            fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, rec, a.bmax);
+            fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, rec, a.bmax, a.objective);
             const float wt = a.w ? a.w[(size_t)f * a.T + t] : 1.0f;
-            bwd_tick(cfg, n, np, xb, vb, work, sh, sa, nz, rec, a.bmax, wt);
+            bwd_tick(cfg, n, np, xb, vb, work, sh, sa, nz, rec, a.bmax, wt, a.objective);
         }
         if (t0 == 0) init_adjoint(a, f, n, xb, sh, sa);
         for (int i = threadIdx.x; i < n; i += kThreads) {
@@ -1046,6 +1082,7 @@ struct svpf_grad {
     int T = 0;
     unsigned long long seed = 0;
     bool forward_done = false;
+    int objective = 0;
     // device
     int* d_n = nullptr;
     svpf_config_t* d_cfg = nullptr;
@@ -1111,6 +1148,7 @@ GArgs make_gargs(const svpf_grad* g, const float* theta, const float* gamma, con
     a.rec_floats = g->rec_floats;
     a.nseg = g->nseg;
     a.status = g->d_status;
+    a.objective = g->objective;
     return a;
 }
 
@@ -1124,6 +1162,7 @@ int svpf_grad_supported(const svpf_config_t* c) {
     if (c->use_adaptive_mu || c->use_adaptive_sigma || c->use_adaptive_guide) return 0;
     if (c->use_asymmetric_rho || c->use_local_params || c->use_guided || c->use_rejuvenation) return 0;
     if (c->use_newton && !c->use_full_newton) return 0;
+    if (c->stein_min_steps < 1 || c->stein_max_steps < 1) return 0;
     // adaptive beta is a continuous function of the previous tick's KSD, which
     // the adjoint does not differentiate
     if (c->use_annealing && c->use_adaptive_beta) return 0;
@@ -1288,5 +1327,12 @@ int svpf_grad_backward(svpf_grad_t* g, const float* w, double* grad) {
 }
 
 int svpf_grad_checkpoint_every(const svpf_grad_t* g) { return g ? g->k : 0; }
+
+int svpf_grad_set_objective(svpf_grad_t* g, int objective) {
+    if (!g || (objective != SVPF_GRAD_TICK_LOGLIK && objective != SVPF_GRAD_PREDICTIVE)) return SVPF_ERR_INVALID_ARG;
+    g->objective = objective;
+    g->forward_done = false;
+    return SVPF_OK;
+}
 
 }  // extern "C"

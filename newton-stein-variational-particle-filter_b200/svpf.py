@@ -151,6 +151,7 @@ def lib() -> C.CDLL:
         "svpf_grad_forward_device": (_I, [vp, vp, vp, vp, _I, C.c_ulonglong, vp]),
         "svpf_grad_backward_device": (_I, [vp, vp, vp]),
         "svpf_grad_checkpoint_every": (_I, [vp]),
+        "svpf_grad_set_objective": (_I, [vp, _I]),
         "svpf_debug_philox": (_I, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), _I]),
     }
     for name, (res, args) in sig.items():
@@ -584,6 +585,15 @@ class Grad:
     @staticmethod
     def supported(cfg: Config) -> bool:
         return bool(lib().svpf_grad_supported(C.byref(cfg)))
+
+    TICK_LOGLIK = 0
+    PREDICTIVE = 1
+
+    def set_objective(self, objective: int):
+        """0: each tick's loglik as the step reports it; 1: the predictive
+        log p(y_t | y_1:t-1) at the predicted particles."""
+        self._check(lib().svpf_grad_set_objective(self._g, int(objective)))
+        return self
 
     @property
     def checkpoint_every(self) -> int:

@@ -851,6 +851,7 @@ struct GradFilter {
     const oracle_config& c;
     int n;
     double gamma;
+    int predictive = 0;              /* 1: log mean_i p(y_t | predicted h_i) instead of the tick loglik */
     Dual mu, rho, sz, nu;            /* theta */
     std::vector<Dual> h, v, lw, g, curv;
     Dual bw_sq, h_mean_prev, gm, gP; /* bandwidth EMA, previous mean, EKF mean/variance */
@@ -910,6 +911,22 @@ struct GradFilter {
             } else {
                 h[i] = dclamp_h(mu + rho * (hi - mu) + sz * Dual(z) + lev);
             }
+        }
+        /* predictive log-likelihood log p(y_t | y_1:t-1): Student-t log density
+         * of y_t averaged over the predicted particles (before guide and Stein) */
+        Dual ll_pred(0);
+        if (predictive) {
+            const Dual st0 = stc();
+            std::vector<Dual> lp(n);
+            Dual mxp(-1e10);
+            for (int i = 0; i < n; ++i) {
+                const Dual A = Dual(y_t * y_t) / (dsafe_exp(h[i]) + Dual(1e-8)) / nu;
+                lp[i] = st0 - Dual(0.5) * h[i] - (nu + Dual(1)) * Dual(0.5) * dlog1p(A);
+                mxp = dmax(mxp, lp[i]);
+            }
+            Dual sp(0);
+            for (int i = 0; i < n; ++i) sp += dexp(lp[i] - mxp);
+            ll_pred = mxp + dlog(dmax(sp / Dual(n), Dual(1e-10)));
         }
         /* EKF guide (svpf_kernels.cuh:509-541) and the preserving shift (:1006-1039) */
         if (c.use_guide) {
@@ -994,7 +1011,7 @@ struct GradFilter {
         h_mean_prev = sh / Dual(n);
         ksd_prev = ksd_last;
         timestep = t + 1;
-        return ll;
+        return predictive ? ll_pred : ll;
     }
 
     /* gradient pass, Gaussian mixture prior + Student-t likelihood (:354-521) */
@@ -1244,6 +1261,7 @@ int svpf_oracle_grad_supported(const oracle_config* c) {
     if (c->use_adaptive_mu || c->use_adaptive_sigma || c->use_adaptive_guide) return 0;
     if (c->use_asymmetric_rho || c->use_local_params || c->use_guided || c->use_rejuvenation) return 0;
     if (c->use_newton && !c->use_full_newton) return 0;
+    if (c->stein_min_steps < 1 || c->stein_max_steps < 1) return 0;
     /* adaptive beta is a continuous function of the previous tick's KSD, which
      * the adjoint does not differentiate */
     if (c->use_annealing && c->use_adaptive_beta) return 0;
@@ -1256,14 +1274,28 @@ int svpf_oracle_grad_supported(const oracle_config* c) {
  * grad[4] = d(sum_t w_t loglik_t)/d theta (w = NULL: all ones); h_final[n]
  * optional.  Returns 0, or -2 for a configuration outside the
  * differentiable set. */
+int svpf_oracle_grad_run2(const oracle_config* cfg_in, int n, int T, const double* theta, double gamma,
+                          const float* ys, const double* w, uint64_t seed, int filter_id,
+                          double* loglik, double* grad, double* h_final, int objective);
+
 int svpf_oracle_grad_run(const oracle_config* cfg_in, int n, int T, const double* theta, double gamma,
                          const float* ys, const double* w, uint64_t seed, int filter_id,
                          double* loglik, double* grad, double* h_final) {
+    return svpf_oracle_grad_run2(cfg_in, n, T, theta, gamma, ys, w, seed, filter_id, loglik, grad, h_final, 0);
+}
+
+/* objective 0: the tick's log-likelihood (log-weights of its last gradient
+ * pass, the reference's output); 1: the predictive log-likelihood
+ * log p(y_t | y_1:t-1), averaged over the predicted particles. */
+int svpf_oracle_grad_run2(const oracle_config* cfg_in, int n, int T, const double* theta, double gamma,
+                          const float* ys, const double* w, uint64_t seed, int filter_id,
+                          double* loglik, double* grad, double* h_final, int objective) {
     if (!svpf_oracle_grad_supported(cfg_in)) return -2;
     if (n < 1 || T < 0) return -1;
     oracle_config cfg = *cfg_in;
     cfg.nu = (float)theta[3];
     GradFilter f(cfg, n, theta, gamma);
+    f.predictive = objective == 1;
     oracle_noise nzs;
     std::memset(&nzs, 0, sizeof(nzs));
     nzs.mode = 1;

@@ -209,6 +209,11 @@ int svpf_oracle_grad_supported(const oracle_config* cfg);
 int svpf_oracle_grad_run(const oracle_config* cfg, int n, int T, const double* theta, double gamma,
                          const float* ys, const double* w, uint64_t seed, int filter_id,
                          double* loglik, double* grad, double* h_final);
+/* objective 0: tick log-likelihood (as svpf_oracle_grad_run); 1: predictive
+ * log-likelihood log mean_i p(y_t | predicted h_i). */
+int svpf_oracle_grad_run2(const oracle_config* cfg, int n, int T, const double* theta, double gamma,
+                          const float* ys, const double* w, uint64_t seed, int filter_id,
+                          double* loglik, double* grad, double* h_final, int objective);
 
 #ifdef __cplusplus
 }

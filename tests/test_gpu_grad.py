@@ -35,11 +35,12 @@ def paths_for(thetas, T, seed0=10):
                      for f, th in enumerate(thetas)])
 
 
-def check_against_oracle(pkg, oracle_mod, cfg, ns, T, k=64, seed=7, w=None, gamma=None):
+def check_against_oracle(pkg, oracle_mod, cfg, ns, T, k=64, seed=7, w=None, gamma=None, objective=0):
     F = len(ns)
     th = thetas_for(F)
     ys = paths_for(th, T)
     g = pkg.Grad(ns, cfg, T_max=T, checkpoint_every=k)
+    g.set_objective(objective)
     ll, ls = g.forward(th, ys, gamma=gamma, seed=seed)
     grad = g.backward(w)
     g.close()
@@ -47,7 +48,7 @@ def check_against_oracle(pkg, oracle_mod, cfg, ns, T, k=64, seed=7, w=None, gamm
         run = lambda t: oracle_mod.grad_run(oracle_cfg(oracle_mod, cfg), ns[f], t, ys[f],  # noqa: E731
                                             gamma=0.0 if gamma is None else float(gamma[f]),
                                             w=None if w is None else w[f].astype(np.float64), seed=seed,
-                                            filter_id=f)
+                                            filter_id=f, objective=objective)
         base = th[f].astype(np.float64)
         oll, og, _ = run(base)
         assert np.max(np.abs(ll[f] - oll) / np.maximum(1, np.abs(oll))) < LL_TOL, f
@@ -82,6 +83,15 @@ def test_adjoint_matches_oracle_configs(pkg, oracle_mod, name):
 def test_adjoint_matches_oracle_sizes(pkg, oracle_mod, ns):
     cfg = pkg.grad_config(4, 12.0)
     check_against_oracle(pkg, oracle_mod, cfg, ns, T=6)
+
+
+@pytest.mark.parametrize("name", ["full_newton", "plain_predict_no_guide"])
+def test_predictive_objective_matches_oracle(pkg, oracle_mod, name):
+    """The predictive objective log p(y_t | y_1:t-1) at the predicted particles."""
+    kw = dict(CFGS[name])
+    full = kw.pop("full_newton", True)
+    cfg = pkg.grad_config(6, 12.0, full_newton=full, **kw)
+    check_against_oracle(pkg, oracle_mod, cfg, [64, 128, 200], T=12, objective=1)
 
 
 def test_leverage_and_weights(pkg, oracle_mod):

@@ -37,7 +37,7 @@ def test_unsupported_configurations_rejected(oracle_mod):
     assert oracle_mod.grad_supported(grad_cfg(oracle_mod))
     for bad in (dict(use_asymmetric_rho=1), dict(use_rejuvenation=1), dict(use_newton=1, use_full_newton=0),
                 dict(use_two_factor=1), dict(use_adaptive_mu=1), dict(use_student_t_state=1), dict(use_guided=1),
-                dict(use_adaptive_beta=1)):
+                dict(use_adaptive_beta=1), dict(stein_min_steps=0)):
         assert not oracle_mod.grad_supported(grad_cfg(oracle_mod, **bad)), bad
 
 
@@ -51,18 +51,19 @@ def test_primal_matches_main_oracle(oracle_mod, name):
     assert np.max(np.abs(ll - ref) / np.maximum(1, np.abs(ref))) < 1e-6
 
 
+@pytest.mark.parametrize("objective", [0, 1], ids=["tick_loglik", "predictive"])
 @pytest.mark.parametrize("name", sorted(CFGS))
-def test_gradient_matches_central_differences(oracle_mod, name):
+def test_gradient_matches_central_differences(oracle_mod, name, objective):
     cfg = grad_cfg(oracle_mod, **CFGS[name])
     _, ys = tape.sv_path(12, -1.0, 0.97, 0.15, seed=3)
-    _, g, _ = oracle_mod.grad_run(cfg, 64, THETA, ys, seed=7)
+    _, g, _ = oracle_mod.grad_run(cfg, 64, THETA, ys, seed=7, objective=objective)
     for k in range(4):
         h = 1e-7 * max(1.0, abs(THETA[k]))
         tp, tm = THETA.copy(), THETA.copy()
         tp[k] += h
         tm[k] -= h
-        fd = (oracle_mod.grad_run(cfg, 64, tp, ys, seed=7)[0].sum() -
-              oracle_mod.grad_run(cfg, 64, tm, ys, seed=7)[0].sum()) / (2 * h)
+        fd = (oracle_mod.grad_run(cfg, 64, tp, ys, seed=7, objective=objective)[0].sum() -
+              oracle_mod.grad_run(cfg, 64, tm, ys, seed=7, objective=objective)[0].sum()) / (2 * h)
         assert abs(fd - g[k]) <= 1e-5 * max(abs(g[k]), 1e-2), (name, k, fd, g[k])
 
 
