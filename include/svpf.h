@@ -52,6 +52,7 @@ extern "C" {
 #define SVPF_ERR_TAPE_SHORT        4   /* noise tape has fewer slots than the tick draws */
 #define SVPF_ERR_NONFINITE         5   /* NaN/Inf seen in an observation or the outputs */
 #define SVPF_ERR_UNSUPPORTED       6
+#define SVPF_ERR_BUDGET            7   /* request loop: the instrument's state does not fit the HBM budget */
 
 /* ---- model parameters (include/svpf.cuh:257-262) ------------------------- */
 typedef struct {
@@ -478,6 +479,47 @@ int svpf_grad_checkpoint_every(const svpf_grad_t* g);
 #define SVPF_GRAD_TICK_LOGLIK 0
 #define SVPF_GRAD_PREDICTIVE  1
 int svpf_grad_set_objective(svpf_grad_t* g, int objective);
+
+/* ---- request loop over instruments in a fixed HBM budget ------------------
+ * The reference serves each instrument with its own svpf_step_graph call
+ * (svpf_optimized_graph.cu:915-928 dispatching to :744-897 for two factors).
+ * Here a fleet of instruments -- single- or two-factor, each with its own N,
+ * configuration and parameters -- lives in one device pool allocated at
+ * creation: `hbm_budget_bytes` covers the pool and the per-instrument records.
+ * Admission places an instrument's particle state first-fit in the pool and
+ * refuses it with SVPF_ERR_BUDGET when it does not fit; eviction frees it.
+ * A call carries (instrument, y_t) requests; each instrument keeps its own
+ * y_prev on the device.  Requests are served in rounds (the k-th request of
+ * an instrument in round k, so its ticks keep their order), each round one
+ * persistent launch per model pulling work largest cost first.  Tick noise is
+ * keyed by (stream seed, slot, tick), initial draws by (admission seed, slot),
+ * so slot f matches filter f of a batch with the same seeds.  Heun is not
+ * supported here (SVPF_ERR_UNSUPPORTED). */
+typedef struct svpf_stream svpf_stream_t;
+
+svpf_stream_t* svpf_stream_create(int max_instruments, size_t hbm_budget_bytes, int n_max,
+                                  cudaStream_t stream);
+void svpf_stream_destroy(svpf_stream_t* s);
+void svpf_stream_set_seed(svpf_stream_t* s, unsigned long long seed);
+/* Returns the instrument's slot (>= 0) or -SVPF_ERR_* (-SVPF_ERR_BUDGET when
+ * its state does not fit).  The instrument starts as after svpf_initialize. */
+int svpf_stream_admit(svpf_stream_t* s, int n_particles, const svpf_config_t* cfg,
+                      const SVPFParams* params, unsigned long long seed);
+int svpf_stream_evict(svpf_stream_t* s, int slot);
+size_t svpf_stream_bytes_in_use(const svpf_stream_t* s);
+size_t svpf_stream_bytes_budget(const svpf_stream_t* s);
+/* Serve `count` requests (host arrays); out[r] (may be NULL) gets request r's
+ * outputs.  Blocking. */
+int svpf_stream_process(svpf_stream_t* s, int count, const int* slots, const float* y, svpf_out_t* out);
+/* One round from device arrays, stream ordered: d_slots[0, count1) are
+ * single-factor instruments, d_slots[count1, count1 + count2) two-factor
+ * ones, each instrument at most once; d_y and d_out are indexed alike. */
+int svpf_stream_process_device(svpf_stream_t* s, int count1, int count2, const int* d_slots,
+                               const float* d_y, svpf_out_t* d_out);
+int svpf_stream_get_ctl(const svpf_stream_t* s, int slot, svpf_ctl_t* ctl);
+/* n values, or 2n (fast then slow) for a two-factor instrument. */
+int svpf_stream_get_particles(const svpf_stream_t* s, int slot, float* h_out);
+long long svpf_stream_kernel_launches(const svpf_stream_t* s);
 
 #ifdef __cplusplus
 }

@@ -45,7 +45,9 @@ __global__ void __launch_bounds__(kThreads, 2) batch_tick_kernel(const __grid_co
         const FilterIO io{a.h + off, a.hp + off, a.v + off, a.lw + off, n};
         const Noise nz{philox_key(a.seed, f), (uint32_t)ctl.timestep, a.tape_n, a.tape_u,
                        a.slots_n, a.slots_u, a.tape_stride, &pl.flag};
-        const float yt = a.y_t[f], yp = a.y_prev[f];
+        // request mode: y_t from the request, y_prev from the filter's record
+        const float yt = a.req_y ? a.req_y[w] : a.y_t[f];
+        const float yp = a.req_y ? ctl.y_prev : a.y_prev[f];
         switch (a.tile[f]) {
             case 1: run_tick<1, 4>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
             case 2: run_tick<1, 2>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
@@ -53,9 +55,10 @@ __global__ void __launch_bounds__(kThreads, 2) batch_tick_kernel(const __grid_co
             case 4: run_tick<2, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
             default: run_tick<4, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
         }
+        if (a.req_y && threadIdx.x == 0) ctl.y_prev = yt;
         __syncthreads();
         copy_words(&a.ctl[f], &ctl);
-        if (a.out != nullptr) copy_words(&a.out[f], &out);
+        if (a.out != nullptr) copy_words(&a.out[a.req_y ? w : f], &out);
         __syncthreads();
     }
 }
@@ -86,7 +89,9 @@ __global__ void __launch_bounds__(kThreads, 2) batch_tick_2f_kernel(const __grid
         const FilterIO io{a.h + off, a.hp + off, a.v + off, a.lw + off, n};
         const Noise nz{philox_key(a.seed, f), (uint32_t)ctl.timestep, a.tape_n, a.tape_u,
                        a.slots_n, a.slots_u, a.tape_stride, &pl.flag};
-        const float yt = a.y_t[f], yp = a.y_prev[f];
+        // request mode: y_t from the request, y_prev from the filter's record
+        const float yt = a.req_y ? a.req_y[w] : a.y_t[f];
+        const float yp = a.req_y ? ctl.y_prev : a.y_prev[f];
         switch (a.tile[f]) {
             case 1: run_tick_2f<1, 4>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
             case 2: run_tick_2f<1, 2>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
@@ -94,9 +99,10 @@ __global__ void __launch_bounds__(kThreads, 2) batch_tick_2f_kernel(const __grid
             case 4: run_tick_2f<2, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
             default: run_tick_2f<4, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
         }
+        if (a.req_y && threadIdx.x == 0) ctl.y_prev = yt;
         __syncthreads();
         copy_words(&a.ctl[f], &ctl);
-        if (a.out != nullptr) copy_words(&a.out[f], &out);
+        if (a.out != nullptr) copy_words(&a.out[a.req_y ? w : f], &out);
         __syncthreads();
     }
 }

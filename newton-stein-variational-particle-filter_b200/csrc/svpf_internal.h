@@ -59,6 +59,10 @@ struct BatchArgs {
     const float* tape_u;
     int slots_n, slots_u, tape_stride;
     int heun;              // any filter of the batch uses Heun (shared-memory layout)
+    // request mode (request loop): work item w is filter order[w] with
+    // y_t = req_y[w], y_prev = that filter's ctl.y_prev (updated to y_t), and
+    // its outputs go to out[w].  nullptr: batch mode (y_t[f], y_prev[f], out[f]).
+    const float* req_y;
 };
 
 struct InitArgs {
@@ -82,6 +86,7 @@ struct InitArgs {
     const float* sdf;       // stationary sd of the fast / slow factor, per filter or sdf0/sds0
     const float* sds;
     float sdf0, sds0;
+    int key_base;           // filter index of block 0 in the Philox key (request loop: the slot)
     float* h2;              // single filter: separate [2n] arrays for the factors; batch:
     float* hp2;             // nullptr (the filter's own segment holds [fast; slow])
     float* v2;

@@ -22,7 +22,7 @@ __global__ void init_kernel(const InitArgs a) {
     const float mu = a.mu ? a.mu[f] : a.mu0;
     const float sd = a.sd ? a.sd[f] : a.sd0;
     const bool tf = a.tf ? a.tf[f] != 0 : a.tf0 != 0;
-    const uint2 key = philox_key(a.seed, f);
+    const uint2 key = philox_key(a.seed, f + a.key_base);
     auto draw = [&](int i, int slot) {
         if (a.tape0 != nullptr) return a.tape0[(size_t)slot * a.tape_stride + i];
         const uint4 r = philox10(key, make_uint4((uint32_t)i, (uint32_t)slot, 0u, 2u));

@@ -24,7 +24,8 @@ SMOOTH_MAX_LAG = 8
 
 SVPF_OK = 0
 ERRORS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "not initialized",
-          4: "noise tape too short", 5: "non-finite observation or output", 6: "unsupported"}
+          4: "noise tape too short", 5: "non-finite observation or output", 6: "unsupported",
+          7: "does not fit the HBM budget"}
 
 _I, _F = C.c_int, C.c_float
 CONFIG_FIELDS = [
@@ -152,6 +153,18 @@ def lib() -> C.CDLL:
         "svpf_grad_backward_device": (_I, [vp, vp, vp]),
         "svpf_grad_checkpoint_every": (_I, [vp]),
         "svpf_grad_set_objective": (_I, [vp, _I]),
+        "svpf_stream_create": (vp, [_I, C.c_size_t, _I, vp]),
+        "svpf_stream_destroy": (None, [vp]),
+        "svpf_stream_set_seed": (None, [vp, C.c_ulonglong]),
+        "svpf_stream_admit": (_I, [vp, _I, C.POINTER(Config), C.POINTER(Params), C.c_ulonglong]),
+        "svpf_stream_evict": (_I, [vp, _I]),
+        "svpf_stream_bytes_in_use": (C.c_size_t, [vp]),
+        "svpf_stream_bytes_budget": (C.c_size_t, [vp]),
+        "svpf_stream_process": (_I, [vp, _I, C.POINTER(_I), _FP, vp]),
+        "svpf_stream_process_device": (_I, [vp, _I, _I, vp, vp, vp]),
+        "svpf_stream_get_ctl": (_I, [vp, _I, C.POINTER(Ctl)]),
+        "svpf_stream_get_particles": (_I, [vp, _I, _FP]),
+        "svpf_stream_kernel_launches": (C.c_longlong, [vp]),
         "svpf_debug_philox": (_I, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), _I]),
     }
     for name, (res, args) in sig.items():
@@ -633,6 +646,87 @@ class Grad:
 
     def backward_device(self, d_w, d_grad: int):
         self._check(lib().svpf_grad_backward_device(self._g, d_w, d_grad))
+
+
+class Stream:
+    """Request loop over instruments held in a fixed HBM budget
+    (svpf_stream_* in the C ABI)."""
+
+    def __init__(self, max_instruments: int, hbm_budget_bytes: int, n_max: int, stream=None, seed: int = 0):
+        self._s = lib().svpf_stream_create(int(max_instruments), int(hbm_budget_bytes), int(n_max), stream)
+        if not self._s:
+            raise RuntimeError("svpf_stream_create failed (budget below the fixed records, sizes, or device)")
+        lib().svpf_stream_set_seed(self._s, int(seed))
+        self._cfg = {}
+        self._n = {}
+
+    def close(self):
+        if getattr(self, "_s", None):
+            lib().svpf_stream_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def admit(self, n: int, cfg: Config, params: Params, seed: int = 0) -> int:
+        """Slot of the admitted instrument, or -SVPF_ERR_* (-7: does not fit the budget)."""
+        slot = int(lib().svpf_stream_admit(self._s, int(n), C.byref(cfg), C.byref(params), int(seed)))
+        if slot >= 0:
+            self._cfg[slot] = Config.from_buffer_copy(cfg)
+            self._n[slot] = int(n)
+        return slot
+
+    def evict(self, slot: int):
+        rc = lib().svpf_stream_evict(self._s, int(slot))
+        if rc != SVPF_OK:
+            raise RuntimeError(f"evict failed rc={rc}")
+        self._cfg.pop(slot, None)
+        self._n.pop(slot, None)
+
+    @property
+    def bytes_in_use(self) -> int:
+        return int(lib().svpf_stream_bytes_in_use(self._s))
+
+    @property
+    def bytes_budget(self) -> int:
+        return int(lib().svpf_stream_bytes_budget(self._s))
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(lib().svpf_stream_kernel_launches(self._s))
+
+    def process(self, slots, y):
+        """Serve requests (slot, y) in order per instrument; returns Out[count]."""
+        sl = np.ascontiguousarray(slots, dtype=np.int32)
+        yy = _f32(y)
+        out = (Out * max(len(sl), 1))()
+        rc = lib().svpf_stream_process(self._s, len(sl), sl.ctypes.data_as(C.POINTER(_I)), _fp(yy), out)
+        if rc != SVPF_OK:
+            raise RuntimeError(f"svpf_stream_process rc={rc}: {ERRORS.get(rc, '?')}")
+        return out
+
+    def process_device(self, count1: int, count2: int, d_slots: int, d_y: int, d_out: int):
+        rc = lib().svpf_stream_process_device(self._s, int(count1), int(count2), d_slots, d_y, d_out)
+        if rc != SVPF_OK:
+            raise RuntimeError(f"svpf_stream_process_device rc={rc}")
+
+    def ctl(self, slot: int) -> Ctl:
+        c = Ctl()
+        rc = lib().svpf_stream_get_ctl(self._s, int(slot), C.byref(c))
+        if rc != SVPF_OK:
+            raise RuntimeError(f"get_ctl rc={rc}")
+        return c
+
+    def particles(self, slot: int) -> np.ndarray:
+        m = 2 if self._cfg[slot].use_two_factor else 1
+        out = np.empty(m * self._n[slot], np.float32)
+        rc = lib().svpf_stream_get_particles(self._s, int(slot), _fp(out))
+        if rc != SVPF_OK:
+            raise RuntimeError(f"get_particles rc={rc}")
+        return out
 
 
 def autotune(ns, ticks: int = 2):
