@@ -270,6 +270,115 @@ def gradient_workload(pkg, torch, F: int = 256, N: int = 512, T: int = 1000, k: 
     }
 
 
+def stream_workload(pkg, n_instruments: int = 10000, budget_bytes: int = 512 << 20, load: float = 0.8,
+                    sim_seconds: float = 1.0, seed: int = 5):
+    """Two-factor request loop: n_instruments two-factor filters (rho_f 0.80,
+    sigma_f 0.30, rho_s 0.995, sigma_s 0.05, Student-t nu 6; N ~ U{256, 512,
+    1024, 2048}; the reference two-factor test's filter knobs) admitted into a
+    fixed HBM budget.  Capacity is probed with one round over every
+    instrument; Poisson arrivals with log-normal per-instrument rates (median
+    50/s, sigma 1) are then scaled to `load` x capacity and replayed in real
+    time: each svpf_stream_process call serves the first pending request of
+    every instrument with one pending (host arrays in, host outputs back), the
+    clock advances by the call's wall time, and a request's latency is its
+    completion time minus its arrival time."""
+    rng = np.random.default_rng(seed)
+    ns = rng.choice([256, 512, 1024, 2048], size=n_instruments).astype(np.int32)
+    cfg = pkg.default_config(8, 6.0)
+    # the reference's two-factor test knobs (test/test_two_factor.cu:199-280)
+    cfg.update(use_two_factor=1, rho_fast=0.80, sigma_fast=0.30, rho_slow=0.995, sigma_slow=0.05,
+               bw_floor_fast=0.01, bw_floor_slow=0.05, use_svld=1, use_annealing=1, n_anneal_steps=5,
+               temperature=0.45, use_mim=1, mim_jump_prob=0.25, mim_jump_scale=9.0, use_guide=1,
+               use_guide_preserving=1, guide_strength=0.12, use_exact_gradient=1, lik_offset=0.345)
+    prm = pkg.Params(0.995, 0.05, -3.5, 0.0)
+    st = pkg.Stream(n_instruments, budget_bytes, int(ns.max()), seed=seed)
+    admitted = []
+    for i in range(n_instruments):
+        k = st.admit(int(ns[i]), cfg, prm, seed=seed)
+        if k < 0:
+            break
+        admitted.append(k)
+    A = len(admitted)
+    slots = np.array(admitted, np.int32)
+    # observations: each instrument's own two-factor path, consumed in arrival order
+    def y_of(i, count):
+        g = np.random.default_rng(1000 + i)
+        f = 0.30 / np.sqrt(1 - 0.8 ** 2) * g.standard_normal()
+        sl = 0.05 / np.sqrt(1 - 0.995 ** 2) * g.standard_normal()
+        out = np.empty(count, np.float32)
+        for t in range(count):
+            f = 0.8 * f + 0.3 * g.standard_normal()
+            sl = 0.995 * sl + 0.05 * g.standard_normal()
+            out[t] = np.exp((-3.5 + f + sl) / 2) * g.standard_t(6.0)
+        return out
+    # capacity probe: one round over every admitted instrument (after one warm round)
+    y0 = np.array([y_of(i, 1)[0] for i in range(A)], np.float32)
+    st.process(slots, y0)
+    t0 = time.perf_counter()
+    st.process(slots, y0)
+    cap = A / (time.perf_counter() - t0)
+    # arrivals at load x capacity
+    rates = np.exp(np.log(50.0) + rng.standard_normal(A))
+    scale = load * cap / rates.sum()
+    rates *= scale
+    counts = rng.poisson(rates * sim_seconds)
+    arr_t, arr_i = [], []
+    for i in range(A):
+        if counts[i]:
+            arr_t.append(np.sort(rng.uniform(0, sim_seconds, counts[i])))
+            arr_i.append(np.full(counts[i], i))
+    arr_t = np.concatenate(arr_t)
+    arr_i = np.concatenate(arr_i)
+    order = np.argsort(arr_t, kind="stable")
+    arr_t, arr_i = arr_t[order], arr_i[order]
+    ys_i = {i: y_of(i, int(counts[i]) + 2)[2:] for i in range(A) if counts[i]}
+    next_y = np.zeros(A, np.int64)
+    from collections import deque
+    pending = {}
+    lat = []
+    clock, k, busy, rounds, served = 0.0, 0, 0.0, 0, 0
+    total = len(arr_t)
+    while served < total:
+        while k < total and arr_t[k] <= clock:
+            pending.setdefault(int(arr_i[k]), deque()).append(arr_t[k])
+            k += 1
+        if not pending:
+            clock = arr_t[k]
+            continue
+        inst = np.fromiter(pending.keys(), np.int64)
+        yv = np.empty(len(inst), np.float32)
+        for q, i in enumerate(inst):
+            yv[q] = ys_i[i][next_y[i]]
+            next_y[i] += 1
+        w0 = time.perf_counter()
+        st.process(slots[inst], yv)
+        dt = time.perf_counter() - w0
+        clock += dt
+        busy += dt
+        rounds += 1
+        for i in inst:
+            a = pending[i].popleft()
+            lat.append(clock - a)
+            if not pending[i]:
+                del pending[i]
+        served += len(inst)
+    st.close()
+    lat = np.sort(np.array(lat)) * 1e6
+    return {
+        "workload": f"two-factor request loop: {n_instruments} instruments (rho_f 0.80, sigma_f 0.30, rho_s 0.995, "
+                    "sigma_s 0.05, nu 6), N ~ U{256,512,1024,2048}, 5 anneal x 8 Stein steps per tick, Poisson "
+                    f"arrivals with log-normal rates (median 50/s) scaled to {load:.0%} of capacity, "
+                    f"{budget_bytes >> 20} MiB HBM budget",
+        "admitted": A, "budget_bytes": budget_bytes,
+        "capacity_filter_ticks_per_s": cap,
+        "rate_scale": float(scale),
+        "filter_ticks_per_s": served / busy, "served": int(served), "rounds": rounds,
+        "mean_round_size": served / max(rounds, 1),
+        "latency_us": {"p50": float(lat[len(lat) // 2]), "p99": float(lat[int(len(lat) * 0.99)]),
+                       "timing": "arrival to completion; the clock advances by each call's host wall time"},
+    }
+
+
 def workload_config(F: int):
     return {"workload": f"batched SVPF tick: {F} filters per GPU, own theta, N ~ U{{256,512,1024,2048,4096}}, "
                         f"production config (full Newton, <= {MAX_STEPS} Stein iterations, 3 stages)",
@@ -287,6 +396,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--latency-ticks", type=int, default=400)
     ap.add_argument("--no-gradient", action="store_true", help="skip the differentiation workload")
+    ap.add_argument("--no-stream", action="store_true", help="skip the two-factor request loop")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -452,6 +562,9 @@ def main():
     grad_line = {}
     if rank == 0 and not args.no_gradient:
         grad_line = gradient_workload(pkg, torch)
+    stream_line = {}
+    if rank == 0 and not args.no_stream:
+        stream_line = stream_workload(pkg)
 
     cpu = {}
     if rank == 0:
@@ -480,6 +593,7 @@ def main():
             "single_filter_latency": lat,
             "plain_step_loop": plain,
             "gradient": grad_line,
+            "two_factor_request_loop": stream_line,
             "cpu_baseline": cpu,
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
             "status_errors": status_bad,

@@ -107,6 +107,101 @@ __global__ void __launch_bounds__(kThreads, 2) batch_tick_2f_kernel(const __grid
     }
 }
 
+// Two-factor filters on clusters of C CTAs (large N: a filter's tick is
+// split over C SMs as in the single-filter kernel, which shortens the longest
+// tick of a launch C-fold).  Rank 0 takes the next filter from the work
+// counter and writes its index into every member's shared memory; cluster
+// barriers separate the rounds, so no member waits on a flag.
+template <int C>
+__global__ void __launch_bounds__(kThreads) batch_tick_2f_cluster_kernel(const __grid_constant__ BatchArgs a) {
+    extern __shared__ __align__(16) float smem[];
+    __shared__ Plan pl;
+    __shared__ svpf_ctl_t ctl;
+    __shared__ svpf_config_t cfg;
+    __shared__ SVPFParams prm;
+    __shared__ svpf_out_t out;
+    __shared__ int s_next;
+    cg::cluster_group cl = cg::this_cluster();
+    const Team team{(int)cl.block_rank(), C};
+    for (;;) {
+        if (team.rank == 0 && threadIdx.x == 0) {
+            const int w = atomicAdd(a.queue, 1);
+            for (int r = 0; r < C; ++r) *cl.map_shared_rank(&s_next, r) = w;
+        }
+        cl.sync();
+        const int w = s_next;
+        if (w >= a.F) break;
+        const int f = a.order[w];
+        copy_words(&cfg, &a.cfg[f]);
+        copy_words(&prm, &a.prm[f]);
+        copy_words(&ctl, &a.ctl[f]);
+        __syncthreads();
+        const int n = a.n[f];
+        const long long off = a.off[f];
+        const Smem2 sm = carve_2f(smem, n, C, team.rank);
+        const FilterIO io{a.h + off, a.hp + off, a.v + off, a.lw + off, n};
+        const Noise nz{philox_key(a.seed, f), (uint32_t)ctl.timestep, a.tape_n, a.tape_u,
+                       a.slots_n, a.slots_u, a.tape_stride, &pl.flag};
+        const float yt = a.req_y ? a.req_y[w] : a.y_t[f];
+        const float yp = a.req_y ? ctl.y_prev : a.y_prev[f];
+        if ((n + C - 1) / C <= kThreads) run_tick_2f<1, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out);
+        else run_tick_2f<2, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out);
+        if (team.rank == 0) {
+            if (a.req_y && threadIdx.x == 0) ctl.y_prev = yt;
+            __syncthreads();
+            copy_words(&a.ctl[f], &ctl);
+            if (a.out != nullptr) copy_words(&a.out[a.req_y ? w : f], &out);
+        }
+        cl.sync();   // every member is done with this filter before the next index is written
+    }
+}
+
+constexpr int kCluster2f = 4;
+
+int batch_cluster_grid_2f(size_t smem_bytes) {
+    auto kern = batch_tick_2f_cluster_kernel<kCluster2f>;
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn_smem());
+        configured = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kCluster2f, 1, 1);
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem_bytes;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kCluster2f;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess || clusters < 1) {
+        cudaGetLastError();
+        return 0;
+    }
+    return clusters * kCluster2f;
+}
+
+cudaError_t launch_batch_2f_cluster(const BatchArgs& a, size_t smem_bytes, int grid, cudaStream_t s) {
+    if (grid < kCluster2f) return cudaErrorInvalidConfiguration;
+    auto kern = batch_tick_2f_cluster_kernel<kCluster2f>;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid / kCluster2f * kCluster2f, 1, 1);
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem_bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kCluster2f;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, a);
+}
+
 int batch_grid_2f(size_t smem_bytes) {
     static bool configured = false;
     if (!configured) {

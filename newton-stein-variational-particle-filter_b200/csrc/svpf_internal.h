@@ -115,6 +115,10 @@ cudaError_t launch_batch_2f(const BatchArgs& a, size_t smem_bytes, int grid, cud
 cudaError_t launch_init(const InitArgs& a, cudaStream_t s);
 int batch_grid(size_t smem_bytes);
 int batch_grid_2f(size_t smem_bytes);
+// Two-factor persistent kernel on clusters of kCluster2f (= 4) CTAs per filter.
+int batch_cluster_grid_2f(size_t smem_bytes);   // CTAs (a multiple of 4), 0 if it cannot run
+cudaError_t launch_batch_2f_cluster(const BatchArgs& a, size_t smem_bytes, int grid, cudaStream_t s);
+constexpr int kClusterMembers2f = 4;
 cudaError_t debug_philox(uint32_t k0, uint32_t k1, const uint32_t* d_ctr, uint32_t* d_out, int count);
 
 // Process-wide tuner table: tile chosen for a particle count (-1 = none yet).

@@ -39,8 +39,8 @@ struct svpf_stream {
     std::vector<int> ns, active;
     std::vector<svpf_config_t> cfgs;
     std::vector<uint8_t> tiles;
-    size_t smem1 = 0, smem2 = 0;
-    int grid1 = 0, grid2 = 0;
+    size_t smem1 = 0, smem2 = 0, smem2c = 0;
+    int grid1 = 0, grid2 = 0, grid2c = 0;
     long long launches = 0;
     // device
     float* pool = nullptr;        // 4 arrays of pool_floats: h, h_prev, v, log_w
@@ -107,10 +107,22 @@ BatchArgs round_args(svpf_stream* s) {
     return a;
 }
 
-// One round: d_req[0, c1) single-factor slots, d_req[c1, c1 + c2) two-factor
-// slots, each part largest cost first; y and outputs indexed alike.
-int launch_round(svpf_stream* s, int c1, int c2, const int* d_req, const float* d_y, svpf_out_t* d_out) {
-    if (cudaMemsetAsync(s->d_queue, 0, 2 * sizeof(int), s->stream) != cudaSuccess) return SVPF_ERR_CUDA;
+// Two-factor filters with at least this many particles take a cluster of
+// kClusterMembers2f CTAs in the request loop: a round waits for its longest
+// tick, and one CTA needs ~30 ms for an N = 2048 two-factor tick of 40 Stein
+// steps.
+constexpr int kClusterMinN = 1024;
+
+bool big_2f(const svpf_stream* s, int slot) {
+    return s->cfgs[slot].use_two_factor && s->ns[slot] >= kClusterMinN && s->grid2c > 0;
+}
+
+// One round: d_req[0, c1) single-factor slots, then c2 two-factor slots of
+// which the first c2c run on clusters; each part largest cost first; y and
+// outputs indexed alike.
+int launch_round(svpf_stream* s, int c1, int c2, const int* d_req, const float* d_y, svpf_out_t* d_out,
+                 int c2c = 0) {
+    if (cudaMemsetAsync(s->d_queue, 0, 3 * sizeof(int), s->stream) != cudaSuccess) return SVPF_ERR_CUDA;
     BatchArgs a = round_args(s);
     if (c1 > 0) {
         a.F = c1;
@@ -121,12 +133,22 @@ int launch_round(svpf_stream* s, int c1, int c2, const int* d_req, const float* 
         if (launch_batch(a, s->smem1, s->grid1, s->stream) != cudaSuccess) return SVPF_ERR_CUDA;
         ++s->launches;
     }
-    if (c2 > 0) {
-        a.F = c2;
+    if (c2c > 0) {
+        a.F = c2c;
         a.order = d_req + c1;
-        a.queue = s->d_queue + 1;
+        a.queue = s->d_queue + 2;
         a.req_y = d_y + c1;
         a.out = d_out + c1;
+        if (launch_batch_2f_cluster(a, s->smem2c, s->grid2c, s->stream) != cudaSuccess) return SVPF_ERR_CUDA;
+        ++s->launches;
+    }
+    const int c2s = c2 - c2c;
+    if (c2s > 0) {
+        a.F = c2s;
+        a.order = d_req + c1 + c2c;
+        a.queue = s->d_queue + 1;
+        a.req_y = d_y + c1 + c2c;
+        a.out = d_out + c1 + c2c;
         if (launch_batch_2f(a, s->smem2, s->grid2, s->stream) != cudaSuccess) return SVPF_ERR_CUDA;
         ++s->launches;
     }
@@ -161,7 +183,7 @@ svpf_stream_t* svpf_stream_create(int max_instruments, size_t hbm_budget_bytes, 
     size_t acc = 0;
     bool ok = salloc(&s->pool, 4 * s->pool_floats, &acc) && salloc(&s->d_n, C, &acc) && salloc(&s->d_off, C, &acc) &&
               salloc(&s->d_tile, C, &acc) && salloc(&s->d_cfg, C, &acc) && salloc(&s->d_prm, C, &acc) &&
-              salloc(&s->d_ctl, C, &acc) && salloc(&s->d_queue, 2, &acc) && salloc(&s->d_req, C, &acc) &&
+              salloc(&s->d_ctl, C, &acc) && salloc(&s->d_queue, 3, &acc) && salloc(&s->d_req, C, &acc) &&
               salloc(&s->d_y, C, &acc) && salloc(&s->d_out, C, &acc);
     s->fixed_bytes = acc - 4 * s->pool_floats * sizeof(float);
     ok = ok && cudaHostAlloc(&s->h_req, C * sizeof(int), cudaHostAllocDefault) == cudaSuccess &&
@@ -181,6 +203,8 @@ svpf_stream_t* svpf_stream_create(int max_instruments, size_t hbm_budget_bytes, 
         s->smem2 = tick_smem_bytes_2f(n_max, 1);
         if (s->smem1 <= max_dyn_smem()) s->grid1 = batch_grid(s->smem1);
         if (s->smem2 <= max_dyn_smem()) s->grid2 = batch_grid_2f(s->smem2);
+        s->smem2c = tick_smem_bytes_2f(n_max, kClusterMembers2f);
+        if (n_max >= kClusterMinN && s->smem2c <= max_dyn_smem()) s->grid2c = batch_cluster_grid_2f(s->smem2c);
         ok = s->grid1 > 0 || s->grid2 > 0;
     }
     if (!ok) {
@@ -211,7 +235,8 @@ int svpf_stream_admit(svpf_stream_t* s, int n, const svpf_config_t* cfg, const S
                       unsigned long long seed) {
     if (!s || !cfg || !p || n < 1 || n > s->n_max) return -SVPF_ERR_INVALID_ARG;
     if (cfg->use_heun) return -SVPF_ERR_UNSUPPORTED;   // the loop's shared-memory layout has no Heun buffers
-    if ((cfg->use_two_factor ? s->grid2 : s->grid1) < 1) return -SVPF_ERR_UNSUPPORTED;
+    if (!cfg->use_two_factor && s->grid1 < 1) return -SVPF_ERR_UNSUPPORTED;
+    if (cfg->use_two_factor && s->grid2 < 1 && !(n >= kClusterMinN && s->grid2c > 0)) return -SVPF_ERR_UNSUPPORTED;
     if (cfg->use_two_factor && cfg->n_stein_steps < 1) return -SVPF_ERR_INVALID_ARG;
     int slot = -1;
     for (int i = 0; i < s->cap; ++i)
@@ -337,23 +362,26 @@ int svpf_stream_process(svpf_stream_t* s, int count, const int* slots, const flo
     for (int r = 0; r < count; ++r) where[round[r]].push_back(r);
     for (int k = 0; k < rounds; ++k) {
         idx = where[k];
-        // single-factor first, then two-factor, each largest cost first
+        // single-factor, then two-factor on clusters, then two-factor on one
+        // CTA; each part largest cost first
+        auto group = [&](int r) { return !s->cfgs[slots[r]].use_two_factor ? 0 : (big_2f(s, slots[r]) ? 1 : 2); };
         std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
-            const svpf_config_t &ca = s->cfgs[slots[a]], &cb = s->cfgs[slots[b]];
-            if ((ca.use_two_factor != 0) != (cb.use_two_factor != 0)) return cb.use_two_factor != 0;
-            return tick_cost(s->ns[slots[a]], ca) > tick_cost(s->ns[slots[b]], cb);
+            if (group(a) != group(b)) return group(a) < group(b);
+            return tick_cost(s->ns[slots[a]], s->cfgs[slots[a]]) > tick_cost(s->ns[slots[b]], s->cfgs[slots[b]]);
         });
-        int c1 = 0;
+        int c1 = 0, c2c = 0;
         for (size_t q = 0; q < idx.size(); ++q) {
             s->h_req[q] = slots[idx[q]];
             s->h_y[q] = y[idx[q]];
-            if (!s->cfgs[slots[idx[q]]].use_two_factor) ++c1;
+            const int gq = group(idx[q]);
+            if (gq == 0) ++c1;
+            if (gq == 1) ++c2c;
         }
         const int m = (int)idx.size();
         if (cudaMemcpyAsync(s->d_req, s->h_req, m * sizeof(int), cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
             cudaMemcpyAsync(s->d_y, s->h_y, m * sizeof(float), cudaMemcpyHostToDevice, s->stream) != cudaSuccess)
             return SVPF_ERR_CUDA;
-        const int rc = launch_round(s, c1, m - c1, s->d_req, s->d_y, s->d_out);
+        const int rc = launch_round(s, c1, m - c1, s->d_req, s->d_y, s->d_out, c2c);
         if (rc != SVPF_OK) return rc;
         if (cudaMemcpyAsync(s->h_out, s->d_out, m * sizeof(svpf_out_t), cudaMemcpyDeviceToHost, s->stream) !=
                 cudaSuccess ||

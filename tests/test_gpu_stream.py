@@ -149,3 +149,33 @@ def test_device_round_matches_host_round(pkg):
         assert abs(ll_dev[r] - out_c[r].loglik) <= TOL * max(1, abs(out_c[r].loglik)), r
     a.close()
     c.close()
+
+
+def test_large_two_factor_filters_on_clusters(pkg):
+    """Two-factor instruments with N >= 1024 run on 4-CTA clusters in the
+    request loop; their ticks must equal the batch's one-CTA ticks."""
+    ns = np.array([2048, 1024, 300, 1500, 2048, 512, 1024, 1100], np.int32)
+    F = len(ns)
+    cfgs, prms = [], []
+    for f in range(F):
+        c = pkg.default_config(4, 6.0)
+        c.update(**dict(cases.TWO_FACTOR_TEST, n_anneal_steps=2, nu=6.0, rho_fast=0.80, sigma_fast=0.30,
+                        rho_slow=0.995, sigma_slow=0.05))
+        cfgs.append(c)
+        prms.append(pkg.Params(0.995, 0.05, -3.5, 0.0))
+    ys = observations(F, 3, seed=9)
+    b = pkg.Batch(ns, cfgs, prms)
+    b.initialize(seed=SEED)
+    s = pkg.Stream(F, 64 << 20, int(ns.max()), seed=SEED)
+    for f in range(F):
+        assert s.admit(int(ns[f]), cfgs[f], prms[f], seed=SEED) == f
+    for t in range(3):
+        ll, _, hm = b.step(ys[t], ys[t - 1] if t else np.zeros(F, np.float32))
+        out = s.process(np.arange(F), ys[t])
+        for f in range(F):
+            assert abs(out[f].loglik - ll[f]) <= TOL * max(1, abs(ll[f])), (t, f, out[f].loglik, ll[f])
+            assert abs(out[f].h_mean - hm[f]) <= TOL * max(1, abs(hm[f])), (t, f)
+    for f in range(F):
+        assert rel_err(s.particles(f), b.get_particles(f)) < TOL, f
+    b.close()
+    s.close()
