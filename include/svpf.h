@@ -521,6 +521,46 @@ int svpf_stream_get_ctl(const svpf_stream_t* s, int slot, svpf_ctl_t* ctl);
 int svpf_stream_get_particles(const svpf_stream_t* s, int slot, float* h_out);
 long long svpf_stream_kernel_launches(const svpf_stream_t* s);
 
+/* ---- svpf_fully_fused_step_v2 (include/svpf_fully_fused_v2.cuh:43-119) ------
+ * The reference's second, single-kernel tick with its own semantics (Silverman
+ * bandwidth, fixed beta ramp, EKF inside the kernel, adaptive guide strength),
+ * same argument list.  One launch of a thread-block cluster; N up to
+ * SVPF_MAX_PARTICLES (the reference: 1024).  Where the reference takes
+ * curandStatePhilox4_32_10_t*, this takes a device svpf_v2_rng_t record: the
+ * engine's counter-based Philox keyed by (seed, filter) and counted by
+ * (particle, draw, tick), tick advanced by every call, or -- a test hook -- a
+ * device noise tape normals[k*n + i], uniforms[k*n + i]. */
+typedef struct {
+    unsigned long long seed;
+    unsigned int tick;            /* advanced by one per call */
+    unsigned int filter;
+    int status;                   /* SVPF_OK or SVPF_ERR_TAPE_SHORT of the last call */
+    int slots_n, slots_u;
+    int reserved;
+    const float* tape_normals;    /* device, or NULL for Philox */
+    const float* tape_uniforms;
+} svpf_v2_rng_t;
+
+bool svpf_fully_fused_v2_supported(int n_particles);
+cudaError_t svpf_fully_fused_step_v2(
+    float* h, float* h_prev, float* grad_log_p, float* log_weights, float* d_grad_v, float* d_inv_hessian,
+    svpf_v2_rng_t* rng, float y_t, float y_prev, float h_mean_prev, float vol_prev, float ksd_prev,
+    float* d_h_mean, float* d_vol, float* d_loglik, float* d_bandwidth, float* d_ksd, float* d_guide_mean,
+    float* d_guide_var, float rho, float sigma_z, float mu, float nu, float lik_offset, float student_t_const,
+    float student_t_implied_offset, float gamma, float delta_rho, float delta_sigma, float mim_jump_prob,
+    float mim_jump_scale, float guide_strength_base, float guide_strength_max, float guide_innovation_threshold,
+    float guided_alpha_base, float guided_alpha_shock, float guided_innovation_thresh_predict, int use_guide,
+    int use_guided_predict, int use_guide_preserving, int use_newton, int use_full_newton, int use_rejuvenation,
+    float rejuv_ksd_threshold, float rejuv_prob, float rejuv_blend, int use_adaptive_mu, float* d_mu_state,
+    float mu_ema_alpha, int use_adaptive_sigma, float sigma_boost_threshold, float sigma_boost_max,
+    float step_size, float temperature, float rmsprop_rho, float rmsprop_eps, int n_stein_steps,
+    int n_anneal_steps, int stein_sign_mode, int n, int timestep, cudaStream_t stream);
+/* Device record helpers (the record may also be filled by the caller). */
+svpf_v2_rng_t* svpf_fully_fused_v2_rng_create(unsigned long long seed, unsigned int filter);
+void svpf_fully_fused_v2_rng_destroy(svpf_v2_rng_t* rng);
+int svpf_fully_fused_v2_rng_get(const svpf_v2_rng_t* rng, svpf_v2_rng_t* host);
+int svpf_fully_fused_v2_rng_set(svpf_v2_rng_t* rng, const svpf_v2_rng_t* host);
+
 #ifdef __cplusplus
 }
 #endif

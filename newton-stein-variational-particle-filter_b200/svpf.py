@@ -165,6 +165,13 @@ def lib() -> C.CDLL:
         "svpf_stream_get_ctl": (_I, [vp, _I, C.POINTER(Ctl)]),
         "svpf_stream_get_particles": (_I, [vp, _I, _FP]),
         "svpf_stream_kernel_launches": (C.c_longlong, [vp]),
+        "svpf_fully_fused_v2_supported": (C.c_bool, [_I]),
+        "svpf_fully_fused_step_v2": (_I, [vp] * 7 + [_F] * 5 + [vp] * 7 + [_F] * 18 + [_I] * 6 + [_F] * 3 +
+                                     [_I, vp, _F, _I] + [_F] * 6 + [_I] * 5 + [vp]),
+        "svpf_fully_fused_v2_rng_create": (vp, [C.c_ulonglong, C.c_uint]),
+        "svpf_fully_fused_v2_rng_destroy": (None, [vp]),
+        "svpf_fully_fused_v2_rng_get": (_I, [vp, vp]),
+        "svpf_fully_fused_v2_rng_set": (_I, [vp, vp]),
         "svpf_debug_philox": (_I, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), _I]),
     }
     for name, (res, args) in sig.items():
@@ -727,6 +734,106 @@ class Stream:
         if rc != SVPF_OK:
             raise RuntimeError(f"get_particles rc={rc}")
         return out
+
+
+class V2Rng(C.Structure):
+    """svpf_v2_rng_t."""
+    _fields_ = [("seed", C.c_ulonglong), ("tick", C.c_uint), ("filter", C.c_uint), ("status", _I),
+                ("slots_n", _I), ("slots_u", _I), ("reserved", _I), ("tape_normals", C.c_void_p),
+                ("tape_uniforms", C.c_void_p)]
+
+
+# scalar arguments of svpf_fully_fused_step_v2 between the device outputs and
+# the arrays' length, in order (include/svpf_fully_fused_v2.cuh:43-119)
+V2_ARG_ORDER = ["rho", "sigma_z", "mu", "nu", "lik_offset", "student_t_const", "student_t_implied_offset",
+                "gamma", "delta_rho", "delta_sigma", "mim_jump_prob", "mim_jump_scale", "guide_strength_base",
+                "guide_strength_max", "guide_innovation_threshold", "guided_alpha_base", "guided_alpha_shock",
+                "guided_innovation_thresh_predict", "use_guide", "use_guided_predict", "use_guide_preserving",
+                "use_newton", "use_full_newton", "use_rejuvenation", "rejuv_ksd_threshold", "rejuv_prob",
+                "rejuv_blend", "use_adaptive_mu", "@mu_state", "mu_ema_alpha", "use_adaptive_sigma",
+                "sigma_boost_threshold", "sigma_boost_max", "step_size", "temperature", "rmsprop_rho",
+                "rmsprop_eps", "n_stein_steps", "n_anneal_steps", "stein_sign_mode"]
+
+
+class FusedV2:
+    """svpf_fully_fused_step_v2 on device buffers owned by this object (torch
+    tensors): arrays h, h_prev, grad, lw, v, inv_hess [n] and the device
+    scalars.  A test-and-tooling wrapper around the C entry point."""
+
+    ARRAYS = ("h", "h_prev", "grad", "lw", "v", "inv_hess")
+    SCALARS = ("h_mean", "vol", "loglik", "bandwidth", "ksd", "guide_mean", "guide_var", "mu_state")
+
+    def __init__(self, n: int, seed: int = 0, filter_id: int = 0):
+        import torch
+        self.torch = torch
+        self.n = n
+        self.arr = {a: torch.zeros(n, dtype=torch.float32, device="cuda") for a in self.ARRAYS}
+        self.sc = torch.zeros(len(self.SCALARS), dtype=torch.float32, device="cuda")
+        self._rng = lib().svpf_fully_fused_v2_rng_create(int(seed), int(filter_id))
+        if not self._rng:
+            raise RuntimeError("svpf_fully_fused_v2_rng_create failed")
+        self._tape = None
+
+    def close(self):
+        if getattr(self, "_rng", None):
+            lib().svpf_fully_fused_v2_rng_destroy(self._rng)
+            self._rng = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set(self, name, values):
+        if name in self.ARRAYS:
+            self.arr[name].copy_(self.torch.as_tensor(np.asarray(values, np.float32)))
+        else:
+            self.sc[self.SCALARS.index(name)] = float(values)
+
+    def get(self, name):
+        self.torch.cuda.synchronize()
+        if name in self.ARRAYS:
+            return self.arr[name].cpu().numpy()
+        return float(self.sc[self.SCALARS.index(name)].item())
+
+    def rng_state(self) -> V2Rng:
+        r = V2Rng()
+        lib().svpf_fully_fused_v2_rng_get(self._rng, C.byref(r))
+        return r
+
+    def set_tape(self, normals=None, uniforms=None, tick=None):
+        """Device noise tape [slots][n] (None: back to Philox)."""
+        r = self.rng_state()
+        if normals is None:
+            self._tape = None
+            r.tape_normals = r.tape_uniforms = None
+            r.slots_n = r.slots_u = 0
+        else:
+            nrm = self.torch.as_tensor(np.ascontiguousarray(normals, np.float32)).cuda()
+            uni = self.torch.as_tensor(np.ascontiguousarray(uniforms, np.float32)).cuda()
+            self._tape = (nrm, uni)
+            r.tape_normals, r.tape_uniforms = nrm.data_ptr(), uni.data_ptr()
+            r.slots_n, r.slots_u = nrm.shape[0], uni.shape[0]
+        if tick is not None:
+            r.tick = tick
+        lib().svpf_fully_fused_v2_rng_set(self._rng, C.byref(r))
+
+    def step(self, params: dict, y_t, y_prev, h_mean_prev, vol_prev, ksd_prev, timestep, stream=None) -> int:
+        A = self.arr
+        sp = [self.sc[k].data_ptr() for k in range(len(self.SCALARS))]
+        scal = []
+        for k in V2_ARG_ORDER:
+            if k == "@mu_state":
+                scal.append(sp[7])
+            else:
+                scal.append(params[k])
+        args = [A[a].data_ptr() for a in self.ARRAYS] + [self._rng] + \
+               [float(y_t), float(y_prev), float(h_mean_prev), float(vol_prev), float(ksd_prev)] + \
+               [sp[0], sp[1], sp[2], sp[3], sp[4], sp[5], sp[6]] + scal + [self.n, int(timestep), stream]
+        rc = lib().svpf_fully_fused_step_v2(*args)
+        self.torch.cuda.synchronize()
+        return int(rc)
 
 
 def autotune(ns, ticks: int = 2):

@@ -139,6 +139,41 @@ def build(quiet: bool = True) -> None:
 _lib = None
 
 
+
+V2_FIELDS = [("rho", "f"), ("sigma_z", "f"), ("mu", "f"), ("nu", "f"), ("lik_offset", "f"),
+             ("student_t_const", "f"), ("student_t_implied_offset", "f"), ("gamma", "f"),
+             ("delta_rho", "f"), ("delta_sigma", "f"), ("mim_jump_prob", "f"), ("mim_jump_scale", "f"),
+             ("guide_strength_base", "f"), ("guide_strength_max", "f"), ("guide_innovation_threshold", "f"),
+             ("guided_alpha_base", "f"), ("guided_alpha_shock", "f"), ("guided_innovation_thresh_predict", "f"),
+             ("use_guide", "i"), ("use_guided_predict", "i"), ("use_guide_preserving", "i"),
+             ("use_newton", "i"), ("use_full_newton", "i"), ("use_rejuvenation", "i"),
+             ("rejuv_ksd_threshold", "f"), ("rejuv_prob", "f"), ("rejuv_blend", "f"),
+             ("use_adaptive_mu", "i"), ("mu_ema_alpha", "f"), ("use_adaptive_sigma", "i"),
+             ("sigma_boost_threshold", "f"), ("sigma_boost_max", "f"), ("step_size", "f"), ("temperature", "f"),
+             ("rmsprop_rho", "f"), ("rmsprop_eps", "f"), ("n_stein_steps", "i"), ("n_anneal_steps", "i"),
+             ("stein_sign_mode", "i")]
+
+
+class OracleV2Params(C.Structure):
+    """oracle_v2_params: the scalar arguments of svpf_fully_fused_step_v2."""
+    _fields_ = [(k, C.c_float if t == "f" else C.c_int) for k, t in V2_FIELDS]
+
+    def to_dict(self):
+        return {k: getattr(self, k) for k, _ in V2_FIELDS}
+
+    @classmethod
+    def from_dict(cls, d):
+        p = cls()
+        for k, _ in V2_FIELDS:
+            if k in d:
+                setattr(p, k, d[k])
+        return p
+
+
+class OracleV2Out(C.Structure):
+    _fields_ = [("h_mean", C.c_float), ("vol", C.c_float), ("loglik", C.c_float), ("bandwidth", C.c_float),
+                ("ksd", C.c_float)]
+
 def lib():
     global _lib
     if _lib is None:
@@ -164,6 +199,10 @@ def lib():
             C.c_uint64, C.c_uint64, C.c_int, C.POINTER(OracleOut)]
         L.svpf_oracle_grad_supported.restype = C.c_int
         L.svpf_oracle_grad_supported.argtypes = [C.POINTER(OracleConfig)]
+        L.svpf_oracle_v2_tick.restype = C.c_int
+        L.svpf_oracle_v2_tick.argtypes = [C.POINTER(OracleV2Params), C.c_int] + [C.POINTER(C.c_double)] * 6 + [
+            C.c_float] * 5 + [C.c_int] + [C.POINTER(C.c_double)] * 3 + [C.POINTER(OracleNoise), C.POINTER(OracleV2Out),
+                                                                        C.c_int]
         L.svpf_oracle_grad_run2.restype = C.c_int
         L.svpf_oracle_grad_run2.argtypes = [C.POINTER(OracleConfig), C.c_int, C.c_int, C.POINTER(C.c_double),
                                             C.c_double, C.POINTER(C.c_float), C.POINTER(C.c_double),
@@ -231,6 +270,49 @@ def run_loglik(cfg: OracleConfig, n: int, theta, ys, gamma: float = 0.0, seed: i
         out.append(o.loglik)
         yp = float(y)
     return np.array(out)
+
+
+class V2State:
+    """Arrays and device scalars of one svpf_fully_fused_step_v2 filter, FP64."""
+
+    ARRAYS = ("h", "h_prev", "grad", "lw", "v", "inv_hess")
+
+    def __init__(self, n):
+        self.n = n
+        for a in self.ARRAYS:
+            setattr(self, a, np.zeros(n))
+        self.guide_mean = np.zeros(1)
+        self.guide_var = np.zeros(1)
+        self.mu_state = np.zeros(1)
+
+    def copy(self):
+        c = V2State(self.n)
+        for a in self.ARRAYS + ("guide_mean", "guide_var", "mu_state"):
+            setattr(c, a, getattr(self, a).copy())
+        return c
+
+
+def v2_tick(p: OracleV2Params, st: V2State, y_t, y_prev, h_mean_prev, vol_prev, ksd_prev, timestep,
+            normals=None, uniforms=None, seed=0, filter_id=0, precision=0) -> OracleV2Out:
+    nz = OracleNoise()
+    keep = []
+    if normals is not None:
+        nrm = np.ascontiguousarray(normals, np.float32)
+        uni = np.ascontiguousarray(uniforms, np.float32)
+        keep += [nrm, uni]
+        nz.mode, nz.n_normal_slots, nz.n_uniform_slots = 0, nrm.shape[0], uni.shape[0]
+        nz.normals, nz.uniforms = _fptr(nrm), _fptr(uni)
+    else:
+        nz.mode = 1
+    nz.seed, nz.tick, nz.filter_id = seed, timestep, filter_id
+    out = OracleV2Out()
+    rc = lib().svpf_oracle_v2_tick(C.byref(p), st.n, *[_dptr(getattr(st, a)) for a in V2State.ARRAYS],
+                                   float(y_t), float(y_prev), float(h_mean_prev), float(vol_prev), float(ksd_prev),
+                                   int(timestep), _dptr(st.guide_mean), _dptr(st.guide_var), _dptr(st.mu_state),
+                                   C.byref(nz), C.byref(out), precision)
+    if rc != 0:
+        raise RuntimeError(f"oracle v2 tick rc={rc}")
+    return out
 
 
 def philox(k0, k1, c0, c1, c2, c3):
@@ -312,10 +394,32 @@ class RefLib:
         L.svpf_ref_step.argtypes = [C.c_void_p, C.c_float, C.c_float, C.POINTER(OracleParams),
                                     C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_float), C.c_int,
                                     C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.svpf_ref_v2_step.restype = C.c_int
+        L.svpf_ref_v2_step.argtypes = [C.POINTER(OracleV2Params), C.c_int] + [C.POINTER(C.c_double)] * 6 + [
+            C.c_float] * 5 + [C.c_int] + [C.POINTER(C.c_double)] * 3 + [C.POINTER(C.c_float), C.c_int,
+                                                                        C.POINTER(C.c_float), C.c_int,
+                                                                        C.POINTER(OracleV2Out)]
+        L.svpf_ref_v2_time.restype = C.c_int
+        L.svpf_ref_v2_time.argtypes = [C.POINTER(OracleV2Params), C.c_int, C.POINTER(C.c_float), C.c_int,
+                                       C.POINTER(C.c_float)]
         L.svpf_ref_time_steps.restype = C.c_int
         L.svpf_ref_time_steps.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int,
                                           C.POINTER(OracleParams), C.POINTER(C.c_float)]
         self.L = L
+
+
+def ref_v2_step(reflib, p: OracleV2Params, st: V2State, y_t, y_prev, h_mean_prev, vol_prev, ksd_prev, timestep,
+                normals, uniforms):
+    """The reference's svpf_fully_fused_step_v2 (tape build) on st, in place."""
+    nrm = np.ascontiguousarray(normals, np.float32)
+    uni = np.ascontiguousarray(uniforms, np.float32)
+    out = OracleV2Out()
+    flags = reflib.L.svpf_ref_v2_step(C.byref(p), st.n, *[_dptr(getattr(st, a)) for a in V2State.ARRAYS],
+                                      float(y_t), float(y_prev), float(h_mean_prev), float(vol_prev),
+                                      float(ksd_prev), int(timestep), _dptr(st.guide_mean), _dptr(st.guide_var),
+                                      _dptr(st.mu_state), _fptr(nrm), nrm.shape[0], _fptr(uni), uni.shape[0],
+                                      C.byref(out))
+    return flags, out
 
 
 class RefFilter:

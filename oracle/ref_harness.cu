@@ -8,6 +8,7 @@
  * ticks (per-tick parity with state re-sync).
  */
 #include "svpf.cuh"
+#include "svpf_fully_fused_v2.cuh"
 #include "svpf_oracle.h"
 
 #include <cstdio>
@@ -271,6 +272,120 @@ int svpf_ref_step(SVPFState* s, float y_t, float y_prev, const oracle_params* p,
     svpf_step_graph(s, y_t, y_prev, &sp, ll, vol, hm);
     if (check(cudaGetLastError(), "step")) return -1;
     return svpf_ref_tape_flags_take();
+}
+
+/* One svpf_fully_fused_step_v2 call (the reference's single-kernel step) on
+ * host arrays [n], with the noise tape. Returns the tape flags, or -1. */
+int svpf_ref_v2_step(const oracle_v2_params* p, int n, double* h, double* hp, double* grad, double* lw,
+                     double* v, double* ih, float y_t, float y_prev, float h_mean_prev, float vol_prev,
+                     float ksd_prev, int timestep, double* gmean, double* gvar, double* mustate,
+                     const float* normals, int slots_n, const float* uniforms, int slots_u, oracle_v2_out* out) {
+    std::vector<float> buf(7 * (size_t)n);
+    float* d = nullptr;
+    curandStatePhilox4_32_10_t* rng = nullptr;
+    float* sc = nullptr;   // h_mean, vol, loglik, bw, ksd, guide_mean, guide_var, mu_state
+    if (check(cudaMalloc(&d, 6 * (size_t)n * sizeof(float)), "v2 arrays") ||
+        check(cudaMalloc(&rng, (size_t)n * sizeof(*rng)), "v2 rng") || check(cudaMalloc(&sc, 8 * sizeof(float)), "v2 sc"))
+        return -1;
+    double* arrs[6] = {h, hp, grad, lw, v, ih};
+    for (int a = 0; a < 6; ++a)
+        for (int i = 0; i < n; ++i) buf[(size_t)a * n + i] = (float)arrs[a][i];
+    float scal[8] = {0, 0, 0, 0, 0, (float)*gmean, (float)*gvar, (float)*mustate};
+    int rc = 0;
+    if (check(cudaMemcpy(d, buf.data(), 6 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice), "v2 in") ||
+        check(cudaMemcpy(sc, scal, sizeof(scal), cudaMemcpyHostToDevice), "v2 sc in"))
+        rc = -1;
+#ifndef SVPF_REF_STOCK
+    if (!rc && svpf_ref_tape_set(normals, slots_n, uniforms, slots_u, n)) rc = -1;
+    if (!rc) reset_counters_kernel<<<(n + 255) / 256, 256>>>(rng, n);
+#endif
+    if (!rc) {
+        cudaError_t e = svpf_fully_fused_step_v2(
+            d, d + n, d + 2 * n, d + 3 * n, d + 4 * n, d + 5 * n, rng, y_t, y_prev, h_mean_prev, vol_prev, ksd_prev,
+            sc, sc + 1, sc + 2, sc + 3, sc + 4, sc + 5, sc + 6, p->rho, p->sigma_z, p->mu, p->nu, p->lik_offset,
+            p->student_t_const, p->student_t_implied_offset, p->gamma, p->delta_rho, p->delta_sigma,
+            p->mim_jump_prob, p->mim_jump_scale, p->guide_strength_base, p->guide_strength_max,
+            p->guide_innovation_threshold, p->guided_alpha_base, p->guided_alpha_shock,
+            p->guided_innovation_thresh_predict, p->use_guide, p->use_guided_predict, p->use_guide_preserving,
+            p->use_newton, p->use_full_newton, p->use_rejuvenation, p->rejuv_ksd_threshold, p->rejuv_prob,
+            p->rejuv_blend, p->use_adaptive_mu, sc + 7, p->mu_ema_alpha, p->use_adaptive_sigma,
+            p->sigma_boost_threshold, p->sigma_boost_max, p->step_size, p->temperature, p->rmsprop_rho,
+            p->rmsprop_eps, p->n_stein_steps, p->n_anneal_steps, p->stein_sign_mode, n, timestep, 0);
+        if (check(e, "v2 step") || check(cudaDeviceSynchronize(), "v2 sync")) rc = -1;
+    }
+    if (!rc && (check(cudaMemcpy(buf.data(), d, 6 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost), "v2 out") ||
+                check(cudaMemcpy(scal, sc, sizeof(scal), cudaMemcpyDeviceToHost), "v2 sc out")))
+        rc = -1;
+    if (!rc) {
+        for (int a = 0; a < 6; ++a)
+            for (int i = 0; i < n; ++i) arrs[a][i] = buf[(size_t)a * n + i];
+        out->h_mean = scal[0]; out->vol = scal[1]; out->loglik = scal[2]; out->bandwidth = scal[3]; out->ksd = scal[4];
+        *gmean = scal[5]; *gvar = scal[6]; *mustate = scal[7];
+        rc = svpf_ref_tape_flags_take();
+    }
+    cudaFree(d);
+    cudaFree(rng);
+    cudaFree(sc);
+    return rc;
+}
+
+namespace {
+__global__ void v2_rng_init_kernel(curandStatePhilox4_32_10_t* st, int n, unsigned long long seed) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) curand_init(seed, i, 0, &st[i]);
+}
+}  // namespace
+
+/* Latency of the reference's svpf_fully_fused_step_v2: T calls on one filter
+ * (stationary start, its own cuRAND states), CUDA events around each call as
+ * test/test_fully_fused_v2.cu:194-219 does; us_per_call[T]. */
+int svpf_ref_v2_time(const oracle_v2_params* p, int n, const float* ys, int T, float* us_per_call) {
+    float* d = nullptr;
+    curandStatePhilox4_32_10_t* rng = nullptr;
+    float* sc = nullptr;
+    if (check(cudaMalloc(&d, 6 * (size_t)n * sizeof(float)), "v2t arrays") ||
+        check(cudaMalloc(&rng, (size_t)n * sizeof(*rng)), "v2t rng") || check(cudaMalloc(&sc, 8 * sizeof(float)), "v2t sc"))
+        return -1;
+    std::vector<float> h0(6 * (size_t)n, 0.0f);
+    for (int i = 0; i < n; ++i) h0[i] = p->mu + 0.3f * (float)((i * 7919) % 1000 - 500) / 500.0f;
+    float scal[8] = {0, 0, 0, 0, 0, 0, 0, p->mu};
+    cudaMemcpy(d, h0.data(), h0.size() * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(sc, scal, sizeof(scal), cudaMemcpyHostToDevice);
+    v2_rng_init_kernel<<<(n + 255) / 256, 256>>>(rng, n, 1234ull);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float y_prev = 0.0f, h_mean_prev = p->mu, vol_prev = expf(p->mu * 0.5f), ksd_prev = 0.1f;
+    for (int t = 0; t < T; ++t) {
+        cudaEventRecord(a, 0);
+        svpf_fully_fused_step_v2(
+            d, d + n, d + 2 * n, d + 3 * n, d + 4 * n, d + 5 * n, rng, ys[t], y_prev, h_mean_prev, vol_prev, ksd_prev,
+            sc, sc + 1, sc + 2, sc + 3, sc + 4, sc + 5, sc + 6, p->rho, p->sigma_z, p->mu, p->nu, p->lik_offset,
+            p->student_t_const, p->student_t_implied_offset, p->gamma, p->delta_rho, p->delta_sigma,
+            p->mim_jump_prob, p->mim_jump_scale, p->guide_strength_base, p->guide_strength_max,
+            p->guide_innovation_threshold, p->guided_alpha_base, p->guided_alpha_shock,
+            p->guided_innovation_thresh_predict, p->use_guide, p->use_guided_predict, p->use_guide_preserving,
+            p->use_newton, p->use_full_newton, p->use_rejuvenation, p->rejuv_ksd_threshold, p->rejuv_prob,
+            p->rejuv_blend, p->use_adaptive_mu, sc + 7, p->mu_ema_alpha, p->use_adaptive_sigma,
+            p->sigma_boost_threshold, p->sigma_boost_max, p->step_size, p->temperature, p->rmsprop_rho,
+            p->rmsprop_eps, p->n_stein_steps, p->n_anneal_steps, p->stein_sign_mode, n, t, 0);
+        cudaEventRecord(b, 0);
+        cudaEventSynchronize(b);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, a, b);
+        us_per_call[t] = ms * 1000.0f;
+        cudaMemcpy(scal, sc, 5 * sizeof(float), cudaMemcpyDeviceToHost);
+        h_mean_prev = scal[0];
+        vol_prev = scal[1];
+        ksd_prev = scal[4];
+        y_prev = ys[t];
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(d);
+    cudaFree(rng);
+    cudaFree(sc);
+    return check(cudaGetLastError(), "v2 time");
 }
 
 /* Latency probe: CUDA events around each svpf_step_graph call, the way the

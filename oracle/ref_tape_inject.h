@@ -7,6 +7,7 @@
  *
  *   curand_init(seed, subseq, offset, state)  -> remember the particle index
  *   curand_normal(state)                      -> next normal from the tape
+ *   curand_normal4(state)                     -> the next four normals
  *   curand_uniform(state)                     -> next uniform from the tape
  *
  * Each particle keeps one normal counter and one uniform counter in the
@@ -64,7 +65,18 @@ static __device__ __forceinline__ float svpf_ref_tape_uniform(curandStatePhilox4
     return tape[(size_t)k * (size_t)svpf_ref_tape_n + i];
 }
 
+/* curand_normal4: four consecutive normal slots (x, y, z, w). */
+static __device__ __forceinline__ float4 svpf_ref_tape_normal4(curandStatePhilox4_32_10_t* st) {
+    float4 r;
+    r.x = svpf_ref_tape_normal(st);
+    r.y = svpf_ref_tape_normal(st);
+    r.z = svpf_ref_tape_normal(st);
+    r.w = svpf_ref_tape_normal(st);
+    return r;
+}
+
 #define curand_init(a, b, c, d) svpf_ref_tape_init((a), (b), (c), (d))
+#define curand_normal4(s) svpf_ref_tape_normal4(s)
 #define curand_normal(s) svpf_ref_tape_normal(s)
 #define curand_uniform(s) svpf_ref_tape_uniform(s)
 

@@ -1320,3 +1320,255 @@ int svpf_oracle_grad_run2(const oracle_config* cfg_in, int n, int T, const doubl
 }
 
 }  // extern "C"
+
+/* ======================================================================== */
+/* svpf_fully_fused_step_v2 restated (src/svpf_fully_fused_v2.cu:90-745).   */
+/* ======================================================================== */
+namespace {
+
+template <typename R>
+int v2_tick(const oracle_v2_params& P, int n, double* hd, double* hpd, double* gd, double* lwd, double* vd,
+            double* ihd, float yt, float yp, float hmp, float volp, float ksdp, int timestep,
+            double* gmean, double* gvar, double* mustate, const oracle_noise* noise, oracle_v2_out* out) {
+    Noise<R> nz(noise, n);
+    const R y_t = yt, y_prev = yp, h_mean_prev = hmp;
+    const R rho = P.rho, sz = P.sigma_z, mu = P.mu, nu = P.nu;
+    /* phase 0 (:190-267) */
+    R eff_mu = P.use_adaptive_mu ? (R)*mustate : mu;
+    R prev_gm = (R)*gmean, gv = (R)*gvar;
+    if (gv < (R)1e-6) {
+        prev_gm = mu;
+        gv = sz * sz / (1 - rho * rho);
+    }
+    R boost = 1;
+    if (P.use_adaptive_sigma && timestep > 0) {
+        R ve = std::max((R)volp, (R)1e-4);
+        R rz = std::fabs(y_t) / ve;
+        if (rz > (R)P.sigma_boost_threshold) {
+            R sev = std::min((rz - (R)P.sigma_boost_threshold) / 3, (R)1);
+            boost = 1 + ((R)P.sigma_boost_max - 1) * sev;
+        }
+    }
+    const R eff_sigma = sz * boost;
+    R gm, gs;
+    if (P.use_guide) {
+        R m_pred = eff_mu + rho * (prev_gm - eff_mu);
+        R P_pred = rho * rho * gv + sz * sz;
+        R ly2 = std::log(y_t * y_t + (R)1e-8);
+        R obs_offset = -(R)P.student_t_implied_offset;
+        R S = P_pred + (R)(4.93 + 2.0);
+        R K = P_pred / (S + (R)1e-8);
+        R innov = ly2 - (m_pred + obs_offset);
+        gm = m_pred + K * innov;
+        gv = (1 - K) * P_pred;
+        *gmean = (double)gm;
+        *gvar = (double)gv;
+        R ve = std::max((R)volp, (R)1e-4);
+        R rz = std::fabs(y_t) / ve;
+        if (rz > (R)P.guide_innovation_threshold) {
+            R sev = std::min((rz - (R)P.guide_innovation_threshold) / 3, (R)1);
+            gs = (R)P.guide_strength_base + ((R)P.guide_strength_max - (R)P.guide_strength_base) * sev;
+        } else {
+            gs = (R)P.guide_strength_base;
+        }
+    } else {
+        gm = h_mean_prev;
+        gv = 1;
+        gs = 0;
+    }
+    const R inv_s2 = 1 / (eff_sigma * eff_sigma), inv_2s2 = (R)0.5 * inv_s2;
+    /* phase 1: predict (:274-357) */
+    std::vector<R> h(n), muk(n), zd(n), lw(n), g(n), sg(n), sh(n), v(n), ksd_i(n, 0);
+    std::vector<int> kn(n, 4);
+    for (int i = 0; i < n; ++i) {
+        R h_old = (R)hd[i];
+        muk[i] = eff_mu + rho * (h_old - eff_mu) + (R)P.gamma * y_prev / (std::exp(h_old * (R)0.5) + (R)1e-8);
+        R lrho = rho, lsig = eff_sigma;
+        if (P.delta_rho > 0 || P.delta_sigma > 0) {
+            R dev = h_old - h_mean_prev;
+            lrho = std::min(std::max(rho + (R)P.delta_rho * std::tanh(dev), (R)0), (R)0.999);
+            lsig = eff_sigma * (1 + (R)P.delta_sigma * std::fabs(dev));
+        }
+        R lev = 0;
+        if (std::fabs(P.gamma) > 1e-6f) lev = (R)P.gamma * y_prev / (std::exp(h_old * (R)0.5) + (R)1e-8);
+        R prior = eff_mu + lrho * (h_old - eff_mu) + lev;
+        R z_state = nz.normal(i, 0);
+        zd[i] = nz.normal(i, 1);
+        R jump = nz.uniform(i, 0) < (R)P.mim_jump_prob ? (R)1 : (R)0;
+        R msig = lsig * (1 + jump * ((R)P.mim_jump_scale - 1));
+        R hi;
+        if (P.use_guided_predict) {
+            R ly2 = std::log(y_t * y_t + (R)1e-10);
+            R implied = std::max(ly2 + (R)P.student_t_implied_offset, (R)-5);
+            R zs = (implied - prior) / (R)2.5;
+            R act = zs > (R)P.guided_innovation_thresh_predict ? std::tanh(zs - (R)P.guided_innovation_thresh_predict) : (R)0;
+            R alpha = (R)P.guided_alpha_base + ((R)P.guided_alpha_shock - (R)P.guided_alpha_base) * act;
+            hi = (1 - alpha) * prior + alpha * implied + msig * z_state;
+        } else {
+            hi = prior + msig * z_state;
+        }
+        hpd[i] = (double)h_old;
+        h[i] = clamp_h(hi);
+    }
+    /* phase 2: guide (:363-378) */
+    if (P.use_guide && gs > 0) {
+        for (int i = 0; i < n; ++i) {
+            R hi = P.use_guide_preserving ? h[i] + gs * (gm - h_mean_prev) : (1 - gs) * h[i] + gs * gm;
+            h[i] = clamp_h(hi);
+        }
+    }
+    /* phase 3: Silverman bandwidth (:384-410) */
+    R sum = 0;
+    for (int i = 0; i < n; ++i) sum += h[i];
+    const R mean = sum / (R)n;
+    R ss = 0;
+    for (int i = 0; i < n; ++i) ss += (h[i] - mean) * (h[i] - mean);
+    const R sd = std::sqrt(std::max(ss / (R)n, (R)1e-6));
+    const R bw = std::min(std::max((R)1.06 * sd * (R)std::pow((double)n, -0.2), (R)0.05), (R)2);
+    const R inv_bw2 = 1 / (bw * bw);
+    /* phase 4: Stein loop (:416-640) */
+    for (int i = 0; i < n; ++i) v[i] = (R)vd[i];
+    const int na = P.n_anneal_steps < 1 ? 1 : P.n_anneal_steps;
+    const int ns = P.n_stein_steps < 1 ? 1 : P.n_stein_steps;
+    const int spa = ns / na, rem = ns - spa * na;
+    const R sign = P.stein_sign_mode == 1 ? (R)1 : (R)-1;
+    const R hess_prior = -inv_s2;
+    const R nu1 = nu + 1;
+    int gstep = 0;
+    for (int ai = 0; ai < na; ++ai) {
+        R beta;
+        if (na <= 1) beta = 1;
+        else if (ai == na - 1) beta = 1;
+        else beta = (R)0.3 + ((R)ai / (R)(na - 1)) * (R)0.5;
+        const int si = spa + (ai == na - 1 ? rem : 0);
+        for (int s = 0; s < si; ++s) {
+            ++gstep;
+            const bool last = gstep == ns;
+            for (int i = 0; i < n; ++i) {
+                const R hi = h[i];
+                R lmax = (R)-1e10;
+                for (int k = 0; k < n; ++k) { R d = hi - muk[k]; lmax = std::max(lmax, -d * d * inv_2s2); }
+                R sr = 0, wg = 0;
+                for (int k = 0; k < n; ++k) {
+                    R d = hi - muk[k];
+                    R r = std::exp(-d * d * inv_2s2 - lmax);
+                    sr += r;
+                    wg -= r * d * inv_s2;
+                }
+                R gp = std::min(std::max(wg / (sr + (R)1e-8), (R)-10), (R)10);
+                R vol = std::exp(hi * (R)0.5);
+                R A = y_t * y_t / (vol * vol + (R)1e-8) / nu;
+                R opA = 1 + A;
+                lw[i] = (R)P.student_t_const - (R)0.5 * hi - (R)0.5 * nu1 * std::log(opA);
+                R gl = (R)-0.5 + (R)0.5 * nu1 * A / opA - (R)P.lik_offset;
+                R gg = std::min(std::max(gp + beta * gl, (R)-10), (R)10);
+                g[i] = gg;
+                R hl = (R)-0.5 * nu1 * A / (opA * opA);
+                R curv = std::min(std::max(-(hl + hess_prior), (R)0.1), (R)100);
+                R invH = 1 / curv;
+                if (P.use_newton || P.use_full_newton) ihd[i] = (double)curv;
+                if (P.use_full_newton) { sg[i] = gg; sh[i] = curv; }
+                else if (P.use_newton) { sg[i] = (R)0.7 * gg * invH; sh[i] = invH; }
+                else { sg[i] = gg; sh[i] = 1; }
+            }
+            std::vector<R> hn(n);
+            const R es = (R)P.step_size * std::sqrt(beta);
+            for (int i = 0; i < n; ++i) {
+                const R hi = h[i];
+                R ks = 0, gk = 0, Hw = 0, Ks = 0, kq = 0;
+                for (int j = 0; j < n; ++j) {
+                    R diff = hi - h[j];
+                    R dist2 = diff * diff * inv_bw2;
+                    R K = 1 / (1 + dist2), K2 = K * K;
+                    ks += K * sg[j];
+                    if (P.use_newton) gk += sign * 2 * diff * inv_bw2 * K2 * sh[j];
+                    else gk += sign * 2 * diff * inv_bw2 * K2;
+                    if (P.use_full_newton) {
+                        Hw += sh[j] * K;
+                        Hw += 2 * inv_bw2 * K2 * std::fabs(3 * dist2 - 1);
+                        Ks += K;
+                    }
+                    if (last) {
+                        R raw_i = g[i];
+                        R raw_j = P.use_newton ? sg[j] / ((R)0.7 * sh[j] + (R)1e-8) : sg[j];
+                        R gxk = -2 * diff * inv_bw2 * K2;
+                        R hxy = 2 * inv_bw2 * K2 * (4 * dist2 * K - 1);
+                        kq += K * raw_i * raw_j + raw_i * (-gxk) + raw_j * gxk + hxy;
+                    }
+                }
+                R phi;
+                if (P.use_full_newton) {
+                    R H = std::min(std::max(Hw / std::max(Ks, (R)1e-6), (R)0.1), (R)100);
+                    phi = (ks + gk) / (R)n / H * (R)0.7;
+                } else {
+                    phi = (ks + gk) / (R)n;
+                }
+                R vn = (R)P.rmsprop_rho * v[i] + (1 - (R)P.rmsprop_rho) * phi * phi;
+                v[i] = vn;
+                R drift = es * phi / std::sqrt(vn + (R)P.rmsprop_eps);
+                R diffu = 0;
+                if (P.temperature > 1e-6f) {
+                    diffu = std::sqrt(2 * es * (R)P.temperature) * zd[i];
+                    zd[i] = nz.normal(i, kn[i]++);
+                }
+                hn[i] = clamp_h(hi + drift + diffu);
+                if (last) ksd_i[i] = kq;
+            }
+            h.swap(hn);
+        }
+    }
+    /* phase 5: rejuvenation (:646-658) */
+    if (P.use_rejuvenation && ksdp > P.rejuv_ksd_threshold && timestep > 10) {
+        for (int i = 0; i < n; ++i) {
+            R u = nz.uniform(i, 1);
+            if (u < (R)P.rejuv_prob) {
+                R gstd = std::sqrt(std::max(gv, (R)1e-6));
+                R target = gm + gstd * nz.normal(i, kn[i]++);
+                h[i] = clamp_h((1 - (R)P.rejuv_blend) * h[i] + (R)P.rejuv_blend * target);
+            }
+        }
+    }
+    /* phase 6: outputs (:664-706) */
+    R ks2 = 0, sh_ = 0, sv = 0, mx = (R)-1e10;
+    for (int i = 0; i < n; ++i) {
+        ks2 += ksd_i[i];
+        sh_ += h[i];
+        sv += std::exp(h[i] * (R)0.5);
+        mx = std::max(mx, lw[i]);
+    }
+    R sw = 0;
+    for (int i = 0; i < n; ++i) sw += std::exp(lw[i] - mx);
+    const R hm = sh_ / (R)n;
+    out->ksd = (float)std::sqrt(std::max(ks2 / (R)n / (R)n, (R)0));
+    out->h_mean = (float)hm;
+    out->vol = (float)(sv / (R)n);
+    out->loglik = (float)(mx + std::log(std::max(sw, (R)1e-10) / (R)n));
+    out->bandwidth = (float)bw;
+    if (P.use_adaptive_mu && timestep > 10) {
+        R mo = (R)*mustate;
+        R mn = (R)P.mu_ema_alpha * hm + (1 - (R)P.mu_ema_alpha) * mo;
+        *mustate = (double)std::min(std::max(mn, (R)-10), (R)0);
+    }
+    for (int i = 0; i < n; ++i) {
+        hd[i] = (double)h[i];
+        gd[i] = (double)g[i];
+        lwd[i] = (double)lw[i];
+        vd[i] = (double)v[i];
+    }
+    return nz.bad ? -3 : 0;
+}
+
+}  // namespace
+
+extern "C" int svpf_oracle_v2_tick(const oracle_v2_params* p, int n, double* h, double* h_prev, double* grad,
+                                   double* lw, double* v, double* inv_hess, float y_t, float y_prev,
+                                   float h_mean_prev, float vol_prev, float ksd_prev, int timestep,
+                                   double* guide_mean, double* guide_var, double* mu_state,
+                                   const oracle_noise* noise, oracle_v2_out* out, int precision) {
+    if (n < 1) return -1;
+    if (precision == 1)
+        return v2_tick<float>(*p, n, h, h_prev, grad, lw, v, inv_hess, y_t, y_prev, h_mean_prev, vol_prev,
+                              ksd_prev, timestep, guide_mean, guide_var, mu_state, noise, out);
+    return v2_tick<double>(*p, n, h, h_prev, grad, lw, v, inv_hess, y_t, y_prev, h_mean_prev, vol_prev,
+                           ksd_prev, timestep, guide_mean, guide_var, mu_state, noise, out);
+}

@@ -169,6 +169,41 @@ typedef struct {
  * success, a negative code on bad arguments or when the tape runs short.
  * With use_two_factor, h / h_prev / v hold 2n values: the fast factor then
  * the slow factor. */
+/* ---- svpf_fully_fused_step_v2 (include/svpf_fully_fused_v2.cuh:43-119) ----- */
+typedef struct {
+    float rho, sigma_z, mu, nu, lik_offset, student_t_const, student_t_implied_offset, gamma;
+    float delta_rho, delta_sigma;
+    float mim_jump_prob, mim_jump_scale;
+    float guide_strength_base, guide_strength_max, guide_innovation_threshold;
+    float guided_alpha_base, guided_alpha_shock, guided_innovation_thresh_predict;
+    int   use_guide, use_guided_predict, use_guide_preserving;
+    int   use_newton, use_full_newton;
+    int   use_rejuvenation;
+    float rejuv_ksd_threshold, rejuv_prob, rejuv_blend;
+    int   use_adaptive_mu;
+    float mu_ema_alpha;
+    int   use_adaptive_sigma;
+    float sigma_boost_threshold, sigma_boost_max;
+    float step_size, temperature, rmsprop_rho, rmsprop_eps;
+    int   n_stein_steps, n_anneal_steps, stein_sign_mode;
+} oracle_v2_params;
+
+typedef struct {
+    float h_mean, vol, loglik, bandwidth, ksd;
+} oracle_v2_out;
+
+/* One svpf_fully_fused_step_v2 call (src/svpf_fully_fused_v2.cu:90-745).
+ * Arrays [n] (grad, lw, inv_hess: last Stein iteration's values); guide_mean,
+ * guide_var and mu_state are the device scalars it reads and writes.  Noise
+ * slots per particle: normals 0..3 from the curand_normal4 draw (0 state, 1
+ * first diffusion), then one normal per Stein iteration with SVLD
+ * (refresh), then the rejuvenation normal; uniforms 0 (MIM), 1 (rejuvenation). */
+int svpf_oracle_v2_tick(const oracle_v2_params* p, int n, double* h, double* h_prev, double* grad,
+                        double* lw, double* v, double* inv_hess, float y_t, float y_prev,
+                        float h_mean_prev, float vol_prev, float ksd_prev, int timestep,
+                        double* guide_mean, double* guide_var, double* mu_state,
+                        const oracle_noise* noise, oracle_v2_out* out, int precision);
+
 int svpf_oracle_tick(const oracle_config* cfg, const oracle_params* p,
                      oracle_ctl* ctl, int n,
                      double* h, double* h_prev, double* v, double* log_w,

@@ -124,3 +124,41 @@ def normal_slots(case) -> int:
     if cfg.get("use_student_t_state", 0) and cfg.get("nu_state", 5.0) <= 30.0:
         pred = 1 + max(int(cfg.get("nu_state", 5.0) + 0.5), 3)
     return pred + max_steps + 1
+
+
+# ---- svpf_fully_fused_step_v2 cases (include/svpf_fully_fused_v2.cuh:43-119) ----
+# V2_REFERENCE_TEST is the parameter set of the reference's own v2 test
+# (test/test_fully_fused_v2.cu:60-110), with nu = 5 and its constants.
+V2_REFERENCE_TEST = dict(rho=0.98, sigma_z=0.10, mu=-4.5, nu=5.0, lik_offset=0.345, gamma=0.0, delta_rho=0.0,
+                         delta_sigma=0.0, mim_jump_prob=0.25, mim_jump_scale=9.0, guide_strength_base=0.05,
+                         guide_strength_max=0.30, guide_innovation_threshold=1.0, guided_alpha_base=0.0,
+                         guided_alpha_shock=0.40, guided_innovation_thresh_predict=1.5, use_guide=1,
+                         use_guided_predict=1, use_guide_preserving=1, use_newton=1, use_full_newton=1,
+                         use_rejuvenation=1, rejuv_ksd_threshold=0.05, rejuv_prob=0.30, rejuv_blend=0.30,
+                         use_adaptive_mu=0, mu_ema_alpha=0.01, use_adaptive_sigma=1, sigma_boost_threshold=0.95,
+                         sigma_boost_max=3.2, step_size=0.25, temperature=0.45, rmsprop_rho=0.9, rmsprop_eps=1e-6,
+                         n_stein_steps=10, n_anneal_steps=5, stein_sign_mode=0)
+
+V2_CASES = {
+    "v2_reference_test_n512": dict(n=512, p=V2_REFERENCE_TEST, path=(-4.5, 0.98, 0.10), ticks=14),
+    "v2_vanilla_local_n256": dict(n=256, p=dict(V2_REFERENCE_TEST, use_newton=0, use_full_newton=0,
+                                                use_guided_predict=0, use_rejuvenation=0, temperature=0.0,
+                                                use_adaptive_mu=1, mu_ema_alpha=0.05, delta_rho=0.02,
+                                                delta_sigma=0.1, gamma=-0.3, stein_sign_mode=1, n_stein_steps=6,
+                                                n_anneal_steps=2, mu=-1.0, rho=0.97, sigma_z=0.15, nu=12.0,
+                                                step_size=0.1),
+                                  path=(-1.0, 0.97, 0.15), ticks=14),
+    "v2_newton_blend_n300": dict(n=300, p=dict(V2_REFERENCE_TEST, use_newton=1, use_full_newton=0,
+                                               use_guide_preserving=0, rejuv_ksd_threshold=0.0, n_stein_steps=7,
+                                               n_anneal_steps=3, mu=-2.0, rho=0.95, sigma_z=0.2, nu=8.0),
+                                 path=(-2.0, 0.95, 0.2), ticks=14),
+    "v2_full_newton_noguide_n128": dict(n=128, p=dict(V2_REFERENCE_TEST, use_newton=0, use_full_newton=1,
+                                                      use_guide=0, temperature=1.0, n_stein_steps=5,
+                                                      n_anneal_steps=1, mu=-1.5, rho=0.97, sigma_z=0.15, nu=30.0),
+                                        path=(-1.5, 0.97, 0.15), ticks=14),
+}
+
+
+def v2_normal_slots(case) -> int:
+    """curand_normal4 (4) + one refresh per Stein step + the rejuvenation normal."""
+    return 4 + max(case["p"]["n_stein_steps"], 1) + 1

@@ -16,6 +16,15 @@ pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
+def results_dir() -> str:
+    """Where the measured comparisons are written: $SVPF_RESULTS_DIR, else a
+    results folder under the system temporary directory."""
+    import tempfile
+    d = os.environ.get("SVPF_RESULTS_DIR") or os.path.join(tempfile.gettempdir(), "svpf_results")
+    os.makedirs(d, exist_ok=True)
+    return d
+
+
 def _ref_stock():
     import oracle
     return oracle, oracle.RefLib("stock")
@@ -88,9 +97,7 @@ def test_rmse_matches_reference_cuda_step(pkg, n):
                              "ours_p99_us": float(np.percentile(lat_ours[w:], 99))})
     res["rmse_ref"] = float(np.mean(r_ref))
     res["rmse_ours"] = float(np.mean(r_ours))
-    out_dir = os.path.join(ROOT, "gpurun_out")
-    os.makedirs(out_dir, exist_ok=True)
-    with open(os.path.join(out_dir, f"reference_compare_n{n}.json"), "w") as fh:
+    with open(os.path.join(results_dir(), f"reference_compare_n{n}.json"), "w") as fh:
         json.dump(res, fh, indent=1)
     assert abs(res["rmse_ours"] - res["rmse_ref"]) <= 0.02 * res["rmse_ref"], res
 
@@ -99,7 +106,7 @@ def test_reference_plain_step_loop_on_batched_workload(pkg):
     """The reference's svpf_step_graph looped over a sample of the batched
     workload (own theta and N per filter, production configuration), the way
     test/profile_svpf.cu:687-790 loops instruments; the engine's own plain
-    step over the same filters beside it.  Rates go to gpurun_out."""
+    step over the same filters beside it.  Rates go to the results folder."""
     import ctypes as C
     import sys
     import time
@@ -154,7 +161,50 @@ def test_reference_plain_step_loop_on_batched_workload(pkg):
     out = {"filters": F, "ticks": 4, "reference_plain_loop_filter_ticks_per_s": ref_rate,
            "engine_plain_loop_filter_ticks_per_s": our_rate,
            "sample": "first 32 filters of the batched workload (bench.make_workload seed 0)"}
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    with open(os.path.join(ROOT, "gpurun_out", "reference_plain_loop.json"), "w") as fh:
+    with open(os.path.join(results_dir(), "reference_plain_loop.json"), "w") as fh:
         json.dump(out, fh, indent=1)
     assert ref_rate > 0 and our_rate > 0
+
+
+def test_v2_latency_vs_reference_kernel(pkg, oracle_mod):
+    """svpf_fully_fused_step_v2: the engine's cluster kernel and the
+    reference's single-block kernel (unmodified build, its own cuRAND), both
+    timed with CUDA events around each call, N = 512 and 1024 (the reference's
+    limit), the reference test's parameters."""
+    import torch
+    from test_oracle_v2 import v2_params
+    _, reflib = _ref_stock()
+    params = v2_params(oracle_mod, cases.V2_REFERENCE_TEST)
+    res = {}
+    for n in (512, 1024):
+        T = 200
+        _, ys = tape.sv_path(T, -4.5, 0.98, 0.10, seed=11)
+        ref_us = np.zeros(T, np.float32)
+        import ctypes as C
+        rc = reflib.L.svpf_ref_v2_time(C.byref(params), n, ys.ctypes.data_as(C.POINTER(C.c_float)), T,
+                                       ref_us.ctypes.data_as(C.POINTER(C.c_float)))
+        assert rc == 0
+        f = pkg.FusedV2(n, seed=3)
+        f.set("h", np.clip(-4.5 + 0.3 * tape.init_normals(2, n), -15, 5))
+        f.set("mu_state", -4.5)
+        ours = []
+        hmp, volp, ksdp, yp = -4.5, float(np.exp(-2.25)), 0.1, 0.0
+        pd = params.to_dict()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for t in range(T):
+            e0.record()
+            rc = f.step(pd, ys[t], yp, hmp, volp, ksdp, t, stream=torch.cuda.current_stream().cuda_stream)
+            e1.record()
+            e1.synchronize()
+            assert rc == 0
+            ours.append(e0.elapsed_time(e1) * 1000.0)
+            hmp, volp, ksdp, yp = f.get("h_mean"), f.get("vol"), f.get("ksd"), float(ys[t])
+        f.close()
+        ours = np.sort(np.array(ours[20:]))
+        ref = np.sort(ref_us[20:])
+        res[str(n)] = {"engine_p50_us": float(ours[len(ours) // 2]), "engine_p99_us": float(ours[int(len(ours) * .99)]),
+                       "reference_p50_us": float(ref[len(ref) // 2]),
+                       "reference_p99_us": float(ref[int(len(ref) * .99)])}
+        assert np.all(np.isfinite(ref)) and ours[0] > 0
+    with open(os.path.join(results_dir(), "v2_latency.json"), "w") as fh:
+        json.dump(res, fh, indent=1)

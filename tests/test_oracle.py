@@ -52,7 +52,12 @@ def test_fp32_mirror_tracks_fp64(oracle_mod, name):
 
 
 def _fixtures():
-    return sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+    """Fixtures of the svpf_step_graph path (the v2 entry point's start with v2_)."""
+    return sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz")) if not os.path.basename(p).startswith("v2_"))
+
+
+def _v2_fixtures():
+    return sorted(glob.glob(os.path.join(GOLDEN, "v2_*.npz")))
 
 
 def test_fixtures_present():
