@@ -379,6 +379,65 @@ def stream_workload(pkg, n_instruments: int = 10000, budget_bytes: int = 512 << 
     }
 
 
+def profile_case(pkg, name: str):
+    """Small fixed cases of the secondary kernels for profiler captures (no
+    timing, no output): `grad` -- value and adjoint of 64 filters, N = 512,
+    64 ticks; `stream` -- one request-loop round over 296 two-factor
+    instruments of N = 1024 / 2048 (the cluster kernel); `v2` -- 20
+    svpf_fully_fused_step_v2 calls at N = 512."""
+    import torch
+    if name == "grad":
+        F, N, T = 64, 512, 64
+        rng = np.random.default_rng(0)
+        th = np.stack([rng.uniform(-2, 0, F), rng.uniform(0.9, 0.99, F), rng.uniform(0.1, 0.3, F),
+                       rng.uniform(5, 20, F)], 1).astype(np.float32)
+        ys = sv_paths(T, th[:, 1].astype(np.float64), th[:, 2].astype(np.float64), th[:, 0].astype(np.float64),
+                      th[:, 3].astype(np.float64), seed=1).T.copy()
+        g = pkg.Grad([N] * F, pkg.grad_config(MAX_STEPS, 12.0), T_max=T, checkpoint_every=64)
+        g.forward(th, ys, seed=1)
+        g.backward()
+        g.close()
+    elif name == "stream":
+        F = 296
+        ns = np.where(np.arange(F) % 2 == 0, 2048, 1024)
+        c = pkg.default_config(8, 6.0)
+        c.update(use_two_factor=1, rho_fast=0.80, sigma_fast=0.30, rho_slow=0.995, sigma_slow=0.05,
+                 use_svld=1, use_annealing=1, n_anneal_steps=5, temperature=0.45, use_mim=1, mim_jump_prob=0.25,
+                 mim_jump_scale=9.0, use_guide=1, use_guide_preserving=1, guide_strength=0.12, use_exact_gradient=1)
+        st = pkg.Stream(F, 256 << 20, 2048, seed=1)
+        for f in range(F):
+            st.admit(int(ns[f]), c, pkg.Params(0.995, 0.05, -3.5, 0.0), seed=1)
+        st.process(np.arange(F), np.full(F, 0.01, np.float32))
+        st.close()
+    elif name == "v2":
+        n = 512
+        nu = 5.0
+        cfg = pkg.default_config(8, nu)
+        import math
+        stc = math.lgamma((nu + 1) / 2) - math.lgamma(nu / 2) - 0.5 * math.log(math.pi * nu)
+        # the reference's own v2 test parameters (test/test_fully_fused_v2.cu:60-110)
+        pd = dict(rho=0.98, sigma_z=0.10, mu=-4.5, nu=nu, lik_offset=0.345, student_t_const=stc,
+                  student_t_implied_offset=cfg.student_t_implied_offset, gamma=0.0, delta_rho=0.0,
+                  delta_sigma=0.0, mim_jump_prob=0.25, mim_jump_scale=9.0, guide_strength_base=0.05,
+                  guide_strength_max=0.30, guide_innovation_threshold=1.0, guided_alpha_base=0.0,
+                  guided_alpha_shock=0.40, guided_innovation_thresh_predict=1.5, use_guide=1, use_guided_predict=1,
+                  use_guide_preserving=1, use_newton=1, use_full_newton=1, use_rejuvenation=1,
+                  rejuv_ksd_threshold=0.05, rejuv_prob=0.30, rejuv_blend=0.30, use_adaptive_mu=0, mu_ema_alpha=0.01,
+                  use_adaptive_sigma=1, sigma_boost_threshold=0.95, sigma_boost_max=3.2, step_size=0.25,
+                  temperature=0.45, rmsprop_rho=0.9, rmsprop_eps=1e-6, n_stein_steps=10, n_anneal_steps=5,
+                  stein_sign_mode=0)
+        f = pkg.FusedV2(n, seed=2)
+        f.set("h", np.clip(-4.5 + 0.3 * np.random.default_rng(2).standard_normal(n), -15, 5))
+        f.set("mu_state", -4.5)
+        for t in range(20):
+            if f.step(pd, 0.01, 0.0, -4.5, 0.1, 0.1, t) != 0:
+                raise RuntimeError("v2 step failed")
+        f.close()
+    else:
+        raise SystemExit(f"unknown profile case {name!r}")
+    torch.cuda.synchronize()
+
+
 def workload_config(F: int):
     return {"workload": f"batched SVPF tick: {F} filters per GPU, own theta, N ~ U{{256,512,1024,2048,4096}}, "
                         f"production config (full Newton, <= {MAX_STEPS} Stein iterations, 3 stages)",
@@ -397,6 +456,8 @@ def main():
     ap.add_argument("--latency-ticks", type=int, default=400)
     ap.add_argument("--no-gradient", action="store_true", help="skip the differentiation workload")
     ap.add_argument("--no-stream", action="store_true", help="skip the two-factor request loop")
+    ap.add_argument("--profile-case", choices=["grad", "stream", "v2"],
+                    help="run one small case of a secondary kernel for a profiler and exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -406,6 +467,10 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.profile_case:
+        import __graft_entry__ as ge
+        profile_case(ge.load_package(), args.profile_case)
         return
 
     import torch
