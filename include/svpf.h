@@ -561,6 +561,52 @@ void svpf_fully_fused_v2_rng_destroy(svpf_v2_rng_t* rng);
 int svpf_fully_fused_v2_rng_get(const svpf_v2_rng_t* rng, svpf_v2_rng_t* host);
 int svpf_fully_fused_v2_rng_set(svpf_v2_rng_t* rng, const svpf_v2_rng_t* host);
 
+/* ---- multiscale composition on the batch engine --------------------------
+ * The reference's two-scale filter (include/svpf_multiscale.cuh: a REACTIVE
+ * scout and an INERTIAL production filter per instrument, combined per tick)
+ * for many instruments at once: the 2F filters of F instruments form one batch
+ * stepped by one launch per tick (the reference steps two svpf_step_adaptive
+ * calls per instrument).  Configuration, per-scale knobs, output fields and
+ * their combination follow ms_svpf_default_config / ms_svpf_create /
+ * ms_svpf_step (:145-536); field names are the reference's. */
+typedef struct {
+    int   n_particles_reactive, n_particles_inertial;
+    int   n_stein_reactive, n_stein_inertial;
+    float surprise_mild_threshold, surprise_high_threshold;
+    float boost_mild_factor, boost_high_factor;
+    float weight_reactive, weight_inertial;
+} svpf_ms_config_t;
+
+typedef struct {
+    float vol_reactive, vol_inertial, h_reactive, h_inertial, loglik_reactive, loglik_inertial;
+    float vol_combined, h_combined, loglik_combined;
+    float transient_magnitude, transient_ratio;
+    float ksd_reactive, ksd_inertial;
+    int   stein_steps_reactive, stein_steps_inertial;
+    float surprise_reactive;
+    int   cross_scale_boost;
+    float mim_prob_inertial_used;
+    int   is_transient, is_regime_shift, is_calm;
+} svpf_ms_output_t;
+
+typedef struct svpf_ms_batch svpf_ms_batch_t;
+
+svpf_ms_config_t svpf_ms_default_config(void);
+/* base_params[F]: each instrument's model (the INERTIAL scale uses it as is,
+ * the REACTIVE scale with rho 0.92, sigma_z 0.18). */
+svpf_ms_batch_t* svpf_ms_batch_create(int n_instruments, const svpf_ms_config_t* cfg,
+                                      const SVPFParams* base_params, cudaStream_t stream);
+void svpf_ms_batch_destroy(svpf_ms_batch_t* b);
+int svpf_ms_batch_init(svpf_ms_batch_t* b, float initial_vol, unsigned long long seed);
+/* y[F]: this tick's observation of every instrument; out[F]. */
+int svpf_ms_batch_step(svpf_ms_batch_t* b, const float* y, svpf_ms_output_t* out);
+/* The per-filter outputs of the last svpf_batch_step of a batch ([n_filters]). */
+int svpf_batch_last_outputs(const svpf_batch_t* b, svpf_out_t* out);
+/* Configuration of filter f of a batch. */
+int svpf_batch_get_config(const svpf_batch_t* b, int f, svpf_config_t* cfg);
+/* The batch holding the 2F filters (REACTIVE i, INERTIAL F + i). */
+svpf_batch_t* svpf_ms_batch_inner(svpf_ms_batch_t* b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -424,6 +424,18 @@ int svpf_batch_sync(svpf_batch_t* b) {
 }
 
 int svpf_batch_n_filters(const svpf_batch_t* b) { return b ? b->F : 0; }
+
+int svpf_batch_get_config(const svpf_batch_t* b, int f, svpf_config_t* cfg) {
+    if (!b || !cfg || f < 0 || f >= b->F) return SVPF_ERR_INVALID_ARG;
+    *cfg = b->cfgs[f];
+    return SVPF_OK;
+}
+
+int svpf_batch_last_outputs(const svpf_batch_t* b, svpf_out_t* out) {
+    if (!b || !out) return SVPF_ERR_INVALID_ARG;
+    std::memcpy(out, b->h_out, (size_t)b->F * sizeof(svpf_out_t));   // filled by svpf_batch_step
+    return SVPF_OK;
+}
 int svpf_batch_kernel_launches(const svpf_batch_t* b) { return b ? b->launches : 0; }
 
 int svpf_batch_get_ctl(const svpf_batch_t* b, svpf_ctl_t* ctl) {

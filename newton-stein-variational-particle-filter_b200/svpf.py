@@ -95,6 +95,22 @@ _FP = C.POINTER(C.c_float)
 _lib = None
 
 
+class MSConfig(C.Structure):
+    _fields_ = [("n_particles_reactive", _I), ("n_particles_inertial", _I), ("n_stein_reactive", _I),
+                ("n_stein_inertial", _I), ("surprise_mild_threshold", _F), ("surprise_high_threshold", _F),
+                ("boost_mild_factor", _F), ("boost_high_factor", _F), ("weight_reactive", _F),
+                ("weight_inertial", _F)]
+
+
+class MSOutput(C.Structure):
+    _fields_ = [(k, _F) for k in ("vol_reactive", "vol_inertial", "h_reactive", "h_inertial", "loglik_reactive",
+                                  "loglik_inertial", "vol_combined", "h_combined", "loglik_combined",
+                                  "transient_magnitude", "transient_ratio", "ksd_reactive", "ksd_inertial")] + \
+                [("stein_steps_reactive", _I), ("stein_steps_inertial", _I), ("surprise_reactive", _F),
+                 ("cross_scale_boost", _I), ("mim_prob_inertial_used", _F), ("is_transient", _I),
+                 ("is_regime_shift", _I), ("is_calm", _I)]
+
+
 def lib() -> C.CDLL:
     """The engine library.  Raises if it is missing: there is no fallback."""
     global _lib
@@ -166,6 +182,14 @@ def lib() -> C.CDLL:
         "svpf_stream_get_particles": (_I, [vp, _I, _FP]),
         "svpf_stream_kernel_launches": (C.c_longlong, [vp]),
         "svpf_fully_fused_v2_supported": (C.c_bool, [_I]),
+        "svpf_ms_default_config": (MSConfig, []),
+        "svpf_ms_batch_create": (vp, [_I, C.POINTER(MSConfig), C.POINTER(Params), vp]),
+        "svpf_ms_batch_destroy": (None, [vp]),
+        "svpf_ms_batch_init": (_I, [vp, _F, C.c_ulonglong]),
+        "svpf_ms_batch_step": (_I, [vp, _FP, C.POINTER(MSOutput)]),
+        "svpf_ms_batch_inner": (vp, [vp]),
+        "svpf_batch_last_outputs": (_I, [vp, C.POINTER(Out)]),
+        "svpf_batch_get_config": (_I, [vp, _I, C.POINTER(Config)]),
         "svpf_fully_fused_step_v2": (_I, [vp] * 7 + [_F] * 5 + [vp] * 7 + [_F] * 18 + [_I] * 6 + [_F] * 3 +
                                      [_I, vp, _F, _I] + [_F] * 6 + [_I] * 5 + [vp]),
         "svpf_fully_fused_v2_rng_create": (vp, [C.c_ulonglong, C.c_uint]),
@@ -734,6 +758,57 @@ class Stream:
         if rc != SVPF_OK:
             raise RuntimeError(f"get_particles rc={rc}")
         return out
+
+
+class MultiScale:
+    """The reference's two-scale filter (REACTIVE + INERTIAL per instrument,
+    include/svpf_multiscale.cuh) for F instruments on one batch
+    (svpf_ms_batch_* in the C ABI)."""
+
+    def __init__(self, base_params, config=None, stream=None):
+        F = len(base_params)
+        self._prms = (Params * F)(*base_params)
+        cfg = config if config is not None else lib().svpf_ms_default_config()
+        self.config = cfg
+        self._m = lib().svpf_ms_batch_create(F, C.byref(cfg), self._prms, stream)
+        if not self._m:
+            raise RuntimeError("svpf_ms_batch_create failed")
+        self.F = F
+
+    def close(self):
+        if getattr(self, "_m", None):
+            lib().svpf_ms_batch_destroy(self._m)
+            self._m = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init(self, initial_vol: float, seed: int = 0):
+        rc = lib().svpf_ms_batch_init(self._m, float(initial_vol), int(seed))
+        if rc != SVPF_OK:
+            raise RuntimeError(f"ms init rc={rc}")
+
+    def step(self, y):
+        yy = _f32(y)
+        out = (MSOutput * self.F)()
+        rc = lib().svpf_ms_batch_step(self._m, _fp(yy), out)
+        if rc != SVPF_OK:
+            raise RuntimeError(f"ms step rc={rc}")
+        return out
+
+    def inner_outputs(self):
+        b = lib().svpf_ms_batch_inner(self._m)
+        out = (Out * (2 * self.F))()
+        lib().svpf_batch_last_outputs(b, out)
+        return out
+
+    def inner_config(self, f: int) -> Config:
+        c = Config()
+        lib().svpf_batch_get_config(lib().svpf_ms_batch_inner(self._m), int(f), C.byref(c))
+        return c
 
 
 class V2Rng(C.Structure):
