@@ -607,6 +607,39 @@ int svpf_batch_get_config(const svpf_batch_t* b, int f, svpf_config_t* cfg);
 /* The batch holding the 2F filters (REACTIVE i, INERTIAL F + i). */
 svpf_batch_t* svpf_ms_batch_inner(svpf_ms_batch_t* b);
 
+/* ---- the reference's differentiable torch model --------------------------- */
+/* SVPFParamEstimator (py-torch/diff_svpf_torch.py:147-217), which the reference
+ * differentiates with torch autograd, as a batched CUDA forward and adjoint:
+ * F paths of N particles (N even), Gaussian AR(1) prior score per particle,
+ * IMQ^(-1/2) kernel, n_stein fixed Stein steps of size stein_lr, antithetic
+ * predict noise, the predictive log-likelihood before the transport, and the
+ * particle path cut every truncate_every ticks (0: never).  The engine has no
+ * reference C counterpart; it replaces the torch model's forward/backward.
+ * stream NULL: the engine makes its own stream; cudaStreamLegacy names the
+ * legacy default stream. */
+typedef struct svpf_estimator svpf_estimator_t;
+svpf_estimator_t* svpf_estimator_create(int n_paths, int n_particles, int n_stein_steps, float stein_lr,
+                                        int T_max, int checkpoint_every, int truncate_every, cudaStream_t stream);
+void svpf_estimator_destroy(svpf_estimator_t* e);
+/* Floats of one path's noise tape: n initial normals, then n/2 per tick. */
+long long svpf_estimator_tape_floats(int n_particles, int T);
+/* theta[F][4] = (mu, rho, sigma_z, nu), y[F][T] (host).  tape[F][tape_floats]
+ * (host) replays given normals (the torch model's torch.randn draws); NULL
+ * draws them from the counter-based generator keyed by seed.  Outputs (host,
+ * NULL allowed): loglik[F][T] predictive log-likelihoods, vol[F][T] volatility
+ * estimates (mean e^{h/2} after the transport), loglik_sum[F] (FP64). */
+int svpf_estimator_forward(svpf_estimator_t* e, const float* theta, const float* y, int T, unsigned long long seed,
+                           const float* tape, float* loglik, float* vol, double* loglik_sum);
+/* grad[F][4] = d(sum_t w_t loglik_t)/d theta for w[F][T] (host; NULL: all ones),
+ * under the noise of the last forward.  The reference's loss
+ * -mean(loglik[burn_in:]) is w_t = -1/(T - burn_in) for t >= burn_in. */
+int svpf_estimator_backward(svpf_estimator_t* e, const float* w, double* grad);
+/* Device-pointer variants (stream-ordered, no synchronisation): the arrays
+ * must stay valid until the backward has run. */
+int svpf_estimator_forward_device(svpf_estimator_t* e, const float* d_theta, const float* d_y, int T,
+                                  unsigned long long seed, const float* d_tape, float* d_loglik, float* d_vol);
+int svpf_estimator_backward_device(svpf_estimator_t* e, const float* d_w, double* d_grad);
+
 #ifdef __cplusplus
 }
 #endif

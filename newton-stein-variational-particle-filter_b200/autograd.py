@@ -17,13 +17,19 @@ import torch
 from .svpf import Config, Grad
 
 
+def torch_stream_handle(device=None) -> int:
+    """Handle of torch's current CUDA stream for an engine to launch on.  The
+    legacy default stream has handle 0, which the engines read as "make a
+    private stream"; cudaStreamLegacy (handle 1) names it explicitly."""
+    return torch.cuda.current_stream(device).cuda_stream or 1
+
+
 class GradEngine(Grad):
     """A Grad bound to torch's current CUDA stream, so its launches are
     ordered with the surrounding torch work."""
 
     def __init__(self, ns, configs, T_max: int, checkpoint_every: int = 64):
-        stream = torch.cuda.current_stream().cuda_stream
-        super().__init__(ns, configs, T_max, checkpoint_every, stream=stream)
+        super().__init__(ns, configs, T_max, checkpoint_every, stream=torch_stream_handle())
 
 
 class SVPFLogLik(torch.autograd.Function):

@@ -197,6 +197,13 @@ def lib() -> C.CDLL:
         "svpf_fully_fused_v2_rng_get": (_I, [vp, vp]),
         "svpf_fully_fused_v2_rng_set": (_I, [vp, vp]),
         "svpf_debug_philox": (_I, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), _I]),
+        "svpf_estimator_create": (vp, [_I, _I, _I, _F, _I, _I, _I, vp]),
+        "svpf_estimator_destroy": (None, [vp]),
+        "svpf_estimator_tape_floats": (C.c_longlong, [_I, _I]),
+        "svpf_estimator_forward": (_I, [vp, _FP, _FP, _I, C.c_ulonglong, _FP, _FP, _FP, C.POINTER(C.c_double)]),
+        "svpf_estimator_backward": (_I, [vp, _FP, C.POINTER(C.c_double)]),
+        "svpf_estimator_forward_device": (_I, [vp, vp, vp, _I, C.c_ulonglong, vp, vp, vp]),
+        "svpf_estimator_backward_device": (_I, [vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -909,6 +916,86 @@ class FusedV2:
         rc = lib().svpf_fully_fused_step_v2(*args)
         self.torch.cuda.synchronize()
         return int(rc)
+
+
+class Estimator:
+    """The reference's differentiable torch model (SVPFParamEstimator,
+    py-torch/diff_svpf_torch.py:147-217) for F paths on the GPU
+    (svpf_estimator_* in the C ABI): forward gives the predictive
+    log-likelihood and volatility estimate of every tick, backward
+    d(sum_t w_t loglik_t)/d(mu, rho, sigma_z, nu) by the CUDA adjoint."""
+
+    def __init__(self, n_paths: int, n_particles: int = 64, n_stein_steps: int = 2, stein_lr: float = 0.1,
+                 T_max: int = 1000, checkpoint_every: int = 64, truncate_every: int = 0, stream=None):
+        self._e = lib().svpf_estimator_create(int(n_paths), int(n_particles), int(n_stein_steps), float(stein_lr),
+                                              int(T_max), int(checkpoint_every), int(truncate_every), stream)
+        if not self._e:
+            raise RuntimeError("svpf_estimator_create failed (odd or too many particles, sizes, or device)")
+        self.F = int(n_paths)
+        self.n = int(n_particles)
+        self.T_max = int(T_max)
+        self.T = 0
+        self.forward_id = 0
+
+    def close(self):
+        if getattr(self, "_e", None):
+            lib().svpf_estimator_destroy(self._e)
+            self._e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def tape_floats(n_particles: int, T: int) -> int:
+        return int(lib().svpf_estimator_tape_floats(int(n_particles), int(T)))
+
+    @staticmethod
+    def make_tape(tape_init, tape_ticks) -> np.ndarray:
+        """One path's tape from its initial normals [n] and per-tick halves [T, n/2]."""
+        return np.concatenate([_f32(tape_init).ravel(), _f32(tape_ticks).ravel()])
+
+    def _check(self, rc):
+        if rc != SVPF_OK:
+            raise RuntimeError(f"svpf estimator error {rc}: {ERRORS.get(rc, '?')}")
+
+    def forward(self, theta, y, seed: int = 0, tape=None):
+        """theta [F,4] = (mu, rho, sigma_z, nu), y [F,T]; tape [F, tape_floats]
+        or None.  Returns (loglik [F,T], vol [F,T], loglik_sum [F])."""
+        th = _f32(theta).reshape(self.F, 4)
+        yy = _f32(y).reshape(self.F, -1)
+        T = yy.shape[1]
+        tp = None
+        if tape is not None:
+            tp = _f32(tape).reshape(self.F, self.tape_floats(self.n, T))
+        ll = np.zeros((self.F, T), np.float32)
+        vol = np.zeros((self.F, T), np.float32)
+        ls = np.zeros(self.F, np.float64)
+        self._check(lib().svpf_estimator_forward(self._e, _fp(th), _fp(yy), T, int(seed),
+                                                 _fp(tp) if tp is not None else None, _fp(ll), _fp(vol),
+                                                 ls.ctypes.data_as(C.POINTER(C.c_double))))
+        self.T = T
+        self.forward_id += 1
+        return ll, vol, ls
+
+    def backward(self, w=None):
+        """grad [F,4] (float64) of sum_t w_t loglik_t; w [F,T] or None (ones)."""
+        ww = None if w is None else _f32(w).reshape(self.F, self.T)
+        g = np.zeros((self.F, 4), np.float64)
+        self._check(lib().svpf_estimator_backward(self._e, _fp(ww) if ww is not None else None,
+                                                  g.ctypes.data_as(C.POINTER(C.c_double))))
+        return g
+
+    def forward_device(self, d_theta: int, d_y: int, T: int, seed: int, d_tape, d_loglik: int, d_vol: int):
+        self._check(lib().svpf_estimator_forward_device(self._e, d_theta, d_y, int(T), int(seed), d_tape, d_loglik,
+                                                        d_vol))
+        self.T = int(T)
+        self.forward_id += 1
+
+    def backward_device(self, d_w, d_grad: int):
+        self._check(lib().svpf_estimator_backward_device(self._e, d_w, d_grad))
 
 
 def autotune(ns, ticks: int = 2):

@@ -213,6 +213,9 @@ def lib():
                                            C.c_double, C.POINTER(C.c_float), C.POINTER(C.c_double),
                                            C.c_uint64, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                            C.POINTER(C.c_double)]
+        L.svpf_oracle_estimator_run2.restype = C.c_int
+        L.svpf_oracle_estimator_run2.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int] + [
+            C.POINTER(C.c_float)] * 3 + [C.POINTER(C.c_double), C.c_int] + [C.POINTER(C.c_double)] * 6
         _lib = L
     return _lib
 
@@ -270,6 +273,31 @@ def run_loglik(cfg: OracleConfig, n: int, theta, ys, gamma: float = 0.0, seed: i
         out.append(o.loglik)
         yp = float(y)
     return np.array(out)
+
+
+def estimator_run(n: int, n_stein: int, stein_lr: float, theta, ys, tape_init, tape_ticks,
+                  truncate_every: int = 0, w=None, bw_fixed=None, return_bw: bool = False):
+    """FP64 forward-mode restatement of the reference's differentiable torch
+    model (SVPFParamEstimator.forward, py-torch/diff_svpf_torch.py:147-217)
+    on one path with its noise as a tape.  Returns (loglik[T] predictive,
+    vol[T], grad[4] of sum_t w_t loglik_t w.r.t. (mu, rho, sigma_z, nu)), and
+    the per-tick bandwidths when return_bw; bw_fixed[T] replays bandwidths."""
+    ys = np.ascontiguousarray(ys, np.float32)
+    T = int(ys.shape[0])
+    ti = np.ascontiguousarray(tape_init, np.float32)
+    tt = np.ascontiguousarray(tape_ticks, np.float32)
+    assert ti.shape == (n,) and tt.shape == (T, n // 2)
+    th = np.ascontiguousarray(theta, np.float64)
+    ll, vol, g = np.zeros(T), np.zeros(T), np.zeros(4)
+    wv = None if w is None else np.ascontiguousarray(w, np.float64)
+    bf = None if bw_fixed is None else np.ascontiguousarray(bw_fixed, np.float64)
+    bo = np.zeros(T)
+    rc = lib().svpf_oracle_estimator_run2(n, n_stein, float(stein_lr), T, _fptr(ys), _fptr(ti), _fptr(tt), _dptr(th),
+                                          int(truncate_every), _dptr(wv) if wv is not None else None, _dptr(ll),
+                                          _dptr(vol), _dptr(g), _dptr(bf) if bf is not None else None, _dptr(bo))
+    if rc != 0:
+        raise RuntimeError(f"estimator oracle rc={rc}")
+    return (ll, vol, g, bo) if return_bw else (ll, vol, g)
 
 
 class V2State:

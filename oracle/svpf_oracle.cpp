@@ -1572,3 +1572,116 @@ extern "C" int svpf_oracle_v2_tick(const oracle_v2_params* p, int n, double* h, 
     return v2_tick<double>(*p, n, h, h_prev, grad, lw, v, inv_hess, y_t, y_prev, h_mean_prev, vol_prev,
                            ksd_prev, timestep, guide_mean, guide_var, mu_state, noise, out);
 }
+
+/* ======================================================================== */
+/* The reference's differentiable torch model, SVPFParamEstimator            */
+/* (py-torch/diff_svpf_torch.py:147-217), restated in FP64 with forward-mode */
+/* tangents for (mu, rho, sigma_z, nu):                                      */
+/*   init   h = mu + sigma_z / sqrt(1 - rho^2 + 1e-6) z               (:168-170) */
+/*   tick   h_pred = mu + rho (h - mu) + sigma_z eps, eps antithetic  (:183-189) */
+/*          loglik_t = logsumexp_i log t_nu(y_t; scale e^{h_pred/2}) - log N   */
+/*                     (before the transport, :192-198)                       */
+/*          bw = std(h_pred) + 0.1, no derivative through it          (:201)    */
+/*          n_stein times: g = clamp(prior AR score + lik score, +-10),          */
+/*          h += lr (K g / N + sum_j grad K / N), IMQ^(-1/2)   (:204-211, :127-145) */
+/*   TBPTT  the tangents of h are cut at t % truncate_every == 0, t > 0 (:177-179) */
+/* ======================================================================== */
+namespace {
+
+Dual student_t_const(const Dual& nu) {
+    /* lgamma((nu+1)/2) - lgamma(nu/2) - 0.5 log(nu pi)  (:75-80) */
+    return dlgamma((nu + Dual(1.0)) * Dual(0.5)) - dlgamma(nu * Dual(0.5)) - Dual(0.5) * dlog(nu * Dual(kPi));
+}
+
+}  // namespace
+
+extern "C" int svpf_oracle_estimator_run2(int n, int n_stein, double stein_lr, int T, const float* ys,
+                                          const float* tape_init, const float* tape_ticks, const double* theta,
+                                          int truncate_every, const double* w, double* loglik, double* vol,
+                                          double* grad, const double* bw_fixed, double* bw_out) {
+    if (n < 2 || (n & 1) || n_stein < 0 || T < 0 || !ys || !tape_init || !tape_ticks || !theta) return -1;
+    const Dual mu = Dual::var(theta[0], 0), rho = Dual::var(theta[1], 1), sz = Dual::var(theta[2], 2),
+               nu = Dual::var(theta[3], 3);
+    const Dual C = student_t_const(nu);
+    const int half = n / 2;
+    std::vector<Dual> h(n), hp(n), tm(n), g(n), hn(n), lp(n);
+    /* :168-170 */
+    const Dual hstd = sz / dsqrt(Dual(1.0) - rho * rho + Dual(1e-6));
+    for (int i = 0; i < n; ++i) h[i] = mu + hstd * Dual((double)tape_init[i]);
+    if (grad)
+        for (int k = 0; k < 4; ++k) grad[k] = 0;
+    const Dual s2e = sz * sz + Dual(1e-8);
+    for (int t = 0; t < T; ++t) {
+        if (truncate_every > 0 && t > 0 && t % truncate_every == 0)
+            for (int i = 0; i < n; ++i) h[i] = Dual(h[i].v);   /* h.detach() */
+        const float* e = tape_ticks + (size_t)t * half;
+        const Dual y((double)ys[t]);
+        for (int i = 0; i < n; ++i) {
+            const double eps = i < half ? (double)e[i] : -(double)e[i - half];
+            tm[i] = mu + rho * (h[i] - mu);
+            hp[i] = mu + rho * (h[i] - mu) + sz * Dual(eps);
+        }
+        /* predictive log-likelihood (:192-198, _student_t_log_prob :112-119) */
+        double mx = -1e300;
+        for (int i = 0; i < n; ++i) {
+            const Dual sc = dexp(hp[i] * Dual(0.5));
+            const Dual z = y / (sc + Dual(1e-8));
+            lp[i] = C - dlog(sc + Dual(1e-8)) - (nu + Dual(1.0)) * Dual(0.5) * dlog1p(z * z / nu);
+            mx = std::max(mx, lp[i].v);
+        }
+        Dual se(0.0);
+        for (int i = 0; i < n; ++i) se += dexp(lp[i] - Dual(mx));
+        const Dual ll = Dual(mx) + dlog(se) - Dual(std::log((double)n));
+        if (loglik) loglik[t] = ll.v;
+        const double wt = w ? w[t] : 1.0;
+        if (grad)
+            for (int k = 0; k < 4; ++k) grad[k] += wt * ll.d[k];
+        /* bandwidth of the predicted particles, detached (:201) */
+        double m = 0;
+        for (int i = 0; i < n; ++i) m += hp[i].v;
+        m /= n;
+        double var = 0;
+        for (int i = 0; i < n; ++i) var += (hp[i].v - m) * (hp[i].v - m);
+        const double bw = bw_fixed ? bw_fixed[t] : std::sqrt(var / n) + 0.1;
+        if (bw_out) bw_out[t] = bw;
+        const double b = bw * bw + 1e-8;
+        h = hp;
+        for (int s = 0; s < n_stein; ++s) {
+            for (int i = 0; i < n; ++i) {
+                /* :205-209 */
+                const Dual v = dexp(h[i] * Dual(0.5));
+                const Dual A = y * y / (v * v * nu + Dual(1e-8));
+                const Dual gl = Dual(-0.5) + Dual(0.5) * (nu + Dual(1.0)) * A / (Dual(1.0) + A);
+                const Dual gpr = -(h[i] - tm[i]) / s2e;
+                g[i] = dclamp(gpr + gl, -10, 10);
+            }
+            /* _stein_step / _imq_kernel (:127-145) */
+            for (int i = 0; i < n; ++i) {
+                Dual acc(0.0), rep(0.0);
+                for (int j = 0; j < n; ++j) {
+                    const Dual d = h[i] - h[j];
+                    const Dual base = Dual(1.0) + d * d / Dual(b);
+                    const Dual sq = dsqrt(base);
+                    acc += g[j] / sq;
+                    rep += -d / (Dual(b) * base * sq);
+                }
+                hn[i] = h[i] + Dual(stein_lr) * (acc / Dual((double)n) + rep / Dual((double)n));
+            }
+            h.swap(hn);
+        }
+        if (vol) {
+            double sv = 0;
+            for (int i = 0; i < n; ++i) sv += std::exp(h[i].v * 0.5);
+            vol[t] = sv / n;
+        }
+    }
+    return 0;
+}
+
+extern "C" int svpf_oracle_estimator_run(int n, int n_stein, double stein_lr, int T, const float* ys,
+                                         const float* tape_init, const float* tape_ticks, const double* theta,
+                                         int truncate_every, const double* w, double* loglik, double* vol,
+                                         double* grad) {
+    return svpf_oracle_estimator_run2(n, n_stein, stein_lr, T, ys, tape_init, tape_ticks, theta, truncate_every, w,
+                                      loglik, vol, grad, nullptr, nullptr);
+}

@@ -250,6 +250,28 @@ int svpf_oracle_grad_run2(const oracle_config* cfg, int n, int T, const double* 
                           const float* ys, const double* w, uint64_t seed, int filter_id,
                           double* loglik, double* grad, double* h_final, int objective);
 
+/* ---- the reference's differentiable torch model (forward-mode AD, FP64) --- */
+/* SVPFParamEstimator.forward (py-torch/diff_svpf_torch.py:147-217) for one
+ * path: n particles (even), n_stein Stein steps of size stein_lr, T ticks of
+ * ys, the noise the model draws as a tape (tape_init[n]: initial particles;
+ * tape_ticks[T][n/2]: the antithetic half per tick), theta = (mu, rho,
+ * sigma_z, nu), TBPTT every truncate_every ticks (0: none).  Writes
+ * loglik[T] (predictive, before the transport), vol[T] (mean e^{h/2} after
+ * it) and grad[4] = d(sum_t w_t loglik_t)/d theta (w = NULL: all ones).
+ * Returns 0, or -1 for invalid sizes. */
+int svpf_oracle_estimator_run(int n, int n_stein, double stein_lr, int T, const float* ys,
+                              const float* tape_init, const float* tape_ticks, const double* theta,
+                              int truncate_every, const double* w, double* loglik, double* vol,
+                              double* grad);
+/* The same with the per-tick bandwidths replayed from bw_fixed[T] (NULL: the
+ * model's own) and recorded into bw_out[T] (NULL: not recorded): central
+ * differences with the bandwidth frozen are what the detached bandwidth's
+ * derivative means. */
+int svpf_oracle_estimator_run2(int n, int n_stein, double stein_lr, int T, const float* ys,
+                               const float* tape_init, const float* tape_ticks, const double* theta,
+                               int truncate_every, const double* w, double* loglik, double* vol,
+                               double* grad, const double* bw_fixed, double* bw_out);
+
 #ifdef __cplusplus
 }
 #endif
