@@ -270,6 +270,52 @@ def gradient_workload(pkg, torch, F: int = 256, N: int = 512, T: int = 1000, k: 
     }
 
 
+def estimator_workload(pkg, torch, P: int = 1024, N: int = 64, S: int = 2, lr: float = 0.15, T: int = 250,
+                       trunc: int = 50, burn_in: int = 20):
+    """The reference's differentiable torch model (SVPFParamEstimator) at its
+    train() settings (N=64, 2 Stein steps of 0.15, nu=8, windows of T=250
+    ticks, truncation every 50, burn-in 20) for P paths with their own theta:
+    value and gradient of the predictive NLL, timed with CUDA events."""
+    rng = np.random.default_rng(21)
+    th = np.stack([rng.uniform(-4.5, -2.5, P), rng.uniform(0.85, 0.98, P), rng.uniform(0.1, 0.3, P),
+                   np.full(P, 8.0)], 1).astype(np.float32)
+    ys = sv_paths(T, th[:, 1].astype(np.float64), th[:, 2].astype(np.float64), th[:, 0].astype(np.float64),
+                  th[:, 3].astype(np.float64), seed=78).T.copy()
+    w = np.zeros((P, T), np.float32)
+    w[:, burn_in:] = -1.0 / (T - burn_in)
+    stream = torch.cuda.Stream()
+    e = pkg.Estimator(P, N, S, lr, T_max=T, checkpoint_every=50, truncate_every=trunc, stream=stream.cuda_stream)
+    d_th = torch.from_numpy(th).cuda()
+    d_y = torch.from_numpy(ys).cuda()
+    d_w = torch.from_numpy(w).cuda()
+    d_ll = torch.empty((P, T), dtype=torch.float32, device="cuda")
+    d_vol = torch.empty((P, T), dtype=torch.float32, device="cuda")
+    d_g = torch.empty((P, 4), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    for _ in range(2):   # warm-up
+        e.forward_device(d_th.data_ptr(), d_y.data_ptr(), T, 3, None, d_ll.data_ptr(), d_vol.data_ptr())
+        e.backward_device(d_w.data_ptr(), d_g.data_ptr())
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(stream)
+    e.forward_device(d_th.data_ptr(), d_y.data_ptr(), T, 3, None, d_ll.data_ptr(), d_vol.data_ptr())
+    ev[1].record(stream)
+    e.backward_device(d_w.data_ptr(), d_g.data_ptr())
+    ev[2].record(stream)
+    ev[2].synchronize()
+    fwd_ms, bwd_ms = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    g = d_g.cpu().numpy()
+    e.close()
+    return {
+        "workload": f"the reference's torch estimator model (SVPFParamEstimator) at its train() settings: {P} paths, "
+                    f"N={N}, {S} Stein steps of {lr}, T={T}, truncation every {trunc}, burn-in {burn_in}, "
+                    "own theta per path; d NLL / d(mu, rho, sigma_z, nu)",
+        "path_ticks_per_s": P * T / ((fwd_ms + bwd_ms) / 1e3),
+        "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+        "grad_path0": g[0].tolist(),
+    }
+
+
 def stream_workload(pkg, n_instruments: int = 10000, budget_bytes: int = 512 << 20, load: float = 0.8,
                     sim_seconds: float = 1.0, seed: int = 5):
     """Two-factor request loop: n_instruments two-factor filters (rho_f 0.80,
@@ -630,6 +676,9 @@ def main():
     stream_line = {}
     if rank == 0 and not args.no_stream:
         stream_line = stream_workload(pkg)
+    est_line = {}
+    if rank == 0 and not args.no_gradient:
+        est_line = estimator_workload(pkg, torch)
 
     cpu = {}
     if rank == 0:
@@ -658,6 +707,7 @@ def main():
             "single_filter_latency": lat,
             "plain_step_loop": plain,
             "gradient": grad_line,
+            "estimator_model": est_line,
             "two_factor_request_loop": stream_line,
             "cpu_baseline": cpu,
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},

@@ -196,8 +196,199 @@ __device__ inline int stage_of_it(int it, int budget, int na) {
     return a < na - 1 ? a : na - 1;
 }
 
+// ---- pair loops ------------------------------------------------------------
+// Every O(N^2) pass handles two rows per thread in packed FP32x2 (one issue
+// slot for both rows) over columns read four at a time; columns past n hold a
+// far value (positions) or zero (weights) so their terms vanish.
+//
+// Mixture prior in scaled coordinates x' = x psc, psc^2 = log2(e) / (2 s2):
+// exp(-(x - m)^2 / (2 s2)) = 2^-(x' - m')^2.  The row maximum is the nearest
+// sorted mean (binary search: the same value as a scan over all means), so a
+// pair is one FADD2, one FFMA2, one ex2 per row and the accumulations.
+
+__device__ __forceinline__ int mix_len(int n, int np) {
+    const int p2 = pow2_at_least(n);
+    const int a = p2 > np ? p2 : np;
+    return round_up(a, 4);
+}
+
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+
+// Sums over the sorted scaled means of w = 2^-(x' - m')^2 + min: sr = sum w,
+// wg = sum w d', and with MOM the moments m2 = sum w d'^2, m3 = sum w d'^3.
+template <bool MOM>
+__device__ __forceinline__ void mixture_rows(const float* __restrict__ srt, int nk4, float2 xs2, float2 ndm,
+                                             float2& sr, float2& wg, float2& m2, float2& m3) {
+    for (int cb = 0; cb < nk4; cb += 4) {
+        const float4 m4 = ld4(srt + cb);
+        const float mm[4] = {m4.x, m4.y, m4.z, m4.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const float2 d = add2(xs2, f2(-mm[e]));
+            const float2 q = fma2(d, d, ndm);
+            const float2 w = make_float2(ex2_approx(-q.x), ex2_approx(-q.y));
+            sr = add2(sr, w);
+            if (MOM) {
+                const float2 wd = mul2(w, d);
+                wg = add2(wg, wd);
+                const float2 wdd = mul2(wd, d);
+                m2 = add2(m2, wdd);
+                m3 = fma2(wdd, d, m3);
+            } else {
+                wg = fma2(w, d, wg);
+            }
+        }
+    }
+}
+
+// Transport row sums, u = (x_i - x_j)/bw, K = 1/(1 + u^2):
+//   kg = sum K g_j, gk = sum u K^2; FULL: ks = sum K, kc = sum K c_j,
+//   nk = sum K^2 |3u^2 - 1| = sum K |3 - 4K|; KSD: gdk = sum g_j u K^2,
+//   ht = sum K^2 (3 - 4K)  (4 u^2 K - 1 = 3 - 4K).
+template <bool FULL, bool KSD>
+__device__ __forceinline__ void transport_rows(const float* __restrict__ x, const float* __restrict__ g,
+                                               const float* __restrict__ cv, int nk4, float2 xi2, float ib,
+                                               float2& kg, float2& gk, float2& ks, float2& kc, float2& nk,
+                                               float2& gdk, float2& ht) {
+    const float2 mib = f2(-ib);
+    for (int cb = 0; cb < nk4; cb += 4) {
+        const float4 x4 = ld4(x + cb), g4 = ld4(g + cb);
+        float4 c4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (FULL) c4 = ld4(cv + cb);
+        const float xx[4] = {x4.x, x4.y, x4.z, x4.w};
+        const float gg[4] = {g4.x, g4.y, g4.z, g4.w};
+        const float cc[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const float2 u = fma2(f2(xx[e]), mib, xi2);
+            const float2 b = fma2(u, u, f2(1.0f));
+            const float2 K = make_float2(rcp_approx(b.x), rcp_approx(b.y));
+            const float2 K2 = mul2(K, K);
+            kg = fma2(K, f2(gg[e]), kg);
+            const float2 uk2 = mul2(u, K2);
+            gk = add2(gk, uk2);
+            if (FULL || KSD) {
+                const float2 t = fma2(K, f2(-4.0f), f2(3.0f));
+                if (FULL) {
+                    ks = add2(ks, K);
+                    kc = fma2(K, f2(cc[e]), kc);
+                    const float2 kt = mul2(K, t);
+                    nk.x += fabsf(kt.x);
+                    nk.y += fabsf(kt.y);
+                }
+                if (KSD) {
+                    gdk = fma2(f2(gg[e]), uk2, gdk);
+                    ht = fma2(K2, t, ht);
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ float flip_sign(float v, float s) {
+    return __int_as_float(__float_as_int(v) ^ (__float_as_int(s) & 0x80000000));
+}
+
+// Transport adjoint row sums (the row and column terms of one Stein
+// iteration, see the header), with u^2 K = 1 - K, K^2 |3u^2-1| = K |3-4K| and
+// uK^2 (6 sgn - 4 K |3u^2-1|) = sgn(3-4K) uK^2 (16K - 6).  Accumulators:
+//   0 S1 = sum g uK2     1 -S2 = sum K2 t       2 C1 = sum a uK2
+//   3 -C2 = sum a K2 t   4 C3 = sum a K         5 Q1 = sum g (K - K2)
+//   6 -Q2' = sum u K2 t  7 R3 = sum uK2         (t = 3 - 4K, Q2 = Q2' + R3)
+//   FULL: 8 R1 = sum c uK2, 9 R2 = sum f6, 10 D1 = sum hb uK2, 11 D2 = sum hb f6,
+//   12 D3 = sum kb uK2, 13 E1 = sum hb K, 14 W1 = sum c (K - K2), 15 W2 = sum u f6,
+//   16 W3 = sum K |t|, 17 W4 = sum (K - K2).
+constexpr int kAdjAcc = 18;
+template <bool FULL>
+__device__ __forceinline__ void adjoint_rows(const float* __restrict__ xs, const float* __restrict__ g,
+                                             const float* __restrict__ a, const float* __restrict__ cv,
+                                             const float* __restrict__ hwb, const float* __restrict__ knb, int nk4,
+                                             float2 xi2, float ib, float2 (&acc)[kAdjAcc]) {
+    const float2 mib = f2(-ib);
+    for (int cb = 0; cb < nk4; cb += 4) {
+        const float4 x4 = ld4(xs + cb), g4 = ld4(g + cb), a4 = ld4(a + cb);
+        float4 c4 = make_float4(0.f, 0.f, 0.f, 0.f), h4 = c4, k4 = c4;
+        if (FULL) {
+            c4 = ld4(cv + cb);
+            h4 = ld4(hwb + cb);
+            k4 = ld4(knb + cb);
+        }
+        const float xx[4] = {x4.x, x4.y, x4.z, x4.w};
+        const float gg[4] = {g4.x, g4.y, g4.z, g4.w};
+        const float aa[4] = {a4.x, a4.y, a4.z, a4.w};
+        const float cc[4] = {c4.x, c4.y, c4.z, c4.w};
+        const float hh[4] = {h4.x, h4.y, h4.z, h4.w};
+        const float kk[4] = {k4.x, k4.y, k4.z, k4.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const float2 u = fma2(f2(xx[e]), mib, xi2);
+            const float2 b = fma2(u, u, f2(1.0f));
+            const float2 K = make_float2(rcp_approx(b.x), rcp_approx(b.y));
+            const float2 K2 = mul2(K, K);
+            const float2 uk2 = mul2(u, K2);
+            const float2 t = fma2(K, f2(-4.0f), f2(3.0f));
+            const float2 k2t = mul2(K2, t);
+            const float2 km = fma2(make_float2(-K.x, -K.y), K, K);
+            const float2 gj = f2(gg[e]), aj = f2(aa[e]);
+            acc[0] = fma2(gj, uk2, acc[0]);
+            acc[1] = add2(acc[1], k2t);
+            acc[2] = fma2(aj, uk2, acc[2]);
+            acc[3] = fma2(aj, k2t, acc[3]);
+            acc[4] = fma2(aj, K, acc[4]);
+            acc[5] = fma2(gj, km, acc[5]);
+            acc[6] = fma2(u, k2t, acc[6]);
+            acc[7] = add2(acc[7], uk2);
+            if (FULL) {
+                const float2 f6u = mul2(uk2, fma2(K, f2(16.0f), f2(-6.0f)));
+                const float2 f6 = make_float2(flip_sign(f6u.x, t.x), flip_sign(f6u.y, t.y));
+                const float2 kt = mul2(K, t);
+                const float2 cj = f2(cc[e]), hj = f2(hh[e]);
+                acc[8] = fma2(cj, uk2, acc[8]);
+                acc[9] = add2(acc[9], f6);
+                acc[10] = fma2(hj, uk2, acc[10]);
+                acc[11] = fma2(hj, f6, acc[11]);
+                acc[12] = fma2(f2(kk[e]), uk2, acc[12]);
+                acc[13] = fma2(hj, K, acc[13]);
+                acc[14] = fma2(cj, km, acc[14]);
+                acc[15] = fma2(u, f6, acc[15]);
+                acc[16].x += fabsf(kt.x);
+                acc[16].y += fabsf(kt.y);
+                acc[17] = add2(acc[17], km);
+            }
+        }
+    }
+}
+
+// Mixture column sums for dL/dmu_k (rows are prior means k, scaled mk2):
+//   sum_j coef_j r_kj (1 - 2 ln2 d' (d' - dbar'_j)),  r_kj = 2^-(d'^2 - lmin'_j),
+//   d' = x_j psc - m'_k.
+__device__ __forceinline__ float2 mixture_cols(const float* __restrict__ xs, const float* __restrict__ lmx,
+                                               const float* __restrict__ dbr, const float* __restrict__ coef, int nk4,
+                                               float psc, float2 mk2) {
+    const float2 nmk = make_float2(-mk2.x, -mk2.y);
+    float2 acc = f2(0.0f);
+    for (int cb = 0; cb < nk4; cb += 4) {
+        const float4 x4 = ld4(xs + cb), l4 = ld4(lmx + cb), d4 = ld4(dbr + cb), c4 = ld4(coef + cb);
+        const float xx[4] = {x4.x, x4.y, x4.z, x4.w};
+        const float ll[4] = {l4.x, l4.y, l4.z, l4.w};
+        const float db[4] = {d4.x, d4.y, d4.z, d4.w};
+        const float co[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const float2 d = fma2(f2(xx[e]), f2(psc), nmk);
+            const float2 q = fma2(d, d, f2(-ll[e]));
+            const float2 r = make_float2(ex2_approx(-q.x), ex2_approx(-q.y));
+            const float2 uu = mul2(d, add2(d, f2(-db[e])));
+            const float2 fct = fma2(uu, f2(-2.0f * kLn2), f2(1.0f));
+            acc = fma2(mul2(r, f2(co[e])), fct, acc);
+        }
+    }
+    return acc;
+}
+
 // One tick of one filter (CTA-wide).  x, v: positions and RMSProp moments
-// (smem, updated in place); work: 6 np floats of smem scratch.  rec: per-tick
+// (smem, updated in place; x has room for round_up(n, 4) columns); work:
+// 5 np + mix_len floats of smem scratch.  rec: per-tick
 // record for the backward, or nullptr.  Returns loglik on every thread.
 __device__ float fwd_tick(const svpf_config_t& c, int n, int np, float* x, float* v, float* work, Shared& sh,
                           const Noise& nz, float y_t, float y_prev, float* rec, int bmax, int objective) {
@@ -209,6 +400,7 @@ __device__ float fwd_tick(const svpf_config_t& c, int n, int np, float* x, float
     float* curv = work + 2 * np;      // full-Newton curvature
     float* lw = work + 3 * np;        // log-weights of the last gradient pass
     float* muk = work + 4 * np;       // prior means
+    float* srt = work + 5 * np;       // prior means scaled and sorted (mix_len floats)
     const bool full = c.use_newton && c.use_full_newton;
     if (tid == 0) {
         ts.y_t = y_t;
@@ -360,11 +552,22 @@ __device__ float fwd_tick(const svpf_config_t& c, int n, int np, float* x, float
         }
         __syncthreads();
     }
+    // ---- sorted, scaled prior means for the mixture passes
+    const float inv2 = 0.5f / ts.s2, inv = 1.0f / ts.s2;
+    const float psc = sqrtf(kLog2e * inv2);
+    const int nk4 = round_up(n, 4);
+    {
+        const int ml = mix_len(n, np);
+        for (int i = tid; i < ml; i += kThreads) srt[i] = i < n ? muk[i] * psc : kMuPad;
+        // far columns of the transport pair loops
+        for (int i = n + tid; i < nk4; i += kThreads) x[i] = kHPadRaw;
+        __syncthreads();
+        bitonic_sort(srt, pow2_at_least(n));
+    }
     // ---- Stein loop
     const float sign = c.stein_repulsive_sign == 1 ? 1.0f : -1.0f;
     const float temp = c.use_svld ? c.temperature : 0.0f;
     const float y2 = y_t * y_t;
-    const float inv2 = 0.5f / ts.s2, inv = 1.0f / ts.s2;
     const float ib = ts.ib, ib2 = ib * ib;
     const float inv_n = 1.0f / (float)n;
     const int budget = ts.budget;
@@ -374,95 +577,105 @@ __device__ float fwd_tick(const svpf_config_t& c, int n, int np, float* x, float
         const float beta = ts.beta[it];
         const bool last = it == budget - 1;
         float* R = rec ? rec + (size_t)np * (kRecFixed + kRecPerIt * it) : nullptr;
-        // gradient pass (svpf_opt_kernels.cu:354-521)
-        for (int j = tid; j < n; j += kThreads) {
-            const float xj = x[j];
-            float lmax = -1e10f;
-            for (int k = 0; k < n; ++k) {
-                const float d = xj - muk[k];
-                lmax = fmaxf(lmax, -d * d * inv2);
-            }
-            float sr = 0.0f, wg = 0.0f, m2 = 0.0f, m3 = 0.0f;
-            for (int k = 0; k < n; ++k) {
-                const float d = xj - muk[k];
-                const float r = expf(-d * d * inv2 - lmax);
-                sr += r;
-                wg -= r * d * inv;
-                if (R) {
-                    const float rd2 = r * d * d;
-                    m2 += rd2;
-                    m3 += rd2 * d;
+        // gradient pass (svpf_opt_kernels.cu:354-521), two rows per thread
+        for (int i = n + tid; i < nk4; i += kThreads) {
+            g[i] = 0.0f;
+            curv[i] = 0.0f;
+        }
+        for (int base = 0; base < n; base += 2 * kThreads) {
+            const int j0 = base + tid;
+            if (j0 >= n) break;
+            const bool two = j0 + kThreads < n;
+            const int j1 = two ? j0 + kThreads : j0;
+            const float2 xs2 = make_float2(x[j0] * psc, x[j1] * psc);
+            const float2 dm = make_float2(nearest_d2(srt, n, xs2.x), nearest_d2(srt, n, xs2.y));
+            float2 sr2 = f2(0.0f), wg2 = f2(0.0f), m22 = f2(0.0f), m32 = f2(0.0f);
+            if (R) mixture_rows<true>(srt, nk4, xs2, make_float2(-dm.x, -dm.y), sr2, wg2, m22, m32);
+            else mixture_rows<false>(srt, nk4, xs2, make_float2(-dm.x, -dm.y), sr2, wg2, m22, m32);
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                if (r == 1 && !two) break;
+                const int j = r ? j1 : j0;
+                const float xj = x[j];
+                const float sr = r ? sr2.y : sr2.x;
+                // sum_k w d = wg' / psc;  gp = -(sum w d) / s2 / (sum w + 1e-8)
+                const float gp = -((r ? wg2.y : wg2.x) / psc) * inv / (sr + 1e-8f);
+                const float A = y2 / (expf(fminf(xj, 20.0f)) + 1e-8f) / ts.nu;
+                const float opA = 1.0f + A;
+                lw[j] = ts.stc - 0.5f * xj - (ts.nu + 1.0f) * 0.5f * log1pf(fmaxf(A, -0.999f));
+                float glik;
+                if (c.use_exact_gradient) glik = -0.5f + 0.5f * (ts.nu + 1.0f) * A / opA - c.lik_offset;
+                else glik = (logf(y2 + 1e-10f) - xj + c.lik_offset) / 1.4f;
+                const float gpre = gp + beta * glik;
+                g[j] = clampf(gpre, -10.0f, 10.0f);
+                if (full) {
+                    const float hl = -0.5f * (ts.nu + 1.0f) * A / (opA * opA);
+                    curv[j] = clampf(-(hl - inv), 0.1f, 100.0f);
                 }
-            }
-            const float gp = wg / (sr + 1e-8f);
-            const float A = y2 / (expf(fminf(xj, 20.0f)) + 1e-8f) / ts.nu;
-            const float opA = 1.0f + A;
-            lw[j] = ts.stc - 0.5f * xj - (ts.nu + 1.0f) * 0.5f * log1pf(fmaxf(A, -0.999f));
-            float glik;
-            if (c.use_exact_gradient) glik = -0.5f + 0.5f * (ts.nu + 1.0f) * A / opA - c.lik_offset;
-            else glik = (logf(y2 + 1e-10f) - xj + c.lik_offset) / 1.4f;
-            const float gpre = gp + beta * glik;
-            g[j] = clampf(gpre, -10.0f, 10.0f);
-            if (full) {
-                const float hl = -0.5f * (ts.nu + 1.0f) * A / (opA * opA);
-                curv[j] = clampf(-(hl - inv), 0.1f, 100.0f);
-            }
-            if (R) {
-                const float dbar = -gp * ts.s2;              // E_w[d]
-                const float e2 = m2 / sr, e3 = m3 / sr;
-                R[IX * np + j] = xj;
-                R[IV * np + j] = v[j];
-                R[IGPRE * np + j] = gpre;
-                R[IAL * np + j] = A;
-                R[ILMAX * np + j] = lmax;
-                R[IZ * np + j] = sr;
-                R[IDBAR * np + j] = dbar;
-                R[IVARD * np + j] = e2 - dbar * dbar;
-                R[ISKEW * np + j] = e3 - dbar * e2;
+                if (R) {
+                    const float dbar = -gp * ts.s2;              // E_w[d]
+                    const float i2 = 1.0f / (psc * psc);
+                    const float e2 = (r ? m22.y : m22.x) * i2 / sr, e3 = (r ? m32.y : m32.x) * i2 / psc / sr;
+                    R[IX * np + j] = xj;
+                    R[IV * np + j] = v[j];
+                    R[IGPRE * np + j] = gpre;
+                    R[IAL * np + j] = A;
+                    R[ILMAX * np + j] = r ? dm.y : dm.x;      // nearest scaled distance^2
+                    R[IZ * np + j] = sr;
+                    R[IDBAR * np + j] = dbar;
+                    R[IVARD * np + j] = e2 - dbar * dbar;
+                    R[ISKEW * np + j] = e3 - dbar * e2;
+                }
             }
         }
         __syncthreads();
         // transport (vanilla :527-599 or full Newton :912-1103), Jacobi
         const float es = ts.es[it];
-        for (int i = tid; i < n; i += kThreads) {
-            const float xi = x[i], gi = g[i];
-            float ks = 0.0f, gk = 0.0f, hw = 0.0f, kk = 0.0f, kq = 0.0f;
-            for (int j = 0; j < n; ++j) {
-                const float u = (xi - x[j]) * ib;
-                const float K = 1.0f / (1.0f + u * u);
-                const float K2 = K * K;
-                ks += K * g[j];
-                gk += u * K2;
-                if (full) {
-                    hw += curv[j] * K + 2.0f * ib2 * K2 * fabsf(3.0f * u * u - 1.0f);
-                    kk += K;
-                }
-                if (last) {
-                    const float gxk = -2.0f * u * ib * K2;
-                    const float hxy = 2.0f * ib2 * K2 * (4.0f * u * u * K - 1.0f);
-                    kq += K * gi * g[j] + gi * (-gxk) + g[j] * gxk + hxy;
-                }
-            }
-            const float phir = (ks + sign * 2.0f * ib * gk) * inv_n;
-            float phi = phir, hr = 0.0f;
+        for (int base = 0; base < n; base += 2 * kThreads) {
+            const int i0 = base + tid;
+            if (i0 >= n) break;
+            const bool two = i0 + kThreads < n;
+            const int i1 = two ? i0 + kThreads : i0;
+            const float2 xi2 = make_float2(x[i0] * ib, x[i1] * ib);
+            float2 kg = f2(0.0f), gk = f2(0.0f), ks = f2(0.0f), kc = f2(0.0f), nk = f2(0.0f), gdk = f2(0.0f),
+                   ht = f2(0.0f);
             if (full) {
-                hr = hw / fmaxf(kk, 1e-6f);
-                phi = phir / clampf(hr, 0.1f, 100.0f) * 0.7f;
+                if (last) transport_rows<true, true>(x, g, curv, nk4, xi2, ib, kg, gk, ks, kc, nk, gdk, ht);
+                else transport_rows<true, false>(x, g, curv, nk4, xi2, ib, kg, gk, ks, kc, nk, gdk, ht);
+            } else {
+                if (last) transport_rows<false, true>(x, g, curv, nk4, xi2, ib, kg, gk, ks, kc, nk, gdk, ht);
+                else transport_rows<false, false>(x, g, curv, nk4, xi2, ib, kg, gk, ks, kc, nk, gdk, ht);
             }
-            ksd_acc += kq;
-            const float rr = c.rmsprop_rho;
-            const float vn = rr * v[i] + (1.0f - rr) * phi * phi;
-            float diff = 0.0f;
-            if (temp > 1e-6f) diff = sqrtf(2.0f * es * temp) * nz.normal(i, kn);
-            const float xr = xi + es * phi * rsqrtf(vn + c.rmsprop_eps) + diff;
-            xn[i] = clamp_h(xr);
-            v[i] = vn;
-            if (R) {
-                R[IPHIR * np + i] = phir;
-                R[IHR * np + i] = hr;
-                R[IHW * np + i] = hw;
-                R[IKN * np + i] = kk;
-                R[IXR * np + i] = xr;
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                if (r == 1 && !two) break;
+                const int i = r ? i1 : i0;
+                const float xi = x[i], gi = g[i];
+                const float kgr = r ? kg.y : kg.x, gkr = r ? gk.y : gk.x;
+                const float phir = (kgr + sign * 2.0f * ib * gkr) * inv_n;
+                float phi = phir, hr = 0.0f, hw = 0.0f, kk = 0.0f;
+                if (full) {
+                    hw = (r ? kc.y : kc.x) + 2.0f * ib2 * (r ? nk.y : nk.x);
+                    kk = r ? ks.y : ks.x;
+                    hr = hw / fmaxf(kk, 1e-6f);
+                    phi = phir / clampf(hr, 0.1f, 100.0f) * 0.7f;
+                }
+                if (last)
+                    ksd_acc += gi * kgr + 2.0f * ib * (gi * gkr - (r ? gdk.y : gdk.x)) + 2.0f * ib2 * (r ? ht.y : ht.x);
+                const float rr = c.rmsprop_rho;
+                const float vn = rr * v[i] + (1.0f - rr) * phi * phi;
+                float diff = 0.0f;
+                if (temp > 1e-6f) diff = sqrtf(2.0f * es * temp) * nz.normal(i, kn);
+                const float xr = xi + es * phi * rsqrtf(vn + c.rmsprop_eps) + diff;
+                xn[i] = clamp_h(xr);
+                v[i] = vn;
+                if (R) {
+                    R[IPHIR * np + i] = phir;
+                    R[IHR * np + i] = hr;
+                    R[IHW * np + i] = hw;
+                    R[IKN * np + i] = kk;
+                    R[IXR * np + i] = xr;
+                }
             }
         }
         __syncthreads();
@@ -524,6 +737,8 @@ __device__ void bwd_tick(const svpf_config_t& c, int n, int np, float* xb, float
     const bool full = c.use_newton && c.use_full_newton;
     const float sign = c.stein_repulsive_sign == 1 ? 1.0f : -1.0f;
     const float s2 = ts.s2, inv = 1.0f / s2;
+    const float psc = sqrtf(kLog2e * (0.5f / s2));   // mixture scale of the forward
+    const int nk4 = round_up(n, 4);
     const float nu = ts.nu;
     const float ib = ts.ib, ib2 = ib * ib;
     const float inv_n = 1.0f / (float)n;
@@ -591,113 +806,111 @@ __device__ void bwd_tick(const svpf_config_t& c, int n, int np, float* xb, float
             a[i] = pr * inv_n;
         }
         __syncthreads();
-        // (b) transport adjoint: one pass of row sums (row and column terms)
-        for (int i = tid; i < n; i += kThreads) {
-            const float xi = xs[i], gi = g[i], ai = a[i];
-            float S1 = 0.f, S2 = 0.f, C1 = 0.f, C2 = 0.f, C3 = 0.f, Q1 = 0.f, Q2 = 0.f;
-            float R1 = 0.f, R2 = 0.f, R3 = 0.f, D1 = 0.f, D2 = 0.f, D3 = 0.f, E1 = 0.f, W1 = 0.f, W2 = 0.f, W3 = 0.f,
-                  W4 = 0.f;
-            for (int j = 0; j < n; ++j) {
-                const float u = (xi - xs[j]) * ib;
-                const float K = 1.0f / (1.0f + u * u);
-                const float K2 = K * K;
-                const float uK2 = u * K2;
-                const float t43 = K2 * (4.0f * K - 3.0f);
-                const float aj = a[j], gj = g[j];
-                S1 += gj * uK2;
-                S2 += t43;
-                C1 += aj * uK2;
-                C2 += aj * t43;
-                C3 += aj * K;
-                Q1 += gj * u * uK2;
-                Q2 += uK2 * (4.0f * K - 2.0f);
-                if (full) {
-                    const float w = 3.0f * u * u - 1.0f;
-                    const float aw = fabsf(w);
-                    const float sg = w > 0.0f ? 1.0f : (w < 0.0f ? -1.0f : 0.0f);
-                    const float f6 = uK2 * (6.0f * sg - 4.0f * K * aw);
-                    const float cj = cv[j], hbj = hwb[j], kbj = knb[j];
-                    R1 += cj * uK2;
-                    R2 += f6;
-                    R3 += uK2;
-                    D1 += hbj * uK2;
-                    D2 += hbj * f6;
-                    D3 += kbj * uK2;
-                    E1 += hbj * K;
-                    W1 += cj * u * uK2;
-                    W2 += u * f6;
-                    W3 += K2 * aw;
-                    W4 += u * uK2;
-                }
-            }
-            float dx = ib * (ai * (-2.0f * S1 + 2.0f * sign * ib * S2) - 2.0f * gi * C1 - 2.0f * sign * ib * C2);
-            pbw += ai * ib * (2.0f * Q1 - 2.0f * sign * ib * Q2);
-            float gb = C3;
-            if (full) {
-                const float hb = hwb[i], kb = knb[i];
-                dx += ib * (hb * (-2.0f * R1 + 2.0f * ib2 * R2) - 2.0f * kb * R3);
-                dx += ib * (-2.0f * cv[i] * D1 + 2.0f * ib2 * D2 - 2.0f * D3);
-                pbw += hb * (ib * (2.0f * W1 - 2.0f * ib2 * W2) - 4.0f * ib2 * ib * W3) + kb * 2.0f * ib * W4;
-                // curvature adjoint E1 -> A and s2 (clamp [0.1, 100])
-                const float A = R[IAL * np + i];
-                const float opA = 1.0f + A;
-                const float craw = 0.5f * (nu + 1.0f) * A / (opA * opA) + inv;
-                if (craw >= 0.1f && craw <= 100.0f) {
-                    // curv = 0.5 (nu+1) A / (1+A)^2 + 1/s2
-                    const float dcdA = 0.5f * (nu + 1.0f) * (1.0f - A) / (opA * opA * opA);
-                    const float dAdx = (xi < 20.0f) ? -A * expf(xi) / (expf(xi) + 1e-8f) : 0.0f;
-                    dx += E1 * dcdA * dAdx;
-                    pnu += E1 * (0.5f * A / (opA * opA) + dcdA * (-A / nu));
-                    ps2 += E1 * (-inv * inv);
-                }
-            }
-            xb[i] += dx;
-            // (c) gradient adjoint, O(N) part (g = clamp(gp + beta glik))
-            const float gpre = R[IGPRE * np + i];
-            const float gpb = (gpre >= -10.0f && gpre <= 10.0f) ? gb : 0.0f;
-            const float A = R[IAL * np + i];
-            const float opA = 1.0f + A;
-            const float ex = expf(fminf(xi, 20.0f));
-            const float dAdx = (xi < 20.0f) ? -A * ex / (ex + 1e-8f) : 0.0f;
-            const float dAdnu = -A / nu;
-            const float dbar = R[IDBAR * np + i], vard = R[IVARD * np + i], skew = R[ISKEW * np + i];
-            float dgdx = -inv + vard * inv * inv;
-            float dgdnu = 0.0f;
-            if (c.use_exact_gradient) {
-                const float dglA = 0.5f * (nu + 1.0f) / (opA * opA);
-                dgdx += beta * dglA * dAdx;
-                dgdnu = beta * (0.5f * A / opA + dglA * dAdnu);
-            } else {
-                dgdx += beta * (-1.0f / 1.4f);
-            }
-            float dxx = gpb * dgdx;
-            pnu += gpb * dgdnu;
-            ps2 += gpb * (dbar * inv * inv - skew * 0.5f * inv * inv * inv);
-            if (it == budget - 1) {
-                const float lb = lwb[i];
-                const float dlwdA = -(nu + 1.0f) * 0.5f / opA;
-                dxx += lb * (-0.5f + dlwdA * dAdx);
-                pnu += lb * (-0.5f * log1pf(A) + dlwdA * dAdnu);
-            }
-            xb[i] += dxx;
-            coef[i] = gpb * inv / R[IZ * np + i];
-            lmx[i] = R[ILMAX * np + i];
-            dbr[i] = dbar;
+        // far columns of the pair loops: position pad, zero weights
+        for (int i = n + tid; i < nk4; i += kThreads) {
+            xs[i] = kHPadRaw;
+            g[i] = 0.0f;
+            a[i] = 0.0f;
+            cv[i] = 0.0f;
+            hwb[i] = 0.0f;
+            knb[i] = 0.0f;
+            coef[i] = 0.0f;
+            lmx[i] = 0.0f;
+            dbr[i] = 0.0f;
         }
         __syncthreads();
-        // (d) mixture column pass: dL/dmu_k
+        // (b) transport adjoint: one pass of row sums (row and column terms),
+        // two rows per thread; (c) the O(N) gradient adjoint of each row
+        for (int base = 0; base < n; base += 2 * kThreads) {
+            const int i0 = base + tid;
+            if (i0 >= n) break;
+            const bool two = i0 + kThreads < n;
+            const int i1 = two ? i0 + kThreads : i0;
+            float2 acc[kAdjAcc];
+#pragma unroll
+            for (int q = 0; q < kAdjAcc; ++q) acc[q] = f2(0.0f);
+            const float2 xi2 = make_float2(xs[i0] * ib, xs[i1] * ib);
+            if (full) adjoint_rows<true>(xs, g, a, cv, hwb, knb, nk4, xi2, ib, acc);
+            else adjoint_rows<false>(xs, g, a, cv, hwb, knb, nk4, xi2, ib, acc);
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                if (r == 1 && !two) break;
+                const int i = r ? i1 : i0;
+                float v_[kAdjAcc];
+#pragma unroll
+                for (int q = 0; q < kAdjAcc; ++q) v_[q] = r ? acc[q].y : acc[q].x;
+                const float S1 = v_[0], S2 = -v_[1], C1 = v_[2], C2 = -v_[3], C3 = v_[4], Q1 = v_[5];
+                const float Q2 = -v_[6] + v_[7];
+                const float xi = xs[i], gi = g[i], ai = a[i];
+                float dx = ib * (ai * (-2.0f * S1 + 2.0f * sign * ib * S2) - 2.0f * gi * C1 - 2.0f * sign * ib * C2);
+                pbw += ai * ib * (2.0f * Q1 - 2.0f * sign * ib * Q2);
+                float gb = C3;
+                if (full) {
+                    const float R1 = v_[8], R2 = v_[9], R3 = v_[7], D1 = v_[10], D2 = v_[11], D3 = v_[12];
+                    const float E1 = v_[13], W1 = v_[14], W2 = v_[15], W3 = v_[16], W4 = v_[17];
+                    const float hb = hwb[i], kb = knb[i];
+                    dx += ib * (hb * (-2.0f * R1 + 2.0f * ib2 * R2) - 2.0f * kb * R3);
+                    dx += ib * (-2.0f * cv[i] * D1 + 2.0f * ib2 * D2 - 2.0f * D3);
+                    pbw += hb * (ib * (2.0f * W1 - 2.0f * ib2 * W2) - 4.0f * ib2 * ib * W3) + kb * 2.0f * ib * W4;
+                    // curvature adjoint E1 -> A and s2 (clamp [0.1, 100])
+                    const float A = R[IAL * np + i];
+                    const float opA = 1.0f + A;
+                    const float craw = 0.5f * (nu + 1.0f) * A / (opA * opA) + inv;
+                    if (craw >= 0.1f && craw <= 100.0f) {
+                        // curv = 0.5 (nu+1) A / (1+A)^2 + 1/s2
+                        const float dcdA = 0.5f * (nu + 1.0f) * (1.0f - A) / (opA * opA * opA);
+                        const float dAdx = (xi < 20.0f) ? -A * expf(xi) / (expf(xi) + 1e-8f) : 0.0f;
+                        dx += E1 * dcdA * dAdx;
+                        pnu += E1 * (0.5f * A / (opA * opA) + dcdA * (-A / nu));
+                        ps2 += E1 * (-inv * inv);
+                    }
+                }
+                xb[i] += dx;   // rows read a, g, xs of other rows, never xb
+                // (c) gradient adjoint, O(N) part (g = clamp(gp + beta glik))
+                const float gpre = R[IGPRE * np + i];
+                const float gpb = (gpre >= -10.0f && gpre <= 10.0f) ? gb : 0.0f;
+                const float A = R[IAL * np + i];
+                const float opA = 1.0f + A;
+                const float ex = expf(fminf(xi, 20.0f));
+                const float dAdx = (xi < 20.0f) ? -A * ex / (ex + 1e-8f) : 0.0f;
+                const float dAdnu = -A / nu;
+                const float dbar = R[IDBAR * np + i], vard = R[IVARD * np + i], skew = R[ISKEW * np + i];
+                float dgdx = -inv + vard * inv * inv;
+                float dgdnu = 0.0f;
+                if (c.use_exact_gradient) {
+                    const float dglA = 0.5f * (nu + 1.0f) / (opA * opA);
+                    dgdx += beta * dglA * dAdx;
+                    dgdnu = beta * (0.5f * A / opA + dglA * dAdnu);
+                } else {
+                    dgdx += beta * (-1.0f / 1.4f);
+                }
+                float dxx = gpb * dgdx;
+                pnu += gpb * dgdnu;
+                ps2 += gpb * (dbar * inv * inv - skew * 0.5f * inv * inv * inv);
+                if (it == budget - 1) {
+                    const float lb = lwb[i];
+                    const float dlwdA = -(nu + 1.0f) * 0.5f / opA;
+                    dxx += lb * (-0.5f + dlwdA * dAdx);
+                    pnu += lb * (-0.5f * log1pf(A) + dlwdA * dAdnu);
+                }
+                xb[i] += dxx;
+                coef[i] = gpb * inv / R[IZ * np + i];
+                lmx[i] = R[ILMAX * np + i];
+                dbr[i] = dbar * psc;
+            }
+        }
+        __syncthreads();
+        // (d) mixture column pass: dL/dmu_k, two prior means per thread
         {
             const float* MU = rec + (size_t)np * MUK;
-            const float inv2 = 0.5f * inv;
-            for (int k = tid; k < n; k += kThreads) {
-                const float mk = MU[k];
-                float acc = 0.0f;
-                for (int j = 0; j < n; ++j) {
-                    const float d = xs[j] - mk;
-                    const float r = expf(-d * d * inv2 - lmx[j]);
-                    acc += coef[j] * r * (1.0f - d * (d - dbr[j]) * inv);
-                }
-                mub[k] += acc;
+            for (int base = 0; base < n; base += 2 * kThreads) {
+                const int k0 = base + tid;
+                if (k0 >= n) break;
+                const bool two = k0 + kThreads < n;
+                const int k1 = two ? k0 + kThreads : k0;
+                const float2 acc = mixture_cols(xs, lmx, dbr, coef, nk4, psc, make_float2(MU[k0] * psc, MU[k1] * psc));
+                mub[k0] += acc.x;
+                if (two) mub[k1] += acc.y;
             }
         }
         __syncthreads();
