@@ -471,6 +471,13 @@ int svpf_grad_forward_device(svpf_grad_t* g, const float* d_theta, const float* 
                              const float* d_y, int T, unsigned long long seed, float* d_loglik);
 int svpf_grad_backward_device(svpf_grad_t* g, const float* d_w, double* d_grad);
 int svpf_grad_checkpoint_every(const svpf_grad_t* g);
+/* 1 if the backward records a whole checkpoint segment in one forward pass
+ * (k tick records per CTA in device memory) instead of re-running each tick's
+ * forward once more before its adjoint; chosen at create by free memory.
+ * set: 1 forces segment records (SVPF_ERR_CUDA if they do not fit), 0 the
+ * per-tick records.  Both give the same bits. */
+int svpf_grad_segment_records(const svpf_grad_t* g);
+int svpf_grad_set_segment_records(svpf_grad_t* g, int on);
 /* What the run's log-likelihood is made of (before the next forward):
  * SVPF_GRAD_TICK_LOGLIK (default): each tick's loglik as svpf_step_graph
  * reports it (log-mean-exp of the log-weights of the tick's last gradient

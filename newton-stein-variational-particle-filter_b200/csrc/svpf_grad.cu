@@ -65,6 +65,8 @@ struct GAdj {
     double th[4];                  // accumulated d/d(mu, rho, sigma_z, nu)
 };
 
+struct TickScalars;
+
 struct GArgs {
     int F, T, k, np, bmax;
     const int* n;
@@ -88,8 +90,10 @@ struct GArgs {
     // per CTA
     float* seg;                    // [grid][k][2 np] tick inputs of the segment
     GState* segs;                  // [grid][k]
-    float* rec;                    // [grid][rec_floats] per-tick record
+    float* rec;                    // [grid][k or 1][rec_floats] per-tick records
     size_t rec_floats;
+    TickScalars* segts;            // [grid][k] the ticks' scalars (segment records)
+    int seg_rec;                   // 1: record the whole segment in one forward
     int nseg;
     int* status;                   // [F]
     int objective;                 // 0: the tick's log-likelihood, 1: predictive log p(y_t | y_1:t-1)
@@ -228,14 +232,11 @@ __device__ __forceinline__ void mixture_rows(const float* __restrict__ srt, int 
             const float2 q = fma2(d, d, ndm);
             const float2 w = make_float2(ex2_approx(-q.x), ex2_approx(-q.y));
             sr = add2(sr, w);
+            wg = fma2(w, d, wg);   // identical with and without the moments: records replay the forward
             if (MOM) {
-                const float2 wd = mul2(w, d);
-                wg = add2(wg, wd);
-                const float2 wdd = mul2(wd, d);
+                const float2 wdd = mul2(mul2(w, d), d);
                 m2 = add2(m2, wdd);
                 m3 = fma2(wdd, d, m3);
-            } else {
-                wg = fma2(w, d, wg);
             }
         }
     }
@@ -1209,7 +1210,8 @@ __global__ void __launch_bounds__(kThreads) grad_backward_kernel(const GArgs a, 
     float* work = smem + 4 * np;
     float* seg = a.seg + (size_t)blockIdx.x * a.k * 2 * np;
     GState* segs = a.segs + (size_t)blockIdx.x * a.k;
-    float* rec = a.rec + (size_t)blockIdx.x * a.rec_floats;
+    TickScalars* segts = a.segts + (size_t)blockIdx.x * a.k;
+    float* rec = a.rec + (size_t)blockIdx.x * a.rec_floats * (a.seg_rec ? a.k : 1);
     const int t0 = sg * a.k;
     const int t1 = min(a.T, t0 + a.k);
     for (int f = blockIdx.x; f < a.F; f += gridDim.x) {
@@ -1230,6 +1232,31 @@ __global__ void __launch_bounds__(kThreads) grad_backward_kernel(const GArgs a, 
             vb[i] = a.av[(size_t)f * np + i];
         }
         __syncthreads();
+        if (a.seg_rec) {
+            // one forward over the segment recording every tick, then the
+            // ticks' adjoints in reverse from those records
+            for (int t = t0; t < t1; ++t) {
+                float* rt = rec + (size_t)(t - t0) * a.rec_floats;
+                copy_state_to(&segs[t - t0], sh.st);
+                const float yt = a.y[(size_t)f * a.T + t];
+                const float yp = t > 0 ? a.y[(size_t)f * a.T + t - 1] : 0.0f;
+                const Noise nz = make_noise(a.seed, f, sh.st.timestep, n, &sh.flag);
+                __syncthreads();
+                fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, rt, a.bmax, a.objective);
+                if (threadIdx.x == 0) segts[t - t0] = sh.ts;
+            }
+            for (int t = t1 - 1; t >= t0; --t) {
+                const float* rt = rec + (size_t)(t - t0) * a.rec_floats;
+                if (threadIdx.x == 0) {
+                    sh.st = segs[t - t0];
+                    sh.ts = segts[t - t0];
+                }
+                __syncthreads();
+                const Noise nz = make_noise(a.seed, f, sh.st.timestep, n, &sh.flag);
+                const float wt = a.w ? a.w[(size_t)f * a.T + t] : 1.0f;
+                bwd_tick(cfg, n, np, xb, vb, work, sh, sa, nz, rt, a.bmax, wt, a.objective);
+            }
+        } else {
         // recompute the segment, keeping every tick's input state
         for (int t = t0; t < t1; ++t) {
             float* sx = seg + (size_t)(t - t0) * 2 * np;
@@ -1242,9 +1269,9 @@ __global__ void __launch_bounds__(kThreads) grad_backward_kernel(const GArgs a, 
             const float yp = t > 0 ? a.y[(size_t)f * a.T + t - 1] : 0.0f;
             const Noise nz = make_noise(a.seed, f, sh.st.timestep, n, &sh.flag);
             __syncthreads();
-            fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, nullptr, a.bmax, a.objective);
+            if (t + 1 < t1) fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, nullptr, a.bmax, a.objective);
         }
-        // reverse over the segment's ticks
+        // reverse over the segment's ticks, re-recording each
         for (int t = t1 - 1; t >= t0; --t) {
             const float* sx = seg + (size_t)(t - t0) * 2 * np;
             for (int i = threadIdx.x; i < n; i += kThreads) {
@@ -1262,6 +1289,7 @@ __global__ void __launch_bounds__(kThreads) grad_backward_kernel(const GArgs a, 
             fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, rec, a.bmax, a.objective);
             const float wt = a.w ? a.w[(size_t)f * a.T + t] : 1.0f;
             bwd_tick(cfg, n, np, xb, vb, work, sh, sa, nz, rec, a.bmax, wt, a.objective);
+        }
         }
         if (t0 == 0) init_adjoint(a, f, n, xb, sh, sa);
         for (int i = threadIdx.x; i < n; i += kThreads) {
@@ -1316,6 +1344,8 @@ struct svpf_grad {
     float* d_seg = nullptr;
     GState* d_segs = nullptr;
     float* d_rec = nullptr;
+    TickScalars* d_segts = nullptr;
+    bool seg_rec = false;             // records of a whole segment (k ticks per CTA)
     int* d_status = nullptr;
     const float* u_theta = nullptr;   // the arrays the last forward used
     const float* u_gamma = nullptr;
@@ -1359,6 +1389,8 @@ GArgs make_gargs(const svpf_grad* g, const float* theta, const float* gamma, con
     a.segs = g->d_segs;
     a.rec = g->d_rec;
     a.rec_floats = g->rec_floats;
+    a.segts = g->d_segts;
+    a.seg_rec = g->seg_rec ? 1 : 0;
     a.nseg = g->nseg;
     a.status = g->d_status;
     a.objective = g->objective;
@@ -1432,7 +1464,16 @@ svpf_grad_t* svpf_grad_create(int F, const int* ns, const svpf_config_t* cfgs, i
               galloc(&g->d_fv, F * np) && galloc(&g->d_fs, F) && galloc(&g->d_ck, F * g->nseg * 2 * np) &&
               galloc(&g->d_cks, (size_t)F * g->nseg) && galloc(&g->d_ax, F * np) && galloc(&g->d_av, F * np) &&
               galloc(&g->d_as, F) && galloc(&g->d_seg, G * k * 2 * np) && galloc(&g->d_segs, G * k) &&
-              galloc(&g->d_rec, G * g->rec_floats) && galloc(&g->d_status, F);
+              galloc(&g->d_segts, G * k) && galloc(&g->d_status, F);
+    // records of whole segments when they take at most a quarter of the free
+    // device memory (and 16 GiB); else one tick's record per CTA
+    if (ok) {
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        const size_t seg_bytes = G * (size_t)k * g->rec_floats * sizeof(float);
+        g->seg_rec = seg_bytes <= std::min(free_b / 4, (size_t)16 << 30) && galloc(&g->d_rec, G * k * g->rec_floats);
+        if (!g->seg_rec) ok = galloc(&g->d_rec, G * g->rec_floats);
+    }
     ok = ok && cudaMemcpy(g->d_n, ns, F * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(g->d_cfg, cfgs, F * sizeof(svpf_config_t), cudaMemcpyHostToDevice) == cudaSuccess;
     if (!ok) {
@@ -1447,7 +1488,7 @@ void svpf_grad_destroy(svpf_grad_t* g) {
     if (g->stream) cudaStreamSynchronize(g->stream);
     void* ptrs[] = {g->d_n, g->d_cfg, g->d_theta, g->d_gamma, g->d_y, g->d_w, g->d_loglik, g->d_llsum,
                     g->d_fx, g->d_fv, g->d_fs, g->d_ck, g->d_cks, g->d_ax, g->d_av, g->d_as, g->d_seg,
-                    g->d_segs, g->d_rec, g->d_status};
+                    g->d_segs, g->d_rec, g->d_segts, g->d_status};
     for (void* p : ptrs) cudaFree(p);
     if (g->own_stream) cudaStreamDestroy(g->stream);
     delete g;
@@ -1540,6 +1581,21 @@ int svpf_grad_backward(svpf_grad_t* g, const float* w, double* grad) {
 }
 
 int svpf_grad_checkpoint_every(const svpf_grad_t* g) { return g ? g->k : 0; }
+
+int svpf_grad_segment_records(const svpf_grad_t* g) { return g && g->seg_rec ? 1 : 0; }
+
+int svpf_grad_set_segment_records(svpf_grad_t* g, int on) {
+    if (!g) return SVPF_ERR_INVALID_ARG;
+    if ((on != 0) == g->seg_rec) return SVPF_OK;
+    if (cudaStreamSynchronize(g->stream) != cudaSuccess) return SVPF_ERR_CUDA;
+    float* r = nullptr;
+    const size_t per = (size_t)g->grid * g->rec_floats;
+    if (!galloc(&r, on ? per * g->k : per)) return SVPF_ERR_CUDA;
+    cudaFree(g->d_rec);
+    g->d_rec = r;
+    g->seg_rec = on != 0;
+    return SVPF_OK;
+}
 
 int svpf_grad_set_objective(svpf_grad_t* g, int objective) {
     if (!g || (objective != SVPF_GRAD_TICK_LOGLIK && objective != SVPF_GRAD_PREDICTIVE)) return SVPF_ERR_INVALID_ARG;

@@ -168,6 +168,8 @@ def lib() -> C.CDLL:
         "svpf_grad_forward_device": (_I, [vp, vp, vp, vp, _I, C.c_ulonglong, vp]),
         "svpf_grad_backward_device": (_I, [vp, vp, vp]),
         "svpf_grad_checkpoint_every": (_I, [vp]),
+        "svpf_grad_segment_records": (_I, [vp]),
+        "svpf_grad_set_segment_records": (_I, [vp, _I]),
         "svpf_grad_set_objective": (_I, [vp, _I]),
         "svpf_stream_create": (vp, [_I, C.c_size_t, _I, vp]),
         "svpf_stream_destroy": (None, [vp]),
@@ -649,6 +651,15 @@ class Grad:
     @property
     def checkpoint_every(self) -> int:
         return int(lib().svpf_grad_checkpoint_every(self._g))
+
+    @property
+    def segment_records(self) -> bool:
+        """True when the backward records whole checkpoint segments."""
+        return bool(lib().svpf_grad_segment_records(self._g))
+
+    @segment_records.setter
+    def segment_records(self, on: bool):
+        self._check(lib().svpf_grad_set_segment_records(self._g, int(bool(on))))
 
     def _check(self, rc):
         if rc != SVPF_OK:

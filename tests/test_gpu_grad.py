@@ -119,6 +119,25 @@ def test_checkpoint_interval_does_not_change_the_gradient(pkg):
         assert np.array_equal(gr, out[0][1])
 
 
+def test_segment_records_give_the_same_bits(pkg):
+    """Recording a whole checkpoint segment in one forward and re-recording
+    each tick before its adjoint are the same computation."""
+    cfg = pkg.grad_config(4, 12.0)
+    ns = [128, 300, 64]
+    th = thetas_for(3, 6)
+    ys = paths_for(th, 20)
+    out = []
+    for on in (True, False):
+        g = pkg.Grad(ns, cfg, T_max=20, checkpoint_every=7)
+        g.segment_records = on
+        assert g.segment_records == on
+        ll, _ = g.forward(th, ys, seed=2)
+        out.append((ll, g.backward()))
+        g.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+
+
 def test_weights_select_ticks(pkg):
     """A one-hot weight on tick t gives the gradient of loglik_t alone, and
     weights combine linearly."""
