@@ -104,3 +104,47 @@ def sv2_path(T: int, mu: float, rho_fast: float, sigma_fast: float, rho_slow: fl
         h[t] = mu + f + s
         y[t] = np.exp(h[t] / 2.0) * eta
     return h, y.astype(np.float32)
+
+
+SCENARIOS = ("regime", "spike", "jumps", "fat_tails", "crisis")
+
+
+def scenario_path(name: str, T: int, seed: int):
+    """The scenario sweep on the 1-factor SV model (base mu=-1, rho=0.97,
+    sigma_z=0.15, Gaussian eta; counter-based draws as sv_path):
+      regime    mu steps from -1 to +1 at T/2
+      spike     +3 added to h at a seeded 1% of ticks (a shock the AR(1) carries on)
+      jumps     compound Poisson in h: rate 0.01 per tick, N(0, 2^2) sizes
+      fat_tails Student-t eta with nu = 5 (chi-square from 5 squared normals)
+      crisis    sigma_z = 0.4, rho = 0.99
+    Returns (h[T], y[T] float32, filter params (rho, sigma_z, mu), nu of the
+    filter's likelihood)."""
+    mu, rho, sz = -1.0, 0.97, 0.15
+    if name == "crisis":
+        rho, sz = 0.99, 0.4
+    k = 5 if name == "fat_tails" else 0
+    per = 5 + k
+    c = np.arange(per * T + 2, dtype=np.uint64) + np.uint64(seed) * np.uint64(1 << 40) + np.uint64(3 << 38)
+    u = _unit(splitmix64(c))
+    u2 = _unit(splitmix64(c ^ np.uint64(0x3333333333333333))) - (1.0 / 16777216.0)
+    g = np.sqrt(-2.0 * np.log(u)) * np.cos(2.0 * np.pi * u2)
+    h = np.empty(T)
+    y = np.empty(T)
+    hv = mu + sz / np.sqrt(1.0 - rho * rho) * g[0]
+    for t in range(T):
+        b = 1 + per * t
+        m = mu
+        if name == "regime" and t >= T // 2:
+            m = 1.0
+        hv = m + rho * (hv - m) + sz * g[b]
+        if name == "spike" and u[b + 2] < 0.01:
+            hv += 3.0
+        if name == "jumps" and u[b + 3] < 0.01:    # Poisson(0.01): two or more jumps per tick are ~5e-5
+            hv += 2.0 * g[b + 4]
+        eta = g[b + 1]
+        if k:
+            eta = eta / np.sqrt(np.sum(g[b + 5:b + 5 + k] ** 2) / k)
+        h[t] = hv
+        y[t] = np.exp(hv / 2.0) * eta
+    nu = 5.0 if name == "fat_tails" else 30.0
+    return h, y.astype(np.float32), (rho, sz, mu), nu
