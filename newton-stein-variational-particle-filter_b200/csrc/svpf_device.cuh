@@ -486,18 +486,18 @@ __device__ inline Smem carve(float* base, int n, int C, int rank, bool heun) {
 // mixture's log-responsibilities (the reference scans all N twice,
 // :453-459) comes either from the nearest of the means sorted once per tick
 // (binary search; the throughput kernel, where the sort is amortised over a
-// large filter) or, with ONLINE, from a running minimum inside the same pass
-// (the latency kernel: no sort, whose ~log2(N)^2/2 block barriers cost more
-// than the pass itself at N <= 1024 on a cluster).
+// large filter) or, with SCAN, from a branch-free min pass over the unsorted
+// means before the sum pass (the latency kernel: no sort, whose ~log2(N)^2/2
+// block barriers cost more than the extra pass at N <= 1024 on a cluster).
 // ---------------------------------------------------------------------------
-template <int R, int S, bool STUDENT, bool ONLINE = false>
+template <int R, int S, bool STUDENT, bool SCAN = false>
 __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_config_t& cfg,
                           float beta, float* __restrict__ lw_out, const Team& team) {
     // Positions arrive in transport coordinates hs = (h - center) / bw.  The
     // Gaussian prior runs in scaled prior coordinates x = (h - mu_center) * sc
     // with sc^2 = log2(e) / (2 sigma^2), where the log-responsibility in base 2
-    // is -(x - m)^2 and the means m are stored scaled the same way; the pair
-    // then costs one FADD, one FFMA, one ex2 and two accumulations.
+    // is -(x - m)^2 and the sorted means m are stored scaled the same way; the
+    // pair then costs one FADD, one FFMA, one ex2 and two accumulations.
     constexpr int G = kThreads / S;
     const int grp = threadIdx.x / S, q = threadIdx.x % S;
     const float* __restrict__ hc = sm.h[cur];
@@ -512,161 +512,6 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
     const float nus2 = cfg.nu_state * s2, inv_nus2 = 1.0f / nus2, np1 = cfg.nu_state + 1.0f;
     const float half_np1 = 0.5f * np1;
 
-    if constexpr (ONLINE) {
-    for (int base = 0; base < nloc; base += G * R) {
-        float hj[R], xj[R], rm[R], sr[R], wg[R], wh[R];
-        int jl[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            jl[r] = base + r * G + grp;
-            const int j = sm.row0 + min(jl[r], nloc - 1);
-            hj[r] = fmaf(hc[j], pl.bw, pl.center);
-            xj[r] = STUDENT ? hj[r] : (hj[r] - pl.mu_center) * sc;
-            rm[r] = 3.0e38f;
-        }
-        // Online row maximum: q is the negated base-2 log-responsibility
-        // (Gaussian: (x - m)^2 in scaled coordinates; Student-t: (nu+1)/2
-        // lg2(1 + d^2/(nu s2))).  Each thread keeps its running minimum rm of
-        // q and sums relative to it; a chunk of four columns with a smaller q
-        // rescales the sums by 2^(new - old) (rare after the first chunks).
-        // The result is the reference's max-then-sum up to rounding.
-        if (!STUDENT) {
-            float2 x2[R], sr2[R], wg2[R];
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                x2[r] = f2(xj[r]);
-                sr2[r] = f2(0.0f);
-                wg2[r] = f2(0.0f);
-            }
-            for (int cb = q * 4; cb < nv; cb += 4 * S) {
-                const float4 m4 = *reinterpret_cast<const float4*>(mu + cb);
-                const float2 ma = make_float2(m4.x, m4.y), mb = make_float2(m4.z, m4.w);
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const float2 da = fma2(ma, f2(-1.0f), x2[r]);   // x - m
-                    const float2 db = fma2(mb, f2(-1.0f), x2[r]);
-                    const float2 qa = mul2(da, da), qb = mul2(db, db);
-                    const float cm = fminf(fminf(qa.x, qa.y), fminf(qb.x, qb.y));
-                    if (cm < rm[r]) {
-                        const float2 f = f2(ex2_approx(cm - rm[r]));
-                        sr2[r] = mul2(sr2[r], f);
-                        wg2[r] = mul2(wg2[r], f);
-                        rm[r] = cm;
-                    }
-                    const float2 nr = f2(-rm[r]);
-                    const float2 ta = add2(qa, nr), tb = add2(qb, nr);   // >= 0
-                    const float2 wa = make_float2(ex2_approx(-ta.x), ex2_approx(-ta.y));
-                    const float2 wb = make_float2(ex2_approx(-tb.x), ex2_approx(-tb.y));
-                    sr2[r] = add2(sr2[r], wa);
-                    wg2[r] = fma2(wa, da, wg2[r]);
-                    sr2[r] = add2(sr2[r], wb);
-                    wg2[r] = fma2(wb, db, wg2[r]);
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                sr[r] = sr2[r].x + sr2[r].y;
-                wg[r] = wg2[r].x + wg2[r].y;
-                wh[r] = 0.0f;
-            }
-        } else {
-#pragma unroll
-            for (int r = 0; r < R; ++r) sr[r] = wg[r] = wh[r] = 0.0f;
-            for (int cb = q * 4; cb < nv; cb += 4 * S) {
-                const float4 m4 = *reinterpret_cast<const float4*>(mu + cb);
-                const float mm[4] = {m4.x, m4.y, m4.z, m4.w};
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    float d[4], d2[4], qq[4];
-                    float cm = 3.0e38f;
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        d[e] = xj[r] - mm[e];
-                        d2[e] = d[e] * d[e];
-                        qq[e] = half_np1 * lg2_approx(fmaf(d2[e], inv_nus2, 1.0f));
-                        cm = fminf(cm, qq[e]);
-                    }
-                    if (cm < rm[r]) {
-                        const float f = ex2_approx(cm - rm[r]);
-                        sr[r] *= f;
-                        wg[r] *= f;
-                        wh[r] *= f;
-                        rm[r] = cm;
-                    }
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const float w = ex2_approx(rm[r] - qq[e]);
-                        const float iden = rcp_approx(nus2 + d2[e]);
-                        sr[r] += w;
-                        wg[r] = fmaf(w * d[e], iden, wg[r]);
-                        wh[r] = fmaf(w * (nus2 - d2[e]), iden * iden, wh[r]);
-                    }
-                }
-            }
-        }
-        // combine the S column slices at their common minimum
-#pragma unroll
-        for (int o = S / 2; o > 0; o >>= 1) {
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const float om = __shfl_xor_sync(0xffffffffu, rm[r], o);
-                const float osr = __shfl_xor_sync(0xffffffffu, sr[r], o);
-                const float owg = __shfl_xor_sync(0xffffffffu, wg[r], o);
-                const float owh = STUDENT ? __shfl_xor_sync(0xffffffffu, wh[r], o) : 0.0f;
-                const float nm = fminf(rm[r], om);
-                const float fa = ex2_approx(nm - rm[r]), fb = ex2_approx(nm - om);
-                sr[r] = sr[r] * fa + osr * fb;
-                wg[r] = wg[r] * fa + owg * fb;
-                if (STUDENT) wh[r] = wh[r] * fa + owh * fb;
-                rm[r] = nm;
-            }
-        }
-        if (q == 0) {
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                if (jl[r] >= nloc) continue;
-                const int j = sm.row0 + jl[r];
-                const float h = hj[r];
-                float gp, hp;
-                if (!STUDENT) {
-                    gp = -(wg[r] / sc) * inv_s2 / (sr[r] + 1e-8f);
-                    hp = -inv_s2;
-                } else {
-                    gp = -np1 * wg[r] / (sr[r] + 1e-8f);
-                    hp = -np1 * wh[r] / (sr[r] + 1e-8f);
-                }
-                // likelihood (:475-499)
-                const float vol = expf(fminf(h, 20.0f));
-                const float y2 = pl.y_t * pl.y_t;
-                const float A = y2 / (vol + 1e-8f) / nu;
-                const float opA = 1.0f + A;
-                const float lw = pl.fan ? 0.0f
-                                        : pl.stc - 0.5f * h - (nu + 1.0f) * 0.5f * log1pf(fmaxf(A, -0.999f));
-                float glik;
-                if (cfg.use_exact_gradient) glik = -0.5f + 0.5f * (nu + 1.0f) * A / opA - cfg.lik_offset;
-                else glik = (logf(y2 + 1e-10f) - h + cfg.lik_offset) / 1.4f;
-                const float eb = pl.fan ? 1.0f : beta;
-                const float gg = clampf(gp + eb * glik, -10.0f, 10.0f);
-                float score = gg, cc = 0.0f;
-                if (pl.transport != 0) {
-                    const float hl = -0.5f * (nu + 1.0f) * A / (opA * opA);
-                    const float curv = clampf(-(hl + hp), 0.1f, 100.0f);
-                    if (pl.transport == 2) {
-                        cc = curv;
-                    } else {
-                        score = 0.7f * gg / curv;   // precond_grad (:519)
-                        cc = 1.0f / curv;           // 1/curvature (:765)
-                    }
-                }
-                for (int rk = 0; rk < team.size; ++rk) {
-                    team.at(sm.g, rk)[j] = score;
-                    team.at(sm.c, rk)[j] = cc;
-                }
-                lw_out[j] = lw;
-            }
-        }
-    }
-    } else {
     for (int base = 0; base < nloc; base += G * R) {
         float hj[R], xj[R], lm[R], sr[R], wg[R], wh[R];
         int jl[R];
@@ -675,14 +520,41 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
             jl[r] = base + r * G + grp;
             const int j = sm.row0 + min(jl[r], nloc - 1);
             hj[r] = fmaf(hc[j], pl.bw, pl.center);
-            if (STUDENT) {
-                xj[r] = hj[r];
-                lm[r] = nearest_lmax_student(mu, sm.n, hj[r], inv_nus2, half_np1);
-            } else {
-                xj[r] = (hj[r] - pl.mu_center) * sc;
-                lm[r] = nearest_d2(mu, sm.n, xj[r]);
+            xj[r] = STUDENT ? hj[r] : (hj[r] - pl.mu_center) * sc;
+            if (!SCAN) {
+                lm[r] = STUDENT ? nearest_lmax_student(mu, sm.n, hj[r], inv_nus2, half_np1)
+                                : nearest_d2(mu, sm.n, xj[r]);
             }
             sr[r] = 0.0f; wg[r] = 0.0f; wh[r] = 0.0f;
+        }
+        if (SCAN) {
+            // the smallest squared distance to any mean: a min over the row's
+            // columns (this lane's slice, then across the S lanes); the same
+            // value as the nearest sorted mean gives
+            float mn[R];
+            float2 x2[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                mn[r] = 3.0e38f;
+                x2[r] = f2(xj[r]);
+            }
+            for (int cb = q * 4; cb < nv; cb += 4 * S) {
+                const float4 m4 = *reinterpret_cast<const float4*>(mu + cb);
+                const float2 ma = make_float2(m4.x, m4.y), mb = make_float2(m4.z, m4.w);
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const float2 da = fma2(ma, f2(-1.0f), x2[r]), db = fma2(mb, f2(-1.0f), x2[r]);
+                    const float2 qa = mul2(da, da), qb = mul2(db, db);
+                    mn[r] = fminf(mn[r], fminf(fminf(qa.x, qa.y), fminf(qb.x, qb.y)));
+                }
+            }
+#pragma unroll
+            for (int o = S / 2; o > 0; o >>= 1) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) mn[r] = fminf(mn[r], __shfl_xor_sync(0xffffffffu, mn[r], o));
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) lm[r] = STUDENT ? -half_np1 * kLn2 * lg2_approx(fmaf(mn[r], inv_nus2, 1.0f)) : mn[r];
         }
         if (!STUDENT) {
             // two columns per packed op: 3 issue slots and 2 ex2 per column pair
@@ -789,7 +661,6 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
                 lw_out[j] = lw;
             }
         }
-    }
     }
 }
 

@@ -18,7 +18,7 @@ __device__ __forceinline__ void copy_words(T* dst, const T* src) {
     for (int k = threadIdx.x; k < (int)(sizeof(T) / 4); k += kThreads) d[k] = s[k];
 }
 
-template <int R, int S, bool ONLINE>
+template <int R, int S, bool SCAN>
 __global__ void __launch_bounds__(kThreads, 1) single_tick_kernel(const __grid_constant__ SingleArgs a) {
     extern __shared__ __align__(16) float smem[];
     __shared__ Plan pl;
@@ -36,7 +36,7 @@ __global__ void __launch_bounds__(kThreads, 1) single_tick_kernel(const __grid_c
     const Noise nz{philox_key(a.seed, 0), (uint32_t)ctl.timestep, a.tape_n, a.tape_u,
                    a.slots_n, a.slots_u, a.n, &pl.flag};
     const FilterIO io{a.h, a.hp, a.v, a.lw, a.n};
-    run_tick<R, S, ONLINE>(cfg, prm, ctl, a.y_t, a.y_prev, io, nz, sm, pl, team, out);
+    run_tick<R, S, SCAN>(cfg, prm, ctl, a.y_t, a.y_prev, io, nz, sm, pl, team, out);
     if (team.rank == 0) {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -75,15 +75,15 @@ __global__ void __launch_bounds__(kThreads) single_tick_2f_kernel(const __grid_c
     }
 }
 
-// Mixture row maximum of the single-factor tick tracked online up to this many
+// Mixture row maximum of the single-factor tick from a min pass up to this many
 // particles (no sort: measured faster on B200 at N <= 1024), from the sorted
 // prior means above it.
-constexpr int kOnlineMaxN = 1024;
+constexpr int kScanMaxN = 1024;
 
-template <int R, int S, bool TWO_FACTOR = false, bool ONLINE = false>
+template <int R, int S, bool TWO_FACTOR = false, bool SCAN = false>
 static cudaError_t launch_single_t(const SingleArgs& a, int C, cudaStream_t s) {
     const size_t smem = TWO_FACTOR ? tick_smem_bytes_2f(a.n, C) : tick_smem_bytes(a.n, C, a.cfg.use_heun != 0);
-    auto kern = TWO_FACTOR ? single_tick_2f_kernel<R, S> : single_tick_kernel<R, S, ONLINE>;
+    auto kern = TWO_FACTOR ? single_tick_2f_kernel<R, S> : single_tick_kernel<R, S, SCAN>;
     static bool configured[kMaxCluster + 1] = {};
     cudaError_t e;
     if (!configured[0]) {

@@ -40,12 +40,12 @@ __device__ float stein_dispatch(int kind, bool ksd, const Smem& sm, int cur, con
                : stein_rows<R, S, 0, false, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out);
 }
 
-template <int R, int S, bool ONLINE>
+template <int R, int S, bool SCAN>
 __device__ __forceinline__ void grad_dispatch(bool student, const Smem& sm, int cur, const Plan& pl,
                                               const svpf_config_t& cfg, float beta, float* lw,
                                               const Team& team) {
-    if (student) grad_pass<R, S, true, ONLINE>(sm, cur, pl, cfg, beta, lw, team);
-    else grad_pass<R, S, false, ONLINE>(sm, cur, pl, cfg, beta, lw, team);
+    if (student) grad_pass<R, S, true, SCAN>(sm, cur, pl, cfg, beta, lw, team);
+    else grad_pass<R, S, false, SCAN>(sm, cur, pl, cfg, beta, lw, team);
 }
 
 // KSD of the last iteration: block sum, then member partials into rank 0.
@@ -58,10 +58,10 @@ __device__ __forceinline__ void ksd_publish(float ksd_thread, Plan& pl, const Te
 
 // The tick.  cfg/prm/ctl are shared-memory copies owned by the caller; only
 // thread 0 of rank 0 mutates ctl after make_plan.  Returns on every member; the
-// caller stores ctl/out from rank 0 thread 0.  ONLINE: the mixture's row
-// maximum is tracked inside the gradient pass instead of sorting the prior
-// means (the single-filter latency kernel).
-template <int R, int S, bool ONLINE = false>
+// caller stores ctl/out from rank 0 thread 0.  SCAN: the mixture's row
+// maximum comes from a min pass over the unsorted prior means instead of the
+// means sorted once per tick (the single-filter latency kernel).
+template <int R, int S, bool SCAN = false>
 __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_ctl_t& ctl, float y_t,
                          float y_prev, const FilterIO& io, const Noise& nz, const Smem& sm, Plan& pl,
                          const Team& team, svpf_out_t& out) {
@@ -169,7 +169,7 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
         pl.prior_scale = sqrtf(kLog2e * 0.5f / (pl.sz_eff * pl.sz_eff));
     }
     // ---- sort prior means once per tick (used for the per-row maximum)
-    if constexpr (!ONLINE) bitonic_sort(sm.mu, sm.p2);
+    if constexpr (!SCAN) bitonic_sort(sm.mu, sm.p2);
     else __syncthreads();   // plan scalars of thread 0 visible to all
     // ---- Stein-loop coordinates: positions (h - center) / bw, Gaussian prior
     //      means (mu - mu_center) * prior_scale (order preserving)
@@ -194,7 +194,7 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
         const float bf = sqrtf(beta);
         const bool last = it == budget - 1;
         if (!cfg.use_heun) {
-            grad_dispatch<R, S, ONLINE>(student, sm, cur, pl, cfg, beta, io.lw, team);
+            grad_dispatch<R, S, SCAN>(student, sm, cur, pl, cfg, beta, io.lw, team);
             team.sync();
             const float kt = stein_dispatch<R, S, kTransport>(pl.transport, last, sm, cur, pl, cfg, bf, nz, kn, team);
             if (last) ksd_publish(kt, pl, team);
@@ -205,7 +205,7 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
             // kernels svpf_opt_kernels.cu:1293-1566)
             const int nloc = sm.row1 - sm.row0;
             const float es = pl.eps_step * bf;
-            grad_dispatch<R, S, ONLINE>(student, sm, cur, pl, cfg, beta, io.lw, team);
+            grad_dispatch<R, S, SCAN>(student, sm, cur, pl, cfg, beta, io.lw, team);
             team.sync();
             stein_dispatch<R, S, kPhiOnly>(pl.transport, false, sm, cur, pl, cfg, bf, nz, kn, team, sm.phi0);
             __syncthreads();
@@ -217,7 +217,7 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
                 for (int rk = 0; rk < team.size; ++rk) team.at(sm.h[cur ^ 1], rk)[i] = hs;
             }
             team.sync();
-            grad_dispatch<R, S, ONLINE>(student, sm, cur ^ 1, pl, cfg, beta, io.lw, team);
+            grad_dispatch<R, S, SCAN>(student, sm, cur ^ 1, pl, cfg, beta, io.lw, team);
             team.sync();
             stein_dispatch<R, S, kPhiOnly>(pl.transport, false, sm, cur ^ 1, pl, cfg, bf, nz, kn, team, sm.phi1);
             if (last) {
