@@ -48,6 +48,7 @@ __global__ void __launch_bounds__(kThreads, 2) batch_tick_kernel(const __grid_co
         // request mode: y_t from the request, y_prev from the filter's record
         const float yt = a.req_y ? a.req_y[w] : a.y_t[f];
         const float yp = a.req_y ? ctl.y_prev : a.y_prev[f];
+        if (threadIdx.x == 0) pl.have_consts = 0;   // make_plan computes the per-tick constants
         switch (a.tile[f]) {
             case 1: run_tick<1, 4>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
             case 2: run_tick<1, 2>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;

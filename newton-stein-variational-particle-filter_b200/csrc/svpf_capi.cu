@@ -2,6 +2,8 @@
 // entry points over the one-launch-per-tick kernel, and the batch API over the
 // persistent kernel.
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -133,6 +135,9 @@ struct Impl {
     svpf_out_t* res_out = nullptr;
     svpf_ctl_t* dev_res_ctl = nullptr;
     svpf_out_t* dev_res_out = nullptr;
+    unsigned int* done = nullptr;     // host-mapped completion word of the last step
+    unsigned int* dev_done = nullptr;
+    unsigned int seq = 0;
     svpf_ctl_t cache;                 // control fields without an SVPFState counterpart
     svpf_out_t last{};
     float* tape_n = nullptr;
@@ -249,6 +254,31 @@ int pick_cluster_2f(const SVPFState* s, const Impl* im) {
     return C <= 16 ? C : 0;
 }
 
+// Wait for the step launched last: poll its host-mapped completion word for up
+// to 2 ms (a blocking step's result is then read without a stream
+// synchronisation), else synchronise the stream, which also reports a failed
+// launch.  The kernel's other CTAs may still be retiring when the word
+// arrives: every host function below that touches the filter's device arrays
+// outside the stream synchronises it first (quiesce).
+cudaError_t wait_done(Impl* im, cudaStream_t stream) {
+    const volatile unsigned int* w = im->done;
+    const unsigned int want = im->seq;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (unsigned int k = 1;; ++k) {
+        if (*w == want) {
+            std::atomic_thread_fence(std::memory_order_acquire);   // the records written before the word
+            return cudaSuccess;
+        }
+        if ((k & 1023u) == 0u && std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(2)) break;
+    }
+    return cudaStreamSynchronize(stream);
+}
+
+void quiesce(const SVPFState* s) {
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    else cudaDeviceSynchronize();
+}
+
 void step_impl(SVPFState* s, float y_t, float y_prev, const SVPFParams* params,
                unsigned long long seed, float* ll, float* vol, float* hm) {
     Impl* im = impl_of(s);
@@ -282,6 +312,13 @@ void step_impl(SVPFState* s, float y_t, float y_prev, const SVPFParams* params,
     }
     a.ctl_out = im->dev_res_ctl;
     a.out = im->dev_res_out;
+    a.done = im->dev_done;
+    a.seq = ++im->seq;
+    // per-tick constants of the single-factor plan, on the host (svpf_optimized_graph.cu:951-953;
+    // the EKF observation log y^2, include/svpf_kernels.cuh:509-541)
+    a.host_consts = 1;
+    a.stc = lgammaf((s->nu + 1.0f) * 0.5f) - lgammaf(s->nu * 0.5f) - 0.5f * logf(3.14159265358979f * s->nu);
+    a.log_y2 = std::log((double)y_t * (double)y_t + 1e-8);
     const int C = tf ? pick_cluster_2f(s, im) : pick_cluster(s, im);
     if (C < 1) {
         set_err(s, SVPF_ERR_UNSUPPORTED);
@@ -289,7 +326,7 @@ void step_impl(SVPFState* s, float y_t, float y_prev, const SVPFParams* params,
     }
     const int tile = im->tile >= 0 ? im->tile : default_single_tile(s->n_particles, C);
     cudaError_t e = tf ? launch_single_2f(a, C, tile, s->stream) : launch_single(a, C, tile, s->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess) e = wait_done(im, s->stream);
     if (e != cudaSuccess) {
         set_err(s, SVPF_ERR_CUDA);
         return;
@@ -329,6 +366,9 @@ SVPFState* svpf_create(int n_particles, int n_stein_steps, float nu, cudaStream_
          cudaHostAlloc(&im->res_out, sizeof(svpf_out_t), cudaHostAllocMapped) == cudaSuccess;
     ok = ok && cudaHostGetDevicePointer((void**)&im->dev_res_ctl, im->res_ctl, 0) == cudaSuccess &&
          cudaHostGetDevicePointer((void**)&im->dev_res_out, im->res_out, 0) == cudaSuccess;
+    ok = ok && cudaHostAlloc(&im->done, sizeof(unsigned int), cudaHostAllocMapped) == cudaSuccess &&
+         cudaHostGetDevicePointer((void**)&im->dev_done, im->done, 0) == cudaSuccess;
+    if (ok) *im->done = 0;
     if (ok) {
         ok = cudaMemset(s->h, 0, bytes) == cudaSuccess && cudaMemset(s->h_prev, 0, bytes) == cudaSuccess &&
              cudaMemset(s->log_weights, 0, bytes) == cudaSuccess && cudaMemset(s->d_grad_v, 0, bytes) == cudaSuccess &&
@@ -354,6 +394,7 @@ void svpf_destroy(SVPFState* s) {
     if (im) {
         if (im->res_ctl) cudaFreeHost(im->res_ctl);
         if (im->res_out) cudaFreeHost(im->res_out);
+        if (im->done) cudaFreeHost(im->done);
         if (im->tape_n) cudaFree(im->tape_n);
         if (im->tape_u) cudaFree(im->tape_u);
         cudaFree(im->h2);
@@ -371,6 +412,7 @@ void svpf_initialize(SVPFState* s, const SVPFParams* p, unsigned long long seed)
         if (s) set_err(s, SVPF_ERR_INVALID_ARG);
         return;
     }
+    quiesce(s);
     s->timestep = 0;
     s->y_prev = 0.0f;
     s->nu_state = fmaxf(s->nu_state, 2.5f);
@@ -496,6 +538,7 @@ void svpf_run_sequence_device(SVPFState* s, const float* d_obs, int T, const SVP
         return;
     }
     std::vector<float> obs(T), ll(T), vol(T);
+    quiesce(s);
     if (cudaMemcpy(obs.data(), d_obs, T * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) {
         set_err(s, SVPF_ERR_CUDA);
         return;
@@ -507,6 +550,7 @@ void svpf_run_sequence_device(SVPFState* s, const float* d_obs, int T, const SVP
 
 void svpf_get_particles(const SVPFState* s, float* h_out) {
     if (!s || !h_out) return;
+    quiesce(s);
     cudaMemcpy(h_out, s->h, s->n_particles * sizeof(float), cudaMemcpyDeviceToHost);
 }
 
@@ -514,6 +558,7 @@ void svpf_get_stats(const SVPFState* s, float* h_mean, float* h_std) {
     if (!s) return;
     const int n = s->n_particles;
     std::vector<float> h(n);
+    quiesce(s);
     cudaMemcpy(h.data(), s->h, n * sizeof(float), cudaMemcpyDeviceToHost);
     double sum = 0.0;
     for (float x : h) sum += x;
@@ -528,6 +573,7 @@ float svpf_get_ess(const SVPFState* s) {
     if (!s) return 0.0f;
     const int n = s->n_particles;
     std::vector<float> lw(n);
+    quiesce(s);
     cudaMemcpy(lw.data(), s->log_weights, n * sizeof(float), cudaMemcpyDeviceToHost);
     float mx = lw[0];
     for (float x : lw) mx = std::max(mx, x);
@@ -596,6 +642,7 @@ int svpf_set_state(SVPFState* s, const svpf_ctl_t* ctl, const float* h, const fl
     Impl* im = impl_of(s);
     if (!s || !im) return SVPF_ERR_INVALID_ARG;
     const size_t b = (size_t)s->n_particles * sizeof(float);
+    quiesce(s);
     if (ctl) ctl_scatter(ctl, s, im);
     if (h && cudaMemcpy(s->h, h, b, cudaMemcpyHostToDevice) != cudaSuccess) return SVPF_ERR_CUDA;
     if (hp && cudaMemcpy(s->h_prev, hp, b, cudaMemcpyHostToDevice) != cudaSuccess) return SVPF_ERR_CUDA;
@@ -623,6 +670,7 @@ int svpf_set_state_2f(SVPFState* s, const float* hf, const float* hs, const floa
     const size_t n = (size_t)s->n_particles, b = n * sizeof(float);
     float* dst[6] = {im->h2, im->h2 + n, im->hp2, im->hp2 + n, im->v2, im->v2 + n};
     const float* src[6] = {hf, hs, hfp, hsp, vf, vs};
+    quiesce(s);
     for (int k = 0; k < 6; ++k)
         if (src[k] && cudaMemcpy(dst[k], src[k], b, cudaMemcpyHostToDevice) != cudaSuccess) return SVPF_ERR_CUDA;
     return SVPF_OK;
@@ -636,6 +684,7 @@ int svpf_set_noise_tape(SVPFState* s, const float* normals, int ns, const float*
         return SVPF_OK;
     }
     if (ns < 1 || nu_ < 0 || (nu_ > 0 && !uniforms)) return set_err(s, SVPF_ERR_INVALID_ARG);
+    quiesce(s);
     const size_t n = (size_t)s->n_particles;
     if (!grow(&im->tape_n, &im->cap_n, ns * n * sizeof(float)) ||
         !grow(&im->tape_u, &im->cap_u, std::max(nu_, 1) * n * sizeof(float)))

@@ -160,6 +160,8 @@ struct Plan {
     int transport;         // 0 vanilla, 1 Newton, 2 full Newton
     int fan;
     int flag;              // tape overrun etc.
+    int have_consts;       // stc / log_y2 set by the launcher (single-filter tick)
+    double log_y2;
     FactorPlan fac[2];     // two-factor: fast, slow
     float fmean[2];        // two-factor: factor means of the previous tick (guide)
     float gmean2[2];       // two-factor: EKF guide means
@@ -179,6 +181,8 @@ __device__ __forceinline__ float adaptive_beta(float ksd_prev, int ai, int na) {
 }
 
 // Scalar control of a tick; writes the updated EKF/sigma fields into ctl.
+// pl.have_consts: pl.stc and pl.log_y2 were filled by the caller (the
+// single-filter launcher computes them on the host), else they are computed here.
 __device__ inline void make_plan(const svpf_config_t& c, const SVPFParams& p, svpf_ctl_t& s,
                           float y_t, float y_prev, Plan& pl) {
     const int t = s.timestep;
@@ -199,7 +203,8 @@ __device__ inline void make_plan(const svpf_config_t& c, const SVPFParams& p, sv
         s.sigma_z_effective = pl.sz_eff;
     }
     // Student-t normaliser (:951-953) and the create-time implied offset
-    pl.stc = lgammaf((c.nu + 1.0f) * 0.5f) - lgammaf(c.nu * 0.5f) - 0.5f * logf(3.14159265358979f * c.nu);
+    if (!pl.have_consts)
+        pl.stc = lgammaf((c.nu + 1.0f) * 0.5f) - lgammaf(c.nu * 0.5f) - 0.5f * logf(3.14159265358979f * c.nu);
     pl.off = c.student_t_implied_offset;
     pl.rho_up = c.use_asymmetric_rho ? c.rho_up : p.rho;
     pl.rho_dn = c.use_asymmetric_rho ? c.rho_down : p.rho;
@@ -228,7 +233,7 @@ __device__ inline void make_plan(const svpf_config_t& c, const SVPFParams& p, sv
         }
         const double m_pred = mu + rho * (m - mu);
         const double P_pred = rho * rho * P + sz * sz;
-        const double log_y2 = log((double)y_t * (double)y_t + 1e-8);
+        const double log_y2 = pl.have_consts ? pl.log_y2 : log((double)y_t * (double)y_t + 1e-8);
         const double S = P_pred + (4.93 + 2.0);
         const double K = P_pred / (S + 1e-8);
         s.guide_mean = m_pred + K * (log_y2 - (m_pred - (double)pl.off));

@@ -35,6 +35,11 @@ struct SingleArgs {
     int slots_n, slots_u;
     svpf_ctl_t* ctl_out;   // host-mapped
     svpf_out_t* out;       // host-mapped
+    unsigned int* done;    // host-mapped completion word: seq once ctl_out / out are written
+    unsigned int seq;
+    int host_consts;       // 1: stc and log_y2 below were computed on the host
+    float stc;             // Student-t normaliser of cfg.nu
+    double log_y2;         // log(y_t^2 + 1e-8) for the EKF guide
 };
 
 struct BatchArgs {

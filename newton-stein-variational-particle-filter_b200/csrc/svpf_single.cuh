@@ -18,6 +18,15 @@ __device__ __forceinline__ void copy_words(T* dst, const T* src) {
     for (int k = threadIdx.x; k < (int)(sizeof(T) / 4); k += kThreads) d[k] = s[k];
 }
 
+// The host polls a.done instead of synchronising the stream: the result
+// records are made visible system-wide before the sequence number is.
+__device__ __forceinline__ void publish_done(const SingleArgs& a) {
+    if (a.done) {
+        __threadfence_system();
+        *reinterpret_cast<volatile unsigned int*>(a.done) = a.seq;
+    }
+}
+
 template <int R, int S, bool SCAN>
 __global__ void __launch_bounds__(kThreads, 1) single_tick_kernel(const __grid_constant__ SingleArgs a) {
     extern __shared__ __align__(16) float smem[];
@@ -36,12 +45,18 @@ __global__ void __launch_bounds__(kThreads, 1) single_tick_kernel(const __grid_c
     const Noise nz{philox_key(a.seed, 0), (uint32_t)ctl.timestep, a.tape_n, a.tape_u,
                    a.slots_n, a.slots_u, a.n, &pl.flag};
     const FilterIO io{a.h, a.hp, a.v, a.lw, a.n};
+    if (threadIdx.x == 0) {
+        pl.have_consts = a.host_consts;
+        pl.stc = a.stc;
+        pl.log_y2 = a.log_y2;
+    }
     run_tick<R, S, SCAN>(cfg, prm, ctl, a.y_t, a.y_prev, io, nz, sm, pl, team, out);
     if (team.rank == 0) {
         __syncthreads();
         if (threadIdx.x == 0) {
             *a.ctl_out = ctl;
             *a.out = out;
+            publish_done(a);
         }
     }
 }
@@ -71,6 +86,7 @@ __global__ void __launch_bounds__(kThreads) single_tick_2f_kernel(const __grid_c
         if (threadIdx.x == 0) {
             *a.ctl_out = ctl;
             *a.out = out;
+            publish_done(a);
         }
     }
 }
