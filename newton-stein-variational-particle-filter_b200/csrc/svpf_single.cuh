@@ -27,7 +27,7 @@ __device__ __forceinline__ void publish_done(const SingleArgs& a) {
     }
 }
 
-template <int R, int S, bool SCAN>
+template <int R, int S, bool SCAN, bool PROD>
 __global__ void __launch_bounds__(kThreads, 1) single_tick_kernel(const __grid_constant__ SingleArgs a) {
     extern __shared__ __align__(16) float smem[];
     __shared__ Plan pl;
@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(kThreads, 1) single_tick_kernel(const __grid_c
         pl.stc = a.stc;
         pl.log_y2 = a.log_y2;
     }
-    run_tick<R, S, SCAN>(cfg, prm, ctl, a.y_t, a.y_prev, io, nz, sm, pl, team, out);
+    run_tick<R, S, SCAN, PROD>(cfg, prm, ctl, a.y_t, a.y_prev, io, nz, sm, pl, team, out);
     if (team.rank == 0) {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -96,10 +96,16 @@ __global__ void __launch_bounds__(kThreads) single_tick_2f_kernel(const __grid_c
 // prior means above it.
 constexpr int kScanMaxN = 1024;
 
-template <int R, int S, bool TWO_FACTOR = false, bool SCAN = false>
+// The production configuration: full-Newton transport, Gaussian state noise,
+// no Heun step (the kernel compiled for it alone).
+inline bool is_production_tick(const svpf_config_t& c) {
+    return c.use_newton && c.use_full_newton && !c.use_heun && !c.use_student_t_state;
+}
+
+template <int R, int S, bool TWO_FACTOR = false, bool SCAN = false, bool PROD = false>
 static cudaError_t launch_single_t(const SingleArgs& a, int C, cudaStream_t s) {
     const size_t smem = TWO_FACTOR ? tick_smem_bytes_2f(a.n, C) : tick_smem_bytes(a.n, C, a.cfg.use_heun != 0);
-    auto kern = TWO_FACTOR ? single_tick_2f_kernel<R, S> : single_tick_kernel<R, S, SCAN>;
+    auto kern = TWO_FACTOR ? single_tick_2f_kernel<R, S> : single_tick_kernel<R, S, SCAN, PROD>;
     static bool configured[kMaxCluster + 1] = {};
     cudaError_t e;
     if (!configured[0]) {

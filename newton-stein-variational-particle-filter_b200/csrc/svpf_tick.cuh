@@ -60,8 +60,11 @@ __device__ __forceinline__ void ksd_publish(float ksd_thread, Plan& pl, const Te
 // thread 0 of rank 0 mutates ctl after make_plan.  Returns on every member; the
 // caller stores ctl/out from rank 0 thread 0.  SCAN: the mixture's row
 // maximum comes from a min pass over the unsorted prior means instead of the
-// means sorted once per tick (the single-filter latency kernel).
-template <int R, int S, bool SCAN = false>
+// means sorted once per tick (the single-filter latency kernel).  PROD: the
+// caller guarantees full-Newton transport, Gaussian state noise and no Heun
+// step (the production configuration), so only those code paths are compiled
+// and the kernel body stays small (instruction fetch bounds the latency kernel).
+template <int R, int S, bool SCAN = false, bool PROD = false>
 __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_ctl_t& ctl, float y_t,
                          float y_prev, const FilterIO& io, const Noise& nz, const Smem& sm, Plan& pl,
                          const Team& team, svpf_out_t& out) {
@@ -173,7 +176,7 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
     else __syncthreads();   // plan scalars of thread 0 visible to all
     // ---- Stein-loop coordinates: positions (h - center) / bw, Gaussian prior
     //      means (mu - mu_center) * prior_scale (order preserving)
-    const bool student = cfg.use_student_t_state != 0;
+    const bool student = PROD ? false : cfg.use_student_t_state != 0;
     if (pl.budget > 0) {
         for (int i = tid; i < n; i += kThreads) {
             sm.h[0][i] = (sm.h[0][i] - pl.center) * pl.inv_bw;
@@ -193,14 +196,22 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
         const float beta = pl.beta[ai];
         const float bf = sqrtf(beta);
         const bool last = it == budget - 1;
-        if (!cfg.use_heun) {
-            grad_dispatch<R, S, SCAN>(student, sm, cur, pl, cfg, beta, io.lw, team);
-            team.sync();
-            const float kt = stein_dispatch<R, S, kTransport>(pl.transport, last, sm, cur, pl, cfg, bf, nz, kn, team);
+        if (PROD || !cfg.use_heun) {
+            float kt;
+            if constexpr (PROD) {
+                grad_pass<R, S, false, SCAN>(sm, cur, pl, cfg, beta, io.lw, team);
+                team.sync();
+                kt = last ? stein_rows<R, S, 2, true, kTransport>(sm, cur, pl, cfg, bf, nz, kn, team, nullptr)
+                          : stein_rows<R, S, 2, false, kTransport>(sm, cur, pl, cfg, bf, nz, kn, team, nullptr);
+            } else {
+                grad_dispatch<R, S, SCAN>(student, sm, cur, pl, cfg, beta, io.lw, team);
+                team.sync();
+                kt = stein_dispatch<R, S, kTransport>(pl.transport, last, sm, cur, pl, cfg, bf, nz, kn, team);
+            }
             if (last) ksd_publish(kt, pl, team);
             team.sync();
             cur ^= 1;
-        } else {
+        } else if constexpr (!PROD) {
             // Heun predictor-corrector (svpf_optimized_graph.cu:1147-1232,
             // kernels svpf_opt_kernels.cu:1293-1566)
             const int nloc = sm.row1 - sm.row0;
