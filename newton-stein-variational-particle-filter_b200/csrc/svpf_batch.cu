@@ -60,6 +60,7 @@ struct svpf_batch {
     int grid = 0, grid2 = 0;
     int launches = 0;
     int heun = 0;
+    int prod = 0;                // every single-factor filter has the production configuration
     // graph
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -112,6 +113,7 @@ BatchArgs make_args(svpf_batch* b, const float* d_yt, const float* d_yp, svpf_ou
     a.slots_u = b->slots_u;
     a.tape_stride = b->n_max;
     a.heun = b->heun;
+    a.prod = b->prod;
     return a;
 }
 
@@ -157,7 +159,7 @@ extern "C" {
 svpf_batch_t* svpf_batch_create(int F, const int* ns, const svpf_config_t* cfgs, const SVPFParams* prms,
                                 cudaStream_t stream) {
     if (F < 1 || !ns || !cfgs || !prms) return nullptr;
-    int n_max = 0, n_max1 = 0, n_max2 = 0, F1 = 0, heun = 0;
+    int n_max = 0, n_max1 = 0, n_max2 = 0, F1 = 0, heun = 0, prod = 1;
     for (int f = 0; f < F; ++f) {
         if (ns[f] < 1 || ns[f] > SVPF_MAX_PARTICLES) return nullptr;
         n_max = std::max(n_max, ns[f]);
@@ -167,6 +169,7 @@ svpf_batch_t* svpf_batch_create(int F, const int* ns, const svpf_config_t* cfgs,
         } else {
             n_max1 = std::max(n_max1, ns[f]);
             heun |= cfgs[f].use_heun != 0;
+            prod &= is_production_tick(cfgs[f]) ? 1 : 0;
             ++F1;
         }
     }
@@ -174,6 +177,7 @@ svpf_batch_t* svpf_batch_create(int F, const int* ns, const svpf_config_t* cfgs,
     if (F1 < F && tick_smem_bytes_2f(n_max2, 1) > max_dyn_smem()) return nullptr;
     svpf_batch* b = new svpf_batch();
     b->heun = heun;
+    b->prod = prod;
     b->F = F;
     b->F1 = F1;
     b->F2 = F - F1;

@@ -16,6 +16,9 @@ __device__ __forceinline__ void copy_words(T* dst, const T* src) {
     for (int k = threadIdx.x; k < (int)(sizeof(T) / 4); k += kThreads) d[k] = s[k];
 }
 
+// PROD: launched only when every single-factor filter of the batch has the
+// production configuration (a.prod), so only its code paths are compiled.
+template <bool PROD>
 __global__ void __launch_bounds__(kThreads, 2) batch_tick_kernel(const __grid_constant__ BatchArgs a) {
     extern __shared__ __align__(16) float smem[];
     __shared__ Plan pl;
@@ -50,11 +53,11 @@ __global__ void __launch_bounds__(kThreads, 2) batch_tick_kernel(const __grid_co
         const float yp = a.req_y ? ctl.y_prev : a.y_prev[f];
         if (threadIdx.x == 0) pl.have_consts = 0;   // make_plan computes the per-tick constants
         switch (a.tile[f]) {
-            case 1: run_tick<1, 4>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
-            case 2: run_tick<1, 2>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
-            case 3: run_tick<1, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
-            case 4: run_tick<2, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
-            default: run_tick<4, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
+            case 1: run_tick<1, 4, false, PROD>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
+            case 2: run_tick<1, 2, false, PROD>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
+            case 3: run_tick<1, 1, false, PROD>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
+            case 4: run_tick<2, 1, false, PROD>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
+            default: run_tick<4, 1, false, PROD>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
         }
         if (a.req_y && threadIdx.x == 0) ctl.y_prev = yt;
         __syncthreads();
@@ -226,20 +229,23 @@ cudaError_t launch_batch_2f(const BatchArgs& a, size_t smem_bytes, int grid, cud
 int batch_grid(size_t smem_bytes) {
     static bool configured = false;
     if (!configured) {
-        cudaFuncSetAttribute(batch_tick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn_smem());
+        cudaFuncSetAttribute(batch_tick_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn_smem());
+        cudaFuncSetAttribute(batch_tick_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn_smem());
         configured = true;
     }
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_tick_kernel, kThreads, smem_bytes);
+    // both variants are bounded to 2 CTAs per SM by their launch bounds
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_tick_kernel<false>, kThreads, smem_bytes);
     if (per_sm < 1) return 0;
     return sms * per_sm;
 }
 
 cudaError_t launch_batch(const BatchArgs& a, size_t smem_bytes, int grid, cudaStream_t s) {
     if (grid < 1) return cudaErrorInvalidConfiguration;
-    batch_tick_kernel<<<grid, kThreads, smem_bytes, s>>>(a);
+    if (a.prod) batch_tick_kernel<true><<<grid, kThreads, smem_bytes, s>>>(a);
+    else batch_tick_kernel<false><<<grid, kThreads, smem_bytes, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -19,6 +19,12 @@ constexpr TileShape kTiles[kNumTiles] = {{1, 8}, {1, 4}, {1, 2}, {1, 1}, {2, 1},
 constexpr int kBatchTileLo = 1;
 constexpr int kBatchTileHi = 5;
 
+// The production configuration: full-Newton transport, Gaussian state noise,
+// no Heun step (kernels compiled for it alone carry only its code paths).
+inline bool is_production_tick(const svpf_config_t& c) {
+    return c.use_newton && c.use_full_newton && !c.use_heun && !c.use_student_t_state;
+}
+
 struct SingleArgs {
     svpf_config_t cfg;
     SVPFParams prm;
@@ -64,6 +70,7 @@ struct BatchArgs {
     const float* tape_u;
     int slots_n, slots_u, tape_stride;
     int heun;              // any filter of the batch uses Heun (shared-memory layout)
+    int prod;              // every single-factor filter has the production configuration
     // request mode (request loop): work item w is filter order[w] with
     // y_t = req_y[w], y_prev = that filter's ctl.y_prev (updated to y_t), and
     // its outputs go to out[w].  nullptr: batch mode (y_t[f], y_prev[f], out[f]).

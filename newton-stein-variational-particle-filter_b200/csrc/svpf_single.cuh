@@ -96,12 +96,6 @@ __global__ void __launch_bounds__(kThreads) single_tick_2f_kernel(const __grid_c
 // prior means above it.
 constexpr int kScanMaxN = 1024;
 
-// The production configuration: full-Newton transport, Gaussian state noise,
-// no Heun step (the kernel compiled for it alone).
-inline bool is_production_tick(const svpf_config_t& c) {
-    return c.use_newton && c.use_full_newton && !c.use_heun && !c.use_student_t_state;
-}
-
 template <int R, int S, bool TWO_FACTOR = false, bool SCAN = false, bool PROD = false>
 static cudaError_t launch_single_t(const SingleArgs& a, int C, cudaStream_t s) {
     const size_t smem = TWO_FACTOR ? tick_smem_bytes_2f(a.n, C) : tick_smem_bytes(a.n, C, a.cfg.use_heun != 0);
