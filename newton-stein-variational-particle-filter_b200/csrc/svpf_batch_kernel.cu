@@ -160,13 +160,14 @@ __global__ void __launch_bounds__(kThreads) batch_tick_2f_cluster_kernel(const _
     }
 }
 
-constexpr int kCluster2f = 4;
+constexpr int kCluster2f = kClusterMembers2f;
 
 int batch_cluster_grid_2f(size_t smem_bytes) {
     auto kern = batch_tick_2f_cluster_kernel<kCluster2f>;
     static bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn_smem());
+        cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         configured = true;
     }
     cudaLaunchConfig_t cfg = {};
