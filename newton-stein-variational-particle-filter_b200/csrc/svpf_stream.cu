@@ -33,6 +33,8 @@ struct svpf_stream {
     size_t budget = 0, pool_floats = 0, fixed_bytes = 0, used_floats = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaStream_t side[2] = {nullptr, nullptr};   // the round's two-factor kernels, forked from stream
+    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
     unsigned long long seed = 0;
     std::map<long long, long long> free_list;    // offset -> length (floats)
     std::vector<long long> off, len;
@@ -119,11 +121,45 @@ bool big_2f(const svpf_stream* s, int slot) {
 
 // One round: d_req[0, c1) single-factor slots, then c2 two-factor slots of
 // which the first c2c run on clusters; each part largest cost first; y and
-// outputs indexed alike.
+// outputs indexed alike.  The three kernels touch disjoint filters and have
+// their own work counters, so they run concurrently: the clustered two-factor
+// kernel (the longest ticks) and the one-CTA two-factor kernel on two side
+// streams forked from the loop's stream, the single-factor kernel on the loop's
+// stream, which then waits for both.  A kernel's CTAs take the SMs that another
+// kernel's tail frees instead of waiting for the whole kernel to end.
 int launch_round(svpf_stream* s, int c1, int c2, const int* d_req, const float* d_y, svpf_out_t* d_out,
                  int c2c = 0) {
     if (cudaMemsetAsync(s->d_queue, 0, 3 * sizeof(int), s->stream) != cudaSuccess) return SVPF_ERR_CUDA;
+    if (cudaEventRecord(s->fork, s->stream) != cudaSuccess) return SVPF_ERR_CUDA;
     BatchArgs a = round_args(s);
+    const int c2s = c2 - c2c;
+    bool joined[2] = {false, false};
+    if (c2c > 0) {
+        a.F = c2c;
+        a.order = d_req + c1;
+        a.queue = s->d_queue + 2;
+        a.req_y = d_y + c1;
+        a.out = d_out + c1;
+        if (cudaStreamWaitEvent(s->side[0], s->fork, 0) != cudaSuccess ||
+            launch_batch_2f_cluster(a, s->smem2c, s->grid2c, s->side[0]) != cudaSuccess ||
+            cudaEventRecord(s->join[0], s->side[0]) != cudaSuccess)
+            return SVPF_ERR_CUDA;
+        joined[0] = true;
+        ++s->launches;
+    }
+    if (c2s > 0) {
+        a.F = c2s;
+        a.order = d_req + c1 + c2c;
+        a.queue = s->d_queue + 1;
+        a.req_y = d_y + c1 + c2c;
+        a.out = d_out + c1 + c2c;
+        if (cudaStreamWaitEvent(s->side[1], s->fork, 0) != cudaSuccess ||
+            launch_batch_2f(a, s->smem2, s->grid2, s->side[1]) != cudaSuccess ||
+            cudaEventRecord(s->join[1], s->side[1]) != cudaSuccess)
+            return SVPF_ERR_CUDA;
+        joined[1] = true;
+        ++s->launches;
+    }
     if (c1 > 0) {
         a.F = c1;
         a.order = d_req;
@@ -133,25 +169,8 @@ int launch_round(svpf_stream* s, int c1, int c2, const int* d_req, const float* 
         if (launch_batch(a, s->smem1, s->grid1, s->stream) != cudaSuccess) return SVPF_ERR_CUDA;
         ++s->launches;
     }
-    if (c2c > 0) {
-        a.F = c2c;
-        a.order = d_req + c1;
-        a.queue = s->d_queue + 2;
-        a.req_y = d_y + c1;
-        a.out = d_out + c1;
-        if (launch_batch_2f_cluster(a, s->smem2c, s->grid2c, s->stream) != cudaSuccess) return SVPF_ERR_CUDA;
-        ++s->launches;
-    }
-    const int c2s = c2 - c2c;
-    if (c2s > 0) {
-        a.F = c2s;
-        a.order = d_req + c1 + c2c;
-        a.queue = s->d_queue + 1;
-        a.req_y = d_y + c1 + c2c;
-        a.out = d_out + c1 + c2c;
-        if (launch_batch_2f(a, s->smem2, s->grid2, s->stream) != cudaSuccess) return SVPF_ERR_CUDA;
-        ++s->launches;
-    }
+    for (int k = 0; k < 2; ++k)
+        if (joined[k] && cudaStreamWaitEvent(s->stream, s->join[k], 0) != cudaSuccess) return SVPF_ERR_CUDA;
     return SVPF_OK;
 }
 
@@ -179,6 +198,16 @@ svpf_stream_t* svpf_stream_create(int max_instruments, size_t hbm_budget_bytes, 
     } else {
         cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
         s->own_stream = true;
+    }
+    bool side_ok = true;
+    for (int k = 0; k < 2; ++k) {
+        side_ok = side_ok && cudaStreamCreateWithFlags(&s->side[k], cudaStreamNonBlocking) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&s->join[k], cudaEventDisableTiming) == cudaSuccess;
+    }
+    side_ok = side_ok && cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming) == cudaSuccess;
+    if (!side_ok) {
+        svpf_stream_destroy(s);
+        return nullptr;
     }
     size_t acc = 0;
     bool ok = salloc(&s->pool, 4 * s->pool_floats, &acc) && salloc(&s->d_n, C, &acc) && salloc(&s->d_off, C, &acc) &&
@@ -223,6 +252,14 @@ void svpf_stream_destroy(svpf_stream_t* s) {
     if (s->h_req) cudaFreeHost(s->h_req);
     if (s->h_y) cudaFreeHost(s->h_y);
     if (s->h_out) cudaFreeHost(s->h_out);
+    for (int k = 0; k < 2; ++k) {
+        if (s->side[k]) {
+            cudaStreamSynchronize(s->side[k]);
+            cudaStreamDestroy(s->side[k]);
+        }
+        if (s->join[k]) cudaEventDestroy(s->join[k]);
+    }
+    if (s->fork) cudaEventDestroy(s->fork);
     if (s->own_stream) cudaStreamDestroy(s->stream);
     delete s;
 }
