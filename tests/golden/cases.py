@@ -7,7 +7,7 @@ engine replay every tick from the stored pre-tick state with the same tape.
 """
 import tape
 
-# BASELINE configuration 1 mapped onto the reference knobs: N=512, at most 8
+# The plain single-filter workload on the reference knobs: N=512, at most 8
 # Newton-Stein iterations over 3 annealing stages, full Newton, SVLD, MIM,
 # asymmetric rho, preserving EKF guide, rejuvenation, Student-t nu = 30.
 PRODUCTION = dict(use_newton=1, use_full_newton=1, stein_min_steps=4, stein_max_steps=8,

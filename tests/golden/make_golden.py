@@ -123,7 +123,7 @@ def run_v2_case(name, case, reflib):
 
 
 def main():
-    out_dir = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden")
+    out_dir = sys.argv[1] if len(sys.argv) > 1 else HERE
     only = set(sys.argv[2:])
     os.makedirs(out_dir, exist_ok=True)
     reflib = oracle.RefLib("tape")

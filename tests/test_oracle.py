@@ -80,7 +80,7 @@ def rel_err(a, b, floor=1.0):
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor)))
 
 
-# Tolerance of per-tick parity with state re-sync (BASELINE: 1e-4 relative).
+# Tolerance of per-tick parity with state re-sync: 1e-4 relative.
 TOL = 1e-4
 
 
