@@ -242,7 +242,7 @@ bool grow(float** p, size_t* cap, size_t bytes) {
 
 int pick_cluster(const SVPFState* s, const Impl* im) {
     int C = im->cluster > 0 ? im->cluster : default_cluster(s->n_particles);
-    while (C > 1 && tick_smem_bytes(s->n_particles, C, s->use_heun != 0) > max_dyn_smem()) C >>= 1;
+    while (C > 1 && tick_smem_bytes_single(s->n_particles, C, s->use_heun != 0) > max_dyn_smem()) C >>= 1;
     return C;
 }
 

@@ -401,8 +401,10 @@ struct Smem {
     float* v;
     float* phi0;        // Heun: operator at the start point, own rows
     float* phi1;        // Heun: operator at the predicted point, own rows
+    float* pre;         // SVLD normals of own rows drawn before the Stein loop, [kPreIters][Lp], or nullptr
     int n, np, m_len, p2;   // particles, padded row length, padded prior length, sort length
     int row0, row1;     // rows owned by this team member
+    int Lp;             // own rows, padded to 4
 };
 
 __host__ __device__ inline int pow2_at_least(int n) {
@@ -420,6 +422,17 @@ __host__ __device__ inline int smem_floats(int n, int C, bool heun) {
     const int m_len = round_up(p2 > np ? p2 : np, 64);
     const int L = round_up((n + C - 1) / C, 4);
     return 2 * np + np + np + m_len + (heun ? 3 : 1) * L;
+}
+
+// Latency kernel: the SVLD normals of the first kPreIters Stein iterations of
+// a member's own rows are drawn in parallel before the loop (each is a
+// Philox block and a Box-Muller on the row's epilogue path otherwise), when
+// the member owns at most kPreMaxRows rows.
+constexpr int kPreIters = 16;
+constexpr int kPreMaxRows = 256;
+__host__ __device__ inline int pre_floats(int n, int C) {
+    const int L = (n + C - 1) / C;
+    return L <= kPreMaxRows ? kPreIters * round_up(L, 4) : 0;
 }
 
 // Two-factor tick: per factor x[2][np] (transport coordinates, double
@@ -451,6 +464,8 @@ __device__ inline Smem2 carve_2f(float* base, int n, int C, int rank) {
         f.c = nullptr;
         f.mu = nullptr;
         f.phi0 = f.phi1 = nullptr;
+        f.pre = nullptr;
+        f.Lp = Lp;
         f.n = n;
         f.np = np;
         f.m_len = 0;
@@ -478,6 +493,8 @@ __device__ inline Smem carve(float* base, int n, int C, int rank, bool heun) {
     s.v = s.mu + s.m_len;
     s.phi0 = heun ? s.v + Lp : nullptr;
     s.phi1 = heun ? s.phi0 + Lp : nullptr;
+    s.pre = nullptr;
+    s.Lp = Lp;
     s.row0 = min(rank * L, n);
     s.row1 = min(s.row0 + L, n);
     return s;
@@ -687,7 +704,8 @@ enum { kTransport = 0, kPhiOnly = 1, kKsdOnly = 2 };
 template <int R, int S, int KIND, bool KSD, int MODE = kTransport, class P = Plan>
 __device__ float transport_pass(const Smem& sm, int cur, const P& pl, const svpf_config_t& cfg,
                                 float bf, const Noise& nz, int kn, const Team& team,
-                                float* __restrict__ phi_out = nullptr) {
+                                float* __restrict__ phi_out = nullptr,
+                                const float* __restrict__ pre = nullptr) {
     constexpr bool RAW = std::is_same<P, FactorPlan>::value;
     constexpr int G = kThreads / S;
     const int grp = threadIdx.x / S, q = threadIdx.x % S;
@@ -821,7 +839,7 @@ __device__ float transport_pass(const Smem& sm, int cur, const P& pl, const svpf
                 sm.v[li] = vn;
                 const float drift = es * phi * rsqrtf(vn + cfg.rmsprop_eps);
                 float diff = 0.0f;
-                if (pl.temp > 1e-6f) diff = sqrtf(2.0f * es * pl.temp) * nz.normal(i, kn);
+                if (pl.temp > 1e-6f) diff = sqrtf(2.0f * es * pl.temp) * (pre ? pre[li] : nz.normal(i, kn));
                 const float h_new = clamp_h((RAW ? hi[r] : fmaf(hi[r], pl.bw, pl.center)) + drift + diff);
                 const float hs_new = RAW ? h_new : (h_new - pl.center) * inv_bw;
                 for (int rk = 0; rk < team.size; ++rk) team.at(hn, rk)[i] = hs_new;

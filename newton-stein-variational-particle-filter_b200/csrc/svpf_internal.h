@@ -107,6 +107,8 @@ struct InitArgs {
 // Dynamic shared-memory bytes of a tick kernel for n particles on C CTAs
 // (single-factor, and two-factor).
 size_t tick_smem_bytes(int n, int C, bool heun);
+// The single-filter kernel's: the tick's layout plus the pre-drawn SVLD normals.
+size_t tick_smem_bytes_single(int n, int C, bool heun);
 size_t tick_smem_bytes_2f(int n, int C);
 // Largest dynamic shared memory a CTA may use on this device.
 size_t max_dyn_smem();

@@ -66,6 +66,9 @@ __global__ void philox_kernel(uint32_t k0, uint32_t k1, const uint32_t* ctr, uin
 // host side
 // ---------------------------------------------------------------------------
 size_t tick_smem_bytes(int n, int C, bool heun) { return (size_t)smem_floats(n, C, heun) * sizeof(float); }
+size_t tick_smem_bytes_single(int n, int C, bool heun) {
+    return (size_t)(smem_floats(n, C, heun) + pre_floats(n, C)) * sizeof(float);
+}
 size_t tick_smem_bytes_2f(int n, int C) { return (size_t)smem_floats_2f(n, C) * sizeof(float); }
 
 size_t max_dyn_smem() {
@@ -104,7 +107,7 @@ int default_batch_tile(int n) {
 
 cudaError_t launch_single(const SingleArgs& a, int C, int tile, cudaStream_t s) {
     if (C < 1 || C > kMaxCluster || a.n < 1) return cudaErrorInvalidValue;
-    if (tick_smem_bytes(a.n, C, a.cfg.use_heun != 0) > max_dyn_smem()) return cudaErrorInvalidValue;
+    if (tick_smem_bytes_single(a.n, C, a.cfg.use_heun != 0) > max_dyn_smem()) return cudaErrorInvalidValue;
     return tile <= 3 ? launch_single_small(a, C, tile, s) : launch_single_large(a, C, tile, s);
 }
 

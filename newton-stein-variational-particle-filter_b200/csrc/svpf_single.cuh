@@ -41,7 +41,8 @@ __global__ void __launch_bounds__(kThreads, 1) single_tick_kernel(const __grid_c
     copy_words(&cfg, &a.cfg);
     copy_words(&prm, &a.prm);
     __syncthreads();
-    const Smem sm = carve(smem, a.n, team.size, team.rank, a.cfg.use_heun != 0);
+    Smem sm = carve(smem, a.n, team.size, team.rank, a.cfg.use_heun != 0);
+    if (pre_floats(a.n, team.size) > 0) sm.pre = smem + smem_floats(a.n, team.size, a.cfg.use_heun != 0);
     const Noise nz{philox_key(a.seed, 0), (uint32_t)ctl.timestep, a.tape_n, a.tape_u,
                    a.slots_n, a.slots_u, a.n, &pl.flag};
     const FilterIO io{a.h, a.hp, a.v, a.lw, a.n};
@@ -98,7 +99,7 @@ constexpr int kScanMaxN = 1024;
 
 template <int R, int S, bool TWO_FACTOR = false, bool SCAN = false, bool PROD = false>
 static cudaError_t launch_single_t(const SingleArgs& a, int C, cudaStream_t s) {
-    const size_t smem = TWO_FACTOR ? tick_smem_bytes_2f(a.n, C) : tick_smem_bytes(a.n, C, a.cfg.use_heun != 0);
+    const size_t smem = TWO_FACTOR ? tick_smem_bytes_2f(a.n, C) : tick_smem_bytes_single(a.n, C, a.cfg.use_heun != 0);
     auto kern = TWO_FACTOR ? single_tick_2f_kernel<R, S> : single_tick_kernel<R, S, SCAN, PROD>;
     static bool configured[kMaxCluster + 1] = {};
     cudaError_t e;

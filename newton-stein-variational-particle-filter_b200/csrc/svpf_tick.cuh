@@ -21,23 +21,24 @@ struct FilterIO {
 template <int R, int S, int KIND, bool KSD, int MODE>
 __device__ __forceinline__ float stein_rows(const Smem& sm, int cur, const Plan& pl,
                                             const svpf_config_t& cfg, float bf, const Noise& nz,
-                                            int kn, const Team& team, float* phi_out) {
-    return transport_pass<R, S, KIND, KSD, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out);
+                                            int kn, const Team& team, float* phi_out,
+                                            const float* pre = nullptr) {
+    return transport_pass<R, S, KIND, KSD, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out, pre);
 }
 
 template <int R, int S, int MODE>
 __device__ float stein_dispatch(int kind, bool ksd, const Smem& sm, int cur, const Plan& pl,
                                 const svpf_config_t& cfg, float bf, const Noise& nz, int kn,
-                                const Team& team, float* phi_out = nullptr) {
+                                const Team& team, float* phi_out = nullptr, const float* pre = nullptr) {
     if (kind == 2) {
-        return ksd ? stein_rows<R, S, 2, true, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out)
-                   : stein_rows<R, S, 2, false, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out);
+        return ksd ? stein_rows<R, S, 2, true, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out, pre)
+                   : stein_rows<R, S, 2, false, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out, pre);
     } else if (kind == 1) {
-        return ksd ? stein_rows<R, S, 1, true, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out)
-                   : stein_rows<R, S, 1, false, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out);
+        return ksd ? stein_rows<R, S, 1, true, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out, pre)
+                   : stein_rows<R, S, 1, false, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out, pre);
     }
-    return ksd ? stein_rows<R, S, 0, true, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out)
-               : stein_rows<R, S, 0, false, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out);
+    return ksd ? stein_rows<R, S, 0, true, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out, pre)
+               : stein_rows<R, S, 0, false, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out, pre);
 }
 
 template <int R, int S, bool SCAN>
@@ -185,6 +186,16 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
     }
     // ---- own rows' RMSProp state
     for (int li = tid; li < sm.row1 - sm.row0; li += kThreads) sm.v[li] = io.v[sm.row0 + li];
+    // ---- SVLD normals of own rows for the first Stein iterations, drawn in
+    //      parallel (same draws, in the same slots, as the per-row epilogue takes)
+    if (sm.pre != nullptr && pl.temp > 1e-6f && (PROD || !cfg.use_heun)) {
+        const int nloc = sm.row1 - sm.row0;
+        const int iters = min(pl.budget, kPreIters);
+        for (int k = tid; k < iters * nloc; k += kThreads) {
+            const int it = k / nloc, li = k - it * nloc;
+            sm.pre[it * sm.Lp + li] = nz.normal(sm.row0 + li, pl.kn_pred + it);
+        }
+    }
     team.sync();   // every member has read io.h / io.h_prev; smem ready
 
     // ---- annealed Stein loop (svpf_optimized_graph.cu:1120-1317)
@@ -197,16 +208,18 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
         const float bf = sqrtf(beta);
         const bool last = it == budget - 1;
         if (PROD || !cfg.use_heun) {
+            const float* pre = (sm.pre != nullptr && it < kPreIters) ? sm.pre + it * sm.Lp : nullptr;
             float kt;
             if constexpr (PROD) {
                 grad_pass<R, S, false, SCAN>(sm, cur, pl, cfg, beta, io.lw, team);
                 team.sync();
-                kt = last ? stein_rows<R, S, 2, true, kTransport>(sm, cur, pl, cfg, bf, nz, kn, team, nullptr)
-                          : stein_rows<R, S, 2, false, kTransport>(sm, cur, pl, cfg, bf, nz, kn, team, nullptr);
+                kt = last ? stein_rows<R, S, 2, true, kTransport>(sm, cur, pl, cfg, bf, nz, kn, team, nullptr, pre)
+                          : stein_rows<R, S, 2, false, kTransport>(sm, cur, pl, cfg, bf, nz, kn, team, nullptr, pre);
             } else {
                 grad_dispatch<R, S, SCAN>(student, sm, cur, pl, cfg, beta, io.lw, team);
                 team.sync();
-                kt = stein_dispatch<R, S, kTransport>(pl.transport, last, sm, cur, pl, cfg, bf, nz, kn, team);
+                kt = stein_dispatch<R, S, kTransport>(pl.transport, last, sm, cur, pl, cfg, bf, nz, kn, team,
+                                                      nullptr, pre);
             }
             if (last) ksd_publish(kt, pl, team);
             team.sync();
