@@ -531,8 +531,9 @@ long long svpf_stream_kernel_launches(const svpf_stream_t* s);
 /* ---- svpf_fully_fused_step_v2 (include/svpf_fully_fused_v2.cuh:43-119) ------
  * The reference's second, single-kernel tick with its own semantics (Silverman
  * bandwidth, fixed beta ramp, EKF inside the kernel, adaptive guide strength),
- * same argument list.  One launch of a thread-block cluster; N up to
- * SVPF_MAX_PARTICLES (the reference: 1024).  Where the reference takes
+ * same argument list.  One launch of a thread-block cluster; N up to 8064
+ * (shared memory; svpf_fully_fused_v2_supported tells; the reference: 1024).
+ * Where the reference takes
  * curandStatePhilox4_32_10_t*, this takes a device svpf_v2_rng_t record: the
  * engine's counter-based Philox keyed by (seed, filter) and counted by
  * (particle, draw, tick), tick advanced by every call, or -- a test hook -- a

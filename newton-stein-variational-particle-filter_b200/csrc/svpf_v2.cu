@@ -58,6 +58,7 @@ struct Args {
     float *d_h_mean, *d_vol, *d_loglik, *d_bw, *d_ksd, *d_guide_mean, *d_guide_var, *d_mu_state;
     Params p;
     int n, timestep;
+    int npre_cap;   // steps whose diffusion normals fit in shared memory to pre-draw
 };
 
 struct Shared {
@@ -122,6 +123,82 @@ struct V2Noise {
     }
 };
 
+// Steps whose diffusion normals are drawn before the Stein loop (at most).
+constexpr int kPreSteps = 17;
+
+// Lanes per row: a power of two <= 32, as many as fill the CTA with a
+// member's share of rows (nloc of them).
+__host__ __device__ __forceinline__ int lanes_per_row(int nloc) {
+    int S = 1;
+    while (S < 32 && 2 * S * (nloc > 1 ? nloc : 1) <= kT) S <<= 1;
+    return S;
+}
+
+// Padded length of the particle arrays (far positions, zero scores, far
+// means beyond n): a multiple of 32 and of the 4 S columns one chunk sweep
+// covers, so that the pair loops need no masks.
+__host__ __device__ __forceinline__ int padded_rows(int n, int C) {
+    const int S = lanes_per_row((n + C - 1) / C);
+    const int m = 4 * S > 32 ? 4 * S : 32;
+    return (n + m - 1) / m * m;
+}
+
+// Transport row sums of row i over four-column chunks (two columns per packed
+// op): ks = sum K s_j, gk = sum d K^2 (x hess_j with Newton), and for full
+// Newton Hw = sum hess_j K + 2/bw^2 K^2 |3 d^2/bw^2 - 1|, Ks = sum K; LAST adds
+// the KSD row sum kd.  d = h_i - h_j, K = 1 / (1 + d^2/bw^2).
+template <bool FULL, bool LAST>
+__device__ __forceinline__ void v2_transport_row(const float* __restrict__ hc, const float* __restrict__ sg,
+                                                 const float* __restrict__ shs, int nv, int q, int S, float hi,
+                                                 float gi, float ib2, bool use_newton, float& ks, float& gk,
+                                                 float& Hw, float& Ks, float& kd) {
+    const float2 h2 = f2(hi), vib2 = f2(ib2);
+    float2 ks2 = f2(0.0f), gk2 = f2(0.0f), hw2 = f2(0.0f), kk2 = f2(0.0f);
+    float hwa = 0.0f;
+    kd = 0.0f;
+    for (int cb = q * 4; cb < nv; cb += 4 * S) {
+        const float4 x4 = *reinterpret_cast<const float4*>(hc + cb);
+        const float4 s4 = *reinterpret_cast<const float4*>(sg + cb);
+        const float4 e4 = *reinterpret_cast<const float4*>(shs + cb);
+        const float2 xx[2] = {make_float2(x4.x, x4.y), make_float2(x4.z, x4.w)};
+        const float2 ss[2] = {make_float2(s4.x, s4.y), make_float2(s4.z, s4.w)};
+        const float2 ee[2] = {make_float2(e4.x, e4.y), make_float2(e4.z, e4.w)};
+#pragma unroll
+        for (int hf = 0; hf < 2; ++hf) {
+            const float2 diff = fma2(xx[hf], f2(-1.0f), h2);
+            const float2 dist2 = mul2(mul2(diff, diff), vib2);
+            const float2 b = add2(dist2, f2(1.0f));
+            const float2 K = make_float2(rcp_approx(b.x), rcp_approx(b.y));
+            const float2 K2 = mul2(K, K);
+            ks2 = fma2(K, ss[hf], ks2);
+            const float2 rep = mul2(diff, K2);
+            gk2 = use_newton ? fma2(rep, ee[hf], gk2) : add2(gk2, rep);
+            if (FULL) {
+                hw2 = fma2(ee[hf], K, hw2);
+                const float2 t = fma2(dist2, f2(3.0f), f2(-1.0f));
+                hwa = fmaf(K2.x, fabsf(t.x), hwa);
+                hwa = fmaf(K2.y, fabsf(t.y), hwa);
+                kk2 = add2(kk2, K);
+            }
+            if (LAST) {
+                const float dd[2] = {diff.x, diff.y}, d2[2] = {dist2.x, dist2.y}, kv[2] = {K.x, K.y},
+                            k2v[2] = {K2.x, K2.y}, sj[2] = {ss[hf].x, ss[hf].y}, hj[2] = {ee[hf].x, ee[hf].y};
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const float rj = use_newton ? __fdividef(sj[c], 0.7f * hj[c] + 1e-8f) : sj[c];
+                    const float gxk = -2.0f * dd[c] * ib2 * k2v[c];
+                    const float hxy = 2.0f * ib2 * k2v[c] * (4.0f * d2[c] * kv[c] - 1.0f);
+                    kd += kv[c] * gi * rj + gi * (-gxk) + rj * gxk + hxy;
+                }
+            }
+        }
+    }
+    ks = ks2.x + ks2.y;
+    gk = gk2.x + gk2.y;
+    Hw = FULL ? hw2.x + hw2.y + 2.0f * ib2 * hwa : 0.0f;
+    Ks = FULL ? kk2.x + kk2.y : 0.0f;
+}
+
 __global__ void __launch_bounds__(kT) v2_kernel(const __grid_constant__ Args a) {
     namespace cg = cooperative_groups;
     extern __shared__ __align__(16) float smem[];
@@ -130,7 +207,7 @@ __global__ void __launch_bounds__(kT) v2_kernel(const __grid_constant__ Args a) 
     const int rank = (int)cl.block_rank(), C = (int)cl.num_blocks();
     const int tid = threadIdx.x;
     const int n = a.n;
-    const int np = round_up(n, 32);
+    const int np = padded_rows(n, C);
     const int L = (n + C - 1) / C;
     const int row0 = min(rank * L, n), row1 = min(row0 + L, n);
     float* hb[2] = {smem, smem + np};
@@ -142,6 +219,7 @@ __global__ void __launch_bounds__(kT) v2_kernel(const __grid_constant__ Args a) 
     float* vr = smem + 7 * np;       // own rows: RMSProp moment
     float* zd = vr + L;              // own rows: pending diffusion normal
     float* gown = zd + L;            // own rows: clamped score g (the KSD's raw score of row i)
+    float* zpre = gown + L;          // own rows: the diffusion normals of the first npre_cap steps, [npre_cap][L]
     const Params& P = a.p;
     const float y_t = a.y_t, y_prev = a.y_prev, hmp = a.h_mean_prev;
     const float rho = P.rho, sz = P.sigma_z, mu = P.mu, nu = P.nu;
@@ -227,9 +305,20 @@ __global__ void __launch_bounds__(kT) v2_kernel(const __grid_constant__ Args a) 
             hi = clamp_h(P.use_guide_preserving ? hi + sh.gs * (sh.gm - hmp) : (1.0f - sh.gs) * hi + sh.gs * sh.gm);
         h[i] = hi;
     }
+    // own rows' moments; the diffusion normals, drawn in parallel up front:
+    // entry g is draw 1 (g = 0) or draw 3 + g, the normal step g + 1 adds
+    // (entry n_stein_steps is the draw the last step takes and leaves unused).
+    // The row epilogue draws the rest one by one, so the set of draws is the
+    // same whatever fits.
+    const int nsteps = P.n_stein_steps < 1 ? 1 : P.n_stein_steps;
+    const int npre = P.temperature > 1e-6f ? min(nsteps + 1, a.npre_cap) : 0;
     for (int li = tid; li < row1 - row0; li += kT) {
         vr[li] = a.v[row0 + li];
-        zd[li] = nz.normal(row0 + li, 1);
+        if (npre == 0) zd[li] = nz.normal(row0 + li, 1);
+    }
+    for (int k = tid; k < npre * (row1 - row0); k += kT) {
+        const int g = k / (row1 - row0), li = k - g * (row1 - row0);
+        zpre[g * L + li] = nz.normal(row0 + li, g == 0 ? 1 : 3 + g);
     }
     __syncthreads();
     // ---- phase 3: Silverman bandwidth (:384-410)
@@ -258,12 +347,14 @@ __global__ void __launch_bounds__(kT) v2_kernel(const __grid_constant__ Args a) 
     const float y2 = y_t * y_t;
     int cur = 0, gstep = 0;
     const int kn0 = 4;
-    // S lanes per row (a power of two <= 32 filling the CTA), G rows per sweep
+    // S lanes per row (a power of two <= 32 filling the CTA with L rows; the
+    // same on every member, so that the padding covers its chunks), G rows
+    // per sweep
     const int nloc = row1 - row0;
-    int S = 1;
-    while (S < 32 && 2 * S * max(nloc, 1) <= kT) S <<= 1;
+    const int S = lanes_per_row(L);
     const int G = kT / S;
     const int grp = tid / S, q = tid % S;
+    const int nv = round_up(n, 4 * S);   // <= np: four columns per chunk, pads beyond n
     const float c2 = inv_2s2 * 1.4426950408889634f;   // log2(e) / (2 sigma^2)
     const bool use_newton = P.use_newton != 0, full = P.use_full_newton != 0;
     for (int ai = 0; ai < na; ++ai) {
@@ -278,21 +369,36 @@ __global__ void __launch_bounds__(kT) v2_kernel(const __grid_constant__ Args a) 
             for (int base = 0; base < nloc; base += G) {
                 const int li = base + grp;
                 const bool valid = li < nloc;
-                const int i = row0 + (valid ? li : 0);
+                const int i = valid ? row0 + li : 0;
                 const float hi = hc[i];
-                float lmax = -1e30f;
-                for (int k = q; k < n; k += S) {
-                    const float d = hi - muk[k];
-                    lmax = fmaxf(lmax, -d * d * c2);
+                // row maximum of -d^2 c2: the smallest d^2 over the row's
+                // columns (four per chunk, two per packed op; far-value pads)
+                const float2 h2 = f2(hi);
+                float mn = 3.0e38f;
+                for (int cb = q * 4; cb < nv; cb += 4 * S) {
+                    const float4 m4 = *reinterpret_cast<const float4*>(muk + cb);
+                    const float2 da = fma2(make_float2(m4.x, m4.y), f2(-1.0f), h2);
+                    const float2 db = fma2(make_float2(m4.z, m4.w), f2(-1.0f), h2);
+                    const float2 qa = mul2(da, da), qb = mul2(db, db);
+                    mn = fminf(mn, fminf(fminf(qa.x, qa.y), fminf(qb.x, qb.y)));
                 }
-                for (int o = S >> 1; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-                float sr = 0.0f, wd = 0.0f;
-                for (int k = q; k < n; k += S) {
-                    const float d = hi - muk[k];
-                    const float r = ex2_approx(-d * d * c2 - lmax);
-                    sr += r;
-                    wd = fmaf(r, d, wd);
+                for (int o = S >> 1; o > 0; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+                const float lmax = -(mn * c2);
+                float2 sr2 = f2(0.0f), wd2 = f2(0.0f);
+                const float2 nc2 = f2(-c2), nl = f2(-lmax);
+                for (int cb = q * 4; cb < nv; cb += 4 * S) {
+                    const float4 m4 = *reinterpret_cast<const float4*>(muk + cb);
+                    const float2 da = fma2(make_float2(m4.x, m4.y), f2(-1.0f), h2);
+                    const float2 db = fma2(make_float2(m4.z, m4.w), f2(-1.0f), h2);
+                    const float2 ta = fma2(mul2(da, da), nc2, nl), tb = fma2(mul2(db, db), nc2, nl);
+                    const float2 wa = make_float2(ex2_approx(ta.x), ex2_approx(ta.y));
+                    const float2 wb = make_float2(ex2_approx(tb.x), ex2_approx(tb.y));
+                    sr2 = add2(sr2, wa);
+                    wd2 = fma2(wa, da, wd2);
+                    sr2 = add2(sr2, wb);
+                    wd2 = fma2(wb, db, wd2);
                 }
+                float sr = sr2.x + sr2.y, wd = wd2.x + wd2.y;
                 for (int o = S >> 1; o > 0; o >>= 1) {
                     sr += __shfl_xor_sync(0xffffffffu, sr, o);
                     wd += __shfl_xor_sync(0xffffffffu, wd, o);
@@ -328,30 +434,16 @@ __global__ void __launch_bounds__(kT) v2_kernel(const __grid_constant__ Args a) 
             for (int base = 0; base < nloc; base += G) {
                 const int li = base + grp;
                 const bool valid = li < nloc;
-                const int i = row0 + (valid ? li : 0);
+                const int i = valid ? row0 + li : 0;
                 const float hi = hc[i];
                 const float gi = valid ? gown[li] : 0.0f;
-                float ks = 0.0f, gk = 0.0f, Hw = 0.0f, Ks = 0.0f, kd = 0.0f;
-                for (int j = q; j < n; j += S) {
-                    const float diff = hi - hc[j];
-                    const float dist2 = diff * diff * ib2;
-                    const float K = rcp_approx(1.0f + dist2);
-                    const float K2 = K * K;
-                    const float sj = sg[j], hj = shs[j];
-                    ks = fmaf(K, sj, ks);
-                    const float rep = diff * K2;
-                    gk = use_newton ? fmaf(rep, hj, gk) : gk + rep;
-                    if (full) {
-                        Hw = fmaf(hj, K, Hw);
-                        Hw = fmaf(2.0f * ib2 * K2, fabsf(3.0f * dist2 - 1.0f), Hw);
-                        Ks += K;
-                    }
-                    if (last) {
-                        const float rj = use_newton ? __fdividef(sj, 0.7f * hj + 1e-8f) : sj;
-                        const float gxk = -2.0f * diff * ib2 * K2;
-                        const float hxy = 2.0f * ib2 * K2 * (4.0f * dist2 * K - 1.0f);
-                        kd += K * gi * rj + gi * (-gxk) + rj * gxk + hxy;
-                    }
+                float ks, gk, Hw, Ks, kd;
+                if (full) {
+                    if (last) v2_transport_row<true, true>(hc, sg, shs, nv, q, S, hi, gi, ib2, use_newton, ks, gk, Hw, Ks, kd);
+                    else v2_transport_row<true, false>(hc, sg, shs, nv, q, S, hi, gi, ib2, use_newton, ks, gk, Hw, Ks, kd);
+                } else {
+                    if (last) v2_transport_row<false, true>(hc, sg, shs, nv, q, S, hi, gi, ib2, use_newton, ks, gk, Hw, Ks, kd);
+                    else v2_transport_row<false, false>(hc, sg, shs, nv, q, S, hi, gi, ib2, use_newton, ks, gk, Hw, Ks, kd);
                 }
                 for (int o = S >> 1; o > 0; o >>= 1) {
                     ks += __shfl_xor_sync(0xffffffffu, ks, o);
@@ -376,8 +468,8 @@ __global__ void __launch_bounds__(kT) v2_kernel(const __grid_constant__ Args a) 
                 const float drift = es * phi * rsqrtf(vn + P.rmsprop_eps);
                 float diffu = 0.0f;
                 if (P.temperature > 1e-6f) {
-                    diffu = sqrtf(2.0f * es * P.temperature) * zd[li];
-                    zd[li] = nz.normal(i, kn0 + gstep - 1);
+                    diffu = sqrtf(2.0f * es * P.temperature) * (gstep - 1 < npre ? zpre[(gstep - 1) * L + li] : zd[li]);
+                    if (gstep >= npre) zd[li] = nz.normal(i, kn0 + gstep - 1);   // past the pre-drawn steps
                 }
                 const float hnew = clamp_h(hi + drift + diffu);
                 for (int r = 0; r < C; ++r) cl.map_shared_rank(hn, r)[i] = hnew;
@@ -448,16 +540,27 @@ using namespace svpf;
 
 namespace {
 
-size_t v2_smem_bytes(int n, int C) {
-    const int np = round_up(n, 32);
+// Dynamic shared memory of one member: seven padded particle arrays, then
+// three own-row arrays and `pre` pre-drawn normals per own row.
+size_t v2_smem_bytes(int n, int C, int pre) {
+    const int np = v2::padded_rows(n, C);
     const int L = (n + C - 1) / C;
-    return (size_t)(7 * np + 3 * L) * sizeof(float);
+    return (size_t)(7 * np + (3 + pre) * L) * sizeof(float);
 }
 
 int v2_cluster(int n) {
     int C = default_cluster(n);
-    while (C > 1 && v2_smem_bytes(n, C) > max_dyn_smem()) C >>= 1;
+    while (C > 1 && v2_smem_bytes(n, C, 0) > max_dyn_smem()) C >>= 1;
     return C;
+}
+
+// Pre-drawn steps that fit beside the cluster's arrays (up to kPreSteps).
+int v2_pre_steps(int n, int C) {
+    const size_t base = v2_smem_bytes(n, C, 0), cap = max_dyn_smem();
+    if (base >= cap) return 0;
+    const size_t row = (size_t)((n + C - 1) / C) * sizeof(float);
+    const size_t fit = (cap - base) / row;
+    return (int)(fit < (size_t)v2::kPreSteps ? fit : (size_t)v2::kPreSteps);
 }
 
 }  // namespace
@@ -466,7 +569,7 @@ extern "C" {
 
 bool svpf_fully_fused_v2_supported(int n_particles) {
     return n_particles >= 1 && n_particles <= SVPF_MAX_PARTICLES &&
-           v2_smem_bytes(n_particles, 16) <= max_dyn_smem();
+           v2_smem_bytes(n_particles, 16, 0) <= max_dyn_smem();
 }
 
 cudaError_t svpf_fully_fused_step_v2(
@@ -511,6 +614,7 @@ cudaError_t svpf_fully_fused_step_v2(
     a.n = n;
     a.timestep = timestep;
     const int C = v2_cluster(n);
+    a.npre_cap = v2_pre_steps(n, C);
     static bool configured = false;
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(v2::v2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -523,7 +627,7 @@ cudaError_t svpf_fully_fused_step_v2(
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(C, 1, 1);
     cfg.blockDim = dim3(v2::kT, 1, 1);
-    cfg.dynamicSmemBytes = v2_smem_bytes(n, C);
+    cfg.dynamicSmemBytes = v2_smem_bytes(n, C, a.npre_cap);
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;

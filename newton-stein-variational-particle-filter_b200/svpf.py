@@ -866,6 +866,11 @@ class FusedV2:
         if not self._rng:
             raise RuntimeError("svpf_fully_fused_v2_rng_create failed")
         self._tape = None
+        # the buffers never move (set() copies into them): their addresses
+        # once, so that a call does no tensor work on the host
+        base = self.sc.data_ptr()
+        self._sp = [base + 4 * k for k in range(len(self.SCALARS))]
+        self._arr_ptrs = [self.arr[a].data_ptr() for a in self.ARRAYS] + [self._rng]
 
     def close(self):
         if getattr(self, "_rng", None):
@@ -912,20 +917,17 @@ class FusedV2:
             r.tick = tick
         lib().svpf_fully_fused_v2_rng_set(self._rng, C.byref(r))
 
-    def step(self, params: dict, y_t, y_prev, h_mean_prev, vol_prev, ksd_prev, timestep, stream=None) -> int:
-        A = self.arr
-        sp = [self.sc[k].data_ptr() for k in range(len(self.SCALARS))]
-        scal = []
-        for k in V2_ARG_ORDER:
-            if k == "@mu_state":
-                scal.append(sp[7])
-            else:
-                scal.append(params[k])
-        args = [A[a].data_ptr() for a in self.ARRAYS] + [self._rng] + \
-               [float(y_t), float(y_prev), float(h_mean_prev), float(vol_prev), float(ksd_prev)] + \
-               [sp[0], sp[1], sp[2], sp[3], sp[4], sp[5], sp[6]] + scal + [self.n, int(timestep), stream]
-        rc = lib().svpf_fully_fused_step_v2(*args)
-        self.torch.cuda.synchronize()
+    def step(self, params: dict, y_t, y_prev, h_mean_prev, vol_prev, ksd_prev, timestep, stream=None,
+             sync: bool = True) -> int:
+        """One call on `stream` (None: the legacy default stream); waits for
+        the device unless sync is False, as the C entry point itself does not."""
+        sp = self._sp
+        scal = [sp[7] if k == "@mu_state" else params[k] for k in V2_ARG_ORDER]
+        rc = lib().svpf_fully_fused_step_v2(
+            *self._arr_ptrs, float(y_t), float(y_prev), float(h_mean_prev), float(vol_prev), float(ksd_prev),
+            *sp[:7], *scal, self.n, int(timestep), stream)
+        if sync:
+            self.torch.cuda.synchronize()
         return int(rc)
 
 

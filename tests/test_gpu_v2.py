@@ -124,4 +124,7 @@ def test_v2_philox_mode_and_tape_errors(pkg, oracle_mod):
     assert f.step(params, 0.01, 0.0, -4.5, 0.1, 0.1, 3) == 0
     assert f.rng_state().status == 4                   # SVPF_ERR_TAPE_SHORT
     assert not pkg.lib().svpf_fully_fused_v2_supported(100000)
+    # the largest N whose arrays fit a 16-member cluster (227 KB per CTA)
+    assert pkg.lib().svpf_fully_fused_v2_supported(8064)
+    assert not pkg.lib().svpf_fully_fused_v2_supported(8065)
     f.close()
