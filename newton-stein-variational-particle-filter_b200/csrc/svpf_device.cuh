@@ -512,6 +512,27 @@ __device__ inline Smem carve(float* base, int n, int C, int rank, bool heun) {
 // means before the sum pass (the latency kernel: no sort, whose ~log2(N)^2/2
 // block barriers cost more than the extra pass at N <= 1024 on a cluster).
 // ---------------------------------------------------------------------------
+// Pushes each row's values from lane 0 of its S lanes into every team
+// member: the row's lanes take the members in turn (lane q: members q, q + S,
+// ...), so that the remote stores of a row go out in parallel.  TWO: a second
+// array b with values vb.  Every lane of the warp calls it.
+template <int R, int S, bool TWO>
+__device__ __forceinline__ void push_rows(float* a, float* b, const float (&va)[R], const float (&vb)[R],
+                                          const int (&jl)[R], int nloc, int row0, int q, const Team& team) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const float x = S > 1 ? __shfl_sync(0xffffffffu, va[r], 0, S) : va[r];
+        float y = 0.0f;
+        if (TWO) y = S > 1 ? __shfl_sync(0xffffffffu, vb[r], 0, S) : vb[r];
+        if (jl[r] >= nloc) continue;
+        const int j = row0 + jl[r];
+        for (int rk = q; rk < team.size; rk += S) {
+            team.at(a, rk)[j] = x;
+            if (TWO) team.at(b, rk)[j] = y;
+        }
+    }
+}
+
 template <int R, int S, bool STUDENT, bool SCAN = false>
 __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_config_t& cfg,
                           float beta, float* __restrict__ lw_out, const Team& team) {
@@ -639,6 +660,9 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
                 if (STUDENT) wh[r] += __shfl_xor_sync(0xffffffffu, wh[r], o);
             }
         }
+        float psc[R], pcc[R];   // the row's pushed score and curvature (lane 0 of the row)
+#pragma unroll
+        for (int r = 0; r < R; ++r) psc[r] = pcc[r] = 0.0f;
         if (q == 0) {
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -676,13 +700,16 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
                         cc = 1.0f / curv;           // 1/curvature (:765)
                     }
                 }
-                for (int rk = 0; rk < team.size; ++rk) {
-                    team.at(sm.g, rk)[j] = score;
-                    team.at(sm.c, rk)[j] = cc;
+                if (team.size == 1) {
+                    sm.g[j] = score;
+                    sm.c[j] = cc;
                 }
+                psc[r] = score;
+                pcc[r] = cc;
                 lw_out[j] = lw;
             }
         }
+        if (team.size > 1) push_rows<R, S, true>(sm.g, sm.c, psc, pcc, jl, nloc, sm.row0, q, team);
     }
 }
 
@@ -816,6 +843,9 @@ __device__ float transport_pass(const Smem& sm, int cur, const P& pl, const svpf
                 }
             }
         }
+        float pnew[R];   // the row's new position (lane 0 of the row)
+#pragma unroll
+        for (int r = 0; r < R; ++r) pnew[r] = 0.0f;
         if (q == 0) {
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -842,9 +872,12 @@ __device__ float transport_pass(const Smem& sm, int cur, const P& pl, const svpf
                 if (pl.temp > 1e-6f) diff = sqrtf(2.0f * es * pl.temp) * (pre ? pre[li] : nz.normal(i, kn));
                 const float h_new = clamp_h((RAW ? hi[r] : fmaf(hi[r], pl.bw, pl.center)) + drift + diff);
                 const float hs_new = RAW ? h_new : (h_new - pl.center) * inv_bw;
-                for (int rk = 0; rk < team.size; ++rk) team.at(hn, rk)[i] = hs_new;
+                if (team.size == 1) hn[i] = hs_new;
+                pnew[r] = hs_new;
             }
         }
+        if (MODE == kTransport && team.size > 1)
+            push_rows<R, S, false>(hn, hn, pnew, pnew, il, nloc, sm.row0, q, team);
     }
     return ksd_thread;
 }
