@@ -512,6 +512,23 @@ __device__ inline Smem carve(float* base, int n, int C, int rank, bool heun) {
 // means before the sum pass (the latency kernel: no sort, whose ~log2(N)^2/2
 // block barriers cost more than the extra pass at N <= 1024 on a cluster).
 // ---------------------------------------------------------------------------
+// Column chunks per sweep unrolled in the cluster kernels (one warp pair per
+// scheduler: four chunks' loads in flight).  The batch kernel, at its register
+// limit, leaves the unrolling to the compiler.
+constexpr int kClusterUnroll = 4;
+
+// The column-chunk loop of the pair sweeps: cb = c0, c0 + step, ... < nv.
+// U > 0 unrolls it U times; U = 0 leaves the unrolling to the compiler.
+template <int U, class F>
+__device__ __forceinline__ void chunk_loop(int c0, int nv, int step, F&& body) {
+    if constexpr (U > 0) {
+#pragma unroll U
+        for (int cb = c0; cb < nv; cb += step) body(cb);
+    } else {
+        for (int cb = c0; cb < nv; cb += step) body(cb);
+    }
+}
+
 // Pushes each row's values from lane 0 of its S lanes into every team
 // member: the row's lanes take the members in turn (lane q: members q, q + S,
 // ...), so that the remote stores of a row go out in parallel.  TWO: a second
@@ -533,7 +550,7 @@ __device__ __forceinline__ void push_rows(float* a, float* b, const float (&va)[
     }
 }
 
-template <int R, int S, bool STUDENT, bool SCAN = false>
+template <int R, int S, bool STUDENT, bool SCAN = false, int U = 0>
 __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_config_t& cfg,
                           float beta, float* __restrict__ lw_out, const Team& team) {
     // Positions arrive in transport coordinates hs = (h - center) / bw.  The
@@ -581,7 +598,7 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
                 mn[r] = 3.0e38f;
                 x2[r] = f2(xj[r]);
             }
-            for (int cb = q * 4; cb < nv; cb += 4 * S) {
+            chunk_loop<U>(q * 4, nv, 4 * S, [&](int cb) {
                 const float4 m4 = *reinterpret_cast<const float4*>(mu + cb);
                 const float2 ma = make_float2(m4.x, m4.y), mb = make_float2(m4.z, m4.w);
 #pragma unroll
@@ -590,7 +607,7 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
                     const float2 qa = mul2(da, da), qb = mul2(db, db);
                     mn[r] = fminf(mn[r], fminf(fminf(qa.x, qa.y), fminf(qb.x, qb.y)));
                 }
-            }
+            });
 #pragma unroll
             for (int o = S / 2; o > 0; o >>= 1) {
 #pragma unroll
@@ -609,7 +626,7 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
                 sr2[r] = f2(0.0f);
                 wg2[r] = f2(0.0f);
             }
-            for (int cb = q * 4; cb < nv; cb += 4 * S) {
+            chunk_loop<U>(q * 4, nv, 4 * S, [&](int cb) {
                 const float4 m4 = *reinterpret_cast<const float4*>(mu + cb);
                 const float2 mm[2] = {make_float2(m4.x, m4.y), make_float2(m4.z, m4.w)};
 #pragma unroll
@@ -623,7 +640,7 @@ __device__ void grad_pass(const Smem& sm, int cur, const Plan& pl, const svpf_co
                         wg2[r] = fma2(w, d, wg2[r]);
                     }
                 }
-            }
+            });
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 sr[r] = sr2[r].x + sr2[r].y;
@@ -728,7 +745,7 @@ enum { kTransport = 0, kPhiOnly = 1, kKsdOnly = 2 };
 // (h - center) / bw) or FactorPlan (one factor of the two-factor tick:
 // positions stored in log-volatility units, scaled inside the pair FMA as
 // u = h_i / bw - h_j / bw, so the stiff per-factor priors read exact positions).
-template <int R, int S, int KIND, bool KSD, int MODE = kTransport, class P = Plan>
+template <int R, int S, int KIND, bool KSD, int MODE = kTransport, class P = Plan, int U = 0>
 __device__ float transport_pass(const Smem& sm, int cur, const P& pl, const svpf_config_t& cfg,
                                 float bf, const Noise& nz, int kn, const Team& team,
                                 float* __restrict__ phi_out = nullptr,
@@ -774,7 +791,7 @@ __device__ float transport_pass(const Smem& sm, int cur, const P& pl, const svpf
                 ks2[r] = kg2[r] = gk2[r] = kc2[r] = gkr2[r] = gdk2[r] = hs2[r] = f2(0.0f);
                 nks[r] = 0.0f;
             }
-            for (int cb = q * 4; cb < nv; cb += 4 * S) {
+            chunk_loop<U>(q * 4, nv, 4 * S, [&](int cb) {
                 const float4 h4 = *reinterpret_cast<const float4*>(hc + cb);
                 const float4 g4 = *reinterpret_cast<const float4*>(gs + cb);
                 float4 c4 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -812,7 +829,7 @@ __device__ float transport_pass(const Smem& sm, int cur, const P& pl, const svpf
                         }
                     }
                 }
-            }
+            });
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 ks[r] = ks2[r].x + ks2[r].y;

@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(kThreads, 1) single_tick_kernel(const __grid_c
         pl.stc = a.stc;
         pl.log_y2 = a.log_y2;
     }
-    run_tick<R, S, SCAN, PROD>(cfg, prm, ctl, a.y_t, a.y_prev, io, nz, sm, pl, team, out);
+    run_tick<R, S, SCAN, PROD, kClusterUnroll>(cfg, prm, ctl, a.y_t, a.y_prev, io, nz, sm, pl, team, out);
     if (team.rank == 0) {
         __syncthreads();
         if (threadIdx.x == 0) {

@@ -18,12 +18,12 @@ struct FilterIO {
     int n;
 };
 
-template <int R, int S, int KIND, bool KSD, int MODE>
+template <int R, int S, int KIND, bool KSD, int MODE, int U = 0>
 __device__ __forceinline__ float stein_rows(const Smem& sm, int cur, const Plan& pl,
                                             const svpf_config_t& cfg, float bf, const Noise& nz,
                                             int kn, const Team& team, float* phi_out,
                                             const float* pre = nullptr) {
-    return transport_pass<R, S, KIND, KSD, MODE>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out, pre);
+    return transport_pass<R, S, KIND, KSD, MODE, Plan, U>(sm, cur, pl, cfg, bf, nz, kn, team, phi_out, pre);
 }
 
 template <int R, int S, int MODE>
@@ -65,7 +65,7 @@ __device__ __forceinline__ void ksd_publish(float ksd_thread, Plan& pl, const Te
 // caller guarantees full-Newton transport, Gaussian state noise and no Heun
 // step (the production configuration), so only those code paths are compiled
 // and the kernel body stays small (instruction fetch bounds the latency kernel).
-template <int R, int S, bool SCAN = false, bool PROD = false>
+template <int R, int S, bool SCAN = false, bool PROD = false, int U = 0>
 __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_ctl_t& ctl, float y_t,
                          float y_prev, const FilterIO& io, const Noise& nz, const Smem& sm, Plan& pl,
                          const Team& team, svpf_out_t& out) {
@@ -211,10 +211,10 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
             const float* pre = (sm.pre != nullptr && it < kPreIters) ? sm.pre + it * sm.Lp : nullptr;
             float kt;
             if constexpr (PROD) {
-                grad_pass<R, S, false, SCAN>(sm, cur, pl, cfg, beta, io.lw, team);
+                grad_pass<R, S, false, SCAN, U>(sm, cur, pl, cfg, beta, io.lw, team);
                 team.sync();
-                kt = last ? stein_rows<R, S, 2, true, kTransport>(sm, cur, pl, cfg, bf, nz, kn, team, nullptr, pre)
-                          : stein_rows<R, S, 2, false, kTransport>(sm, cur, pl, cfg, bf, nz, kn, team, nullptr, pre);
+                kt = last ? stein_rows<R, S, 2, true, kTransport, U>(sm, cur, pl, cfg, bf, nz, kn, team, nullptr, pre)
+                          : stein_rows<R, S, 2, false, kTransport, U>(sm, cur, pl, cfg, bf, nz, kn, team, nullptr, pre);
             } else {
                 grad_dispatch<R, S, SCAN>(student, sm, cur, pl, cfg, beta, io.lw, team);
                 team.sync();
