@@ -651,7 +651,9 @@ def main():
             lib.svpf_step_graph(s._s, float(ys[1, f]), float(ys[0, f]), C.byref(s.params), None, None, None)
         dtp = time.perf_counter() - t0
         plain = {"value": sample / dtp, "unit": "filter-ticks/s", "sample": f"{sample} filters of the workload, "
-                 "one blocking svpf_step_graph call each"}
+                 "one blocking svpf_step_graph call each",
+                 "step": "this engine's own single-filter step; the reference's step looped over the same "
+                         "workload is timed on the same GPU by tests/test_gpu_reference.py"}
         for s in filt:
             s.close()
 

@@ -548,15 +548,30 @@ size_t v2_smem_bytes(int n, int C, int pre) {
     return (size_t)(7 * np + (3 + pre) * L) * sizeof(float);
 }
 
+// Dynamic shared memory a v2 member may take: the device's opt-in limit per
+// block less the kernel's own static shared memory.
+size_t v2_smem_cap() {
+    static size_t cached = 0;
+    if (cached == 0) {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        cudaFuncAttributes fa{};
+        if (cudaFuncGetAttributes(&fa, v2::v2_kernel) != cudaSuccess) return 0;
+        cached = (size_t)v > fa.sharedSizeBytes ? (size_t)v - fa.sharedSizeBytes : 0;
+    }
+    return cached;
+}
+
 int v2_cluster(int n) {
     int C = default_cluster(n);
-    while (C > 1 && v2_smem_bytes(n, C, 0) > max_dyn_smem()) C >>= 1;
+    while (C > 1 && v2_smem_bytes(n, C, 0) > v2_smem_cap()) C >>= 1;
     return C;
 }
 
 // Pre-drawn steps that fit beside the cluster's arrays (up to kPreSteps).
 int v2_pre_steps(int n, int C) {
-    const size_t base = v2_smem_bytes(n, C, 0), cap = max_dyn_smem();
+    const size_t base = v2_smem_bytes(n, C, 0), cap = v2_smem_cap();
     if (base >= cap) return 0;
     const size_t row = (size_t)((n + C - 1) / C) * sizeof(float);
     const size_t fit = (cap - base) / row;
@@ -569,7 +584,7 @@ extern "C" {
 
 bool svpf_fully_fused_v2_supported(int n_particles) {
     return n_particles >= 1 && n_particles <= SVPF_MAX_PARTICLES &&
-           v2_smem_bytes(n_particles, 16, 0) <= max_dyn_smem();
+           v2_smem_bytes(n_particles, 16, 0) <= v2_smem_cap();
 }
 
 cudaError_t svpf_fully_fused_step_v2(
@@ -618,7 +633,7 @@ cudaError_t svpf_fully_fused_step_v2(
     static bool configured = false;
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(v2::v2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)max_dyn_smem());
+                                             (int)v2_smem_cap());
         if (e != cudaSuccess) return e;
         e = cudaFuncSetAttribute(v2::v2_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         if (e != cudaSuccess) return e;
