@@ -666,10 +666,18 @@ def main():
     mean_s = (sum(step_ms) / len(step_ms)) / 1e3
     achieved = mean_pairs / mean_s / 1e9
     # per pair-iteration (one mixture-prior pair + one full-Newton transport pair):
-    # 2 MUFU evaluations (ex2, rcp) at 16/clk/SM and 13 FP32 operations at
-    # 128/clk/SM -> the MUFU bounds it at 8 pair-iterations per clock per SM
-    PAIRS_PER_CLK = min(16.0 / 2.0, 128.0 / 13.0)
-    peak = sms * sm_mhz * 1e6 * PAIRS_PER_CLK / 1e9
+    # 2 MUFU evaluations (ex2, rcp) and 13 FP32 operations.  Nominal rates
+    # 16 MUFU and 128 FP32 results per clock per SM -> 8 pair-iterations per
+    # clock per SM (MUFU-bound); the peak used is the same bound from the
+    # rates measured on this GPU (svpf_measure_pipe_rates), the nominal beside it
+    PAIRS_PER_CLK_NOMINAL = min(16.0 / 2.0, 128.0 / 13.0)
+    try:
+        rates = pkg.pipe_rates()
+        pairs_per_clk, peak_src = rates["pairs_per_clk_sm"], "measured"
+    except RuntimeError as exc:
+        rates, pairs_per_clk, peak_src = {"error": str(exc)}, PAIRS_PER_CLK_NOMINAL, "nominal"
+    peak = sms * sm_mhz * 1e6 * pairs_per_clk / 1e9
+    peak_nominal = sms * sm_mhz * 1e6 * PAIRS_PER_CLK_NOMINAL / 1e9
     traffic = read_ncu_traffic()
 
     grad_line = {}
@@ -702,10 +710,13 @@ def main():
                               "same ticks as the device-timed steps"},
             "gpu_launches": launches,
             "roofline": {"bound": "fp32+mufu", "achieved": achieved, "peak": peak, "unit": "Gpair/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "note": "pair = one (i,j) Stein iteration: mixture-prior pair + transport pair; peak = "
-                                 f"{sms} SMs x {sm_mhz:.0f} MHz (measured) x 8 pair/clk/SM (2 MUFU evaluations per "
-                                 "pair at 16/clk/SM; 13 FP32 ops at 128/clk/SM)"},
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                         "pipe_rates": rates, "peak_nominal": peak_nominal,
+                         "note": "pair = one (i,j) Stein iteration: mixture-prior pair + transport pair (2 MUFU "
+                                 "evaluations, 13 FP32 ops); peak = "
+                                 f"{sms} SMs x {sm_mhz:.0f} MHz (sampled) x min(MUFU/2, FP32/13) pair/clk/SM from "
+                                 "the MUFU and FP32 results per SM clock measured on this GPU "
+                                 "(nominal 16 and 128: 8 pair/clk/SM)"},
             "single_filter_latency": lat,
             "plain_step_loop": plain,
             "gradient": grad_line,

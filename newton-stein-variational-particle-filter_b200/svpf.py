@@ -199,6 +199,7 @@ def lib() -> C.CDLL:
         "svpf_fully_fused_v2_rng_get": (_I, [vp, vp]),
         "svpf_fully_fused_v2_rng_set": (_I, [vp, vp]),
         "svpf_debug_philox": (_I, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), _I]),
+        "svpf_measure_pipe_rates": (_I, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "svpf_estimator_create": (vp, [_I, _I, _I, _F, _I, _I, _I, vp]),
         "svpf_estimator_destroy": (None, [vp]),
         "svpf_estimator_tape_floats": (C.c_longlong, [_I, _I]),
@@ -1033,6 +1034,17 @@ def philox(k0: int, k1: int, counters: np.ndarray) -> np.ndarray:
     if rc != SVPF_OK:
         raise RuntimeError(f"philox failed: {ERRORS.get(rc, rc)}")
     return out
+
+
+def pipe_rates() -> dict:
+    """Measured MUFU and FP32 results per SM clock on the current device
+    (svpf_measure_pipe_rates) and the pair-iteration peak they give."""
+    mufu, fp32 = C.c_double(0.0), C.c_double(0.0)
+    rc = lib().svpf_measure_pipe_rates(C.byref(mufu), C.byref(fp32))
+    if rc != SVPF_OK:
+        raise RuntimeError(f"svpf_measure_pipe_rates failed: {ERRORS.get(rc, rc)}")
+    return {"mufu_per_clk_sm": mufu.value, "fp32_per_clk_sm": fp32.value,
+            "pairs_per_clk_sm": min(mufu.value / 2.0, fp32.value / 13.0)}
 
 
 def build_info() -> str:
