@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(kThreads, 1) single_tick_kernel(const __grid_c
 
 // Two-factor tick: a.h / a.hp / a.v hold [fast (n); slow (n)].
 template <int R, int S>
-__global__ void __launch_bounds__(kThreads) single_tick_2f_kernel(const __grid_constant__ SingleArgs a) {
+__global__ void __launch_bounds__(kThreads, 1) single_tick_2f_kernel(const __grid_constant__ SingleArgs a) {
     extern __shared__ __align__(16) float smem[];
     __shared__ Plan pl;
     __shared__ svpf_ctl_t ctl;
