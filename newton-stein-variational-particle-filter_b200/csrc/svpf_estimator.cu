@@ -390,7 +390,7 @@ __global__ void __launch_bounds__(kThreads) est_forward_kernel(const EArgs a, in
     }
 }
 
-__global__ void __launch_bounds__(kThreads) est_backward_kernel(const EArgs a, int sg) {
+__global__ void __launch_bounds__(kThreads, 4) est_backward_kernel(const EArgs a, int sg) {
     extern __shared__ __align__(16) float smem[];
     __shared__ TickShared sh;
     const Arrays s = carve(smem, a.np, a.S);
