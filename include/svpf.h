@@ -43,6 +43,7 @@ extern "C" {
 /* Engine limits. */
 #define SVPF_MAX_PARTICLES         8192   /* per filter */
 #define SVPF_MAX_ANNEAL_STEPS      16
+#define SVPF_MAX_STEIN_STEPS       256    /* Stein iterations of one tick, all stages */
 
 /* Error codes returned by svpf_last_error() and the batch API. */
 #define SVPF_OK                    0
@@ -399,11 +400,25 @@ int svpf_batch_kernel_launches(const svpf_batch_t* b);  /* launches issued so fa
 int svpf_batch_get_ctl(const svpf_batch_t* b, svpf_ctl_t* ctl_host);          /* [n_filters] */
 /* h_out receives n values, or 2n (fast then slow) for a two-factor filter. */
 int svpf_batch_get_particles(const svpf_batch_t* b, int filter, float* h_out);
+/* State of filter f (host arrays; any pointer may be NULL): control record,
+ * h / h_prev / RMSProp v of n values (2n, fast then slow, for a two-factor
+ * filter) and the n log-weights.  Both wait for the batch's stream.  Used for
+ * checkpoints and for per-tick parity checks with state re-sync. */
+int svpf_batch_get_state(const svpf_batch_t* b, int filter, svpf_ctl_t* ctl, float* h, float* h_prev, float* v,
+                         float* log_w);
+int svpf_batch_set_state(svpf_batch_t* b, int filter, const svpf_ctl_t* ctl, const float* h, const float* h_prev,
+                         const float* v, const float* log_w);
 int svpf_batch_set_noise_tape(svpf_batch_t* b, const float* normals, int n_normal_slots,
                               const float* uniforms, int n_uniform_slots);   /* same tape for all, [k][n_max] */
 /* Tile shape (rows per thread R, column split S) used for filters of size n;
  * -1 when no choice was made. */
 int svpf_batch_tile_of(const svpf_batch_t* b, int n, int* rows_per_thread, int* col_split);
+/* The tile shape filter f runs with, and -- to test or pin a shape -- force
+ * one: (rows_per_thread, col_split) must be a compiled batch tile, (1,4)
+ * (1,2) (1,1) (2,1) (4,1); SVPF_ERR_INVALID_ARG otherwise.  Forcing a tile
+ * waits for the batch's stream and drops its captured graph. */
+int svpf_batch_tile_of_filter(const svpf_batch_t* b, int filter, int* rows_per_thread, int* col_split);
+int svpf_batch_set_tile(svpf_batch_t* b, int filter, int rows_per_thread, int col_split);
 
 /* One tick of a batch whose buffers the caller owns, with no allocation of any
  * kind.  No counterpart in the reference: it serves callers that cannot call
@@ -411,17 +426,26 @@ int svpf_batch_tile_of(const svpf_batch_t* b, int n, int* rows_per_thread, int* 
  * a plugin inside another framework's memory manager, a latency-critical loop
  * that must not take the device synchronisation an allocation may cause).
  * Every buffer is a device pointer the caller allocated: particle counts d_n,
- * packed-array offsets d_off (16-float aligned, as the batch layout), per-filter
- * configuration, parameters and control records (updated in place), the packed
- * particle arrays (updated in place), this tick's observations and, optionally,
- * the outputs.  The kernel's scratch (work counter, work order, tile per
- * filter) is a fixed array inside the library, resident on every GPU that
- * loads it until the process exits; at most SVPF_NOALLOC_MAX_FILTERS filters
- * per call, larger batches are rejected with SVPF_ERR_INVALID_ARG.  The first
- * call on a device looks up that array's device address (make it before any
- * stream capture).  All calls share the one array and each call rewrites what
- * it uses; calls that overlap on the GPU race, so issue them in one stream or
- * order them.  Asynchronous on `stream`. */
+ * packed-array offsets d_off, per-filter configuration, parameters and control
+ * records (updated in place), the packed particle arrays (updated in place),
+ * this tick's observations and, optionally, the outputs.
+ * Single-factor filters only.  Each filter must have 1 <= d_n[f] <= n_max, an
+ * offset d_off[f] >= 0 that is a multiple of 16 floats, use_heun only when
+ * any_heun is 1, and loop counts within SVPF_MAX_STEIN_STEPS; its n floats at
+ * d_off[f] must lie inside each packed array (that size is not passed and is
+ * not checked).  A filter that breaks one of the checked rules is left out of
+ * the tick on the device, before anything reads its particles: its control
+ * record's status becomes SVPF_ERR_INVALID_ARG (SVPF_ERR_UNSUPPORTED for a
+ * two-factor filter) and its arrays and outputs are not written; the other
+ * filters tick as usual.
+ * The kernel's scratch (work counter, work order, tile per filter) is a fixed
+ * array inside the library, resident on every GPU that loads it until the
+ * process exits; at most SVPF_NOALLOC_MAX_FILTERS filters per call, larger
+ * batches are rejected with SVPF_ERR_INVALID_ARG.  The first call on a device
+ * looks up that array's device address (make it before any stream capture).
+ * All calls share the one array and each call rewrites what it uses; calls
+ * that overlap on the GPU race, so issue them in one stream or order them.
+ * Asynchronous on `stream`. */
 #define SVPF_NOALLOC_MAX_FILTERS   16384
 int svpf_batch_tick_noalloc(int n_filters, const int* d_n, const long long* d_off,
                             const svpf_config_t* d_cfg, const SVPFParams* d_params,
@@ -478,6 +502,15 @@ int svpf_grad_forward_device(svpf_grad_t* g, const float* d_theta, const float* 
                              const float* d_y, int T, unsigned long long seed, float* d_loglik);
 int svpf_grad_backward_device(svpf_grad_t* g, const float* d_w, double* d_grad);
 int svpf_grad_checkpoint_every(const svpf_grad_t* g);
+/* Parameter domain: every theta component finite, nu > 0, sigma_z > 0,
+ * |rho| < 1, leverage finite.  svpf_grad_forward checks the host theta and
+ * returns SVPF_ERR_INVALID_ARG before any launch.  With device theta
+ * (svpf_grad_forward_device, the torch path) a filter outside the domain is
+ * left out on the device: its status becomes SVPF_ERR_INVALID_ARG, its
+ * log-likelihoods and gradient NaN; the other filters are unaffected.
+ * status [n_filters] (host): the status of each filter after the last
+ * forward / backward (waits for the engine's stream). */
+int svpf_grad_get_status(svpf_grad_t* g, int* status);
 /* 1 if the backward records a whole checkpoint segment in one forward pass
  * (k tick records per CTA in device memory) instead of re-running each tick's
  * forward once more before its adjoint; chosen at create by free memory.
@@ -654,6 +687,11 @@ int svpf_estimator_backward(svpf_estimator_t* e, const float* w, double* grad);
 int svpf_estimator_forward_device(svpf_estimator_t* e, const float* d_theta, const float* d_y, int T,
                                   unsigned long long seed, const float* d_tape, float* d_loglik, float* d_vol);
 int svpf_estimator_backward_device(svpf_estimator_t* e, const float* d_w, double* d_grad);
+/* theta outside the domain (any component non-finite, nu <= 0, sigma_z <= 0,
+ * |rho| >= 1): svpf_estimator_forward returns SVPF_ERR_INVALID_ARG before any
+ * launch; the device variants mark that path SVPF_ERR_INVALID_ARG, NaN its
+ * outputs and gradient and leave the other paths unaffected.  status [F]. */
+int svpf_estimator_get_status(svpf_estimator_t* e, int* status);
 
 #ifdef __cplusplus
 }

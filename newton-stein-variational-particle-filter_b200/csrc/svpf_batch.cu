@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <utility>
 #include <vector>
 
 #include "svpf.h"
@@ -161,7 +162,7 @@ svpf_batch_t* svpf_batch_create(int F, const int* ns, const svpf_config_t* cfgs,
     if (F < 1 || !ns || !cfgs || !prms) return nullptr;
     int n_max = 0, n_max1 = 0, n_max2 = 0, F1 = 0, heun = 0, prod = 1;
     for (int f = 0; f < F; ++f) {
-        if (ns[f] < 1 || ns[f] > SVPF_MAX_PARTICLES) return nullptr;
+        if (ns[f] < 1 || ns[f] > SVPF_MAX_PARTICLES || !config_loops_ok(cfgs[f])) return nullptr;
         n_max = std::max(n_max, ns[f]);
         if (cfgs[f].use_two_factor) {
             if (cfgs[f].n_stein_steps < 1) return nullptr;
@@ -457,6 +458,37 @@ int svpf_batch_get_particles(const svpf_batch_t* b, int f, float* h_out) {
                ? SVPF_OK : SVPF_ERR_CUDA;
 }
 
+int svpf_batch_get_state(const svpf_batch_t* b, int f, svpf_ctl_t* ctl, float* h, float* hp, float* v, float* lw) {
+    if (!b || f < 0 || f >= b->F) return SVPF_ERR_INVALID_ARG;
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return SVPF_ERR_CUDA;
+    const size_t len = (size_t)(b->tf[f] ? 2 : 1) * b->ns[f], off = (size_t)b->offs[f];
+    const std::pair<float*, const float*> arrs[] = {{h, b->d_h}, {hp, b->d_hp}, {v, b->d_v}};
+    for (const auto& a : arrs)
+        if (a.first && cudaMemcpy(a.first, a.second + off, len * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return SVPF_ERR_CUDA;
+    if (lw && cudaMemcpy(lw, b->d_lw + off, b->ns[f] * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return SVPF_ERR_CUDA;
+    if (ctl && cudaMemcpy(ctl, b->d_ctl + f, sizeof(svpf_ctl_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return SVPF_ERR_CUDA;
+    return SVPF_OK;
+}
+
+int svpf_batch_set_state(svpf_batch_t* b, int f, const svpf_ctl_t* ctl, const float* h, const float* hp,
+                         const float* v, const float* lw) {
+    if (!b || f < 0 || f >= b->F) return SVPF_ERR_INVALID_ARG;
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return SVPF_ERR_CUDA;
+    const size_t len = (size_t)(b->tf[f] ? 2 : 1) * b->ns[f], off = (size_t)b->offs[f];
+    const std::pair<const float*, float*> arrs[] = {{h, b->d_h}, {hp, b->d_hp}, {v, b->d_v}};
+    for (const auto& a : arrs)
+        if (a.first && cudaMemcpy(a.second + off, a.first, len * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+            return SVPF_ERR_CUDA;
+    if (lw && cudaMemcpy(b->d_lw + off, lw, b->ns[f] * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+        return SVPF_ERR_CUDA;
+    if (ctl && cudaMemcpy(b->d_ctl + f, ctl, sizeof(svpf_ctl_t), cudaMemcpyHostToDevice) != cudaSuccess)
+        return SVPF_ERR_CUDA;
+    return SVPF_OK;
+}
+
 int svpf_batch_set_noise_tape(svpf_batch_t* b, const float* normals, int ns, const float* uniforms, int nu_) {
     if (!b) return SVPF_ERR_INVALID_ARG;
     if (b->tape_n) cudaFree(b->tape_n);
@@ -492,65 +524,100 @@ int svpf_batch_tile_of(const svpf_batch_t* b, int n, int* R, int* S) {
 // Autotuner: for each particle count, time every batch tile shape on a
 // synthetic batch that fills the GPU (one filter per resident CTA) and keep
 // the fastest.  Production configuration, fixed budget (stein_min = max).
+// Any failed call (allocation, copy, launch, a tile's tick) ends the tuning
+// with SVPF_ERR_CUDA and records no choice for that size.
+namespace {
+
+int tune_one(int n, int ticks, int* best_tile) {
+    const size_t smem = tick_smem_bytes(n, 1, false);
+    if (smem > max_dyn_smem()) return SVPF_ERR_INVALID_ARG;
+    const int F = batch_grid(smem);
+    if (F < 1) return SVPF_ERR_CUDA;
+    svpf_config_t c;
+    svpf_config_init(&c, 8, 30.0f);
+    c.use_newton = 1;
+    c.use_full_newton = 1;
+    c.stein_min_steps = 8;
+    c.stein_max_steps = 8;
+    std::vector<int> nv(F, n);
+    std::vector<svpf_config_t> cv(F, c);
+    std::vector<SVPFParams> pv(F, SVPFParams{0.97f, 0.15f, -1.0f, 0.0f});
+    svpf_batch_t* b = svpf_batch_create(F, nv.data(), cv.data(), pv.data(), nullptr);
+    if (!b) return SVPF_ERR_CUDA;
+    float* d_y = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = svpf_batch_initialize(b, 1234);
+    if (rc == SVPF_OK && !dalloc(&d_y, 2 * (size_t)F)) rc = SVPF_ERR_CUDA;
+    if (rc == SVPF_OK) {
+        std::vector<float> ys(2 * (size_t)F);
+        std::fill(ys.begin(), ys.begin() + F, 0.3f);
+        std::fill(ys.begin() + F, ys.end(), 0.2f);
+        if (cudaMemcpy(d_y, ys.data(), ys.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+            rc = SVPF_ERR_CUDA;
+    }
+    float best = 1e30f;
+    int best_t = -1;
+    for (int t = kBatchTileLo; rc == SVPF_OK && t <= kBatchTileHi; ++t) {
+        std::fill(b->tiles.begin(), b->tiles.end(), (uint8_t)t);
+        if (cudaMemcpy(b->d_tile, b->tiles.data(), F, cudaMemcpyHostToDevice) != cudaSuccess) {
+            rc = SVPF_ERR_CUDA;
+            break;
+        }
+        rc = enqueue_tick(b, d_y, d_y + F, nullptr);   // warm
+        if (rc == SVPF_OK && cudaEventRecord(e0, b->stream) != cudaSuccess) rc = SVPF_ERR_CUDA;
+        for (int i = 0; rc == SVPF_OK && i < ticks; ++i) rc = enqueue_tick(b, d_y, d_y + F, nullptr);
+        if (rc == SVPF_OK && (cudaEventRecord(e1, b->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess))
+            rc = SVPF_ERR_CUDA;
+        float ms = 0.0f;
+        if (rc == SVPF_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) rc = SVPF_ERR_CUDA;
+        if (rc == SVPF_OK && ms < best) {
+            best = ms;
+            best_t = t;
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(d_y);
+    svpf_batch_destroy(b);
+    if (rc == SVPF_OK && best_t < 0) rc = SVPF_ERR_CUDA;
+    if (rc == SVPF_OK) *best_tile = best_t;
+    return rc;
+}
+
+}  // namespace
+
 int svpf_autotune(const int* ns, int count, int ticks) {
     if (!ns || count < 1) return SVPF_ERR_INVALID_ARG;
     ticks = std::max(ticks, 1);
+    for (int k = 0; k < count; ++k)
+        if (ns[k] < 1 || ns[k] > SVPF_MAX_PARTICLES) return SVPF_ERR_INVALID_ARG;
     for (int k = 0; k < count; ++k) {
-        const int n = ns[k];
-        if (n < 1 || n > SVPF_MAX_PARTICLES) return SVPF_ERR_INVALID_ARG;
-        const size_t smem = tick_smem_bytes(n, 1, false);
-        if (smem > max_dyn_smem()) return SVPF_ERR_INVALID_ARG;
-        const int grid = batch_grid(smem);
-        if (grid < 1) return SVPF_ERR_CUDA;
-        const int F = grid;
-        SVPFState* proto = svpf_create(std::min(n, 64), 8, 30.0f, nullptr);
-        if (!proto) return SVPF_ERR_CUDA;
-        svpf_config_t c;
-        svpf_get_config(proto, &c);
-        svpf_destroy(proto);
-        c.use_newton = 1;
-        c.use_full_newton = 1;
-        c.stein_min_steps = 8;
-        c.stein_max_steps = 8;
-        std::vector<int> nv(F, n);
-        std::vector<svpf_config_t> cv(F, c);
-        std::vector<SVPFParams> pv(F, SVPFParams{0.97f, 0.15f, -1.0f, 0.0f});
-        svpf_batch_t* b = svpf_batch_create(F, nv.data(), cv.data(), pv.data(), nullptr);
-        if (!b) return SVPF_ERR_CUDA;
-        svpf_batch_initialize(b, 1234);
-        std::vector<float> y(F, 0.3f), yp(F, 0.2f);
-        float* d_y = nullptr;
-        dalloc(&d_y, 2 * (size_t)F);
-        std::vector<float> ys(2 * F);
-        std::copy(y.begin(), y.end(), ys.begin());
-        std::copy(yp.begin(), yp.end(), ys.begin() + F);
-        cudaMemcpy(d_y, ys.data(), 2 * F * sizeof(float), cudaMemcpyHostToDevice);
-        cudaEvent_t e0, e1;
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
-        float best = 1e30f;
-        int best_t = default_batch_tile(n);
-        for (int t = kBatchTileLo; t <= kBatchTileHi; ++t) {
-            std::fill(b->tiles.begin(), b->tiles.end(), (uint8_t)t);
-            cudaMemcpy(b->d_tile, b->tiles.data(), F, cudaMemcpyHostToDevice);
-            enqueue_tick(b, d_y, d_y + F, nullptr);   // warm
-            cudaEventRecord(e0, b->stream);
-            for (int i = 0; i < ticks; ++i) enqueue_tick(b, d_y, d_y + F, nullptr);
-            cudaEventRecord(e1, b->stream);
-            if (cudaEventSynchronize(e1) != cudaSuccess) break;
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (ms < best) {
-                best = ms;
-                best_t = t;
-            }
-        }
-        set_tuned_batch_tile(n, best_t);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        cudaFree(d_y);
-        svpf_batch_destroy(b);
+        int t = -1;
+        const int rc = tune_one(ns[k], ticks, &t);
+        if (rc != SVPF_OK) return rc;
+        set_tuned_batch_tile(ns[k], t);
     }
+    return SVPF_OK;
+}
+
+int svpf_batch_set_tile(svpf_batch_t* b, int f, int R, int S) {
+    if (!b || f < 0 || f >= b->F) return SVPF_ERR_INVALID_ARG;
+    int tile = -1;
+    for (int t = kBatchTileLo; t <= kBatchTileHi; ++t)
+        if (kTiles[t].R == R && kTiles[t].S == S) tile = t;
+    if (tile < 0) return SVPF_ERR_INVALID_ARG;
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return SVPF_ERR_CUDA;
+    b->tiles[f] = (uint8_t)tile;
+    drop_graph(b);
+    return cudaMemcpy(b->d_tile + f, &b->tiles[f], 1, cudaMemcpyHostToDevice) == cudaSuccess ? SVPF_OK
+                                                                                          : SVPF_ERR_CUDA;
+}
+
+int svpf_batch_tile_of_filter(const svpf_batch_t* b, int f, int* R, int* S) {
+    if (!b || f < 0 || f >= b->F) return SVPF_ERR_INVALID_ARG;
+    if (R) *R = kTiles[b->tiles[f]].R;
+    if (S) *S = kTiles[b->tiles[f]].S;
     return SVPF_OK;
 }
 

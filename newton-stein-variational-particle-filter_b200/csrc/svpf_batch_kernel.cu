@@ -164,11 +164,9 @@ constexpr int kCluster2f = kClusterMembers2f;
 
 int batch_cluster_grid_2f(size_t smem_bytes) {
     auto kern = batch_tick_2f_cluster_kernel<kCluster2f>;
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn_smem());
-        cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        configured = true;
+    if (configure_kernel((const void*)kern, (int)max_dyn_smem(), true) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(kCluster2f, 1, 1);
@@ -208,10 +206,9 @@ cudaError_t launch_batch_2f_cluster(const BatchArgs& a, size_t smem_bytes, int g
 }
 
 int batch_grid_2f(size_t smem_bytes) {
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(batch_tick_2f_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn_smem());
-        configured = true;
+    if (configure_kernel((const void*)batch_tick_2f_kernel, (int)max_dyn_smem(), false) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
     }
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
@@ -228,11 +225,10 @@ cudaError_t launch_batch_2f(const BatchArgs& a, size_t smem_bytes, int grid, cud
 }
 
 int batch_grid(size_t smem_bytes) {
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(batch_tick_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn_smem());
-        cudaFuncSetAttribute(batch_tick_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn_smem());
-        configured = true;
+    if (configure_kernel((const void*)batch_tick_kernel<false>, (int)max_dyn_smem(), false) != cudaSuccess ||
+        configure_kernel((const void*)batch_tick_kernel<true>, (int)max_dyn_smem(), false) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
     }
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);

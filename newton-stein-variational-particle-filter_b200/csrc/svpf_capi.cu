@@ -294,6 +294,10 @@ void step_impl(SVPFState* s, float y_t, float y_prev, const SVPFParams* params,
     SingleArgs a;
     std::memset(&a, 0, sizeof(a));
     config_from_state(s, &a.cfg);
+    if (!config_loops_ok(a.cfg)) {
+        set_err(s, SVPF_ERR_INVALID_ARG);
+        return;
+    }
     a.prm = *params;
     ctl_gather(s, im, &a.ctl);
     a.y_t = y_t;

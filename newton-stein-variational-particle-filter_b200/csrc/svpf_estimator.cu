@@ -38,6 +38,8 @@
 
 #include "svpf.h"
 #include "svpf_device.cuh"
+#include "svpf_internal.h"
+#include "svpf_math.h"
 
 namespace svpf {
 namespace est {
@@ -67,6 +69,7 @@ struct TickShared {
     float mx, se, b;        // logsumexp max and sum, kernel scale b
     float red[8][kWarps];
     double acc[4];
+    int bad;                // this path's theta is outside the domain (theta_ok)
 };
 
 __device__ __forceinline__ size_t tape_stride(const EArgs& a) { return (size_t)a.n + (size_t)a.T * (a.n / 2); }
@@ -240,16 +243,6 @@ __device__ float fwd_tick(const EArgs& a, int f, int t, const Arrays& s, TickSha
     return ll;
 }
 
-// d/dnu of lgamma((nu+1)/2) - lgamma(nu/2) - log(nu pi)/2 (:75-80), psi by
-// the recurrence up to 8 and the asymptotic series (Abramowitz-Stegun 6.3.18).
-__device__ inline double digamma_est(double x) {
-    double acc = 0.0;
-    while (x < 8.0) { acc -= 1.0 / x; x += 1.0; }
-    const double r = 1.0 / x, r2 = r * r;
-    return acc + log(x) - 0.5 * r -
-           r2 * (1.0 / 12 - r2 * (1.0 / 120 - r2 * (1.0 / 252 - r2 * (1.0 / 240 - r2 * (1.0 / 132)))));
-}
-
 // Backward of tick t: s.xb holds d loss / d(output particles) on entry and
 // d loss / d(input particles) on exit; theta adjoints accumulate in sh.acc.
 // Requires the recorded forward of the same tick (s.m, s.lp, s.h, rec, sh.mx,
@@ -330,7 +323,8 @@ __device__ void bwd_tick(const EArgs& a, int f, int t, const Arrays& s, TickShar
     float v[5] = {pmu, prho, psz, pnu, ps2e};
     block_sum<5>(v, sh);
     if (tid == 0) {
-        const double dC = 0.5 * digamma_est(0.5 * ((double)nu + 1.0)) - 0.5 * digamma_est(0.5 * (double)nu) -
+        // d/dnu of the normaliser lgamma((nu+1)/2) - lgamma(nu/2) - log(nu pi)/2 (:75-80)
+        const double dC = 0.5 * digamma_bounded(0.5 * ((double)nu + 1.0)) - 0.5 * digamma_bounded(0.5 * (double)nu) -
                           0.5 / (double)nu;
         sh.acc[0] += v[0];
         sh.acc[1] += v[1];
@@ -348,6 +342,7 @@ __device__ inline void load_theta(const EArgs& a, int f, TickShared& sh) {
     sh.nu = a.theta[4 * f + 3];
     const float nu = sh.nu;
     sh.C = lgammaf((nu + 1.0f) * 0.5f) - lgammaf(nu * 0.5f) - 0.5f * logf(nu * 3.14159265358979f);
+    sh.bad = !theta_ok(sh.mu, sh.rho, sh.sz, sh.nu);
 }
 
 __global__ void __launch_bounds__(kThreads) est_forward_kernel(const EArgs a, int t0, int t1) {
@@ -358,6 +353,19 @@ __global__ void __launch_bounds__(kThreads) est_forward_kernel(const EArgs a, in
     for (int f = blockIdx.x; f < a.F; f += gridDim.x) {
         if (threadIdx.x == 0) load_theta(a, f, sh);
         __syncthreads();
+        if (sh.bad) {
+            // parameters no filter can run with: report them and leave the path out
+            for (int t = t0 + threadIdx.x; t < t1; t += kThreads) {
+                if (a.loglik) a.loglik[(size_t)f * a.T + t] = NAN;
+                if (a.vol) a.vol[(size_t)f * a.T + t] = NAN;
+            }
+            if (threadIdx.x == 0) {
+                a.status[f] = SVPF_ERR_INVALID_ARG;
+                a.ll_sum[f] = NAN;
+            }
+            __syncthreads();
+            continue;
+        }
         if (t0 == 0) {
             // :168-170
             const float hs = sh.sz / sqrtf(1.0f - sh.rho * sh.rho + 1e-6f);
@@ -404,6 +412,14 @@ __global__ void __launch_bounds__(kThreads, 4) est_backward_kernel(const EArgs a
             for (int q = 0; q < 4; ++q) sh.acc[q] = a.ath[4 * (size_t)f + q];
         }
         __syncthreads();
+        if (sh.bad) {
+            if (threadIdx.x == 0) {
+                for (int q = 0; q < 4; ++q) a.ath[4 * (size_t)f + q] = NAN;
+                a.status[f] = SVPF_ERR_INVALID_ARG;
+            }
+            __syncthreads();
+            continue;
+        }
         const float* ck = a.ck + ((size_t)f * a.nseg + sg) * np;
         for (int i = threadIdx.x; i < n; i += kThreads) {
             s.xin[i] = ck[i];
@@ -552,8 +568,15 @@ svpf_estimator_t* svpf_estimator_create(int n_filters, int n_particles, int n_st
         cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
         e->own_stream = true;
     }
-    cudaFuncSetAttribute(est_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->smem);
-    cudaFuncSetAttribute(est_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e->smem);
+    // the opt-in is the device's whole limit (engines of different sizes share the kernels)
+    if (configure_kernel((const void*)est_forward_kernel, (int)kernel_smem_cap((const void*)est_forward_kernel),
+                         false) != cudaSuccess ||
+        configure_kernel((const void*)est_backward_kernel, (int)kernel_smem_cap((const void*)est_backward_kernel),
+                         false) != cudaSuccess) {
+        cudaGetLastError();
+        svpf_estimator_destroy(e);
+        return nullptr;
+    }
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, est_backward_kernel, kThreads, e->smem);
     e->grid = std::min(n_filters, std::max(1, per_sm) * std::max(sms, 1));
@@ -620,6 +643,8 @@ int svpf_estimator_forward(svpf_estimator_t* e, const float* theta, const float*
                            const float* tape, float* loglik, float* vol, double* loglik_sum) {
     if (!e || !theta || !y || T < 1 || T > e->T_max) return SVPF_ERR_INVALID_ARG;
     const size_t F = (size_t)e->F;
+    for (size_t f = 0; f < F; ++f)
+        if (!theta_ok(theta[4 * f], theta[4 * f + 1], theta[4 * f + 2], theta[4 * f + 3])) return SVPF_ERR_INVALID_ARG;
     if (cudaMemcpyAsync(e->d_theta, theta, 4 * F * sizeof(float), cudaMemcpyHostToDevice, e->stream) != cudaSuccess ||
         cudaMemcpyAsync(e->d_y, y, F * T * sizeof(float), cudaMemcpyHostToDevice, e->stream) != cudaSuccess)
         return SVPF_ERR_CUDA;
@@ -651,6 +676,13 @@ int svpf_estimator_forward(svpf_estimator_t* e, const float* theta, const float*
     for (int s : st)
         if (s) return s;
     return SVPF_OK;
+}
+
+int svpf_estimator_get_status(svpf_estimator_t* e, int* status) {
+    if (!e || !status) return SVPF_ERR_INVALID_ARG;
+    if (cudaStreamSynchronize(e->stream) != cudaSuccess) return SVPF_ERR_CUDA;
+    return cudaMemcpy(status, e->d_status, (size_t)e->F * sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess
+               ? SVPF_OK : SVPF_ERR_CUDA;
 }
 
 int svpf_estimator_backward(svpf_estimator_t* e, const float* w, double* grad) {

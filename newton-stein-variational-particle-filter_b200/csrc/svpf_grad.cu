@@ -45,6 +45,7 @@
 #include "svpf.h"
 #include "svpf_device.cuh"
 #include "svpf_internal.h"
+#include "svpf_math.h"
 
 namespace svpf {
 namespace grad {
@@ -101,16 +102,6 @@ struct GArgs {
 
 __host__ __device__ inline size_t rec_floats_for(int np, int bmax) {
     return (size_t)np * (kRecFixed + kRecPerIt * bmax + 2);
-}
-
-// psi(x), x > 0: shift to x >= 8 with psi(x) = psi(x+1) - 1/x, then the
-// asymptotic series (Abramowitz & Stegun 6.3.18).
-__device__ inline double digamma_d(double x) {
-    double acc = 0.0;
-    while (x < 8.0) { acc -= 1.0 / x; x += 1.0; }
-    const double r = 1.0 / x, r2 = r * r;
-    return acc + log(x) - 0.5 * r -
-           r2 * (1.0 / 12 - r2 * (1.0 / 120 - r2 * (1.0 / 252 - r2 * (1.0 / 240 - r2 * (1.0 / 132)))));
 }
 
 // ---- block reductions over kThreads threads ----------------------------------
@@ -189,6 +180,7 @@ struct Shared {
     TickScalars ts;
     GState st;
     int flag;
+    int bad;          // this filter's theta is outside the domain (theta_ok)
     double acc[8];
 };
 
@@ -927,7 +919,7 @@ __device__ void bwd_tick(const svpf_config_t& c, int n, int np, float* xb, float
         reduce_sum<2>(s, sh.red);
         if (tid == 0) {
             TickScalars& t = sh.ts;
-            const double dstc = 0.5 * digamma_d(0.5 * ((double)nu + 1.0)) - 0.5 * digamma_d(0.5 * (double)nu) -
+            const double dstc = 0.5 * digamma_bounded(0.5 * ((double)nu + 1.0)) - 0.5 * digamma_bounded(0.5 * (double)nu) -
                                 0.5 / (double)nu;
             sh.acc[3] = dstc * (double)s[1];
             const float bwb = s[0];
@@ -1077,6 +1069,11 @@ __device__ inline void load_theta(const GArgs& a, int f, TickScalars& ts) {
     ts.gamma = a.gamma ? a.gamma[f] : 0.0f;
 }
 
+// 1 when filter f's parameters cannot be run (see theta_ok; leverage finite).
+__device__ inline int theta_bad(const TickScalars& ts) {
+    return !theta_ok(ts.mu, ts.rho, ts.sz, ts.nu) || !(fabsf(ts.gamma) < INFINITY);
+}
+
 // svpf_initialize (svpf_optimized_graph.cu:349-451), single factor, Philox draw 0 of stream 2.
 __device__ void init_filter(const GArgs& a, int f, int n, float* x, float* v, Shared& sh) {
     const TickScalars& ts = sh.ts;
@@ -1150,8 +1147,20 @@ __global__ void __launch_bounds__(kThreads) grad_forward_kernel(const GArgs a, i
             cfg = a.cfg[f];
             sh.flag = 0;
             load_theta(a, f, sh.ts);
+            sh.bad = theta_bad(sh.ts);
         }
         __syncthreads();
+        if (sh.bad) {
+            // parameters no filter can run with: report them and leave the filter out
+            if (a.loglik)
+                for (int t = t0 + threadIdx.x; t < t1; t += kThreads) a.loglik[(size_t)f * a.T + t] = NAN;
+            if (threadIdx.x == 0) {
+                a.status[f] = SVPF_ERR_INVALID_ARG;
+                a.ll_sum[f] = NAN;
+            }
+            __syncthreads();
+            continue;
+        }
         const int n = a.n[f];
         if (t0 == 0) {
             init_filter(a, f, n, x, v, sh);
@@ -1220,10 +1229,19 @@ __global__ void __launch_bounds__(kThreads) grad_backward_kernel(const GArgs a, 
             cfg = a.cfg[f];
             sh.flag = 0;
             load_theta(a, f, sh.ts);
+            sh.bad = theta_bad(sh.ts);
             sh.st = a.cks[(size_t)f * a.nseg + sg];
             sa = a.as[f];
         }
         __syncthreads();
+        if (sh.bad) {
+            if (threadIdx.x == 0) {
+                for (int q = 0; q < 4; ++q) a.as[f].th[q] = NAN;
+                a.status[f] = SVPF_ERR_INVALID_ARG;
+            }
+            __syncthreads();
+            continue;
+        }
         const float* ck = a.ck + ((size_t)f * a.nseg + sg) * 2 * np;
         for (int i = threadIdx.x; i < n; i += kThreads) {
             x[i] = ck[i];
@@ -1451,8 +1469,15 @@ svpf_grad_t* svpf_grad_create(int F, const int* ns, const svpf_config_t* cfgs, i
         delete g;
         return nullptr;
     }
-    cudaFuncSetAttribute(grad_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g->smem);
-    cudaFuncSetAttribute(grad_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g->smem);
+    // the opt-in is the device's whole limit (engines of different sizes share the kernels)
+    if (configure_kernel((const void*)grad_forward_kernel, (int)kernel_smem_cap((const void*)grad_forward_kernel),
+                         false) != cudaSuccess ||
+        configure_kernel((const void*)grad_backward_kernel, (int)kernel_smem_cap((const void*)grad_backward_kernel),
+                         false) != cudaSuccess) {
+        cudaGetLastError();
+        delete g;
+        return nullptr;
+    }
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grad_backward_kernel, kThreads, g->smem);
     g->grid = std::min(F, std::max(1, per_sm) * sms);
@@ -1538,6 +1563,10 @@ int svpf_grad_forward(svpf_grad_t* g, const float* theta, const float* gamma, co
                       unsigned long long seed, float* loglik, double* loglik_sum) {
     if (!g || !theta || !y || T < 1 || T > g->T_max) return SVPF_ERR_INVALID_ARG;
     const size_t F = (size_t)g->F;
+    for (size_t f = 0; f < F; ++f) {
+        if (!theta_ok(theta[4 * f], theta[4 * f + 1], theta[4 * f + 2], theta[4 * f + 3])) return SVPF_ERR_INVALID_ARG;
+        if (gamma && !(std::fabs(gamma[f]) < INFINITY)) return SVPF_ERR_INVALID_ARG;
+    }
     if (cudaMemcpyAsync(g->d_theta, theta, 4 * F * sizeof(float), cudaMemcpyHostToDevice, g->stream) != cudaSuccess)
         return SVPF_ERR_CUDA;
     if (gamma && cudaMemcpyAsync(g->d_gamma, gamma, F * sizeof(float), cudaMemcpyHostToDevice, g->stream) != cudaSuccess)
@@ -1578,6 +1607,13 @@ int svpf_grad_backward(svpf_grad_t* g, const float* w, double* grad) {
     if (rc == SVPF_OK && cudaStreamSynchronize(g->stream) != cudaSuccess) rc = SVPF_ERR_CUDA;
     cudaFree(d_grad);
     return rc;
+}
+
+int svpf_grad_get_status(svpf_grad_t* g, int* status) {
+    if (!g || !status) return SVPF_ERR_INVALID_ARG;
+    if (cudaStreamSynchronize(g->stream) != cudaSuccess) return SVPF_ERR_CUDA;
+    return cudaMemcpy(status, g->d_status, (size_t)g->F * sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess
+               ? SVPF_OK : SVPF_ERR_CUDA;
 }
 
 int svpf_grad_checkpoint_every(const svpf_grad_t* g) { return g ? g->k : 0; }

@@ -1,11 +1,13 @@
 // svpf_internal.h -- launch interface between the C ABI (svpf_capi.cu) and
-// the kernels (svpf_kernels.cu).  Host-only declarations.
+// the kernels (svpf_kernels.cu).  Host declarations, plus small helpers
+// (SVPF_HD) that device code uses too.
 #pragma once
 
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "svpf.h"
+#include "svpf_math.h"
 
 namespace svpf {
 
@@ -110,8 +112,29 @@ size_t tick_smem_bytes(int n, int C, bool heun);
 // The single-filter kernel's: the tick's layout plus the pre-drawn SVLD normals.
 size_t tick_smem_bytes_single(int n, int C, bool heun);
 size_t tick_smem_bytes_2f(int n, int C);
-// Largest dynamic shared memory a CTA may use on this device.
+// Largest dynamic shared memory a CTA may use on the current device.
 size_t max_dyn_smem();
+// Current device index in [0, kMaxDevices), or -1.
+constexpr int kMaxDevices = 64;
+int current_device();
+// Set a kernel's dynamic shared-memory opt-in (and, if asked, non-portable
+// cluster sizes) on the current device, once per (device, kernel); thread safe.
+cudaError_t configure_kernel(const void* func, int dyn_smem_bytes, bool nonportable_cluster);
+// Dynamic shared memory a kernel may opt into on the current device (the
+// device's per-block opt-in limit less the kernel's static shared memory).
+size_t kernel_smem_cap(const void* func);
+// Loop counts a tick runs are bounded (the Stein budget of one tick over all
+// stages at most SVPF_MAX_STEIN_STEPS, annealing stages at most
+// SVPF_MAX_ANNEAL_STEPS), so no configuration keeps a kernel running for long.
+SVPF_HD inline bool config_loops_ok(const svpf_config_t& c) {
+    if (c.use_two_factor) {
+        const int na = c.use_annealing ? c.n_anneal_steps : 1;
+        return c.n_stein_steps >= 1 && na >= 1 && na <= SVPF_MAX_ANNEAL_STEPS &&
+               (long long)na * c.n_stein_steps <= SVPF_MAX_STEIN_STEPS;
+    }
+    return c.stein_min_steps >= 0 && c.stein_min_steps <= SVPF_MAX_STEIN_STEPS && c.stein_max_steps >= 0 &&
+           c.stein_max_steps <= SVPF_MAX_STEIN_STEPS;
+}
 
 // Default tile of the single-filter kernel for n particles on C CTAs, and of
 // the batch kernel for n particles.

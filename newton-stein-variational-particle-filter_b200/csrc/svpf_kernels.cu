@@ -7,7 +7,9 @@
 //                            persistent grid pulling filters largest-first
 #include <cstdio>
 #include <mutex>
+#include <set>
 #include <unordered_map>
+#include <utility>
 
 #include "svpf_internal.h"
 #include "svpf_tick.cuh"
@@ -71,17 +73,55 @@ size_t tick_smem_bytes_single(int n, int C, bool heun) {
 }
 size_t tick_smem_bytes_2f(int n, int C) { return (size_t)smem_floats_2f(n, C) * sizeof(float); }
 
+// ---- per-device facts and kernel attributes --------------------------------
+// Function attributes and device limits belong to a device, so every cache
+// below is keyed by the current device; one process may drive several GPUs,
+// from several host threads.
+static std::mutex g_dev_mu;
+static size_t g_max_dyn_smem[kMaxDevices] = {};
+static std::set<std::pair<int, const void*>> g_configured;
+
+int current_device() {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -1;
+    return dev;
+}
+
 size_t max_dyn_smem() {
-    static size_t cached = 0;
-    if (cached == 0) {
-        int dev = 0, v = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const int dev = current_device();
+    if (dev < 0) return 0;
+    std::lock_guard<std::mutex> lk(g_dev_mu);
+    if (g_max_dyn_smem[dev] == 0) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
         const size_t static_bytes = sizeof(Plan) + sizeof(svpf_ctl_t) + sizeof(svpf_config_t) +
                                     sizeof(SVPFParams) + sizeof(svpf_out_t) + 64;
-        cached = (size_t)v > static_bytes ? (size_t)v - static_bytes : 0;
+        g_max_dyn_smem[dev] = (size_t)v > static_bytes ? (size_t)v - static_bytes : 0;
     }
-    return cached;
+    return g_max_dyn_smem[dev];
+}
+
+size_t kernel_smem_cap(const void* func) {
+    const int dev = current_device();
+    int v = 0;
+    cudaFuncAttributes fa{};
+    if (dev < 0 || cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, func) != cudaSuccess)
+        return 0;
+    return (size_t)v > fa.sharedSizeBytes ? (size_t)v - fa.sharedSizeBytes : 0;
+}
+
+cudaError_t configure_kernel(const void* func, int dyn_smem_bytes, bool nonportable_cluster) {
+    const int dev = current_device();
+    if (dev < 0) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_dev_mu);
+    if (g_configured.count({dev, func})) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_smem_bytes);
+    if (e == cudaSuccess && nonportable_cluster)
+        e = cudaFuncSetAttribute(func, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+    g_configured.insert({dev, func});
+    return cudaSuccess;
 }
 
 int default_cluster(int n) {

@@ -28,6 +28,7 @@ constexpr int kOrderOff = 64;
 constexpr int kTileOff = kOrderOff + kMax;
 constexpr int kScratchWords = kTileOff + kMax / 4;
 constexpr int kBuckets = 14;   // particle counts grouped by bit length (n <= 8192)
+static_assert(kBatchTileLo >= 1, "tile 0 marks a filter the setup left out");
 
 static __device__ __align__(256) int g_noalloc_scratch[kScratchWords];
 
@@ -49,32 +50,60 @@ __device__ int bucket_of(int n) {
     return b;
 }
 
-// One CTA: zero the counter, choose tiles, order filters largest first
+// One CTA, before the tick: check every filter against what the launch was
+// sized for, choose tiles, and order the valid filters largest first
 // (bucketed by particle count; the order inside a bucket is free because the
-// filters are independent).  Every call rewrites all the scratch it uses.
-__global__ void noalloc_setup_kernel(int F, const int* __restrict__ n) {
+// filters are independent).  A filter with n outside [1, n_max], an offset
+// that is negative or not a multiple of 16 floats, Heun while any_heun is 0,
+// or loop counts beyond the engine's limits gets SVPF_ERR_INVALID_ARG in its
+// control record (two-factor filters SVPF_ERR_UNSUPPORTED) and is never
+// touched by the tick: rejected filters take the first positions of the work
+// order and the work counter starts past them.  Every call rewrites all the
+// scratch it uses.
+__global__ void noalloc_setup_kernel(int F, const int* __restrict__ n, const long long* __restrict__ off,
+                                     const svpf_config_t* __restrict__ cfg, svpf_ctl_t* ctl, int n_max,
+                                     int any_heun) {
     __shared__ int hist[kBuckets];
     __shared__ int start[kBuckets];
+    __shared__ int n_bad, bad_pos;
     int* scratch = g_noalloc_scratch;
     uint8_t* tiles = reinterpret_cast<uint8_t*>(scratch + kTileOff);
     if (threadIdx.x < kBuckets) hist[threadIdx.x] = 0;
-    if (threadIdx.x == 0) scratch[0] = 0;
+    if (threadIdx.x == 0) {
+        n_bad = 0;
+        bad_pos = 0;
+    }
     __syncthreads();
     for (int f = threadIdx.x; f < F; f += blockDim.x) {
-        tiles[f] = (uint8_t)tile_for(n[f]);
-        atomicAdd(&hist[bucket_of(n[f])], 1);
+        const int nf = n[f];
+        const long long of = off[f];
+        const svpf_config_t& c = cfg[f];
+        int st = SVPF_OK;
+        if (c.use_two_factor) st = SVPF_ERR_UNSUPPORTED;
+        else if (nf < 1 || nf > n_max || of < 0 || (of & 15) != 0 || (c.use_heun && !any_heun) ||
+                 !config_loops_ok(c))
+            st = SVPF_ERR_INVALID_ARG;
+        if (st != SVPF_OK) {
+            ctl[f].status = st;
+            tiles[f] = 0;   // no batch tile is 0: marks the filter as left out
+            atomicAdd(&n_bad, 1);
+        } else {
+            tiles[f] = (uint8_t)tile_for(nf);
+            atomicAdd(&hist[bucket_of(nf)], 1);
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        int acc = 0;
+        int acc = n_bad;
         for (int b = kBuckets - 1; b >= 0; --b) {   // largest bucket first
             start[b] = acc;
             acc += hist[b];
         }
+        scratch[0] = n_bad;   // the work counter starts past the rejected filters
     }
     __syncthreads();
     for (int f = threadIdx.x; f < F; f += blockDim.x) {
-        const int pos = atomicAdd(&start[bucket_of(n[f])], 1);
+        const int pos = tiles[f] == 0 ? atomicAdd(&bad_pos, 1) : atomicAdd(&start[bucket_of(n[f])], 1);
         scratch[kOrderOff + pos] = f;
     }
 }
@@ -127,7 +156,7 @@ int svpf_batch_tick_noalloc(int n_filters, const int* d_n, const long long* d_of
     if (!scratch) return err;
     const int grid = batch_grid(smem);
     if (grid < 1) return SVPF_ERR_CUDA;
-    noalloc_setup_kernel<<<1, kThreads, 0, stream>>>(n_filters, d_n);
+    noalloc_setup_kernel<<<1, kThreads, 0, stream>>>(n_filters, d_n, d_off, d_cfg, d_ctl, n_max, any_heun != 0);
     if (cudaGetLastError() != cudaSuccess) return SVPF_ERR_CUDA;
     BatchArgs a;
     std::memset(&a, 0, sizeof(a));

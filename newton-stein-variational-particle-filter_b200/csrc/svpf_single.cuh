@@ -101,15 +101,8 @@ template <int R, int S, bool TWO_FACTOR = false, bool SCAN = false, bool PROD = 
 static cudaError_t launch_single_t(const SingleArgs& a, int C, cudaStream_t s) {
     const size_t smem = TWO_FACTOR ? tick_smem_bytes_2f(a.n, C) : tick_smem_bytes_single(a.n, C, a.cfg.use_heun != 0);
     auto kern = TWO_FACTOR ? single_tick_2f_kernel<R, S> : single_tick_kernel<R, S, SCAN, PROD>;
-    static bool configured[kMaxCluster + 1] = {};
-    cudaError_t e;
-    if (!configured[0]) {
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn_smem());
-        if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        if (e != cudaSuccess) return e;
-        configured[0] = true;
-    }
+    const cudaError_t e = configure_kernel((const void*)kern, (int)max_dyn_smem(), true);
+    if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(C, 1, 1);
     cfg.blockDim = dim3(kThreads, 1, 1);

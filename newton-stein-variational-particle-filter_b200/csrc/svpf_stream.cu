@@ -275,6 +275,7 @@ int svpf_stream_admit(svpf_stream_t* s, int n, const svpf_config_t* cfg, const S
     if (!cfg->use_two_factor && s->grid1 < 1) return -SVPF_ERR_UNSUPPORTED;
     if (cfg->use_two_factor && s->grid2 < 1 && !(n >= kClusterMinN && s->grid2c > 0)) return -SVPF_ERR_UNSUPPORTED;
     if (cfg->use_two_factor && cfg->n_stein_steps < 1) return -SVPF_ERR_INVALID_ARG;
+    if (!config_loops_ok(*cfg)) return -SVPF_ERR_INVALID_ARG;
     int slot = -1;
     for (int i = 0; i < s->cap; ++i)
         if (!s->active[i]) { slot = i; break; }

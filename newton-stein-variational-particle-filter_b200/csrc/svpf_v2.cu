@@ -25,6 +25,7 @@
 // passes where the reference passes curand states.
 #include <cooperative_groups.h>
 #include <cstring>
+#include <mutex>
 
 #include "svpf.h"
 #include "svpf_device.cuh"
@@ -551,16 +552,19 @@ size_t v2_smem_bytes(int n, int C, int pre) {
 // Dynamic shared memory a v2 member may take: the device's opt-in limit per
 // block less the kernel's own static shared memory.
 size_t v2_smem_cap() {
-    static size_t cached = 0;
-    if (cached == 0) {
-        int dev = 0, v = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    static std::mutex mu;
+    static size_t cached[kMaxDevices] = {};
+    const int dev = current_device();
+    if (dev < 0) return 0;
+    std::lock_guard<std::mutex> lk(mu);
+    if (cached[dev] == 0) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
         cudaFuncAttributes fa{};
         if (cudaFuncGetAttributes(&fa, v2::v2_kernel) != cudaSuccess) return 0;
-        cached = (size_t)v > fa.sharedSizeBytes ? (size_t)v - fa.sharedSizeBytes : 0;
+        cached[dev] = (size_t)v > fa.sharedSizeBytes ? (size_t)v - fa.sharedSizeBytes : 0;
     }
-    return cached;
+    return cached[dev];
 }
 
 int v2_cluster(int n) {
@@ -601,6 +605,8 @@ cudaError_t svpf_fully_fused_step_v2(
     float step_size, float temperature, float rmsprop_rho, float rmsprop_eps, int n_stein_steps,
     int n_anneal_steps, int stein_sign_mode, int n, int timestep, cudaStream_t stream) {
     if (!svpf_fully_fused_v2_supported(n)) return cudaErrorInvalidConfiguration;
+    if (n_stein_steps > SVPF_MAX_STEIN_STEPS || n_anneal_steps > SVPF_MAX_ANNEAL_STEPS)
+        return cudaErrorInvalidValue;   // bounded loop counts: no call keeps the kernel running for long
     if (!h || !h_prev || !grad_log_p || !log_weights || !d_grad_v || !d_inv_hessian || !rng || !d_h_mean ||
         !d_vol || !d_loglik || !d_bandwidth || !d_ksd || !d_guide_mean || !d_guide_var || !d_mu_state)
         return cudaErrorInvalidValue;
@@ -630,14 +636,9 @@ cudaError_t svpf_fully_fused_step_v2(
     a.timestep = timestep;
     const int C = v2_cluster(n);
     a.npre_cap = v2_pre_steps(n, C);
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(v2::v2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)v2_smem_cap());
+    {
+        const cudaError_t e = configure_kernel((const void*)v2::v2_kernel, (int)v2_smem_cap(), true);
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(v2::v2_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        if (e != cudaSuccess) return e;
-        configured = true;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(C, 1, 1);

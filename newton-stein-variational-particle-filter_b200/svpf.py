@@ -157,6 +157,10 @@ def lib() -> C.CDLL:
         "svpf_batch_get_particles": (_I, [vp, _I, _FP]),
         "svpf_batch_set_noise_tape": (_I, [vp, _FP, _I, _FP, _I]),
         "svpf_batch_tile_of": (_I, [vp, _I, C.POINTER(_I), C.POINTER(_I)]),
+        "svpf_batch_tile_of_filter": (_I, [vp, _I, C.POINTER(_I), C.POINTER(_I)]),
+        "svpf_batch_set_tile": (_I, [vp, _I, _I, _I]),
+        "svpf_batch_get_state": (_I, [vp, _I, C.POINTER(Ctl), _FP, _FP, _FP, _FP]),
+        "svpf_batch_set_state": (_I, [vp, _I, C.POINTER(Ctl), _FP, _FP, _FP, _FP]),
         "svpf_autotune": (_I, [C.POINTER(_I), _I, _I]),
         "svpf_tile_choice": (_I, [_I, C.POINTER(_I), C.POINTER(_I)]),
         "svpf_build_info": (C.c_char_p, []),
@@ -171,6 +175,7 @@ def lib() -> C.CDLL:
         "svpf_grad_segment_records": (_I, [vp]),
         "svpf_grad_set_segment_records": (_I, [vp, _I]),
         "svpf_grad_set_objective": (_I, [vp, _I]),
+        "svpf_grad_get_status": (_I, [vp, C.POINTER(_I)]),
         "svpf_stream_create": (vp, [_I, C.c_size_t, _I, vp]),
         "svpf_stream_destroy": (None, [vp]),
         "svpf_stream_set_seed": (None, [vp, C.c_ulonglong]),
@@ -207,6 +212,7 @@ def lib() -> C.CDLL:
         "svpf_estimator_backward": (_I, [vp, _FP, C.POINTER(C.c_double)]),
         "svpf_estimator_forward_device": (_I, [vp, vp, vp, _I, C.c_ulonglong, vp, vp, vp]),
         "svpf_estimator_backward_device": (_I, [vp, vp, vp]),
+        "svpf_estimator_get_status": (_I, [vp, C.POINTER(_I)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -577,6 +583,21 @@ class Batch:
         self._check(lib().svpf_batch_get_particles(self._b, int(f), _fp(out)))
         return out
 
+    def get_state(self, f: int):
+        """(ctl, h, h_prev, v, log_w) of filter f (h/h_prev/v [2n] for two factors)."""
+        n = int(self._ns[f])
+        m = (2 if self._cfgs[f].use_two_factor else 1) * n
+        ctl = Ctl()
+        h, hp, v = (np.empty(m, np.float32) for _ in range(3))
+        lw = np.empty(n, np.float32)
+        self._check(lib().svpf_batch_get_state(self._b, int(f), C.byref(ctl), _fp(h), _fp(hp), _fp(v), _fp(lw)))
+        return ctl, h, hp, v, lw
+
+    def set_state(self, f: int, ctl=None, h=None, hp=None, v=None, lw=None):
+        arrs = [None if a is None else _f32(a) for a in (h, hp, v, lw)]
+        self._check(lib().svpf_batch_set_state(self._b, int(f), None if ctl is None else C.byref(ctl),
+                                               *[None if a is None else _fp(a) for a in arrs]))
+
     def set_noise_tape(self, normals=None, uniforms=None):
         if normals is None:
             self._check(lib().svpf_batch_set_noise_tape(self._b, None, 0, None, 0))
@@ -589,6 +610,16 @@ class Batch:
         r, s = C.c_int(), C.c_int()
         lib().svpf_batch_tile_of(self._b, int(n), C.byref(r), C.byref(s))
         return r.value, s.value
+
+    def tile_of_filter(self, f: int):
+        """(rows per thread, column split) filter f runs with."""
+        r, s = C.c_int(), C.c_int()
+        self._check(lib().svpf_batch_tile_of_filter(self._b, int(f), C.byref(r), C.byref(s)))
+        return r.value, s.value
+
+    def set_tile(self, f: int, rows_per_thread: int, col_split: int):
+        """Force filter f's tile shape (a compiled batch tile)."""
+        self._check(lib().svpf_batch_set_tile(self._b, int(f), int(rows_per_thread), int(col_split)))
 
 
 def grad_config(n_stein: int = 8, nu: float = 12.0, full_newton: bool = True, **kw) -> Config:
@@ -696,6 +727,13 @@ class Grad:
 
     def backward_device(self, d_w, d_grad: int):
         self._check(lib().svpf_grad_backward_device(self._g, d_w, d_grad))
+
+    def status(self) -> np.ndarray:
+        """Per-filter status of the last forward/backward (SVPF_ERR_INVALID_ARG
+        for a theta outside the domain)."""
+        st = np.zeros(self.F, np.int32)
+        self._check(lib().svpf_grad_get_status(self._g, st.ctypes.data_as(C.POINTER(_I))))
+        return st
 
 
 class Stream:
@@ -1010,6 +1048,12 @@ class Estimator:
 
     def backward_device(self, d_w, d_grad: int):
         self._check(lib().svpf_estimator_backward_device(self._e, d_w, d_grad))
+
+    def status(self) -> np.ndarray:
+        """Per-path status of the last forward/backward."""
+        st = np.zeros(self.F, np.int32)
+        self._check(lib().svpf_estimator_get_status(self._e, st.ctypes.data_as(C.POINTER(_I))))
+        return st
 
 
 def autotune(ns, ticks: int = 2):

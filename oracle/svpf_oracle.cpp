@@ -824,11 +824,13 @@ inline bool operator>(const Dual& a, const Dual& b) { return a.v > b.v; }
 inline double val(const Dual& a) { return a.v; }
 inline double val(double a) { return a; }
 
-/* psi(x), x > 0: recurrence psi(x) = psi(x+1) - 1/x up to x >= 8, then the
- * asymptotic series (Abramowitz & Stegun 6.3.18). */
+/* psi(x), x > 0: recurrence psi(x) = psi(x+1) - 1/x up to x >= 8 (at most
+ * eight shifts), then the asymptotic series (Abramowitz & Stegun 6.3.18);
+ * NaN for x <= 0 or NaN. */
 double digamma(double x) {
+    if (!(x > 0)) return std::nan("");
     double acc = 0;
-    while (x < 8) { acc -= 1 / x; x += 1; }
+    for (int k = 0; k < 8 && x < 8; ++k) { acc -= 1 / x; x += 1; }
     double r = 1 / x, r2 = r * r;
     return acc + std::log(x) - 0.5 * r -
            r2 * (1.0 / 12 - r2 * (1.0 / 120 - r2 * (1.0 / 252 - r2 * (1.0 / 240 - r2 * (1.0 / 132)))));
@@ -1250,6 +1252,8 @@ int svpf_oracle_batch_tick_f32(int nf, const oracle_config* cfgs, const oracle_p
 
 /* ---- gradient oracle entry points ---------------------------------------- */
 extern "C" {
+
+double svpf_oracle_digamma(double x) { return digamma(x); }
 
 /* 1 if the configuration is inside the differentiable set: single factor,
  * plain or MIM predict with the model's rho, preserving or blending EKF guide

@@ -1,0 +1,167 @@
+"""Parity of the batched engine's headline path with the FP64 oracle.
+
+The benchmark ticks the persistent batch kernel through
+svpf_batch_graph_launch (one captured launch per tick, replayed), with the
+tile shape per particle count the autotuner picks.  Here that same call is
+checked against the oracle (the per-filter tick of the reference,
+src/svpf_optimized_graph.cu:915-1389):
+
+* every compiled batch tile (rows per thread, column split) at particle
+  counts 64 ... 4096, forced per filter in one batch;
+* the first 16 filters of the benchmark's own workload (own theta, own nu,
+  N drawn from {256, ..., 4096}) with the autotuner's tiles, over 12 ticks,
+  which crosses t = 10 where the KSD-driven Stein budget and rejuvenation
+  switch on.
+
+Before every tick the oracle takes the engine's state (control record,
+particles, previous particles, RMSProp moments); both sides draw the same
+noise tape (captured once in the graph and replayed).  Tolerance 1e-4
+relative (floor 1), as the other parity tests; KSD 1e-3.
+"""
+import concurrent.futures as cf
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import tape
+from test_oracle import TOL, rel_err
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+TILES = [(1, 4), (1, 2), (1, 1), (2, 1), (4, 1)]
+SIZES = [64, 100, 256, 300, 1024, 2048, 4096]
+
+
+def _twin(oracle_mod, batch, f, cfg, params):
+    ctl, h, hp, v, lw = batch.get_state(f)
+    o = oracle_mod.OracleFilter(h.shape[0], oracle_mod.config_from_dict(cfg.to_dict()),
+                                oracle_mod.OracleParams(*params))
+    o.ctl = oracle_mod.ctl_from_dict({k: getattr(ctl, k) for k, _ in ctl._fields_ if not k.startswith("smooth_")})
+    o.h, o.h_prev, o.v, o.log_w = (a.astype(np.float64) for a in (h, hp, v, lw))
+    return o
+
+
+def _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks, tiles=None, tape_seed=31):
+    """Tick a batch through svpf_batch_graph_launch and the oracle side by side."""
+    import torch
+
+    F = len(ns)
+    n_max = max(ns)
+    b = pkg.Batch(ns, cfgs, [pkg.Params(*p) for p in params])
+    b.set_noise_tape(tape.init_normals(tape_seed, n_max)[None, :], np.ones((1, n_max), np.float32))
+    b.initialize(seed=1)
+    if tiles is not None:
+        for f, (R, S) in enumerate(tiles):
+            b.set_tile(f, R, S)
+    used = [b.tile_of_filter(f) for f in range(F)]
+    slots = 2 + max(c.stein_max_steps for c in cfgs) + 7
+    nrm, uni = tape.tape(tape_seed + 1, 0, n_max, slots, 2)
+    b.set_noise_tape(nrm, uni)   # one tape for every tick: the graph is captured once, then replayed
+    d_yt = torch.empty(F, dtype=torch.float32, device="cuda")
+    d_yp = torch.zeros(F, dtype=torch.float32, device="cuda")
+    d_out = torch.zeros((F, 8), dtype=torch.float32, device="cuda")
+    launches0 = b.kernel_launches
+    pool = cf.ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1))
+    for t in range(ticks):
+        twins = [_twin(oracle_mod, b, f, cfgs[f], params[f]) for f in range(F)]
+        yp = ys[t - 1] if t > 0 else np.zeros(F, np.float32)
+        d_yt.copy_(torch.from_numpy(np.ascontiguousarray(ys[t])))
+        d_yp.copy_(torch.from_numpy(np.ascontiguousarray(yp)))
+        torch.cuda.synchronize()
+        b.graph_launch(d_yt.data_ptr(), d_yp.data_ptr(), d_out.data_ptr())
+        b.sync()
+        out = d_out.cpu().numpy()
+        steps = out.view(np.int32)[:, 6]
+        rejuv = out.view(np.int32)[:, 7]
+        # the oracle's ticks run in threads: each is a ctypes call, which releases the GIL
+        oo = list(pool.map(lambda f: twins[f].step(ys[t, f], yp[f], nrm[:, :ns[f]], uni[:, :ns[f]]), range(F)))
+        ctl = b.ctl()
+        for f in range(F):
+            tag = (t, f, ns[f], used[f])
+            assert ctl[f].status == 0, tag
+            assert steps[f] == oo[f].steps_used, tag
+            assert rejuv[f] == oo[f].rejuv_fired, tag
+            h = b.get_particles(f)
+            assert rel_err(h, twins[f].h) < TOL, (tag, rel_err(h, twins[f].h))
+            for col, name in ((0, "loglik"), (1, "vol"), (2, "h_mean")):
+                want = getattr(oo[f], name)
+                assert abs(out[f, col] - want) < TOL * max(1.0, abs(want)), (tag, name, out[f, col], want)
+            assert abs(out[f, 5] - oo[f].ksd) < 1e-3 * max(1.0, abs(oo[f].ksd)), (tag, out[f, 5], oo[f].ksd)
+    pool.shutdown()
+    # one captured launch per tick, replayed: no more kernels than ticks
+    assert b.kernel_launches - launches0 == ticks
+    b.close()
+    return used
+
+
+def test_every_batch_tile_matches_oracle(pkg, oracle_mod):
+    """Each compiled tile at each size, forced per filter, 3 graph-replayed ticks."""
+    ns, tiles, params, cfgs = [], [], [], []
+    for i, n in enumerate(SIZES):
+        for j, tl in enumerate(TILES):
+            ns.append(n)
+            tiles.append(tl)
+            params.append((0.93 + 0.01 * j, 0.12 + 0.04 * (i % 4), -1.5 + 0.2 * j, -0.1 * (i % 2)))
+            cfgs.append(pkg.production_config(5.0 + 4.0 * j, 8))
+    F = len(ns)
+    _, y = tape.sv_path(4, -1.0, 0.97, 0.2, seed=3)
+    ys = np.tile(y[:, None], (1, F)).astype(np.float32) * np.linspace(0.6, 1.4, F, dtype=np.float32)[None, :]
+    used = _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks=3, tiles=tiles)
+    assert used == tiles
+
+
+def test_benchmark_workload_slice_matches_oracle(pkg, oracle_mod):
+    """The first 16 filters of the benchmark's workload (own theta and nu, N up
+    to 4096) with the autotuner's tiles, 12 graph-replayed ticks."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    ns_all, rho, sz, mu, nu = bench.make_workload(4096, seed=0)
+    Fs = 16
+    ns = [int(n) for n in ns_all[:Fs]]
+    assert max(ns) == 4096
+    chosen = pkg.autotune(sorted(set(ns)), ticks=1)
+    ys = bench.sv_paths(12, rho, sz, mu, nu, seed=0)[:, :Fs]
+    params = [(float(rho[f]), float(sz[f]), float(mu[f]), 0.0) for f in range(Fs)]
+    cfgs = [pkg.production_config(float(nu[f]), bench.MAX_STEPS) for f in range(Fs)]
+    used = _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks=12)
+    for f, n in enumerate(ns):
+        assert used[f] == tuple(chosen[n]), (n, used[f], chosen[n])
+
+
+def test_tile_hook_rejects_unknown_shapes(pkg):
+    b = pkg.Batch([256, 512], pkg.production_config(30.0, 8), pkg.Params(0.97, 0.15, -1.0, 0.0))
+    for R, S in ((8, 1), (1, 8), (3, 1), (0, 0)):
+        with pytest.raises(RuntimeError):
+            b.set_tile(0, R, S)
+    with pytest.raises(RuntimeError):
+        b.set_tile(2, 1, 4)   # no such filter
+    b.set_tile(1, 1, 2)
+    assert b.tile_of_filter(1) == (1, 2)
+    b.close()
+
+
+def test_loop_counts_are_bounded(pkg):
+    """Configurations whose Stein budget would keep a kernel running for long
+    are refused before any launch (SVPF_MAX_STEIN_STEPS = 256 per tick)."""
+    ok = pkg.production_config(30.0, 8)
+    bad = pkg.production_config(30.0, 8)
+    bad.stein_max_steps = 1 << 30
+    with pytest.raises(RuntimeError):
+        pkg.Batch([256, 256], [ok, bad], pkg.Params(0.97, 0.15, -1.0, 0.0))
+    neg = pkg.production_config(30.0, 8)
+    neg.stein_min_steps = -(1 << 30)
+    with pytest.raises(RuntimeError):
+        pkg.Batch([256], [neg], pkg.Params(0.97, 0.15, -1.0, 0.0))
+    f = pkg.SVPF(256, 8, 30.0)
+    f.initialize(0.97, 0.15, -1.0, 0.0, seed=1)
+    f.configure(stein_max_steps=100000)
+    rc, _ = f.step_raw(0.1, 0.0)
+    assert rc == 1   # SVPF_ERR_INVALID_ARG, nothing launched
+    f.configure(stein_max_steps=8)
+    rc, _ = f.step_raw(0.1, 0.0)
+    assert rc == 0
+    f.close()
