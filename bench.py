@@ -31,6 +31,7 @@ sys.path.insert(0, ROOT)
 
 N_CHOICES = (256, 512, 1024, 2048, 4096)
 MAX_STEPS = 8
+PLAIN_PER_CLASS = 13   # plain-step loop sample: filters per particle count (65 filters)
 METRIC = "filter-ticks/s batched vs plain step on 1 B200 at matched RMSE; p50/p99 µs/tick"
 
 
@@ -123,46 +124,84 @@ def read_ncu_traffic():
     return None
 
 
-def oracle_cpu_rate(F_sample: int, ns, rho, sz, mu, nu, ys, n_threads: int, reps: int = 1):
-    """Filter-ticks/s of the oracle's FP32 mirror (OpenMP over filters) on a
-    bounded sample of the same workload: one tick of the first F_sample
-    filters, repeated ``reps`` times."""
+def stratified(ns, per_class: int) -> np.ndarray:
+    """Indices of the first `per_class` filters of each particle count.  The
+    workload draws counts uniformly from N_CHOICES, so equal counts per class
+    give a sample with the workload's distribution of tick costs."""
+    idx = []
+    for n in N_CHOICES:
+        idx.extend(np.where(np.asarray(ns) == n)[0][:per_class].tolist())
+    return np.array(idx, np.int64)
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def config1_path(T: int = 5000, seed: int = 0):
+    """The plain single-filter workload: h_t = mu + rho (h_{t-1} - mu) + sigma_z eps
+    with mu = -1, rho = 0.97, sigma_z = 0.15, h_0 stationary, y_t = e^{h_t/2} eta
+    with Gaussian eta, T = 5000, seed 0 (the project's counter-based generator
+    in tests/golden/tape.py, exact on every machine).  Returns (h, y)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import tape
+    return tape.sv_path(T, -1.0, 0.97, 0.15, seed=seed)
+
+
+def oracle_cpu_run(idx, ns, rho, sz, mu, nu, ys, n_threads: int, t_timed0: int, t_end: int):
+    """The oracle's FP32 mirror (OpenMP over filters, all host threads) on the
+    filters `idx` of the workload for ticks 0 .. t_end-1, timing ticks
+    t_timed0 .. t_end-1.  Returns (filter-ticks/s, pair-iterations/s, seconds
+    timed); a pair-iteration is one (i, j) pair of one Stein iteration."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle  # test infrastructure, used here only as the CPU baseline
 
     L = oracle.lib()
-    Fs = int(F_sample)
+    idx = np.asarray(idx, np.int64)
+    Fs = int(idx.shape[0])
     cfgs = (oracle.OracleConfig * Fs)()
     prms = (oracle.OracleParams * Fs)()
     ctls = (oracle.OracleCtl * Fs)()
     outs = (oracle.OracleOut * Fs)()
-    n_max = int(ns[:Fs].max())
+    nsel = np.ascontiguousarray(np.asarray(ns)[idx], np.int32)
+    n_max = int(nsel.max())
     h = np.zeros((Fs, n_max), np.float32)
     hp, v, lw = np.zeros_like(h), np.zeros_like(h), np.zeros_like(h)
-    for f in range(Fs):
+    for k, f in enumerate(idx):
         c = oracle.default_config(MAX_STEPS, float(nu[f]))
         c.use_newton, c.use_full_newton, c.stein_min_steps, c.stein_max_steps, c.n_anneal_steps = 1, 1, 4, MAX_STEPS, 3
-        cfgs[f] = c
-        prms[f] = oracle.OracleParams(float(rho[f]), float(sz[f]), float(mu[f]), 0.0)
-        ctls[f] = oracle.default_ctl()
-        hh, hpp, vv = (np.zeros(int(ns[f])) for _ in range(3))
-        L.svpf_oracle_initialize(C.byref(cfgs[f]), C.byref(prms[f]), C.byref(ctls[f]), int(ns[f]),
+        cfgs[k] = c
+        prms[k] = oracle.OracleParams(float(rho[f]), float(sz[f]), float(mu[f]), 0.0)
+        ctls[k] = oracle.default_ctl()
+        hh, hpp, vv = (np.zeros(int(nsel[k])) for _ in range(3))
+        L.svpf_oracle_initialize(C.byref(cfgs[k]), C.byref(prms[k]), C.byref(ctls[k]), int(nsel[k]),
                                  hh.ctypes.data_as(C.POINTER(C.c_double)), hpp.ctypes.data_as(C.POINTER(C.c_double)),
-                                 vv.ctypes.data_as(C.POINTER(C.c_double)), None, 1, f)
-        h[f, :ns[f]] = hh
-        hp[f, :ns[f]] = hpp
-    nsa = np.ascontiguousarray(ns[:Fs], np.int32)
+                                 vv.ctypes.data_as(C.POINTER(C.c_double)), None, 1, int(f))
+        h[k, :nsel[k]] = hh
+        hp[k, :nsel[k]] = hpp
+    n2 = nsel.astype(np.float64) ** 2
     fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))  # noqa: E731
-    t0 = time.perf_counter()
-    for r in range(reps):
-        yt = np.ascontiguousarray(ys[r % ys.shape[0], :Fs])
-        yp = np.ascontiguousarray(ys[(r - 1) % ys.shape[0], :Fs]) if r else np.zeros(Fs, np.float32)
-        rc = L.svpf_oracle_batch_tick_f32(Fs, cfgs, prms, ctls, nsa.ctypes.data_as(C.POINTER(C.c_int)), n_max,
-                                          fp(h), fp(hp), fp(v), fp(lw), fp(yt), fp(yp), 1, r, n_threads, outs)
+    dt, pairs = 0.0, 0.0
+    for t in range(t_end):
+        yt = np.ascontiguousarray(ys[t, idx], np.float32)
+        yp = np.ascontiguousarray(ys[t - 1, idx], np.float32) if t else np.zeros(Fs, np.float32)
+        t0 = time.perf_counter()
+        rc = L.svpf_oracle_batch_tick_f32(Fs, cfgs, prms, ctls, nsel.ctypes.data_as(C.POINTER(C.c_int)), n_max,
+                                          fp(h), fp(hp), fp(v), fp(lw), fp(yt), fp(yp), 1, t, n_threads, outs)
+        el = time.perf_counter() - t0
         if rc != 0:
             raise RuntimeError(f"oracle batch tick rc={rc}")
-    dt = time.perf_counter() - t0
-    return Fs * reps / dt, dt
+        if t >= t_timed0:
+            dt += el
+            pairs += float(sum(outs[k].steps_used * n2[k] for k in range(Fs)))
+    return Fs * (t_end - t_timed0) / dt, pairs / dt, dt
 
 
 def cpu_threads() -> int:
@@ -172,30 +211,129 @@ def cpu_threads() -> int:
         return os.cpu_count() or 1
 
 
+def cpu_sample(threads: int) -> int:
+    """Filters per particle count in a CPU sample: enough to keep every host
+    thread busy (OpenMP over filters)."""
+    return max(1, -(-threads // len(N_CHOICES)))
+
+
+def reference_cuda_step(args, ns, rho, sz, mu, nu, ys):
+    """The reference's own CUDA step (its sources compiled unmodified for
+    sm_100a into oracle/_ref/libsvpf_ref_stock.so, cuRAND noise) on this GPU:
+    (1) svpf_step_graph looped over the plain-step sample of the workload on
+    the same ticks as the batched steps, one blocking call per filter-tick,
+    host wall clock per call, the way test/profile_svpf.cu:687-790 loops
+    instruments; (2) the plain single-filter workload (N = 512, T = 5000,
+    seed 0): CUDA events around each call (test/profile_svpf.cu:98-164) for
+    p50/p99, and the filtered log-vol RMSE."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+        reflib = oracle.RefLib("stock")
+    except Exception as exc:  # noqa: BLE001
+        return {"unavailable": f"reference build not loadable: {exc}"}
+    L = reflib.L
+    L.svpf_step_graph.restype = None
+    L.svpf_step_graph.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.svpf_ref_steps_used.restype = C.c_int
+    L.svpf_ref_steps_used.argtypes = [C.c_void_p]
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import tape
+
+    def make(n, nu_f, params):
+        r = oracle.RefFilter(reflib, int(n), MAX_STEPS, float(nu_f))
+        c = r.read_config()
+        c.use_newton, c.use_full_newton, c.stein_min_steps, c.stein_max_steps, c.n_anneal_steps = 1, 1, 4, MAX_STEPS, 3
+        r.apply_config(c)
+        r.initialize(params, tape.init_normals(1, int(n)))
+        return r
+
+    # (1) plain step looped over the sample, timed ticks warmup .. warmup+steps-1
+    idx = stratified(ns, PLAIN_PER_CLASS)
+    filt = [(make(ns[f], nu[f], oracle.OracleParams(float(rho[f]), float(sz[f]), float(mu[f]), 0.0)), f) for f in idx]
+    ll, vol, hm = C.c_float(), C.c_float(), C.c_float()
+    t_end = args.warmup + args.steps
+    dt, pairs = 0.0, 0.0
+    for t in range(t_end):
+        for r, f in filt:
+            yp = float(ys[t - 1, f]) if t else 0.0
+            p = C.byref(oracle.OracleParams(float(rho[f]), float(sz[f]), float(mu[f]), 0.0))
+            t0 = time.perf_counter()
+            L.svpf_step_graph(r.s, float(ys[t, f]), yp, p, C.byref(ll), C.byref(vol), C.byref(hm))
+            el = time.perf_counter() - t0
+            if t >= args.warmup:
+                dt += el
+                pairs += float(L.svpf_ref_steps_used(r.s)) * float(ns[f]) ** 2
+    for r, _ in filt:
+        r.close()
+    loop = {"value": len(idx) * args.steps / dt, "unit": "filter-ticks/s", "pair_iterations_per_s": pairs / dt,
+            "sample": f"{len(idx)} filters of the workload ({PLAIN_PER_CLASS} per particle count), ticks "
+                      f"{args.warmup}..{t_end - 1} (the batched steps' ticks), one blocking svpf_step_graph "
+                      "call per filter-tick, host wall clock per call"}
+    # (2) the plain single-filter workload
+    h_true, y1 = config1_path()
+    p1 = oracle.OracleParams(0.97, 0.15, -1.0, 0.0)
+    r = make(512, 30.0, p1)
+    us = np.zeros(y1.shape[0], np.float32)
+    L.svpf_ref_time_steps(r.s, y1.ctypes.data_as(C.POINTER(C.c_float)), y1.shape[0], C.byref(p1),
+                          us.ctypes.data_as(C.POINTER(C.c_float)))
+    r.close()
+    r = make(512, 30.0, p1)
+    hms = np.zeros(y1.shape[0])
+    yp = 0.0
+    for t in range(y1.shape[0]):
+        L.svpf_step_graph(r.s, float(y1[t]), yp, C.byref(p1), C.byref(ll), C.byref(vol), C.byref(hm))
+        hms[t] = hm.value
+        yp = float(y1[t])
+    r.close()
+    lat = np.sort(us[20:])
+    return {
+        "build": "the reference's src/svpf_opt_kernels.cu, svpf_optimized_graph.cu, svpf_two_factor.cu, "
+                 "svpf_fully_fused_v2.cu compiled unmodified (its flags, sm_100a), cuRAND noise",
+        "plain_step_loop": loop,
+        "single_filter": {"n": 512, "ticks": int(y1.shape[0]), "p50_us": float(lat[len(lat) // 2]),
+                          "p99_us": float(lat[int(len(lat) * 0.99)]),
+                          "timing": "CUDA events around each svpf_step_graph call (test/profile_svpf.cu:98-164)",
+                          "rmse_logvol": float(np.sqrt(np.mean((hms[100:] - h_true[100:]) ** 2))),
+                          "rmse": "filtered h_mean vs the true log-vol, ticks 100..4999"},
+    }
+
+
 def run_reference(args, rank: int, world: int):
-    """Reference arm: the reference has no CPU implementation of the step, so
-    the CPU restatement (oracle FP32 mirror, OpenMP over filters, all host
-    threads) is timed on a bounded sample of the same workload."""
+    """Reference arm.  The reference has no CPU implementation of the step, so
+    `value` is the CPU restatement (the oracle's FP32 mirror, OpenMP over
+    filters, all host threads) on a stratified sample of the same workload and
+    the same ticks as the batched steps.  The reference's own CUDA step on this
+    GPU is reported beside it (`reference_cuda_step`): its plain step looped
+    over the same filters and ticks as this engine's `plain_step_loop`, and its
+    single-filter latency and RMSE on the plain single-filter workload."""
     if rank != 0:
         return
     F = args.filters
     ns, rho, sz, mu, nu = make_workload(F, seed=0)
-    ys = sv_paths(args.warmup + args.steps + 1, rho, sz, mu, nu, seed=0)
+    t_end = args.warmup + args.steps
+    ys = sv_paths(t_end + 1, rho, sz, mu, nu, seed=0)
     threads = cpu_threads()
-    sample = max(2 * threads, 32)
-    # warm-up: one small rep
-    oracle_cpu_rate(min(sample, 16), ns, rho, sz, mu, nu, ys, threads, reps=1)
-    rate, dt = oracle_cpu_rate(sample, ns, rho, sz, mu, nu, ys, threads, reps=max(1, args.steps))
+    k = cpu_sample(threads)
+    idx = stratified(ns, k)
+    rate, prate, dt = oracle_cpu_run(idx, ns, rho, sz, mu, nu, ys, threads, args.warmup, t_end)
+    ref_cuda = reference_cuda_step(args, ns, rho, sz, mu, nu, ys) if not args.no_reference_cuda else {}
     line = {
         "metric": METRIC, "value": rate, "unit": "filter-ticks/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * dt / max(1, args.steps), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
         "impl": "reference",
         "config": workload_config(F),
-        "cpu_baseline": {"value": rate, "unit": "filter-ticks/s", "cores": threads, "kind": "port",
-                         "sample": f"{sample} filters of the workload x {max(1, args.steps)} ticks per run "
-                                   f"(the reference has no CPU step; oracle FP32 mirror, OpenMP)"},
+        "cpu_baseline": {"value": rate, "unit": "filter-ticks/s", "pair_iterations_per_s": prate, "cores": threads,
+                         "cpu_model": cpu_model(), "kind": "port",
+                         "sample": f"{len(idx)} filters of the workload ({k} per particle count) x ticks "
+                                   f"{args.warmup}..{t_end - 1}; the reference has no CPU step: the oracle's FP32 "
+                                   "mirror, OpenMP over filters"},
         "e2e": {"value": rate, "unit": "filter-ticks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_cuda_step": ref_cuda,
     }
     print(json.dumps(line), flush=True)
 
@@ -484,6 +622,74 @@ def profile_case(pkg, name: str):
     torch.cuda.synchronize()
 
 
+def config1_engine(pkg):
+    """This engine on the plain single-filter workload (N = 512, production
+    configuration, nu = 30, T = 5000, seed 0): host wall clock of each blocking
+    svpf_step_graph call (launch and wait included) and the filtered log-vol
+    RMSE against the true path (ticks 100..4999)."""
+    h_true, y1 = config1_path()
+    f1 = pkg.SVPF(512, MAX_STEPS, 30.0)
+    f1.configure(**pkg.production_config(30.0, MAX_STEPS).to_dict())
+    f1.initialize(0.97, 0.15, -1.0, 0.0, seed=0)
+    lib = pkg.lib()
+    p = C.byref(f1.params)
+    hm = C.c_float()
+    us = np.zeros(y1.shape[0])
+    hms = np.zeros(y1.shape[0])
+    yprev = 0.0
+    for t in range(y1.shape[0]):
+        t0 = time.perf_counter()
+        lib.svpf_step_graph(f1._s, float(y1[t]), yprev, p, None, None, C.byref(hm))
+        us[t] = (time.perf_counter() - t0) * 1e6
+        hms[t] = hm.value
+        yprev = float(y1[t])
+    f1.close()
+    lat = np.sort(us[20:])
+    return {"n": 512, "ticks": int(y1.shape[0]), "p50_us": float(lat[len(lat) // 2]),
+            "p99_us": float(lat[int(len(lat) * 0.99)]), "mean_us": float(lat.mean()),
+            "timing": "host wall clock per blocking svpf_step_graph call (ctypes, launch and wait included)",
+            "rmse_logvol": float(np.sqrt(np.mean((hms[100:] - h_true[100:]) ** 2))),
+            "rmse": "filtered h_mean vs the true log-vol, ticks 100..4999",
+            "workload": "h_t = -1 + 0.97 (h_{t-1} + 1) + 0.15 eps, Gaussian returns, T = 5000, seed 0, N = 512, "
+                        "production config, nu = 30"}
+
+
+def plain_step_loop(pkg, args, ns, rho, sz, mu, nu, ys):
+    """This engine's single-filter step looped over the plain-step sample of
+    the workload (PLAIN_PER_CLASS filters of each particle count), one
+    blocking svpf_step_graph call per filter-tick, on the batched steps' ticks
+    (warmup .. warmup+steps-1; earlier ticks run untimed).  Rates in
+    filter-ticks/s and pair-iterations/s (steps used x N^2)."""
+    lib = pkg.lib()
+    idx = stratified(ns, PLAIN_PER_CLASS)
+    filt = []
+    for f in idx:
+        s = pkg.SVPF(int(ns[f]), MAX_STEPS, float(nu[f]))
+        s.configure(**pkg.production_config(float(nu[f]), MAX_STEPS).to_dict())
+        s.initialize(float(rho[f]), float(sz[f]), float(mu[f]), 0.0, seed=int(f))
+        filt.append((s, f))
+    t_end = args.warmup + args.steps
+    dt, pairs = 0.0, 0.0
+    for t in range(t_end):
+        for s, f in filt:
+            yp = float(ys[t - 1, f]) if t else 0.0
+            p = C.byref(s.params)
+            t0 = time.perf_counter()
+            lib.svpf_step_graph(s._s, float(ys[t, f]), yp, p, None, None, None)
+            el = time.perf_counter() - t0
+            if t >= args.warmup:
+                dt += el
+                pairs += float(s.last_output().steps_used) * float(ns[f]) ** 2
+    for s, _ in filt:
+        s.close()
+    return {"value": len(idx) * args.steps / dt, "unit": "filter-ticks/s", "pair_iterations_per_s": pairs / dt,
+            "sample": f"{len(idx)} filters of the workload ({PLAIN_PER_CLASS} per particle count), ticks "
+                      f"{args.warmup}..{t_end - 1} (the batched steps' ticks), one blocking svpf_step_graph call "
+                      "per filter-tick, host wall clock per call",
+            "step": "this engine's single-filter step; the reference's step on the same filters and ticks is "
+                    "the --impl reference line's reference_cuda_step.plain_step_loop"}
+
+
 def workload_config(F: int):
     return {"workload": f"batched SVPF tick: {F} filters per GPU, own theta, N ~ U{{256,512,1024,2048,4096}}, "
                         f"production config (full Newton, <= {MAX_STEPS} Stein iterations, 3 stages)",
@@ -499,7 +705,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--filters", type=int, default=4096)
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--latency-ticks", type=int, default=400)
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="reference arm: skip the reference's CUDA step (its CPU restatement only)")
     ap.add_argument("--no-gradient", action="store_true", help="skip the differentiation workload")
     ap.add_argument("--no-stream", action="store_true", help="skip the two-factor request loop")
     ap.add_argument("--profile-case", choices=["grad", "stream", "v2"],
@@ -533,10 +740,17 @@ def main():
     shard = importlib.import_module("svpf_b200.shard")
     dev = torch.device("cuda", local)
 
-    F = args.filters
-    ns, rho, sz, mu, nu = make_workload(F, seed=rank)
+    # The global workload holds `filters` filters per GPU; filters are
+    # independent, so each rank takes a share balanced by tick cost (no
+    # per-tick exchange) and the end-of-run gather puts results in global order.
+    F_all = args.filters * world
+    ns_g, rho_g, sz_g, mu_g, nu_g = make_workload(F_all, seed=0)
     T = args.warmup + args.steps + 2
-    ys = sv_paths(T, rho, sz, mu, nu, seed=rank)
+    ys_g = sv_paths(T, rho_g, sz_g, mu_g, nu_g, seed=0)
+    mine = shard.partition(ns_g, MAX_STEPS, world)[rank] if world > 1 else np.arange(F_all)
+    ns, rho, sz, mu, nu = ns_g[mine], rho_g[mine], sz_g[mine], mu_g[mine], nu_g[mine]
+    ys = np.ascontiguousarray(ys_g[:, mine])
+    F = int(mine.shape[0])
     tiles = {}
     if not args.no_autotune:
         tiles = pkg.autotune(sorted(set(ns.tolist())), ticks=2)
@@ -568,6 +782,7 @@ def main():
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    n2 = torch.from_numpy(ns.astype(np.float64)).to("cuda") ** 2
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             flush.zero_()
@@ -578,7 +793,6 @@ def main():
             e1.record(stream)
             e1.synchronize()
             steps = d_out.view(torch.int32)[:, 6].to(torch.float64)   # svpf_out_t.steps_used
-            n2 = torch.from_numpy(ns.astype(np.float64)).to("cuda") ** 2
             pairs.append(float((steps * n2).sum()))
         torch.cuda.synchronize()
     if world > 1:
@@ -586,7 +800,7 @@ def main():
     launches = batch.kernel_launches - launches0
     step_ms = [ev[k][0].elapsed_time(ev[k][1]) for k in range(args.steps)]
     total_ms = shard.max_over_ranks(float(sum(step_ms)), dev)
-    value = world * F * args.steps / (total_ms / 1e3)
+    value = F_all * args.steps / (total_ms / 1e3)
 
     # ---- end to end through the C ABI with host buffers: a second batch with the
     #      same seed replays exactly the timed ticks (same states, same budgets)
@@ -603,59 +817,21 @@ def main():
         batch_e2e.step(ys[t], ys[t - 1])
         e2e_s += time.perf_counter() - t0
     e2e_s = shard.max_over_ranks(e2e_s, dev)
-    e2e_value = world * F * args.steps / e2e_s
+    e2e_value = F_all * args.steps / e2e_s
     batch_e2e.close()
 
     # ---- end-of-run exchange: per-filter FP64 log-likelihood sums of every rank
     ctl = batch.ctl()
-    ll_all = shard.gather_by_filter(np.arange(F) + rank * F, [c.loglik_sum for c in ctl], world * F, dev)
+    ll_all = shard.gather_by_filter(mine, [c.loglik_sum for c in ctl], F_all, dev)
     status_bad = sum(1 for c in ctl if c.status != 0)
 
-    # ---- single-filter latency (configuration 1: N=512) and the plain-step loop
+    # ---- the plain single-filter workload (N = 512, T = 5000, seed 0) and the
+    #      plain step looped over a sample of the batched workload
     lat = {}
     plain = {}
     if rank == 0:
-        f1 = pkg.SVPF(512, MAX_STEPS, 30.0)
-        f1.configure(**pkg.production_config(30.0, MAX_STEPS).to_dict())
-        f1.initialize(0.97, 0.15, -1.0, 0.0, seed=0)
-        yl = sv_paths(args.latency_ticks + 20, np.array([0.97]), np.array([0.15]), np.array([-1.0]),
-                      np.array([1e6]), seed=5)[:, 0]
-        us = []
-        yprev = 0.0
-        lib = pkg.lib()
-        p = C.byref(f1.params)
-        for t in range(args.latency_ticks + 20):
-            t0 = time.perf_counter()
-            lib.svpf_step_graph(f1._s, float(yl[t]), yprev, p, None, None, None)
-            dt = time.perf_counter() - t0
-            yprev = float(yl[t])
-            if t >= 20:
-                us.append(dt * 1e6)
-        us.sort()
-        lat = {"n": 512, "p50_us": us[len(us) // 2], "p99_us": us[int(len(us) * 0.99)],
-               "mean_us": float(np.mean(us)), "ticks": len(us), "timing": "host wall clock per blocking call"}
-        f1.close()
-        # plain step looped over a sample of the batch's filters (one tick each)
-        sample = 64
-        filt = []
-        for f in range(sample):
-            s = pkg.SVPF(int(ns[f]), MAX_STEPS, float(nu[f]))
-            s.configure(**cfgs[f].to_dict())
-            s.initialize(float(rho[f]), float(sz[f]), float(mu[f]), 0.0, seed=f)
-            filt.append(s)
-        for s in filt:   # warm (t = 0 tick)
-            lib.svpf_step_graph(s._s, float(ys[0, 0]), 0.0, C.byref(s.params), None, None, None)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for f, s in enumerate(filt):
-            lib.svpf_step_graph(s._s, float(ys[1, f]), float(ys[0, f]), C.byref(s.params), None, None, None)
-        dtp = time.perf_counter() - t0
-        plain = {"value": sample / dtp, "unit": "filter-ticks/s", "sample": f"{sample} filters of the workload, "
-                 "one blocking svpf_step_graph call each",
-                 "step": "this engine's own single-filter step; the reference's step looped over the same "
-                         "workload is timed on the same GPU by tests/test_gpu_reference.py"}
-        for s in filt:
-            s.close()
+        lat = config1_engine(pkg)
+        plain = plain_step_loop(pkg, args, ns_g, rho_g, sz_g, mu_g, nu_g, ys_g)
 
     # ---- roofline: pair-interactions per launch / mean launch time
     props = torch.cuda.get_device_properties(local)
@@ -693,17 +869,29 @@ def main():
     cpu = {}
     if rank == 0:
         threads = cpu_threads()
-        sample = max(2 * threads, 32)
-        rate, dt = oracle_cpu_rate(sample, ns, rho, sz, mu, nu, ys, threads, reps=1)
-        cpu = {"value": rate, "unit": "filter-ticks/s", "cores": threads, "kind": "port",
-               "sample": f"one tick of {sample} filters of the workload ({dt:.1f} s); oracle FP32 mirror, OpenMP"}
+        k = cpu_sample(threads)
+        idx = stratified(ns_g, k)
+        rate, prate, dt = oracle_cpu_run(idx, ns_g, rho_g, sz_g, mu_g, nu_g, ys_g, threads, 0, 2)
+        cpu = {"value": rate, "unit": "filter-ticks/s", "pair_iterations_per_s": prate, "cores": threads,
+               "cpu_model": cpu_model(), "kind": "port",
+               "sample": f"ticks 0-1 of {len(idx)} filters of the workload ({k} per particle count; {dt:.1f} s); "
+                         "the oracle's FP32 mirror, OpenMP over filters (the reference has no CPU step). Ticks "
+                         "t < 10 run the full Stein budget: compare pair_iterations_per_s"}
+
+    ratios = {}
+    if rank == 0 and plain:
+        ratios = {"filter_ticks": value / world / plain["value"],
+                  "pair_iterations": achieved * 1e9 / plain["pair_iterations_per_s"],
+                  "note": "this engine's batched tick over its own plain step looped on the same ticks (per GPU); "
+                          "against the reference's plain step divide by the --impl reference line's "
+                          "reference_cuda_step.plain_step_loop (same filters and ticks)"}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "filter-ticks/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-            "config": dict(workload_config(F), tiles={str(k): list(v) for k, v in tiles.items()}),
+            "config": dict(workload_config(args.filters), tiles={str(k): list(v) for k, v in tiles.items()}),
             "e2e": {"value": e2e_value, "unit": "filter-ticks/s", "h2d_bytes_per_step": 2 * F * 4,
                     "d2h_bytes_per_step": F * 32,
                     "timing": "host wall clock around each svpf_batch_step call (host y in, host outputs back), "
@@ -717,8 +905,10 @@ def main():
                                  f"{sms} SMs x {sm_mhz:.0f} MHz (sampled) x min(MUFU/2, FP32/13) pair/clk/SM from "
                                  "the MUFU and FP32 results per SM clock measured on this GPU "
                                  "(nominal 16 and 128: 8 pair/clk/SM)"},
+            "pair_iterations_per_s": achieved * 1e9,
             "single_filter_latency": lat,
             "plain_step_loop": plain,
+            "batched_over_plain": ratios,
             "gradient": grad_line,
             "estimator_model": est_line,
             "two_factor_request_loop": stream_line,

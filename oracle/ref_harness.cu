@@ -422,4 +422,8 @@ int svpf_ref_time_steps(SVPFState* s, const float* ys, int T, const oracle_param
     return check(cudaGetLastError(), "time");
 }
 
+/* Stein iterations the last svpf_step_graph call ran (the reference keeps it
+ * in the state, svpf_optimized_graph.cu:1490-1493). */
+int svpf_ref_steps_used(const SVPFState* s) { return s->stein_steps_used; }
+
 }  // extern "C"

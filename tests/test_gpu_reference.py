@@ -102,6 +102,29 @@ def test_rmse_matches_reference_cuda_step(pkg, n):
     assert abs(res["rmse_ours"] - res["rmse_ref"]) <= 0.02 * res["rmse_ref"], res
 
 
+def test_plain_workload_exactly_matches_reference_rmse(pkg):
+    """The plain single-filter workload exactly as specified: mu = -1, rho =
+    0.97, sigma_z = 0.15, h_0 stationary, Gaussian returns, T = 5000, seed 0,
+    N = 512, production configuration, nu = 30.  Engine and reference
+    (unmodified build, cuRAND) each filter the same path with their own
+    noise; filtered log-vol RMSE (ticks 100..4999) within 2%."""
+    oracle, reflib = _ref_stock()
+    h_true, ys = tape.sv_path(5000, -1.0, 0.97, 0.15, seed=0)
+    cfg = pkg.production_config(30.0, 8).to_dict()
+    params = (0.97, 0.15, -1.0, 0.0)
+    hm_ref, lat_ref = run_reference(oracle, reflib, cfg, params, ys, 512, 8, 30.0)
+    hm_ours, lat_ours = run_engine(pkg, cfg, params, ys, 512, 8, 30.0, seed=0)
+    r_ref = float(np.sqrt(np.mean((hm_ref[100:] - h_true[100:]) ** 2)))
+    r_ours = float(np.sqrt(np.mean((hm_ours[100:] - h_true[100:]) ** 2)))
+    res = {"n": 512, "T": 5000, "seed": 0, "rmse_ref": r_ref, "rmse_ours": r_ours,
+           "ref_p50_us": float(np.percentile(lat_ref[20:], 50)), "ref_p99_us": float(np.percentile(lat_ref[20:], 99)),
+           "ours_p50_us": float(np.percentile(lat_ours[20:], 50)),
+           "ours_p99_us": float(np.percentile(lat_ours[20:], 99))}
+    with open(os.path.join(results_dir(), "plain_workload_n512_T5000.json"), "w") as fh:
+        json.dump(res, fh, indent=1)
+    assert abs(r_ours - r_ref) <= 0.02 * r_ref, res
+
+
 def test_reference_plain_step_loop_on_batched_workload(pkg):
     """The reference's svpf_step_graph looped over a sample of the batched
     workload (own theta and N per filter, production configuration), the way

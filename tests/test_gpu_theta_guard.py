@@ -55,7 +55,7 @@ def test_grad_engine_leaves_out_bad_theta(pkg):
         g.forward_device(d_th.data_ptr(), None, d_y.data_ptr(), T, 3, d_ll.data_ptr())
         st_fwd = g.status()
         g.backward_device(None, d_g.data_ptr())
-        st = g.status()
+        st = g.status()   # waits for the engine's own stream before the copies below
         return d_ll.cpu().numpy(), d_g.cpu().numpy(), st_fwd, st
 
     ll_ref, g_ref, st0, st1 = run(good)
@@ -95,7 +95,8 @@ def test_estimator_leaves_out_bad_theta(pkg):
         torch.cuda.synchronize()
         e.forward_device(d_th.data_ptr(), d_y.data_ptr(), T, 2, None, d_ll.data_ptr(), d_v.data_ptr())
         e.backward_device(None, d_g.data_ptr())
-        return d_ll.cpu().numpy(), d_g.cpu().numpy(), e.status()
+        st = e.status()   # waits for the engine's own stream before the copies below
+        return d_ll.cpu().numpy(), d_g.cpu().numpy(), st
 
     ll_ref, g_ref, st0 = run(good)
     assert not st0.any()
