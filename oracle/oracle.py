@@ -128,12 +128,21 @@ def _fptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
+def reference_dir() -> str:
+    """Where the reference's source tree is read from when the checker builds
+    it: $SVPF_REFERENCE_DIR, else the build container's copy."""
+    return os.environ.get("SVPF_REFERENCE_DIR") or "/root/reference"
+
+
 def build(quiet: bool = True) -> None:
-    """Compile the oracle (and, where the reference tree exists, the reference build)."""
+    """Compile the oracle and, where the reference tree exists, the reference
+    build and the reference callers linked to this engine (test checkers)."""
     out = subprocess.DEVNULL if quiet else None
     subprocess.run(["make", "-C", HERE, "all"], check=True, stdout=out)
-    if os.path.isdir("/root/reference/src"):
-        subprocess.run(["make", "-C", HERE, "ref"], check=True, stdout=out)
+    ref = reference_dir()
+    if os.path.isdir(os.path.join(ref, "src")):
+        env = dict(os.environ, SVPF_REFERENCE_DIR=ref)
+        subprocess.run(["make", "-C", HERE, "ref", "callers"], check=True, stdout=out, env=env)
 
 
 _lib = None

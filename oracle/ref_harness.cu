@@ -7,13 +7,15 @@
  * a pre-drawn noise tape and with its full state loaded and read back between
  * ticks (per-tick parity with state re-sync).
  */
-#include "svpf.cuh"
-#include "svpf_fully_fused_v2.cuh"
-#include "svpf_oracle.h"
-
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
+
+#include "svpf.cuh"
+#include "svpf_fully_fused_v2.cuh"
+#include "svpf_multiscale.cuh"
+#include "svpf_oracle.h"
 
 /* Built twice: with the tape header forced in (parity build), and stock
  * (SVPF_REF_STOCK, timing build: curand untouched, counters never reset). */
@@ -420,6 +422,41 @@ int svpf_ref_time_steps(SVPFState* s, const float* ys, int T, const oracle_param
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     return check(cudaGetLastError(), "time");
+}
+
+/* ---- the reference's two-scale composition (include/svpf_multiscale.cuh),
+ * driven unmodified: ms_svpf_create / ms_svpf_init / ms_svpf_step.  In the
+ * tape build both scales draw from one tape of stride n_max, particle i of
+ * either scale reading column i (the layout of one tape shared by a batch). */
+MS_SVPF* svpf_ref_ms_create(void) { return ms_svpf_create(NULL); }
+
+void svpf_ref_ms_destroy(MS_SVPF* ms) { ms_svpf_destroy(ms); }
+
+/* which: 0 = REACTIVE, 1 = INERTIAL (for svpf_ref_get_state / set_state). */
+SVPFState* svpf_ref_ms_filter(MS_SVPF* ms, int which) { return which ? ms->inertial : ms->reactive; }
+
+int svpf_ref_ms_init(MS_SVPF* ms, float initial_vol, const oracle_params* p, const float* init_normals, int n_max) {
+    float one = 1.0f;
+    if (svpf_ref_tape_set(init_normals, 1, &one, 0, n_max)) return -1;
+    SVPFParams sp = {p->rho, p->sigma_z, p->mu, p->gamma};
+    ms_svpf_init(ms, initial_vol, &sp, 0u);
+    cudaDeviceSynchronize();
+    return svpf_ref_tape_flags_take();
+}
+
+int svpf_ref_ms_step(MS_SVPF* ms, float y_t, const oracle_params* p, const float* normals, int n_normal_slots,
+                     const float* uniforms, int n_uniform_slots, int n_max, MS_SVPF_Output* out) {
+#ifndef SVPF_REF_STOCK
+    SVPFState* fs[2] = {ms->reactive, ms->inertial};
+    for (SVPFState* s : fs)
+        reset_counters_kernel<<<(s->n_particles + 255) / 256, 256, 0, s->stream>>>(s->rng_states, s->n_particles);
+    cudaDeviceSynchronize();
+#endif
+    if (svpf_ref_tape_set(normals, n_normal_slots, uniforms, n_uniform_slots, n_max)) return -1;
+    SVPFParams sp = {p->rho, p->sigma_z, p->mu, p->gamma};
+    ms_svpf_step(ms, y_t, &sp, out);
+    cudaDeviceSynchronize();
+    return svpf_ref_tape_flags_take();
 }
 
 /* Stein iterations the last svpf_step_graph call ran (the reference keeps it

@@ -123,7 +123,9 @@ def run_case(mod, torch, case):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle"))
+    import oracle
+    ref = sys.argv[1] if len(sys.argv) > 1 else oracle.reference_dir()
     out = sys.argv[2] if len(sys.argv) > 2 else HERE
     mod = load_reference(ref)
     import torch

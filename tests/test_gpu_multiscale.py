@@ -1,9 +1,19 @@
 """The reference's two-scale composition (include/svpf_multiscale.cuh) on the
 batch engine: per-scale knobs as ms_svpf_create sets them, one batch launch
-per tick for all 2F filters, and each instrument's output combined from its
-two filters' outputs the way ms_svpf_step combines them."""
+per tick for all 2F filters, each instrument's output combined from its two
+filters' outputs the way ms_svpf_step combines them, and -- pinned to the
+reference itself -- the outputs of the reference's own ms_svpf_step
+recorded tick by tick (tests/golden/ms_composition.npz, made by
+tests/golden/make_ms_golden.py from the unmodified header and sources)."""
+import ctypes as C
+import json
+import os
+
 import numpy as np
 import pytest
+
+import tape
+from test_oracle import TOL
 
 pytestmark = pytest.mark.gpu
 
@@ -49,4 +59,54 @@ def test_combination_follows_ms_svpf_step(pkg):
             assert o.is_calm == int(r.vol < 0.02 and n.vol < 0.02)
             assert o.cross_scale_boost == 0
             vol_prev[k] = o.vol_combined
+    m.close()
+
+
+FIXTURE = os.path.join(os.path.dirname(__file__), "golden", "ms_composition.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(FIXTURE), reason="fixture not recorded")
+def test_composition_matches_reference_ms_svpf_step(pkg):
+    """Both scales of every instrument start each tick from the reference's
+    recorded state (after the first tick, which starts from the engine's own
+    initialisation on the recorded initial-draw tape) and draw the recorded
+    tape; every output field of the composition must match the reference's
+    ms_svpf_step within 1e-4 relative (integers and flags exactly)."""
+    z = np.load(FIXTURE)
+    fields = json.loads(str(z["fields"]))
+    ctls = json.loads(str(z["ctl"]))
+    F = z["params"].shape[0]
+    n_max = int(z["n_max"])
+    ns_slots = int(z["normal_slots"])
+    seed = int(z["tape_seed"])
+    L = pkg.lib()
+    m = pkg.MultiScale([pkg.Params(*[float(x) for x in p]) for p in z["params"]])
+    inner = L.svpf_ms_batch_inner(m._m)
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))  # noqa: E731
+    init = np.ascontiguousarray(tape.init_normals(seed, n_max)[None, :])
+    ones = np.ones((1, n_max), np.float32)
+    assert L.svpf_batch_set_noise_tape(inner, fp(init), 1, fp(ones), 1) == 0
+    m.init(float(z["initial_vol"]), seed=0)
+    sizes = (m.config.n_particles_reactive, m.config.n_particles_inertial)
+    T = z["ys"].shape[1]
+    for t in range(T):
+        if t > 0:
+            for i in range(F):
+                for s, n in enumerate(sizes):
+                    c = pkg.Ctl()
+                    for k, v in ctls[i][t - 1][s].items():
+                        if hasattr(c, k) and not isinstance(v, list):
+                            setattr(c, k, type(getattr(c, k))(v))
+                    arrs = [np.ascontiguousarray(z[k][i, t - 1, s, :n]) for k in ("h", "hp", "v", "lw")]
+                    assert L.svpf_batch_set_state(inner, i + s * F, C.byref(c), *[fp(a) for a in arrs]) == 0
+        nrm, uni = tape.tape(seed, t, n_max, ns_slots, 2)
+        assert L.svpf_batch_set_noise_tape(inner, fp(nrm), ns_slots, fp(uni), 2) == 0
+        out = m.step(z["ys"][:, t])
+        for i in range(F):
+            for q, k in enumerate(fields):
+                got, want = getattr(out[i], k), z["outs"][i, t, q]
+                if isinstance(got, int):
+                    assert got == int(want), (t, i, k, got, want)
+                else:
+                    assert abs(got - want) <= TOL * max(1.0, abs(want)), (t, i, k, got, want)
     m.close()

@@ -7,7 +7,7 @@ import pytest
 
 import cases
 import tape
-from test_oracle import TOL, TWO_FACTOR_SCALARS, _fixtures, load_fixture, rel_err
+from test_oracle import TOL, TWO_FACTOR_SCALARS, _fixtures, ctl_mismatches, load_fixture, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -75,6 +75,34 @@ def test_engine_matches_reference_ticks(pkg, path, cluster):
         for k in SCALARS + (TWO_FACTOR_SCALARS if tf else ()):
             a, b = getattr(ctl, k), post[k]
             assert abs(a - b) <= TOL * max(1.0, abs(b)), (t, k, a, b)
+    f.close()
+
+
+@pytest.mark.parametrize("path", _fixtures(), ids=lambda p: p.split("/")[-1][:-4])
+def test_engine_initialize_matches_reference(pkg, path):
+    """svpf_initialize on the engine (svpf_optimized_graph.cu:349-451 and the
+    backend quirks at :483-494: stationary draw, reset control record,
+    previous mean -3.5): from the fixture's initial-draw tape the engine lands
+    on the reference's recorded post-initialise state (fixture tick 0) --
+    particles, previous particles, RMSProp moments, log-weights and every
+    recorded control field."""
+    fx = load_fixture(path)
+    n = fx["n"]
+    cfg = fx["config"]
+    tf = bool(cfg.get("use_two_factor", 0))
+    f = pkg.SVPF(n, cfg["n_stein_steps"], cfg["nu"])
+    f.configure(**cfg)
+    f.set_noise_tape(tape.init_normals(fx["tape_seed"], n, 3 if tf else 1).reshape(-1, n),
+                     np.ones((1, n), np.float32))
+    f.initialize(*[float(x) for x in fx["params"]], seed=1)
+    ctl, h, hp, v, lw = f.get_state()
+    if tf:
+        h, hp, v = f.get_state_2f()
+    assert rel_err(h, fx["h"][0]) < TOL, rel_err(h, fx["h"][0])
+    assert rel_err(hp, fx["hp"][0]) < TOL
+    assert np.array_equal(v, fx["v"][0]) and np.array_equal(lw, fx["lw"][0])
+    bad = ctl_mismatches(ctl, fx["ctl"][0])
+    assert not bad, bad
     f.close()
 
 

@@ -127,3 +127,35 @@ def test_oracle_replays_reference_ticks(oracle_mod, path):
 # Two-factor control fields compared after every replayed tick.
 TWO_FACTOR_SCALARS = ("h_fast_mean", "h_slow_mean", "guide_mean_fast", "guide_mean_slow", "guide_var_fast",
                       "guide_var_slow", "guide_2f_initialized", "timestep")
+
+
+def ctl_mismatches(ctl, want: dict, tol: float = TOL):
+    """Fields of a control record (oracle or engine) that differ from a
+    recorded one: every scalar and every smoother slot the record holds."""
+    bad = {}
+    for k, b in want.items():
+        if not hasattr(ctl, k):
+            continue
+        a = getattr(ctl, k)
+        if isinstance(b, list):
+            a = list(a)
+            if any(abs(x - y) > tol * max(1.0, abs(y)) for x, y in zip(a, b)):
+                bad[k] = (a, b)
+        elif abs(a - b) > tol * max(1.0, abs(b)):
+            bad[k] = (a, b)
+    return bad
+
+
+@pytest.mark.parametrize("path", _fixtures(), ids=lambda p: os.path.basename(p)[:-4])
+def test_oracle_initialize_matches_reference(oracle_mod, path):
+    """svpf_initialize (svpf_optimized_graph.cu:349-451, backend quirks
+    :483-494): from the fixture's initial-draw tape, the oracle lands on the
+    reference's recorded post-initialise state (tick 0 of the fixture)."""
+    fx = load_fixture(path)
+    n = fx["n"]
+    cfg = oracle_mod.config_from_dict(fx["config"])
+    f = oracle_mod.OracleFilter(n, cfg, oracle_mod.OracleParams(*[float(x) for x in fx["params"]]))
+    f.initialize(tape.init_normals(fx["tape_seed"], n, 3 if cfg.use_two_factor else 1))
+    assert rel_err(f.h, fx["h"][0]) < TOL and rel_err(f.h_prev, fx["hp"][0]) < TOL
+    assert np.array_equal(f.v, fx["v"][0]) and np.array_equal(f.log_w, fx["lw"][0])
+    assert not ctl_mismatches(f.ctl, fx["ctl"][0])
