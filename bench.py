@@ -565,19 +565,21 @@ def stream_workload(pkg, n_instruments: int = 10000, budget_bytes: int = 512 << 
 
 def profile_case(pkg, name: str):
     """Small fixed cases of the secondary kernels for profiler captures (no
-    timing, no output): `grad` -- value and adjoint of 64 filters, N = 512,
-    64 ticks; `stream` -- one request-loop round over 296 two-factor
+    timing, no output): `grad` -- value and adjoint of 296 filters (two per
+    SM, the benchmark's occupancy), N = 512, 16 ticks in one checkpoint
+    segment; `stream` -- one request-loop round over 296 two-factor
     instruments of N = 1024 / 2048 (the cluster kernel); `v2` -- 20
     svpf_fully_fused_step_v2 calls at N = 512."""
     import torch
     if name == "grad":
-        F, N, T = 64, 512, 64
+        F, N, T = 296, 512, 16
         rng = np.random.default_rng(0)
         th = np.stack([rng.uniform(-2, 0, F), rng.uniform(0.9, 0.99, F), rng.uniform(0.1, 0.3, F),
                        rng.uniform(5, 20, F)], 1).astype(np.float32)
         ys = sv_paths(T, th[:, 1].astype(np.float64), th[:, 2].astype(np.float64), th[:, 0].astype(np.float64),
                       th[:, 3].astype(np.float64), seed=1).T.copy()
-        g = pkg.Grad([N] * F, pkg.grad_config(MAX_STEPS, 12.0), T_max=T, checkpoint_every=64)
+        g = pkg.Grad([N] * F, pkg.grad_config(MAX_STEPS, 12.0), T_max=T, checkpoint_every=T)
+        g.set_objective(g.PREDICTIVE)
         g.forward(th, ys, seed=1)
         g.backward()
         g.close()
