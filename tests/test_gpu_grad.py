@@ -180,6 +180,41 @@ def test_adjoint_matches_fp64_central_differences(pkg, oracle_mod):
         assert abs(fd - grad[k]) <= 1e-3 * max(abs(grad[k]), 1e-2), (k, fd, grad[k])
 
 
+def test_production_adjoint_matches_fp64_fd_and_forward_mode(pkg):
+    """The benchmark's differentiation check settled in FP64: its first four
+    filters (production gradient configuration: full Newton, 8 Stein
+    iterations over 3 stages, SVLD, MIM, EKF guide, nu free; N = 512, 200
+    ticks, the predictive objective) with the FP64 oracle's forward-mode
+    gradient and its central differences at step 1e-4 max(1, |theta|)
+    recorded by tests/golden/make_grad_fd.py.
+
+    * CUDA adjoint vs the FP64 forward-mode gradient: 2e-4 relative (floor
+      1e-3) or four times the run's sensitivity to a 1e-7 change of theta.
+    * CUDA adjoint vs the FP64 central differences: 1e-3 wherever the FP64
+      differences agree with the FP64 forward-mode gradient to 1e-3
+      (kink-free: no clamp switches inside the step).  The recorded kinks:
+      filter 1's differences are biased by 2.8e-3 (mu), 3.4e-2 (rho) and
+      4.2e-2 (sigma_z) against the exact FP64 derivative, which the adjoint
+      matches instead."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "grad_fd_production.npz"))
+    th, ys, n, seed = z["theta"], z["ys"], int(z["n"]), int(z["seed"])
+    F, T = ys.shape
+    g = pkg.Grad([n] * F, pkg.grad_config(8, 12.0), T_max=T, checkpoint_every=64)
+    g.set_objective(g.PREDICTIVE)
+    _, ls = g.forward(th, ys, seed=seed)
+    grad = g.backward()
+    g.close()
+    assert np.allclose(ls, z["loglik_sum"], rtol=1e-5, atol=1e-3), (ls, z["loglik_sum"])
+    fm, fd = z["grad"], z["fd"]
+    rel_fm = np.abs(grad - fm) / np.maximum(np.abs(fm), 1e-3)
+    assert np.all(rel_fm < np.maximum(G_TOL, 4 * z["sens"][:, None])), rel_fm
+    kink_free = np.abs(fd - fm) / np.maximum(np.abs(fm), 1e-3) < 1e-3
+    assert kink_free.sum() >= 12 and not kink_free[1, 1:3].any()
+    rel_fd = np.abs(grad - fd) / np.maximum(np.abs(fd), 1e-3)
+    assert np.all(rel_fd[kink_free] < 1e-3), rel_fd
+
+
 def test_unsupported_configuration_is_rejected(pkg):
     cfg = pkg.grad_config(4, 12.0)
     assert pkg.Grad.supported(cfg)
