@@ -462,14 +462,6 @@ int svpf_tile_choice(int n, int* rows_per_thread, int* col_split);
 
 /* Library facts. */
 const char* svpf_build_info(void);
-int svpf_debug_philox(uint32_t k0, uint32_t k1, const uint32_t* ctr4, uint32_t* out4, int count);
-/* Measured issue rates of the pipes the pair sweeps run on, on the current
- * device, per SM clock: MUFU results (ex2.approx / rcp.approx) and FP32
- * results (packed FFMA2), medians over one CTA per SM.  The roofline of the
- * pair-iteration (one ex2 + one rcp + 13 FP32 operations) is
- * min(mufu / 2, fp32 / 13) pair-iterations per clock per SM.  No reference
- * counterpart (a diagnostic of this engine). */
-int svpf_measure_pipe_rates(double* mufu_per_clk_sm, double* fp32_per_clk_sm);
 
 
 /* ---- gradients of the log-likelihood (adjoint) ---------------------------
@@ -692,6 +684,22 @@ int svpf_estimator_backward_device(svpf_estimator_t* e, const float* d_w, double
  * launch; the device variants mark that path SVPF_ERR_INVALID_ARG, NaN its
  * outputs and gradient and leave the other paths unaffected.  status [F]. */
 int svpf_estimator_get_status(svpf_estimator_t* e, int* status);
+
+/* ---- test and measurement hooks ------------------------------------------
+ * Not part of the filtering surface and without reference counterparts; the
+ * parity tests and the benchmark use them. */
+
+/* The engine's counter-based Philox4x32-10 on the device: out4[4k..4k+3] for
+ * key (k0, k1) and counter ctr4[4k..4k+3], count counters (host arrays). */
+int svpf_debug_philox(uint32_t k0, uint32_t k1, const uint32_t* ctr4, uint32_t* out4, int count);
+
+/* Measured issue rates of the pipes the pair sweeps run on, on the current
+ * device, per SM clock: MUFU results (ex2.approx / rcp.approx) and FP32
+ * results (packed FFMA2), medians over one CTA per SM.  The roofline of the
+ * pair-iteration (one ex2 + one rcp + 13 FP32 operations) is
+ * min(mufu / 2, fp32 / 13) pair-iterations per clock per SM; the benchmark
+ * uses it as its roofline denominator. */
+int svpf_measure_pipe_rates(double* mufu_per_clk_sm, double* fp32_per_clk_sm);
 
 #ifdef __cplusplus
 }
