@@ -400,6 +400,11 @@ int svpf_batch_kernel_launches(const svpf_batch_t* b);  /* launches issued so fa
 int svpf_batch_get_ctl(const svpf_batch_t* b, svpf_ctl_t* ctl_host);          /* [n_filters] */
 /* h_out receives n values, or 2n (fast then slow) for a two-factor filter. */
 int svpf_batch_get_particles(const svpf_batch_t* b, int filter, float* h_out);
+/* Model parameters of filter f.  Setting them is stream ordered (ticks already
+ * enqueued keep the old ones) and waits for the batch's stream; the next
+ * svpf_batch_initialize draws the stationary law from them. */
+int svpf_batch_get_params(const svpf_batch_t* b, int filter, SVPFParams* params);
+int svpf_batch_set_params(svpf_batch_t* b, int filter, const SVPFParams* params);
 /* State of filter f (host arrays; any pointer may be NULL): control record,
  * h / h_prev / RMSProp v of n values (2n, fast then slow, for a two-factor
  * filter) and the n log-weights.  Both wait for the batch's stream.  Used for
@@ -632,8 +637,10 @@ typedef struct {
 typedef struct svpf_ms_batch svpf_ms_batch_t;
 
 svpf_ms_config_t svpf_ms_default_config(void);
-/* base_params[F]: each instrument's model (the INERTIAL scale uses it as is,
- * the REACTIVE scale with rho 0.92, sigma_z 0.18). */
+/* base_params[F]: each instrument's model (the INERTIAL scale ticks with it as
+ * is, the REACTIVE scale with rho 0.92, sigma_z 0.18).  As ms_svpf_init does,
+ * svpf_ms_batch_init draws the INERTIAL scale's initial state from its own
+ * dynamics (rho 0.98, sigma_z 0.10) and the base mu and gamma. */
 svpf_ms_batch_t* svpf_ms_batch_create(int n_instruments, const svpf_ms_config_t* cfg,
                                       const SVPFParams* base_params, cudaStream_t stream);
 void svpf_ms_batch_destroy(svpf_ms_batch_t* b);

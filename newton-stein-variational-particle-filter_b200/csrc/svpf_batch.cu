@@ -458,6 +458,21 @@ int svpf_batch_get_particles(const svpf_batch_t* b, int f, float* h_out) {
                ? SVPF_OK : SVPF_ERR_CUDA;
 }
 
+int svpf_batch_get_params(const svpf_batch_t* b, int f, SVPFParams* p) {
+    if (!b || !p || f < 0 || f >= b->F) return SVPF_ERR_INVALID_ARG;
+    *p = b->prms[f];
+    return SVPF_OK;
+}
+
+int svpf_batch_set_params(svpf_batch_t* b, int f, const SVPFParams* p) {
+    if (!b || !p || f < 0 || f >= b->F) return SVPF_ERR_INVALID_ARG;
+    b->prms[f] = *p;
+    // stream ordered: ticks already enqueued keep the old parameters
+    return cudaMemcpyAsync(b->d_prm + f, &b->prms[f], sizeof(SVPFParams), cudaMemcpyHostToDevice, b->stream) ==
+                   cudaSuccess && cudaStreamSynchronize(b->stream) == cudaSuccess
+               ? SVPF_OK : SVPF_ERR_CUDA;
+}
+
 int svpf_batch_get_state(const svpf_batch_t* b, int f, svpf_ctl_t* ctl, float* h, float* hp, float* v, float* lw) {
     if (!b || f < 0 || f >= b->F) return SVPF_ERR_INVALID_ARG;
     if (cudaStreamSynchronize(b->stream) != cudaSuccess) return SVPF_ERR_CUDA;

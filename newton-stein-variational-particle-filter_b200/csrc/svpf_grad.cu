@@ -51,9 +51,9 @@ namespace svpf {
 namespace grad {
 
 constexpr int kRecFixed = 4;       // XS, HPR, HGR, MUK
-constexpr int kRecPerIt = 14;      // X V GPRE AL LMAX Z DBAR VARD SKEW PHIR HR HW KN XR
+constexpr int kRecPerIt = 15;      // X V GPRE AL LMAX Z DBAR VARD SKEW PHIR HR HW KN XR NK
 enum { XS = 0, HPR = 1, HGR = 2, MUK = 3 };
-enum { IX = 0, IV, IGPRE, IAL, ILMAX, IZ, IDBAR, IVARD, ISKEW, IPHIR, IHR, IHW, IKN, IXR };
+enum { IX = 0, IV, IGPRE, IAL, ILMAX, IZ, IDBAR, IVARD, ISKEW, IPHIR, IHR, IHW, IKN, IXR, INK };
 
 struct GState {
     double m, P;                   // EKF guide mean / variance
@@ -283,15 +283,15 @@ __device__ __forceinline__ float flip_sign(float v, float s) {
 }
 
 // Transport adjoint row sums (the row and column terms of one Stein
-// iteration, see the header), with u^2 K = 1 - K, K^2 |3u^2-1| = K |3-4K| and
+// iteration, see the header), with K^2 |3u^2-1| = K |3-4K| and
 // uK^2 (6 sgn - 4 K |3u^2-1|) = sgn(3-4K) uK^2 (16K - 6).  Accumulators:
-//   0 S1 = sum g uK2     1 -S2 = sum K2 t       2 C1 = sum a uK2
-//   3 -C2 = sum a K2 t   4 C3 = sum a K         5 Q1 = sum g (K - K2)
-//   6 -Q2' = sum u K2 t  7 R3 = sum uK2         (t = 3 - 4K, Q2 = Q2' + R3)
-//   FULL: 8 R1 = sum c uK2, 9 R2 = sum f6, 10 D1 = sum hb uK2, 11 D2 = sum hb f6,
-//   12 D3 = sum kb uK2, 13 E1 = sum hb K, 14 W1 = sum c (K - K2), 15 W2 = sum u f6,
-//   16 W3 = sum K |t|, 17 W4 = sum (K - K2).
-constexpr int kAdjAcc = 18;
+//   0 S1 = sum g uK2     1 -S2 = sum K2 t      2 C1 = sum a uK2
+//   3 -C2 = sum a K2 t   4 C3 = sum a K        5 R3 = sum uK2       (t = 3 - 4K)
+//   FULL: 6 R1 = sum c uK2, 7 R2 = sum f6, 8 D1 = sum hb uK2, 9 D2 = sum hb f6,
+//   10 D3 = sum kb uK2, 11 E1 = sum hb K.
+// The bandwidth adjoint takes no pair sums of its own (bwd_tick derives it
+// from the position adjoint by homogeneity).
+constexpr int kAdjAcc = 12;
 template <bool FULL>
 __device__ __forceinline__ void adjoint_rows(const float* __restrict__ xs, const float* __restrict__ g,
                                              const float* __restrict__ a, const float* __restrict__ cv,
@@ -321,32 +321,23 @@ __device__ __forceinline__ void adjoint_rows(const float* __restrict__ xs, const
             const float2 uk2 = mul2(u, K2);
             const float2 t = fma2(K, f2(-4.0f), f2(3.0f));
             const float2 k2t = mul2(K2, t);
-            const float2 km = fma2(make_float2(-K.x, -K.y), K, K);
             const float2 gj = f2(gg[e]), aj = f2(aa[e]);
             acc[0] = fma2(gj, uk2, acc[0]);
             acc[1] = add2(acc[1], k2t);
             acc[2] = fma2(aj, uk2, acc[2]);
             acc[3] = fma2(aj, k2t, acc[3]);
             acc[4] = fma2(aj, K, acc[4]);
-            acc[5] = fma2(gj, km, acc[5]);
-            acc[6] = fma2(u, k2t, acc[6]);
-            acc[7] = add2(acc[7], uk2);
+            acc[5] = add2(acc[5], uk2);
             if (FULL) {
                 const float2 f6u = mul2(uk2, fma2(K, f2(16.0f), f2(-6.0f)));
                 const float2 f6 = make_float2(flip_sign(f6u.x, t.x), flip_sign(f6u.y, t.y));
-                const float2 kt = mul2(K, t);
                 const float2 cj = f2(cc[e]), hj = f2(hh[e]);
-                acc[8] = fma2(cj, uk2, acc[8]);
-                acc[9] = add2(acc[9], f6);
-                acc[10] = fma2(hj, uk2, acc[10]);
-                acc[11] = fma2(hj, f6, acc[11]);
-                acc[12] = fma2(f2(kk[e]), uk2, acc[12]);
-                acc[13] = fma2(hj, K, acc[13]);
-                acc[14] = fma2(cj, km, acc[14]);
-                acc[15] = fma2(u, f6, acc[15]);
-                acc[16].x += fabsf(kt.x);
-                acc[16].y += fabsf(kt.y);
-                acc[17] = add2(acc[17], km);
+                acc[6] = fma2(cj, uk2, acc[6]);
+                acc[7] = add2(acc[7], f6);
+                acc[8] = fma2(hj, uk2, acc[8]);
+                acc[9] = fma2(hj, f6, acc[9]);
+                acc[10] = fma2(f2(kk[e]), uk2, acc[10]);
+                acc[11] = fma2(hj, K, acc[11]);
             }
         }
     }
@@ -668,6 +659,7 @@ __device__ float fwd_tick(const svpf_config_t& c, int n, int np, float* x, float
                     R[IHW * np + i] = hw;
                     R[IKN * np + i] = kk;
                     R[IXR * np + i] = xr;
+                    R[INK * np + i] = full ? (r ? nk.y : nk.x) : 0.0f;
                 }
             }
         }
@@ -832,19 +824,21 @@ __device__ void bwd_tick(const svpf_config_t& c, int n, int np, float* xb, float
                 float v_[kAdjAcc];
 #pragma unroll
                 for (int q = 0; q < kAdjAcc; ++q) v_[q] = r ? acc[q].y : acc[q].x;
-                const float S1 = v_[0], S2 = -v_[1], C1 = v_[2], C2 = -v_[3], C3 = v_[4], Q1 = v_[5];
-                const float Q2 = -v_[6] + v_[7];
+                const float S1 = v_[0], S2 = -v_[1], C1 = v_[2], C2 = -v_[3], C3 = v_[4], R3 = v_[5];
                 const float xi = xs[i], gi = g[i], ai = a[i];
                 float dx = ib * (ai * (-2.0f * S1 + 2.0f * sign * ib * S2) - 2.0f * gi * C1 - 2.0f * sign * ib * C2);
-                pbw += ai * ib * (2.0f * Q1 - 2.0f * sign * ib * Q2);
+                // parts of the iteration's objective of degree -1 (repulsion, 2 s uK^2 / bw) and
+                // -2 (the Hessian's 2 K^2 |3u^2 - 1| / bw^2) under (x, bw) -> (l x, l bw)
+                float gm1 = 2.0f * sign * ib * ai * R3, gm2 = 0.0f;
                 float gb = C3;
                 if (full) {
-                    const float R1 = v_[8], R2 = v_[9], R3 = v_[7], D1 = v_[10], D2 = v_[11], D3 = v_[12];
-                    const float E1 = v_[13], W1 = v_[14], W2 = v_[15], W3 = v_[16], W4 = v_[17];
+                    const float R1 = v_[6], R2 = v_[7], D1 = v_[8], D2 = v_[9], D3 = v_[10], E1 = v_[11];
                     const float hb = hwb[i], kb = knb[i];
                     dx += ib * (hb * (-2.0f * R1 + 2.0f * ib2 * R2) - 2.0f * kb * R3);
                     dx += ib * (-2.0f * cv[i] * D1 + 2.0f * ib2 * D2 - 2.0f * D3);
-                    pbw += hb * (ib * (2.0f * W1 - 2.0f * ib2 * W2) - 4.0f * ib2 * ib * W3) + kb * 2.0f * ib * W4;
+                    gm2 = 2.0f * ib2 * hb * R[INK * np + i];
+                    // bandwidth adjoint by homogeneity, before the curvature path joins dx (below)
+                    pbw -= ib * ((xi - ts.mean) * dx + gm1 + 2.0f * gm2);
                     // curvature adjoint E1 -> A and s2 (clamp [0.1, 100])
                     const float A = R[IAL * np + i];
                     const float opA = 1.0f + A;
@@ -857,6 +851,8 @@ __device__ void bwd_tick(const svpf_config_t& c, int n, int np, float* xb, float
                         pnu += E1 * (0.5f * A / (opA * opA) + dcdA * (-A / nu));
                         ps2 += E1 * (-inv * inv);
                     }
+                } else {
+                    pbw -= ib * ((xi - ts.mean) * dx + gm1);
                 }
                 xb[i] += dx;   // rows read a, g, xs of other rows, never xb
                 // (c) gradient adjoint, O(N) part (g = clamp(gp + beta glik))

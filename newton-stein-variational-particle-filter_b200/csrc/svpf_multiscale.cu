@@ -130,10 +130,26 @@ void svpf_ms_batch_destroy(svpf_ms_batch_t* m) {
     delete m;
 }
 
-// ms_svpf_init (:383-405): both scales from the same seed
+// ms_svpf_init (:383-405): both scales from the same seed.  The INERTIAL scale
+// is initialised with the scale's own dynamics (rho_inertial 0.98, sigma_z_inertial
+// 0.10, :269-270, :388-390) -- its stationary draw, EKF variance and effective
+// sigma_z -- while its ticks use the instrument's base parameters (:468).
 int svpf_ms_batch_init(svpf_ms_batch_t* m, float initial_vol, unsigned long long seed) {
     if (!m) return SVPF_ERR_INVALID_ARG;
-    const int rc = svpf_batch_initialize(m->batch, seed);
+    const int F = m->F;
+    std::vector<SVPFParams> base(F);
+    for (int i = 0; i < F; ++i) {
+        svpf_batch_get_params(m->batch, F + i, &base[i]);
+        SVPFParams pi = base[i];
+        pi.rho = 0.98f;
+        pi.sigma_z = 0.10f;
+        svpf_batch_set_params(m->batch, F + i, &pi);
+    }
+    int rc = svpf_batch_initialize(m->batch, seed);
+    for (int i = 0; i < F; ++i) {
+        const int r = svpf_batch_set_params(m->batch, F + i, &base[i]);
+        if (rc == SVPF_OK) rc = r;
+    }
     std::fill(m->vol_prev.begin(), m->vol_prev.end(), initial_vol);
     std::fill(m->y_prev.begin(), m->y_prev.end(), 0.0f);
     std::fill(m->surprise_ema.begin(), m->surprise_ema.end(), 0.0f);

@@ -160,6 +160,8 @@ def lib() -> C.CDLL:
         "svpf_batch_tile_of_filter": (_I, [vp, _I, C.POINTER(_I), C.POINTER(_I)]),
         "svpf_batch_set_tile": (_I, [vp, _I, _I, _I]),
         "svpf_batch_get_state": (_I, [vp, _I, C.POINTER(Ctl), _FP, _FP, _FP, _FP]),
+        "svpf_batch_get_params": (_I, [vp, _I, C.POINTER(Params)]),
+        "svpf_batch_set_params": (_I, [vp, _I, C.POINTER(Params)]),
         "svpf_batch_set_state": (_I, [vp, _I, C.POINTER(Ctl), _FP, _FP, _FP, _FP]),
         "svpf_autotune": (_I, [C.POINTER(_I), _I, _I]),
         "svpf_tile_choice": (_I, [_I, C.POINTER(_I), C.POINTER(_I)]),
