@@ -53,9 +53,10 @@ def test_fp32_mirror_tracks_fp64(oracle_mod, name):
 
 def _fixtures():
     """Fixtures of the svpf_step_graph path (the v2 entry point's start with
-    v2_, the torch estimator model's with estimator_)."""
+    v2_, the torch estimator model's with estimator_, the gradient check's with
+    grad_, the two-scale composition's with ms_)."""
     return sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith(("v2_", "estimator_")))
+                  if not os.path.basename(p).startswith(("v2_", "estimator_", "grad_", "ms_")))
 
 
 def _v2_fixtures():
