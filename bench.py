@@ -363,15 +363,24 @@ def gradient_workload(pkg, torch, F: int = 256, N: int = 512, T: int = 1000, k: 
     g.forward_device(d_th.data_ptr(), None, d_y.data_ptr(), min(T, 64), 1, d_ll.data_ptr())   # warm-up
     g.backward_device(None, d_g.data_ptr())
     torch.cuda.synchronize()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-    ev[0].record(stream)
-    g.forward_device(d_th.data_ptr(), None, d_y.data_ptr(), T, 1, d_ll.data_ptr())
-    ev[1].record(stream)
+
+    def timed():
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record(stream)
+        g.forward_device(d_th.data_ptr(), None, d_y.data_ptr(), T, 1, d_ll.data_ptr())
+        ev[1].record(stream)
+        g.backward_device(None, d_g.data_ptr())
+        ev[2].record(stream)
+        ev[2].synchronize()
+        return ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), d_g.cpu().numpy()
+
+    run_records = g.run_records
+    fwd_ms, bwd_ms, grad = timed()
+    # the checkpointed path: the backward recomputes each segment from its checkpoint
+    g.run_records = False
+    g.forward_device(d_th.data_ptr(), None, d_y.data_ptr(), min(T, 64), 1, d_ll.data_ptr())   # warm-up
     g.backward_device(None, d_g.data_ptr())
-    ev[2].record(stream)
-    ev[2].synchronize()
-    fwd_ms, bwd_ms = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
-    grad = d_g.cpu().numpy()
+    ck_fwd_ms, ck_bwd_ms, ck_grad = timed()
     g.close()
     # central differences on a subset, step 1e-4 (float-rounded: the exact step used)
     Fs, Ts = 4, 200
@@ -399,6 +408,13 @@ def gradient_workload(pkg, torch, F: int = 256, N: int = 512, T: int = 1000, k: 
                     "ticks, full Newton <= 8 Stein iterations, own theta per filter, Student-t paths",
         "filter_ticks_per_s": F * T / ((fwd_ms + bwd_ms) / 1e3),
         "forward_ms": fwd_ms, "backward_ms": bwd_ms, "backward_over_forward": bwd_ms / fwd_ms,
+        "records": ("run records: the forward keeps every tick's record, the backward recomputes nothing"
+                    if run_records else "checkpoint segments recomputed in the backward"),
+        "checkpoint_recompute": {
+            "filter_ticks_per_s": F * T / ((ck_fwd_ms + ck_bwd_ms) / 1e3), "forward_ms": ck_fwd_ms,
+            "backward_ms": ck_bwd_ms, "backward_over_forward": ck_bwd_ms / ck_fwd_ms,
+            "same_bits": bool(np.array_equal(grad, ck_grad)),
+            "note": "checkpoint every 64 ticks, each segment recomputed once from its checkpoint"},
         "grad_filter0": grad[0].tolist(),
         "fd_check": {"step": "1e-4 * max(1, |theta|)", "filters": Fs, "ticks": Ts,
                      "median_rel_err": {n: float(np.median(rel[:, q])) for q, n in enumerate(names)},

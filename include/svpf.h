@@ -515,6 +515,15 @@ int svpf_grad_get_status(svpf_grad_t* g, int* status);
  * per-tick records.  Both give the same bits. */
 int svpf_grad_segment_records(const svpf_grad_t* g);
 int svpf_grad_set_segment_records(svpf_grad_t* g, int on);
+/* 1 if the forward keeps every tick's record (T_max records per filter in
+ * device memory) so that the backward recomputes nothing; chosen at create
+ * when they take at most half of the free device memory.  Checkpoints are
+ * still written.  set: 1 allocates them (SVPF_ERR_CUDA if they do not fit),
+ * 0 frees them (the backward then recomputes from the checkpoints); either
+ * way a new forward must run before the next backward.  All modes give the
+ * same bits. */
+int svpf_grad_run_records(const svpf_grad_t* g);
+int svpf_grad_set_run_records(svpf_grad_t* g, int on);
 /* What the run's log-likelihood is made of (before the next forward):
  * SVPF_GRAD_TICK_LOGLIK (default): each tick's loglik as svpf_step_graph
  * reports it (log-mean-exp of the log-weights of the tick's last gradient

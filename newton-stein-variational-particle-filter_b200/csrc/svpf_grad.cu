@@ -95,6 +95,11 @@ struct GArgs {
     size_t rec_floats;
     TickScalars* segts;            // [grid][k] the ticks' scalars (segment records)
     int seg_rec;                   // 1: record the whole segment in one forward
+    // run records: the forward keeps every tick's record (nullptr: recompute)
+    float* run_rec;                // [F][T_max][rec_floats]
+    GState* run_st;                // [F][T_max] state at each tick's start
+    TickScalars* run_ts;           // [F][T_max] the ticks' scalars
+    int T_max;
     int nseg;
     int* status;                   // [F]
     int objective;                 // 0: the tick's log-likelihood, 1: predictive log p(y_t | y_1:t-1)
@@ -1182,11 +1187,17 @@ __global__ void __launch_bounds__(kThreads) grad_forward_kernel(const GArgs a, i
             const float yt = a.y[(size_t)f * a.T + t];
             const float yp = t > 0 ? a.y[(size_t)f * a.T + t - 1] : 0.0f;
             const Noise nz = make_noise(a.seed, f, sh.st.timestep, n, &sh.flag);
+            float* rt = nullptr;
+            if (a.run_rec) {   // keep this tick's record: the backward replays none of the forward
+                rt = a.run_rec + ((size_t)f * a.T_max + t) * a.rec_floats;
+                copy_state_to(&a.run_st[(size_t)f * a.T_max + t], sh.st);
+            }
             __syncthreads();
-            const float ll = fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, nullptr, a.bmax, a.objective);
+            const float ll = fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, rt, a.bmax, a.objective);
             if (threadIdx.x == 0) {
                 if (a.loglik) a.loglik[(size_t)f * a.T + t] = ll;
                 a.ll_sum[f] += (double)ll;
+                if (a.run_rec) a.run_ts[(size_t)f * a.T_max + t] = sh.ts;
             }
         }
         for (int i = threadIdx.x; i < n; i += kThreads) {
@@ -1246,7 +1257,20 @@ __global__ void __launch_bounds__(kThreads) grad_backward_kernel(const GArgs a, 
             vb[i] = a.av[(size_t)f * np + i];
         }
         __syncthreads();
-        if (a.seg_rec) {
+        if (a.run_rec) {
+            // the forward kept every tick's record: adjoints in reverse, nothing recomputed
+            for (int t = t1 - 1; t >= t0; --t) {
+                const float* rt = a.run_rec + ((size_t)f * a.T_max + t) * a.rec_floats;
+                if (threadIdx.x == 0) {
+                    sh.st = a.run_st[(size_t)f * a.T_max + t];
+                    sh.ts = a.run_ts[(size_t)f * a.T_max + t];
+                }
+                __syncthreads();
+                const Noise nz = make_noise(a.seed, f, sh.st.timestep, n, &sh.flag);
+                const float wt = a.w ? a.w[(size_t)f * a.T + t] : 1.0f;
+                bwd_tick(cfg, n, np, xb, vb, work, sh, sa, nz, rt, a.bmax, wt, a.objective);
+            }
+        } else if (a.seg_rec) {
             // one forward over the segment recording every tick, then the
             // ticks' adjoints in reverse from those records
             for (int t = t0; t < t1; ++t) {
@@ -1360,6 +1384,9 @@ struct svpf_grad {
     float* d_rec = nullptr;
     TickScalars* d_segts = nullptr;
     bool seg_rec = false;             // records of a whole segment (k ticks per CTA)
+    float* d_run_rec = nullptr;       // run records: every tick's record kept by the forward
+    GState* d_run_st = nullptr;
+    TickScalars* d_run_ts = nullptr;
     int* d_status = nullptr;
     const float* u_theta = nullptr;   // the arrays the last forward used
     const float* u_gamma = nullptr;
@@ -1371,6 +1398,28 @@ namespace {
 template <class T>
 bool galloc(T** p, size_t count) {
     return cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T)) == cudaSuccess;
+}
+
+size_t run_record_bytes(const svpf_grad* g) {
+    return (size_t)g->F * g->T_max * (g->rec_floats * sizeof(float) + sizeof(GState) + sizeof(TickScalars));
+}
+
+void free_run_records(svpf_grad* g) {
+    cudaFree(g->d_run_rec);
+    cudaFree(g->d_run_st);
+    cudaFree(g->d_run_ts);
+    g->d_run_rec = nullptr;
+    g->d_run_st = nullptr;
+    g->d_run_ts = nullptr;
+}
+
+bool alloc_run_records(svpf_grad* g) {
+    const size_t FT = (size_t)g->F * g->T_max;
+    if (galloc(&g->d_run_rec, FT * g->rec_floats) && galloc(&g->d_run_st, FT) && galloc(&g->d_run_ts, FT))
+        return true;
+    free_run_records(g);
+    cudaGetLastError();
+    return false;
 }
 
 GArgs make_gargs(const svpf_grad* g, const float* theta, const float* gamma, const float* y, const float* w,
@@ -1405,6 +1454,10 @@ GArgs make_gargs(const svpf_grad* g, const float* theta, const float* gamma, con
     a.rec_floats = g->rec_floats;
     a.segts = g->d_segts;
     a.seg_rec = g->seg_rec ? 1 : 0;
+    a.run_rec = g->d_run_rec;
+    a.run_st = g->d_run_st;
+    a.run_ts = g->d_run_ts;
+    a.T_max = g->T_max;
     a.nseg = g->nseg;
     a.status = g->d_status;
     a.objective = g->objective;
@@ -1486,14 +1539,24 @@ svpf_grad_t* svpf_grad_create(int F, const int* ns, const svpf_config_t* cfgs, i
               galloc(&g->d_cks, (size_t)F * g->nseg) && galloc(&g->d_ax, F * np) && galloc(&g->d_av, F * np) &&
               galloc(&g->d_as, F) && galloc(&g->d_seg, G * k * 2 * np) && galloc(&g->d_segs, G * k) &&
               galloc(&g->d_segts, G * k) && galloc(&g->d_status, F);
-    // records of whole segments when they take at most a quarter of the free
-    // device memory (and 16 GiB); else one tick's record per CTA
+    // Records, in order of preference: every tick's record kept by the forward
+    // (run records: the backward recomputes nothing) when they take at most
+    // half of the free device memory (and 96 GiB); else the records of whole
+    // segments, recomputed once per segment from its checkpoint, when they take
+    // at most a quarter (and 16 GiB); else one tick's record per CTA.
     if (ok) {
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
-        const size_t seg_bytes = G * (size_t)k * g->rec_floats * sizeof(float);
-        g->seg_rec = seg_bytes <= std::min(free_b / 4, (size_t)16 << 30) && galloc(&g->d_rec, G * k * g->rec_floats);
-        if (!g->seg_rec) ok = galloc(&g->d_rec, G * g->rec_floats);
+        const size_t run_bytes = run_record_bytes(g);
+        if (run_bytes <= std::min(free_b / 2, (size_t)96 << 30)) alloc_run_records(g);
+        if (g->d_run_rec) {
+            ok = galloc(&g->d_rec, G * g->rec_floats);
+        } else {
+            const size_t seg_bytes = G * (size_t)k * g->rec_floats * sizeof(float);
+            g->seg_rec = seg_bytes <= std::min(free_b / 4, (size_t)16 << 30) &&
+                         galloc(&g->d_rec, G * k * g->rec_floats);
+            if (!g->seg_rec) ok = galloc(&g->d_rec, G * g->rec_floats);
+        }
     }
     ok = ok && cudaMemcpy(g->d_n, ns, F * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(g->d_cfg, cfgs, F * sizeof(svpf_config_t), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -1511,6 +1574,7 @@ void svpf_grad_destroy(svpf_grad_t* g) {
                     g->d_fx, g->d_fv, g->d_fs, g->d_ck, g->d_cks, g->d_ax, g->d_av, g->d_as, g->d_seg,
                     g->d_segs, g->d_rec, g->d_segts, g->d_status};
     for (void* p : ptrs) cudaFree(p);
+    free_run_records(g);
     if (g->own_stream) cudaStreamDestroy(g->stream);
     delete g;
 }
@@ -1627,6 +1691,20 @@ int svpf_grad_set_segment_records(svpf_grad_t* g, int on) {
     g->d_rec = r;
     g->seg_rec = on != 0;
     return SVPF_OK;
+}
+
+int svpf_grad_run_records(const svpf_grad_t* g) { return g && g->d_run_rec ? 1 : 0; }
+
+int svpf_grad_set_run_records(svpf_grad_t* g, int on) {
+    if (!g) return SVPF_ERR_INVALID_ARG;
+    if ((on != 0) == (g->d_run_rec != nullptr)) return SVPF_OK;
+    if (cudaStreamSynchronize(g->stream) != cudaSuccess) return SVPF_ERR_CUDA;
+    g->forward_done = false;   // the records come from a forward made in this mode
+    if (!on) {
+        free_run_records(g);
+        return SVPF_OK;
+    }
+    return alloc_run_records(g) ? SVPF_OK : SVPF_ERR_CUDA;
 }
 
 int svpf_grad_set_objective(svpf_grad_t* g, int objective) {

@@ -178,6 +178,8 @@ def lib() -> C.CDLL:
         "svpf_grad_set_segment_records": (_I, [vp, _I]),
         "svpf_grad_set_objective": (_I, [vp, _I]),
         "svpf_grad_get_status": (_I, [vp, C.POINTER(_I)]),
+        "svpf_grad_run_records": (_I, [vp]),
+        "svpf_grad_set_run_records": (_I, [vp, _I]),
         "svpf_stream_create": (vp, [_I, C.c_size_t, _I, vp]),
         "svpf_stream_destroy": (None, [vp]),
         "svpf_stream_set_seed": (None, [vp, C.c_ulonglong]),
@@ -694,6 +696,15 @@ class Grad:
     @segment_records.setter
     def segment_records(self, on: bool):
         self._check(lib().svpf_grad_set_segment_records(self._g, int(bool(on))))
+
+    @property
+    def run_records(self) -> bool:
+        """True when the forward keeps every tick's record (no recomputation)."""
+        return bool(lib().svpf_grad_run_records(self._g))
+
+    @run_records.setter
+    def run_records(self, on: bool):
+        self._check(lib().svpf_grad_set_run_records(self._g, int(bool(on))))
 
     def _check(self, rc):
         if rc != SVPF_OK:

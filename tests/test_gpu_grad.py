@@ -119,23 +119,26 @@ def test_checkpoint_interval_does_not_change_the_gradient(pkg):
         assert np.array_equal(gr, out[0][1])
 
 
-def test_segment_records_give_the_same_bits(pkg):
-    """Recording a whole checkpoint segment in one forward and re-recording
-    each tick before its adjoint are the same computation."""
+def test_record_modes_give_the_same_bits(pkg):
+    """The forward keeping every tick's record (no recomputation), recording a
+    whole checkpoint segment in one forward, and re-recording each tick before
+    its adjoint are the same computation."""
     cfg = pkg.grad_config(4, 12.0)
     ns = [128, 300, 64]
     th = thetas_for(3, 6)
     ys = paths_for(th, 20)
     out = []
-    for on in (True, False):
+    for run, seg in ((True, False), (False, True), (False, False)):
         g = pkg.Grad(ns, cfg, T_max=20, checkpoint_every=7)
-        g.segment_records = on
-        assert g.segment_records == on
+        g.run_records = run
+        g.segment_records = seg
+        assert g.run_records == run and g.segment_records == seg
         ll, _ = g.forward(th, ys, seed=2)
         out.append((ll, g.backward()))
         g.close()
-    assert np.array_equal(out[0][0], out[1][0])
-    assert np.array_equal(out[0][1], out[1][1])
+    for ll, gr in out[1:]:
+        assert np.array_equal(out[0][0], ll)
+        assert np.array_equal(out[0][1], gr)
 
 
 def test_weights_select_ticks(pkg):
