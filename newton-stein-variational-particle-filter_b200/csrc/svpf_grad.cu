@@ -1702,6 +1702,12 @@ int svpf_grad_set_run_records(svpf_grad_t* g, int on) {
     g->forward_done = false;   // the records come from a forward made in this mode
     if (!on) {
         free_run_records(g);
+        // the backward recomputes from now on: segment records when they fit (as at create)
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        const size_t seg_bytes = (size_t)g->grid * g->k * g->rec_floats * sizeof(float);
+        if (!g->seg_rec && seg_bytes <= std::min(free_b / 4, (size_t)16 << 30)) svpf_grad_set_segment_records(g, 1);
+        cudaGetLastError();
         return SVPF_OK;
     }
     return alloc_run_records(g) ? SVPF_OK : SVPF_ERR_CUDA;

@@ -119,17 +119,19 @@ def test_checkpoint_interval_does_not_change_the_gradient(pkg):
         assert np.array_equal(gr, out[0][1])
 
 
-def test_record_modes_give_the_same_bits(pkg):
+@pytest.mark.parametrize("objective", [0, 1])
+def test_record_modes_give_the_same_bits(pkg, objective):
     """The forward keeping every tick's record (no recomputation), recording a
     whole checkpoint segment in one forward, and re-recording each tick before
     its adjoint are the same computation."""
-    cfg = pkg.grad_config(4, 12.0)
-    ns = [128, 300, 64]
-    th = thetas_for(3, 6)
+    cfg = pkg.grad_config(8 if objective else 4, 12.0)
+    ns = [128, 300, 64, 512]
+    th = thetas_for(4, 6)
     ys = paths_for(th, 20)
     out = []
     for run, seg in ((True, False), (False, True), (False, False)):
         g = pkg.Grad(ns, cfg, T_max=20, checkpoint_every=7)
+        g.set_objective(objective)
         g.run_records = run
         g.segment_records = seg
         assert g.run_records == run and g.segment_records == seg
