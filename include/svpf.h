@@ -524,6 +524,18 @@ int svpf_grad_set_segment_records(svpf_grad_t* g, int on);
  * same bits. */
 int svpf_grad_run_records(const svpf_grad_t* g);
 int svpf_grad_set_run_records(svpf_grad_t* g, int on);
+/* Truncated backpropagation through time (the reference's torch model cuts
+ * its particle path the same way, py-torch/diff_svpf_torch.py:177-179): for
+ * t > 0 with t % every == 0, the state carried into tick t (particles,
+ * RMSProp moments, EKF guide, bandwidth average, previous mean) is held
+ * constant in theta, so each tick's log-likelihood is differentiated through
+ * at most `every` ticks of the filter.  0 (default): the exact gradient of the
+ * whole run.  The exact gradient can grow exponentially with the run's length
+ * (narrow state noise makes the particle map expanding); a filter whose
+ * gradient overflows gets SVPF_ERR_NONFINITE in svpf_grad_get_status.
+ * Applies to the next backward. */
+int svpf_grad_set_truncation(svpf_grad_t* g, int every);
+int svpf_grad_truncation(const svpf_grad_t* g);
 /* What the run's log-likelihood is made of (before the next forward):
  * SVPF_GRAD_TICK_LOGLIK (default): each tick's loglik as svpf_step_graph
  * reports it (log-mean-exp of the log-weights of the tick's last gradient

@@ -100,6 +100,7 @@ struct GArgs {
     GState* run_st;                // [F][T_max] state at each tick's start
     TickScalars* run_ts;           // [F][T_max] the ticks' scalars
     int T_max;
+    int trunc;                     // > 0: truncated backpropagation every trunc ticks
     int nseg;
     int* status;                   // [F]
     int objective;                 // 0: the tick's log-likelihood, 1: predictive log p(y_t | y_1:t-1)
@@ -1134,6 +1135,25 @@ __device__ inline void copy_state_to(GState* dst, const GState& src) {
     if (threadIdx.x == 0) *dst = src;
 }
 
+// Truncated backpropagation through time: after the adjoint of tick t, for
+// t > 0 with t % trunc == 0, the state carried into tick t (particles,
+// RMSProp moments, EKF mean and variance, bandwidth average, previous mean)
+// is held constant in theta -- its adjoint is dropped; theta's is kept.
+__device__ inline void truncate_after(const GArgs& a, int t, int n, float* xb, float* vb, GAdj& sa) {
+    if (a.trunc <= 0 || t == 0 || t % a.trunc != 0) return;
+    for (int i = threadIdx.x; i < n; i += kThreads) {
+        xb[i] = 0.0f;
+        vb[i] = 0.0f;
+    }
+    if (threadIdx.x == 0) {
+        sa.m = 0.0;
+        sa.P = 0.0;
+        sa.bw_sq = 0.0;
+        sa.h_mean = 0.0;
+    }
+    __syncthreads();
+}
+
 // Forward over ticks [t0, t1) for every filter; checkpoint at segment starts.
 __global__ void __launch_bounds__(kThreads) grad_forward_kernel(const GArgs a, int t0, int t1) {
     extern __shared__ __align__(16) float smem[];
@@ -1269,6 +1289,7 @@ __global__ void __launch_bounds__(kThreads) grad_backward_kernel(const GArgs a, 
                 const Noise nz = make_noise(a.seed, f, sh.st.timestep, n, &sh.flag);
                 const float wt = a.w ? a.w[(size_t)f * a.T + t] : 1.0f;
                 bwd_tick(cfg, n, np, xb, vb, work, sh, sa, nz, rt, a.bmax, wt, a.objective);
+                truncate_after(a, t, n, xb, vb, sa);
             }
         } else if (a.seg_rec) {
             // one forward over the segment recording every tick, then the
@@ -1293,6 +1314,7 @@ __global__ void __launch_bounds__(kThreads) grad_backward_kernel(const GArgs a, 
                 const Noise nz = make_noise(a.seed, f, sh.st.timestep, n, &sh.flag);
                 const float wt = a.w ? a.w[(size_t)f * a.T + t] : 1.0f;
                 bwd_tick(cfg, n, np, xb, vb, work, sh, sa, nz, rt, a.bmax, wt, a.objective);
+                truncate_after(a, t, n, xb, vb, sa);
             }
         } else {
         // recompute the segment, keeping every tick's input state
@@ -1327,6 +1349,7 @@ __global__ void __launch_bounds__(kThreads) grad_backward_kernel(const GArgs a, 
             fwd_tick(cfg, n, np, x, v, work, sh, nz, yt, yp, rec, a.bmax, a.objective);
             const float wt = a.w ? a.w[(size_t)f * a.T + t] : 1.0f;
             bwd_tick(cfg, n, np, xb, vb, work, sh, sa, nz, rec, a.bmax, wt, a.objective);
+            truncate_after(a, t, n, xb, vb, sa);
         }
         }
         if (t0 == 0) init_adjoint(a, f, n, xb, sh, sa);
@@ -1337,6 +1360,9 @@ __global__ void __launch_bounds__(kThreads) grad_backward_kernel(const GArgs a, 
         if (threadIdx.x == 0) {
             a.as[f] = sa;
             if (sh.flag) a.status[f] = sh.flag;
+            // an exact gradient can grow exponentially with the run's length: report overflow
+            if (t0 == 0 && !(isfinite(sa.th[0]) && isfinite(sa.th[1]) && isfinite(sa.th[2]) && isfinite(sa.th[3])))
+                a.status[f] = SVPF_ERR_NONFINITE;
         }
         __syncthreads();
     }
@@ -1361,6 +1387,7 @@ struct svpf_grad {
     int T = 0;
     unsigned long long seed = 0;
     bool forward_done = false;
+    int trunc = 0;                    // truncated backpropagation every trunc ticks (0: off)
     int objective = 0;
     // device
     int* d_n = nullptr;
@@ -1458,6 +1485,7 @@ GArgs make_gargs(const svpf_grad* g, const float* theta, const float* gamma, con
     a.run_st = g->d_run_st;
     a.run_ts = g->d_run_ts;
     a.T_max = g->T_max;
+    a.trunc = g->trunc;
     a.nseg = g->nseg;
     a.status = g->d_status;
     a.objective = g->objective;
@@ -1599,7 +1627,9 @@ int svpf_grad_forward_device(svpf_grad_t* g, const float* d_theta, const float* 
 
 int svpf_grad_backward_device(svpf_grad_t* g, const float* d_w, double* d_grad) {
     if (!g || !g->forward_done) return SVPF_ERR_NOT_INITIALIZED;
-    if (cudaMemsetAsync(g->d_ax, 0, (size_t)g->F * g->np * sizeof(float), g->stream) != cudaSuccess ||
+    // statuses are the backward's own from here (parameter domain, overflow)
+    if (cudaMemsetAsync(g->d_status, 0, g->F * sizeof(int), g->stream) != cudaSuccess ||
+        cudaMemsetAsync(g->d_ax, 0, (size_t)g->F * g->np * sizeof(float), g->stream) != cudaSuccess ||
         cudaMemsetAsync(g->d_av, 0, (size_t)g->F * g->np * sizeof(float), g->stream) != cudaSuccess ||
         cudaMemsetAsync(g->d_as, 0, (size_t)g->F * sizeof(GAdj), g->stream) != cudaSuccess)
         return SVPF_ERR_CUDA;
@@ -1692,6 +1722,14 @@ int svpf_grad_set_segment_records(svpf_grad_t* g, int on) {
     g->seg_rec = on != 0;
     return SVPF_OK;
 }
+
+int svpf_grad_set_truncation(svpf_grad_t* g, int every) {
+    if (!g || every < 0) return SVPF_ERR_INVALID_ARG;
+    g->trunc = every;
+    return SVPF_OK;
+}
+
+int svpf_grad_truncation(const svpf_grad_t* g) { return g ? g->trunc : 0; }
 
 int svpf_grad_run_records(const svpf_grad_t* g) { return g && g->d_run_rec ? 1 : 0; }
 

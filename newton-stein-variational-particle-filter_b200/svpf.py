@@ -179,6 +179,8 @@ def lib() -> C.CDLL:
         "svpf_grad_set_objective": (_I, [vp, _I]),
         "svpf_grad_get_status": (_I, [vp, C.POINTER(_I)]),
         "svpf_grad_run_records": (_I, [vp]),
+        "svpf_grad_set_truncation": (_I, [vp, _I]),
+        "svpf_grad_truncation": (_I, [vp]),
         "svpf_grad_set_run_records": (_I, [vp, _I]),
         "svpf_stream_create": (vp, [_I, C.c_size_t, _I, vp]),
         "svpf_stream_destroy": (None, [vp]),
@@ -696,6 +698,15 @@ class Grad:
     @segment_records.setter
     def segment_records(self, on: bool):
         self._check(lib().svpf_grad_set_segment_records(self._g, int(bool(on))))
+
+    @property
+    def truncate_every(self) -> int:
+        """Truncated backpropagation every k ticks (0: the exact gradient)."""
+        return int(lib().svpf_grad_truncation(self._g))
+
+    @truncate_every.setter
+    def truncate_every(self, every: int):
+        self._check(lib().svpf_grad_set_truncation(self._g, int(every)))
 
     @property
     def run_records(self) -> bool:

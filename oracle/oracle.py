@@ -217,6 +217,8 @@ def lib():
                                             C.c_double, C.POINTER(C.c_float), C.POINTER(C.c_double),
                                             C.c_uint64, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                             C.POINTER(C.c_double), C.c_int]
+        L.svpf_oracle_grad_run3.restype = C.c_int
+        L.svpf_oracle_grad_run3.argtypes = L.svpf_oracle_grad_run2.argtypes + [C.c_int]
         L.svpf_oracle_grad_run.restype = C.c_int
         L.svpf_oracle_grad_run.argtypes = [C.POINTER(OracleConfig), C.c_int, C.c_int, C.POINTER(C.c_double),
                                            C.c_double, C.POINTER(C.c_float), C.POINTER(C.c_double),
@@ -246,7 +248,7 @@ def grad_supported(cfg: OracleConfig) -> bool:
 
 
 def grad_run(cfg: OracleConfig, n: int, theta, ys, gamma: float = 0.0, w=None, seed: int = 0,
-             filter_id: int = 0, objective: int = 0):
+             filter_id: int = 0, objective: int = 0, truncate_every: int = 0):
     """FP64 forward-mode gradient oracle of one filter's run: initialisation
     from theta = (mu, rho, sigma_z, nu), then len(ys) ticks (Philox noise keyed
     by seed and filter_id).  Returns (loglik[T], grad[4] of sum_t w_t loglik_t,
@@ -258,9 +260,9 @@ def grad_run(cfg: OracleConfig, n: int, theta, ys, gamma: float = 0.0, w=None, s
     g = np.zeros(4)
     hf = np.zeros(n)
     wv = None if w is None else np.ascontiguousarray(w, np.float64)
-    rc = lib().svpf_oracle_grad_run2(C.byref(cfg), n, T, _dptr(th), float(gamma), _fptr(ys),
+    rc = lib().svpf_oracle_grad_run3(C.byref(cfg), n, T, _dptr(th), float(gamma), _fptr(ys),
                                      _dptr(wv) if wv is not None else None, seed, filter_id,
-                                     _dptr(ll), _dptr(g), _dptr(hf), int(objective))
+                                     _dptr(ll), _dptr(g), _dptr(hf), int(objective), int(truncate_every))
     if rc != 0:
         raise RuntimeError(f"grad oracle rc={rc}")
     return ll, g, hf

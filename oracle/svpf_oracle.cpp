@@ -872,6 +872,18 @@ struct GradFilter {
         h_mean_prev = Dual(-3.5);   /* svpf_optimized_graph.cu:492-494 */
     }
 
+    /* Truncation: the carried state keeps its values and loses its tangents. */
+    void hold_state() {
+        for (int i = 0; i < n; ++i) {
+            h[i] = Dual(h[i].v);
+            v[i] = Dual(v[i].v);
+        }
+        bw_sq = Dual(bw_sq.v);
+        h_mean_prev = Dual(h_mean_prev.v);
+        gm = Dual(gm.v);
+        gP = Dual(gP.v);
+    }
+
     /* svpf_initialize, svpf_optimized_graph.cu:349-451 (single-factor part) */
     void initialize(Noise<double>& nz_init, const float* init_normals, PhiloxKey key) {
         Dual var = sz * sz / (Dual(1) - rho * rho + Dual(1e-6));
@@ -1281,6 +1293,9 @@ int svpf_oracle_grad_supported(const oracle_config* c) {
 int svpf_oracle_grad_run2(const oracle_config* cfg_in, int n, int T, const double* theta, double gamma,
                           const float* ys, const double* w, uint64_t seed, int filter_id,
                           double* loglik, double* grad, double* h_final, int objective);
+int svpf_oracle_grad_run3(const oracle_config* cfg_in, int n, int T, const double* theta, double gamma,
+                          const float* ys, const double* w, uint64_t seed, int filter_id,
+                          double* loglik, double* grad, double* h_final, int objective, int truncate_every);
 
 int svpf_oracle_grad_run(const oracle_config* cfg_in, int n, int T, const double* theta, double gamma,
                          const float* ys, const double* w, uint64_t seed, int filter_id,
@@ -1294,6 +1309,13 @@ int svpf_oracle_grad_run(const oracle_config* cfg_in, int n, int T, const double
 int svpf_oracle_grad_run2(const oracle_config* cfg_in, int n, int T, const double* theta, double gamma,
                           const float* ys, const double* w, uint64_t seed, int filter_id,
                           double* loglik, double* grad, double* h_final, int objective) {
+    return svpf_oracle_grad_run3(cfg_in, n, T, theta, gamma, ys, w, seed, filter_id, loglik, grad, h_final,
+                                 objective, 0);
+}
+
+int svpf_oracle_grad_run3(const oracle_config* cfg_in, int n, int T, const double* theta, double gamma,
+                          const float* ys, const double* w, uint64_t seed, int filter_id,
+                          double* loglik, double* grad, double* h_final, int objective, int truncate_every) {
     if (!svpf_oracle_grad_supported(cfg_in)) return -2;
     if (n < 1 || T < 0) return -1;
     oracle_config cfg = *cfg_in;
@@ -1310,6 +1332,7 @@ int svpf_oracle_grad_run2(const oracle_config* cfg_in, int n, int T, const doubl
     for (int k = 0; k < 4; ++k) grad[k] = 0;
     double y_prev = 0;
     for (int t = 0; t < T; ++t) {
+        if (truncate_every > 0 && t > 0 && t % truncate_every == 0) f.hold_state();
         nzs.tick = (uint64_t)t;
         Noise<double> nz(&nzs, n);
         const Dual ll = f.tick((double)ys[t], y_prev, nz);

@@ -249,6 +249,14 @@ int svpf_oracle_grad_run(const oracle_config* cfg, int n, int T, const double* t
 int svpf_oracle_grad_run2(const oracle_config* cfg, int n, int T, const double* theta, double gamma,
                           const float* ys, const double* w, uint64_t seed, int filter_id,
                           double* loglik, double* grad, double* h_final, int objective);
+/* As svpf_oracle_grad_run2, with truncated backpropagation through time:
+ * for t > 0 with t % truncate_every == 0 the state carried into tick t
+ * (particles, RMSProp moments, EKF guide mean and variance, bandwidth
+ * average, previous mean) is held constant in theta -- in forward mode its
+ * tangents are zeroed (0: no truncation). */
+int svpf_oracle_grad_run3(const oracle_config* cfg, int n, int T, const double* theta, double gamma,
+                          const float* ys, const double* w, uint64_t seed, int filter_id,
+                          double* loglik, double* grad, double* h_final, int objective, int truncate_every);
 
 /* ---- the reference's differentiable torch model (forward-mode AD, FP64) --- */
 /* SVPFParamEstimator.forward (py-torch/diff_svpf_torch.py:147-217) for one

@@ -9,6 +9,8 @@ sensitivity where that is larger: the FP64 gradient's relative change when
 theta moves by 1e-7 relative (FP32-sized input noise).  Most configurations
 have a sensitivity ~1e-5 and the measured agreement is ~1e-5; without SVLD
 noise and annealing the run is ill-conditioned (sensitivity 2e-3 .. 1e-2)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -35,12 +37,13 @@ def paths_for(thetas, T, seed0=10):
                      for f, th in enumerate(thetas)])
 
 
-def check_against_oracle(pkg, oracle_mod, cfg, ns, T, k=64, seed=7, w=None, gamma=None, objective=0):
+def check_against_oracle(pkg, oracle_mod, cfg, ns, T, k=64, seed=7, w=None, gamma=None, objective=0, trunc=0):
     F = len(ns)
     th = thetas_for(F)
     ys = paths_for(th, T)
     g = pkg.Grad(ns, cfg, T_max=T, checkpoint_every=k)
     g.set_objective(objective)
+    g.truncate_every = trunc
     ll, ls = g.forward(th, ys, gamma=gamma, seed=seed)
     grad = g.backward(w)
     g.close()
@@ -48,7 +51,7 @@ def check_against_oracle(pkg, oracle_mod, cfg, ns, T, k=64, seed=7, w=None, gamm
         run = lambda t: oracle_mod.grad_run(oracle_cfg(oracle_mod, cfg), ns[f], t, ys[f],  # noqa: E731
                                             gamma=0.0 if gamma is None else float(gamma[f]),
                                             w=None if w is None else w[f].astype(np.float64), seed=seed,
-                                            filter_id=f, objective=objective)
+                                            filter_id=f, objective=objective, truncate_every=trunc)
         base = th[f].astype(np.float64)
         oll, og, _ = run(base)
         assert np.max(np.abs(ll[f] - oll) / np.maximum(1, np.abs(oll))) < LL_TOL, f
@@ -92,6 +95,44 @@ def test_predictive_objective_matches_oracle(pkg, oracle_mod, name):
     full = kw.pop("full_newton", True)
     cfg = pkg.grad_config(6, 12.0, full_newton=full, **kw)
     check_against_oracle(pkg, oracle_mod, cfg, [64, 128, 200], T=12, objective=1)
+
+
+@pytest.mark.parametrize("objective,trunc,k", [(0, 8, 64), (1, 5, 7)])
+def test_truncated_adjoint_matches_oracle(pkg, oracle_mod, objective, trunc, k):
+    """Truncated backpropagation every `trunc` ticks (cuts aligned and not
+    aligned with the checkpoints) against the FP64 forward-mode oracle with
+    the same cuts (the carried state's tangents zeroed at each cut)."""
+    cfg = pkg.grad_config(6, 12.0)
+    check_against_oracle(pkg, oracle_mod, cfg, [64, 128, 200], T=24, k=k, objective=objective, trunc=trunc)
+
+
+def test_exploding_gradient_is_reported_and_truncation_bounds_it(pkg):
+    """A filter of the benchmark's workload with narrow state noise (sigma_z
+    0.056): its exact gradient grows exponentially with the run's length (the
+    FP64 forward-mode oracle gives 5.8e5 for d/dmu after 200 ticks, 2.2e7 after
+    250) and overflows FP32 within 1000 ticks -- reported as
+    SVPF_ERR_NONFINITE; truncated backpropagation every 64 ticks keeps it
+    finite."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    F = 256
+    rng = np.random.default_rng(12)
+    th = np.stack([rng.uniform(-2.0, 0.0, F), rng.uniform(0.90, 0.995, F), rng.uniform(0.05, 0.4, F),
+                   rng.uniform(4.0, 30.0, F)], 1).astype(np.float32)
+    ys = bench.sv_paths(1000, th[:, 1].astype(np.float64), th[:, 2].astype(np.float64), th[:, 0].astype(np.float64),
+                        th[:, 3].astype(np.float64), seed=77).T.copy()
+    f = 222
+    g = pkg.Grad([512], pkg.grad_config(8, 12.0), T_max=1000, checkpoint_every=64)
+    g.set_objective(g.PREDICTIVE)
+    g.forward(th[f:f + 1], ys[f:f + 1], seed=1)
+    assert not np.isfinite(g.backward()).all()
+    assert g.status()[0] == 5   # SVPF_ERR_NONFINITE
+    g.truncate_every = 64
+    gt = g.backward()
+    assert np.isfinite(gt).all() and np.abs(gt).max() < 1e5, gt
+    assert g.status()[0] == 0
+    g.close()
 
 
 def test_leverage_and_weights(pkg, oracle_mod):
