@@ -71,3 +71,20 @@ def test_config_fields_follow_header_order(pkg, oracle_mod):
     names = re.findall(r"X_(?:INT|FLOAT)\((\w+)\)", block)
     assert names == [f for f, _ in pkg.CONFIG_FIELDS]
     assert names == [f for f, _ in oracle_mod.CONFIG_FIELDS]
+
+
+def test_batch_create_refuses_bad_sizes_before_device_work(pkg):
+    """Empty batches, empty or oversized filters and runaway loop counts are
+    refused on the host, before any device call (so this runs without a GPU)."""
+    import ctypes as C
+    lib = pkg.lib()
+    cfg = pkg.production_config(30.0, 8)
+    prm = pkg.Params(0.97, 0.15, -1.0, 0.0)
+    for ns in ([], [0], [8193], [256, -1]):
+        arr = (C.c_int * max(1, len(ns)))(*ns)
+        cfgs = (pkg.Config * max(1, len(ns)))(*([cfg] * max(1, len(ns))))
+        prms = (pkg.Params * max(1, len(ns)))(*([prm] * max(1, len(ns))))
+        assert not lib.svpf_batch_create(len(ns), arr, cfgs, prms, None), ns
+    bad = pkg.production_config(30.0, 8)
+    bad.stein_max_steps = 257   # > SVPF_MAX_STEIN_STEPS
+    assert not lib.svpf_batch_create(1, (C.c_int * 1)(256), (pkg.Config * 1)(bad), (pkg.Params * 1)(prm), None)

@@ -165,3 +165,53 @@ def test_loop_counts_are_bounded(pkg):
     rc, _ = f.step_raw(0.1, 0.0)
     assert rc == 0
     f.close()
+
+
+def test_maximum_particle_count_matches_oracle(pkg, oracle_mod):
+    """N = SVPF_MAX_PARTICLES (8192), the largest filter the engine takes:
+    the single-filter cluster kernel and the batch kernel (one CTA, ~190 KB
+    of shared memory), 2 ticks each against the FP64 oracle."""
+    import torch
+
+    n = 8192
+    cfg = pkg.production_config(30.0, 8)
+    params = (0.97, 0.15, -1.0, 0.0)
+    _, ys = tape.sv_path(3, -1.0, 0.97, 0.15, seed=8)
+    init = tape.init_normals(41, n)
+    slots = 2 + 8 + 7
+    nrm, uni = tape.tape(42, 0, n, slots, 2)
+    # single filter
+    f = pkg.SVPF(n, 8, 30.0)
+    f.configure(**cfg.to_dict())
+    f.set_noise_tape(init[None, :], np.ones((1, n), np.float32))
+    f.initialize(*params, seed=1)
+    # batch of one
+    b = pkg.Batch([n], cfg, pkg.Params(*params))
+    b.set_noise_tape(init[None, :], np.ones((1, n), np.float32))
+    b.initialize(seed=1)
+    b.set_noise_tape(nrm, uni)
+    f.set_noise_tape(nrm, uni)
+    d_out = torch.zeros((1, 8), dtype=torch.float32, device="cuda")
+    yp = 0.0
+    for t in range(2):
+        ctl, h, hp, v, lw = f.get_state()
+        o1 = oracle_mod.OracleFilter(n, oracle_mod.config_from_dict(cfg.to_dict()), oracle_mod.OracleParams(*params))
+        o1.ctl = oracle_mod.ctl_from_dict({k: getattr(ctl, k) for k, _ in ctl._fields_ if not k.startswith("smooth_")})
+        o1.h, o1.h_prev, o1.v, o1.log_w = (a.astype(np.float64) for a in (h, hp, v, lw))
+        o2 = _twin(oracle_mod, b, 0, cfg, params)
+        rc, out = f.step_raw(ys[t], yp)
+        assert rc == 0
+        d_yt = torch.tensor([ys[t]], dtype=torch.float32, device="cuda")
+        d_yp = torch.tensor([yp], dtype=torch.float32, device="cuda")
+        b.step_device(d_yt.data_ptr(), d_yp.data_ptr(), d_out.data_ptr())
+        b.sync()
+        with cf.ThreadPoolExecutor(2) as ex:
+            oo1, oo2 = ex.map(lambda o: o.step(ys[t], yp, nrm, uni), (o1, o2))
+        yp = float(ys[t])
+        assert rel_err(f.get_particles(), o1.h) < TOL and abs(out.loglik - oo1.loglik) < TOL * max(1, abs(oo1.loglik))
+        assert rel_err(b.get_particles(0), o2.h) < TOL
+        ob = d_out.cpu().numpy()
+        assert abs(ob[0, 0] - oo2.loglik) < TOL * max(1, abs(oo2.loglik))
+        assert out.steps_used == oo1.steps_used and int(ob.view(np.int32)[0, 6]) == oo2.steps_used
+    f.close()
+    b.close()
