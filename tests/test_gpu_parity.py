@@ -94,7 +94,11 @@ def test_engine_initialize_matches_reference(pkg, path):
     f.configure(**cfg)
     f.set_noise_tape(tape.init_normals(fx["tape_seed"], n, 3 if tf else 1).reshape(-1, n),
                      np.ones((1, n), np.float32))
-    f.initialize(*[float(x) for x in fx["params"]], seed=1)
+    # the C entry point itself (the pybind-style initialize() also resets mu_var as pysvpf does)
+    import ctypes as C
+    f.params = pkg.Params(*[float(x) for x in fx["params"]])
+    pkg.lib().svpf_initialize(f._s, C.byref(f.params), 1)
+    assert f.last_error() == 0
     ctl, h, hp, v, lw = f.get_state()
     if tf:
         h, hp, v = f.get_state_2f()
