@@ -139,3 +139,38 @@ def test_noalloc_rejects_bad_arguments_on_the_host(pkg):
     no_h = list(fake)
     no_h[6] = None                                                                 # d_h
     assert lib.svpf_batch_tick_noalloc(4, *no_h, 256, 0, 0, None) == 1
+
+
+@pytest.mark.gpu
+def test_noalloc_tick_on_two_devices_in_one_process(pkg):
+    """The scratch array and the kernels' shared-memory opt-in exist per
+    device: the same call on two GPUs of one process gives the same results
+    (skipped with fewer than two GPUs)."""
+    import torch
+
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    lib = _bind(pkg.lib())
+    ns = [512, 4096, 256]
+    F = len(ns)
+    cfgs = (pkg.Config * F)(*[pkg.production_config(10.0, 8) for _ in range(F)])
+    prms = (pkg.Params * F)(*[pkg.Params(0.97, 0.15, -1.0, 0.0) for _ in range(F)])
+    offs = np.cumsum([0] + [(n + 15) // 16 * 16 for n in ns[:-1]]).astype(np.int64)
+    total = int(offs[-1] + (ns[-1] + 15) // 16 * 16)
+    h0 = (-1.0 + 0.3 * np.random.default_rng(1).standard_normal(total)).astype(np.float32)
+    ctl0 = pkg.Batch([64], pkg.production_config(10.0, 8), pkg.Params(0.97, 0.15, -1.0, 0.0)).ctl()[0]
+    results = []
+    for dev in (0, 1):
+        with torch.cuda.device(dev):
+            d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda(dev)  # noqa: E731
+            d_ctl = _dev_bytes(torch, (pkg.Ctl * F)(*([ctl0] * F))).cuda(dev)
+            bufs = [d(np.array(ns, np.int32)), d(offs), _dev_bytes(torch, cfgs).cuda(dev),
+                    _dev_bytes(torch, prms).cuda(dev), d_ctl, d(h0), d(h0), d(np.zeros(total, np.float32)),
+                    d(np.zeros(total, np.float32)), d(np.full(F, 0.3, np.float32)), d(np.zeros(F, np.float32))]
+            d_out = torch.zeros((F, 8), dtype=torch.float32, device=f"cuda:{dev}")
+            rc = lib.svpf_batch_tick_noalloc(F, *[b.data_ptr() for b in bufs], d_out.data_ptr(), max(ns), 0, 5,
+                                             None)
+            assert rc == 0, (dev, rc)
+            torch.cuda.synchronize(dev)
+            results.append(d_out.cpu().numpy())
+    assert np.isfinite(results[0]).all() and np.array_equal(results[0], results[1])
