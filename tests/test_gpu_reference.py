@@ -125,6 +125,36 @@ def test_plain_workload_exactly_matches_reference_rmse(pkg):
     assert abs(r_ours - r_ref) <= 0.02 * r_ref, res
 
 
+def test_two_factor_rmse_matches_reference_cuda_step(pkg):
+    """The two-factor step (h = mu + h_fast + h_slow) on the reference
+    two-factor test's knobs (5 annealing stages x 8 Stein steps, guide, MIM,
+    SVLD; N = 512, Student-t nu = 7) against the reference's own step
+    (unmodified build, its own noise) on seeded two-factor paths: filtered
+    log-vol RMSE within 2 %; per-call latency of both recorded."""
+    import cases
+    oracle, reflib = _ref_stock()
+    cfg = pkg.default_config(8, 7.0)
+    cfg.update(**cases.TWO_FACTOR_TEST)
+    cfg = cfg.to_dict()
+    params = (0.99, 0.05, -3.5, 0.0)
+    res = {"n": 512, "paths": []}
+    r_ref, r_ours = [], []
+    for seed in (0, 1):
+        h_true, ys = tape.sv2_path(1500, -3.5, 0.90, 0.15, 0.99, 0.05, seed=200 + seed, nu_obs=7.0)
+        hm_ref, lat_ref = run_reference(oracle, reflib, cfg, params, ys, 512, 8, 7.0)
+        hm_ours, lat_ours = run_engine(pkg, cfg, params, ys, 512, 8, 7.0, seed)
+        w = 100
+        r_ref.append(float(np.sqrt(np.mean((hm_ref[w:] - h_true[w:]) ** 2))))
+        r_ours.append(float(np.sqrt(np.mean((hm_ours[w:] - h_true[w:]) ** 2))))
+        res["paths"].append({"seed": seed, "rmse_ref": r_ref[-1], "rmse_ours": r_ours[-1],
+                             "ref_p50_us": float(np.percentile(lat_ref[w:], 50)),
+                             "ours_p50_us": float(np.percentile(lat_ours[w:], 50))})
+    res["rmse_ref"], res["rmse_ours"] = float(np.mean(r_ref)), float(np.mean(r_ours))
+    with open(os.path.join(results_dir(), "reference_compare_two_factor_n512.json"), "w") as fh:
+        json.dump(res, fh, indent=1)
+    assert abs(res["rmse_ours"] - res["rmse_ref"]) <= 0.02 * res["rmse_ref"], res
+
+
 def test_reference_plain_step_loop_on_batched_workload(pkg):
     """The reference's svpf_step_graph looped over a sample of the batched
     workload (own theta and N per filter, production configuration), the way
