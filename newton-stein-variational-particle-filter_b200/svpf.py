@@ -236,6 +236,22 @@ def _f32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float32)
 
 
+def _tape(normals, uniforms, width: int):
+    """A noise tape as the C entry points read it: [slots][width] float32
+    rows.  A 1-D array of ``width`` values is one slot; any other shape is
+    refused here, since the C side reads slots x width values from the
+    pointer and cannot check the buffer's size."""
+    out = []
+    for name, a in (("normals", normals), ("uniforms", uniforms)):
+        a = _f32(a)
+        if a.ndim == 1 and a.shape[0] == width:
+            a = a[None, :]
+        if a.ndim != 2 or a.shape[1] != width or a.shape[0] < 1:
+            raise ValueError(f"{name} tape must be [slots, {width}], got shape {a.shape}")
+        out.append(a)
+    return tuple(out)
+
+
 def default_config(n_stein_steps: int = 8, nu: float = 30.0) -> Config:
     """The reference's svpf_create defaults (svpf_optimized_graph.cu:116-283)."""
     c = Config()
@@ -506,7 +522,7 @@ class SVPF:
         if normals is None:
             self._check(lib().svpf_set_noise_tape(self._s, None, 0, None, 0))
             return
-        self._tape = (_f32(normals), _f32(uniforms))
+        self._tape = _tape(normals, uniforms, self._n)
         nrm, uni = self._tape
         self._check(lib().svpf_set_noise_tape(self._s, _fp(nrm), nrm.shape[0], _fp(uni), uni.shape[0]))
 
@@ -608,7 +624,7 @@ class Batch:
         if normals is None:
             self._check(lib().svpf_batch_set_noise_tape(self._b, None, 0, None, 0))
             return
-        self._tape = (_f32(normals), _f32(uniforms))
+        self._tape = _tape(normals, uniforms, int(self._ns.max()))
         nrm, uni = self._tape
         self._check(lib().svpf_batch_set_noise_tape(self._b, _fp(nrm), nrm.shape[0], _fp(uni), uni.shape[0]))
 

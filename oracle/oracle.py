@@ -441,6 +441,8 @@ class RefLib:
         L.svpf_ref_v2_time.restype = C.c_int
         L.svpf_ref_v2_time.argtypes = [C.POINTER(OracleV2Params), C.c_int, C.POINTER(C.c_float), C.c_int,
                                        C.POINTER(C.c_float)]
+        L.svpf_ref_steps_used.restype = C.c_int
+        L.svpf_ref_steps_used.argtypes = [C.c_void_p]
         L.svpf_ref_time_steps.restype = C.c_int
         L.svpf_ref_time_steps.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int,
                                           C.POINTER(OracleParams), C.POINTER(C.c_float)]
@@ -501,6 +503,10 @@ class RefFilter:
         arrs = [np.ascontiguousarray(a, np.float64) for a in (h, hp, v, lw)]
         rc = self.L.svpf_ref_set_state(self.s, C.byref(ctl), *[_dptr(a) for a in arrs])
         assert rc == 0, rc
+
+    def steps_used(self) -> int:
+        """Stein steps the last svpf_step_graph call ran."""
+        return self.L.svpf_ref_steps_used(self.s)
 
     def step(self, y_t, y_prev, params, normals, uniforms):
         nrm = np.ascontiguousarray(normals, np.float32)

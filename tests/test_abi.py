@@ -88,3 +88,18 @@ def test_batch_create_refuses_bad_sizes_before_device_work(pkg):
     bad = pkg.production_config(30.0, 8)
     bad.stein_max_steps = 257   # > SVPF_MAX_STEIN_STEPS
     assert not lib.svpf_batch_create(1, (C.c_int * 1)(256), (pkg.Config * 1)(bad), (pkg.Params * 1)(prm), None)
+
+
+def test_noise_tape_shape_is_checked_before_the_c_call(pkg):
+    """The C entry points read slots x width floats from the tape pointer and
+    cannot see the buffer's size, so the Python mirror refuses any tape that
+    is not [slots, width] (a 1-D array of width values is one slot)."""
+    import numpy as np
+    n = 64
+    nrm, uni = pkg.svpf._tape(np.zeros(n), np.ones((2, n)), n)
+    assert nrm.shape == (1, n) and uni.shape == (2, n) and nrm.dtype == np.float32
+    for bad in (np.zeros(n + 1), np.zeros((3, n - 1)), np.zeros((0, n)), np.zeros((2, 2, n))):
+        with pytest.raises(ValueError):
+            pkg.svpf._tape(bad, np.ones((1, n)), n)
+    with pytest.raises(ValueError):
+        pkg.svpf._tape(np.zeros((1, n)), np.ones(2 * n), n)

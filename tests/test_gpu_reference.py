@@ -1,7 +1,12 @@
-"""Free-running comparison with the reference's own CUDA step (unmodified
-build, its own cuRAND noise) on seeded synthetic SV paths: filtered log-vol
-RMSE must agree within 2% (independent particle noise on both sides, so the
-check is statistical).  Latency of both steps is recorded alongside."""
+"""Free-running comparison with the reference's own CUDA step on seeded
+synthetic SV paths.
+
+* Against the unmodified build (its own cuRAND noise): filtered log-vol RMSE
+  must agree within a statistical tolerance (independent particle noise on
+  both sides).  Latency of both steps is recorded alongside.
+* Against the tape build (the reference's code with its cuRAND draws replaced
+  by a noise tape) on the tape the engine also reads: the two filtered
+  trajectories, never re-synced, must stay together."""
 import json
 import os
 
@@ -125,21 +130,130 @@ def test_plain_workload_exactly_matches_reference_rmse(pkg):
     assert abs(r_ours - r_ref) <= 0.02 * r_ref, res
 
 
-def test_two_factor_rmse_matches_reference_cuda_step(pkg):
-    """The two-factor step (h = mu + h_fast + h_slow) on the reference
-    two-factor test's knobs (5 annealing stages x 8 Stein steps, guide, MIM,
-    SVLD; N = 512, Student-t nu = 7) against the reference's own step
-    (unmodified build, its own noise) on seeded two-factor paths: filtered
-    log-vol RMSE within 2 %; per-call latency of both recorded."""
-    import cases
-    oracle, reflib = _ref_stock()
+def _two_factor_setup(pkg):
     cfg = pkg.default_config(8, 7.0)
     cfg.update(**cases.TWO_FACTOR_TEST)
-    cfg = cfg.to_dict()
-    params = (0.99, 0.05, -3.5, 0.0)
+    return cfg.to_dict(), (0.99, 0.05, -3.5, 0.0)
+
+
+def test_two_factor_free_run_on_shared_tape_tracks_reference_step(pkg):
+    """The two-factor step (h = mu + h_fast + h_slow) on the reference
+    two-factor test's knobs (5 annealing stages x 8 Stein steps, guide, MIM,
+    SVLD; N = 512, Student-t nu = 7), free-running for 1500 ticks next to the
+    reference's own svpf_step_graph (its tape build: the reference's code with
+    its cuRAND draws replaced by the same noise tape).  Nothing is re-synced:
+    both start from the same initial draws and see the same tape every tick,
+    so the two filtered log-vol trajectories must stay together, h_mean
+    within 1e-4 at every tick, and give the same RMSE against the true
+    log-vol (to 1e-5)."""
+    import oracle
+    reflib = oracle.RefLib("tape")
+    cfg, params = _two_factor_setup(pkg)
+    n, T, w = 512, 1500, 100
+    slots = 2 + 2 * cfg["n_anneal_steps"] * 8
+    res = {"n": n, "T": T, "paths": []}
+    for seed in (0, 1):
+        h_true, ys = tape.sv2_path(T, -3.5, 0.90, 0.15, 0.99, 0.05, seed=200 + seed, nu_obs=7.0)
+        z = tape.init_normals(7 + seed, n, 3)
+        f = pkg.SVPF(n, 8, 7.0)
+        f.configure(**cfg)
+        f.set_noise_tape(z, np.ones((1, n), np.float32))
+        f.initialize(*params, seed=seed)
+        r = oracle.RefFilter(reflib, n, 8, 7.0)
+        r.apply_config(oracle.config_from_dict(cfg))
+        p = oracle.OracleParams(*params)
+        assert r.initialize(p, z) == 0
+        hm_ours = np.zeros(T, np.float32)
+        hm_ref = np.zeros(T, np.float32)
+        yp = 0.0
+        for t in range(T):
+            nrm, uni = tape.tape(300 + seed, t, n, slots, 2)
+            f.set_noise_tape(nrm, uni)
+            rc, out = f.step_raw(ys[t], yp)
+            assert rc == 0, (seed, t, rc)
+            fl, _, _, hm_ref[t] = r.step(ys[t], yp, p, nrm, uni)
+            assert fl == 0, (seed, t, fl)
+            hm_ours[t] = out.h_mean
+            yp = float(ys[t])
+        f.close()
+        r.close()
+        diff = np.abs(hm_ours - hm_ref)
+        r_ref = float(np.sqrt(np.mean((hm_ref[w:] - h_true[w:]) ** 2)))
+        r_ours = float(np.sqrt(np.mean((hm_ours[w:] - h_true[w:]) ** 2)))
+        res["paths"].append({"seed": seed, "rmse_ref": r_ref, "rmse_ours": r_ours,
+                             "max_abs_h_mean_diff": float(diff.max())})
+        assert diff.max() < 1e-4 * max(1.0, float(np.abs(hm_ref).max())), (seed, int(diff.argmax()), diff.max())
+        assert abs(r_ours - r_ref) < 1e-5, (seed, r_ours, r_ref)
+    with open(os.path.join(results_dir(), "reference_tape_free_run_two_factor_n512.json"), "w") as fh:
+        json.dump(res, fh, indent=1)
+
+
+@pytest.mark.parametrize("n", [512, 1024])
+def test_single_factor_free_run_on_shared_tape_tracks_reference_step(pkg, n):
+    """The production single-factor step (nu = 30) free-running for 2500 ticks
+    next to the reference's svpf_step_graph (tape build), same initial draws
+    and the same tape every tick, nothing re-synced.  The two sides sum in
+    different orders; where the posterior is sharp, FP32 rounding differences
+    grow for a few ticks (up to ~1e-3 in h_mean, with identical Stein step
+    counts) before the filter pulls the trajectories back together.  So:
+    h_mean within 1e-4 on at least 95 % of ticks and RMSE against the true
+    log-vol equal to 1e-3 relative; the Stein step counts are recorded."""
+    import oracle
+    reflib = oracle.RefLib("tape")
+    cfg = pkg.production_config(30.0, 8).to_dict()
+    params = (0.97, 0.15, -1.0, 0.0)
+    T, w, slots = 2500, 100, 2 + 8 + 7
+    h_true, ys = tape.sv_path(T, -1.0, 0.97, 0.15, seed=100)
+    z = tape.init_normals(7, n, 1)
+    f = pkg.SVPF(n, 8, 30.0)
+    f.configure(**cfg)
+    f.set_noise_tape(z, np.ones((1, n), np.float32))
+    f.initialize(*params, seed=0)
+    r = oracle.RefFilter(reflib, n, 8, 30.0)
+    r.apply_config(oracle.config_from_dict(cfg))
+    p = oracle.OracleParams(*params)
+    assert r.initialize(p, z) == 0
+    hm = np.zeros((2, T), np.float32)
+    steps = np.zeros((2, T), np.int32)
+    yp = 0.0
+    for t in range(T):
+        nrm, uni = tape.tape(300, t, n, slots, 2)
+        f.set_noise_tape(nrm, uni)
+        rc, out = f.step_raw(ys[t], yp)
+        assert rc == 0, (t, rc)
+        fl, _, _, hm[1, t] = r.step(ys[t], yp, p, nrm, uni)
+        assert fl == 0, (t, fl)
+        hm[0, t], steps[0, t], steps[1, t] = out.h_mean, out.steps_used, r.steps_used()
+        yp = float(ys[t])
+    f.close()
+    r.close()
+    d = np.abs(hm[0] - hm[1])
+    near = d <= 1e-4 * np.maximum(1.0, np.abs(hm[1]))
+    rm = [float(np.sqrt(np.mean((hm[k, w:] - h_true[w:]) ** 2))) for k in (0, 1)]
+    first_part = int(np.argmin(near)) if not near.all() else T
+    first_steps = int(np.argmax(steps[0] != steps[1])) if (steps[0] != steps[1]).any() else T
+    res = {"n": n, "T": T, "frac_within_1e-4": float(near.mean()), "max_abs_diff": float(d.max()),
+           "ticks_steps_differ": int((steps[0] != steps[1]).sum()), "first_parting": first_part,
+           "first_steps_differ": first_steps, "rmse_ours": rm[0], "rmse_ref": rm[1]}
+    with open(os.path.join(results_dir(), f"reference_tape_free_run_n{n}.json"), "w") as fh:
+        json.dump(res, fh, indent=1)
+    assert near.mean() >= 0.95, res
+    assert abs(rm[0] - rm[1]) <= 1e-3 * rm[1], res
+
+
+def test_two_factor_rmse_against_reference_cuda_step(pkg):
+    """The same two-factor setup against the reference's unmodified build (its
+    own cuRAND noise) on 8 seeded two-factor paths of 1500 ticks: per-path
+    RMSE differences (engine minus reference) must have a mean within four
+    standard errors of zero plus 1 % of the reference's RMSE.  Independent
+    particle noise makes a single path's RMSE vary by several per cent, so a
+    tolerance on one or two paths would say nothing; per-call latency of both
+    steps is recorded."""
+    oracle, reflib = _ref_stock()
+    cfg, params = _two_factor_setup(pkg)
     res = {"n": 512, "paths": []}
     r_ref, r_ours = [], []
-    for seed in (0, 1):
+    for seed in range(8):
         h_true, ys = tape.sv2_path(1500, -3.5, 0.90, 0.15, 0.99, 0.05, seed=200 + seed, nu_obs=7.0)
         hm_ref, lat_ref = run_reference(oracle, reflib, cfg, params, ys, 512, 8, 7.0)
         hm_ours, lat_ours = run_engine(pkg, cfg, params, ys, 512, 8, 7.0, seed)
@@ -149,10 +263,13 @@ def test_two_factor_rmse_matches_reference_cuda_step(pkg):
         res["paths"].append({"seed": seed, "rmse_ref": r_ref[-1], "rmse_ours": r_ours[-1],
                              "ref_p50_us": float(np.percentile(lat_ref[w:], 50)),
                              "ours_p50_us": float(np.percentile(lat_ours[w:], 50))})
-    res["rmse_ref"], res["rmse_ours"] = float(np.mean(r_ref)), float(np.mean(r_ours))
+    d = np.array(r_ours) - np.array(r_ref)
+    se = float(d.std(ddof=1) / np.sqrt(len(d)))
+    res.update(rmse_ref=float(np.mean(r_ref)), rmse_ours=float(np.mean(r_ours)), mean_diff=float(d.mean()),
+               se_diff=se)
     with open(os.path.join(results_dir(), "reference_compare_two_factor_n512.json"), "w") as fh:
         json.dump(res, fh, indent=1)
-    assert abs(res["rmse_ours"] - res["rmse_ref"]) <= 0.02 * res["rmse_ref"], res
+    assert abs(d.mean()) <= 4 * se + 0.01 * res["rmse_ref"], res
 
 
 def test_reference_plain_step_loop_on_batched_workload(pkg):
