@@ -515,8 +515,9 @@ int svpf_batch_set_noise_tape(svpf_batch_t* b, const float* normals, int ns, con
     if (ns < 1 || nu_ < 1 || !uniforms) return SVPF_ERR_INVALID_ARG;
     const size_t w = (size_t)b->n_max;
     if (!dalloc(&b->tape_n, ns * w) || !dalloc(&b->tape_u, nu_ * w)) return SVPF_ERR_CUDA;
-    cudaMemcpy(b->tape_n, normals, ns * w * sizeof(float), cudaMemcpyHostToDevice);
-    cudaMemcpy(b->tape_u, uniforms, nu_ * w * sizeof(float), cudaMemcpyHostToDevice);
+    if (cudaMemcpy(b->tape_n, normals, ns * w * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->tape_u, uniforms, nu_ * w * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+        return SVPF_ERR_CUDA;
     b->slots_n = ns;
     b->slots_u = nu_;
     return SVPF_OK;

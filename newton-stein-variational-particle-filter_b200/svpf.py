@@ -243,6 +243,9 @@ def _tape(normals, uniforms, width: int):
     pointer and cannot check the buffer's size."""
     out = []
     for name, a in (("normals", normals), ("uniforms", uniforms)):
+        if a is None and name == "uniforms":   # no uniform slots: the C call takes (NULL, 0)
+            out.append(None)
+            continue
         a = _f32(a)
         if a.ndim == 1 and a.shape[0] == width:
             a = a[None, :]
@@ -524,7 +527,8 @@ class SVPF:
             return
         self._tape = _tape(normals, uniforms, self._n)
         nrm, uni = self._tape
-        self._check(lib().svpf_set_noise_tape(self._s, _fp(nrm), nrm.shape[0], _fp(uni), uni.shape[0]))
+        self._check(lib().svpf_set_noise_tape(self._s, _fp(nrm), nrm.shape[0], None if uni is None else _fp(uni),
+                                                       0 if uni is None else uni.shape[0]))
 
     def set_cluster_size(self, ctas: int):
         self._check(lib().svpf_set_cluster_size(self._s, int(ctas)))
@@ -626,7 +630,8 @@ class Batch:
             return
         self._tape = _tape(normals, uniforms, int(self._ns.max()))
         nrm, uni = self._tape
-        self._check(lib().svpf_batch_set_noise_tape(self._b, _fp(nrm), nrm.shape[0], _fp(uni), uni.shape[0]))
+        self._check(lib().svpf_batch_set_noise_tape(self._b, _fp(nrm), nrm.shape[0], None if uni is None else _fp(uni),
+                                                             0 if uni is None else uni.shape[0]))
 
     def tile_of(self, n: int):
         r, s = C.c_int(), C.c_int()

@@ -103,3 +103,5 @@ def test_noise_tape_shape_is_checked_before_the_c_call(pkg):
             pkg.svpf._tape(bad, np.ones((1, n)), n)
     with pytest.raises(ValueError):
         pkg.svpf._tape(np.zeros((1, n)), np.ones(2 * n), n)
+    nrm, uni = pkg.svpf._tape(np.zeros((3, n)), None, n)   # no uniform slots
+    assert nrm.shape == (3, n) and uni is None
