@@ -334,13 +334,14 @@ int svpf_batch_initialize(svpf_batch_t* b, unsigned long long seed) {
         cudaFree(d_tf);
         return SVPF_ERR_CUDA;
     }
-    cudaMemcpy(d_mu, mu.data(), b->F * sizeof(float), cudaMemcpyHostToDevice);
-    cudaMemcpy(d_sd, sd.data(), b->F * sizeof(float), cudaMemcpyHostToDevice);
-    cudaMemcpy(d_sdf, sdf.data(), b->F * sizeof(float), cudaMemcpyHostToDevice);
-    cudaMemcpy(d_sds, sds.data(), b->F * sizeof(float), cudaMemcpyHostToDevice);
-    cudaMemcpy(d_tf, b->tf.data(), b->F, cudaMemcpyHostToDevice);
-    cudaMemcpy(b->d_cfg, b->cfgs.data(), b->F * sizeof(svpf_config_t), cudaMemcpyHostToDevice);
-    cudaMemcpy(b->d_ctl, ctl.data(), b->F * sizeof(svpf_ctl_t), cudaMemcpyHostToDevice);
+    const bool copied =
+        cudaMemcpy(d_mu, mu.data(), b->F * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess &&
+        cudaMemcpy(d_sd, sd.data(), b->F * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess &&
+        cudaMemcpy(d_sdf, sdf.data(), b->F * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess &&
+        cudaMemcpy(d_sds, sds.data(), b->F * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess &&
+        cudaMemcpy(d_tf, b->tf.data(), b->F, cudaMemcpyHostToDevice) == cudaSuccess &&
+        cudaMemcpy(b->d_cfg, b->cfgs.data(), b->F * sizeof(svpf_config_t), cudaMemcpyHostToDevice) == cudaSuccess &&
+        cudaMemcpy(b->d_ctl, ctl.data(), b->F * sizeof(svpf_ctl_t), cudaMemcpyHostToDevice) == cudaSuccess;
     InitArgs a;
     std::memset(&a, 0, sizeof(a));
     a.h = b->d_h;
@@ -357,7 +358,7 @@ int svpf_batch_initialize(svpf_batch_t* b, unsigned long long seed) {
     a.tf = d_tf;
     a.sdf = d_sdf;
     a.sds = d_sds;
-    cudaError_t e = launch_init(a, b->stream);
+    cudaError_t e = copied ? launch_init(a, b->stream) : cudaErrorInvalidValue;
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     cudaFree(d_mu);
     cudaFree(d_sd);

@@ -548,14 +548,17 @@ void svpf_run_sequence_device(SVPFState* s, const float* d_obs, int T, const SVP
         return;
     }
     svpf_run_sequence(s, obs.data(), T, p, ll.data(), vol.data());
-    if (d_ll) cudaMemcpy(d_ll, ll.data(), T * sizeof(float), cudaMemcpyHostToDevice);
-    if (d_vol) cudaMemcpy(d_vol, vol.data(), T * sizeof(float), cudaMemcpyHostToDevice);
+    if ((d_ll && cudaMemcpy(d_ll, ll.data(), T * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) ||
+        (d_vol && cudaMemcpy(d_vol, vol.data(), T * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess))
+        set_err(s, SVPF_ERR_CUDA);
 }
 
 void svpf_get_particles(const SVPFState* s, float* h_out) {
     if (!s || !h_out) return;
     quiesce(s);
-    cudaMemcpy(h_out, s->h, s->n_particles * sizeof(float), cudaMemcpyDeviceToHost);
+    // void, as the reference declares it: a failed copy is recorded for svpf_last_error
+    if (cudaMemcpy(h_out, s->h, s->n_particles * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+        set_err(const_cast<SVPFState*>(s), SVPF_ERR_CUDA);
 }
 
 void svpf_get_stats(const SVPFState* s, float* h_mean, float* h_std) {
@@ -563,7 +566,12 @@ void svpf_get_stats(const SVPFState* s, float* h_mean, float* h_std) {
     const int n = s->n_particles;
     std::vector<float> h(n);
     quiesce(s);
-    cudaMemcpy(h.data(), s->h, n * sizeof(float), cudaMemcpyDeviceToHost);
+    if (cudaMemcpy(h.data(), s->h, n * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        set_err(const_cast<SVPFState*>(s), SVPF_ERR_CUDA);
+        if (h_mean) *h_mean = NAN;
+        if (h_std) *h_std = NAN;
+        return;
+    }
     double sum = 0.0;
     for (float x : h) sum += x;
     const double m = sum / n;
@@ -578,7 +586,10 @@ float svpf_get_ess(const SVPFState* s) {
     const int n = s->n_particles;
     std::vector<float> lw(n);
     quiesce(s);
-    cudaMemcpy(lw.data(), s->log_weights, n * sizeof(float), cudaMemcpyDeviceToHost);
+    if (cudaMemcpy(lw.data(), s->log_weights, n * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        set_err(const_cast<SVPFState*>(s), SVPF_ERR_CUDA);
+        return 0.0f;
+    }
     float mx = lw[0];
     for (float x : lw) mx = std::max(mx, x);
     double sw = 0.0, sw2 = 0.0;

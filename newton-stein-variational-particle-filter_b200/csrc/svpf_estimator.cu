@@ -672,7 +672,8 @@ int svpf_estimator_forward(svpf_estimator_t* e, const float* theta, const float*
         return SVPF_ERR_CUDA;
     if (cudaStreamSynchronize(e->stream) != cudaSuccess) return SVPF_ERR_CUDA;
     std::vector<int> st(F);
-    cudaMemcpy(st.data(), e->d_status, F * sizeof(int), cudaMemcpyDeviceToHost);
+    if (cudaMemcpy(st.data(), e->d_status, F * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return SVPF_ERR_CUDA;
     for (int s : st)
         if (s) return s;
     return SVPF_OK;

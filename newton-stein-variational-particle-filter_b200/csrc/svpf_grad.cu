@@ -1672,7 +1672,8 @@ int svpf_grad_forward(svpf_grad_t* g, const float* theta, const float* gamma, co
         return SVPF_ERR_CUDA;
     if (cudaStreamSynchronize(g->stream) != cudaSuccess) return SVPF_ERR_CUDA;
     std::vector<int> st(F);
-    cudaMemcpy(st.data(), g->d_status, F * sizeof(int), cudaMemcpyDeviceToHost);
+    if (cudaMemcpy(st.data(), g->d_status, F * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return SVPF_ERR_CUDA;
     for (int s : st)
         if (s) return s;
     return SVPF_OK;
