@@ -291,6 +291,12 @@ void svpf_step_seeded(SVPFState* state, float y_t, const SVPFParams* params,
 void svpf_step_adaptive(SVPFState* state, float y_t, float y_prev, const SVPFParams* params,
                         float* h_loglik_out, float* h_vol_out, float* h_mean_out);
 
+/* svpf_step_optimized (include/svpf.cuh:726-733): declared by the reference but
+ * defined nowhere in its sources; here the production tick without the h_mean
+ * output (svpf_step_graph with h_mean_out = NULL). */
+void svpf_step_optimized(SVPFState* state, float y_t, float y_prev, const SVPFParams* params,
+                         float* h_loglik_out, float* h_vol_out);
+
 /* svpf_step_graph (include/svpf.cuh:843-851): the production tick.  Blocking;
  * NULL output pointers are allowed.  One kernel launch per call. */
 void svpf_step_graph(SVPFState* state, float y_t, float y_prev, const SVPFParams* params,

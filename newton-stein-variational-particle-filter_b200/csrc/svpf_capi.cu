@@ -489,6 +489,10 @@ void svpf_step_adaptive(SVPFState* s, float y_t, float y_prev, const SVPFParams*
     svpf_step_graph(s, y_t, y_prev, p, ll, vol, hm);
 }
 
+void svpf_step_optimized(SVPFState* s, float y_t, float y_prev, const SVPFParams* p, float* ll, float* vol) {
+    svpf_step_graph(s, y_t, y_prev, p, ll, vol, nullptr);
+}
+
 // svpf_step (svpf_optimized_graph.cu:1396-1407)
 void svpf_step(SVPFState* s, float y_t, const SVPFParams* p, SVPFResult* r) {
     if (!s) return;

@@ -125,6 +125,8 @@ def lib() -> C.CDLL:
         "svpf_destroy": (None, [vp]),
         "svpf_initialize": (None, [vp, C.POINTER(Params), C.c_ulonglong]),
         "svpf_step_graph": (None, [vp, _F, _F, C.POINTER(Params), _FP, _FP, _FP]),
+        "svpf_step_optimized": (None, [vp, _F, _F, C.POINTER(Params), _FP, _FP]),
+        "svpf_step_adaptive": (None, [vp, _F, _F, C.POINTER(Params), _FP, _FP, _FP]),
         "svpf_step_seeded": (None, [vp, _F, C.POINTER(Params), C.c_ulonglong, vp]),
         "svpf_run_sequence": (None, [vp, _FP, _I, C.POINTER(Params), _FP, _FP]),
         "svpf_get_particles": (None, [vp, _FP]),

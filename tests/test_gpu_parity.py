@@ -258,3 +258,33 @@ def test_status_codes_and_bad_arguments(pkg):
     assert rc == 0
     f.close()
 
+
+
+def test_step_entry_points_agree(pkg):
+    """svpf_step_optimized and svpf_step_adaptive (declared by the reference's
+    svpf.cuh) tick exactly as svpf_step_graph: three filters from one seed,
+    one per entry point, bit-identical outputs over 20 ticks."""
+    import ctypes as C
+
+    L = pkg.lib()
+    _, ys = tape.sv_path(20, -1.0, 0.97, 0.15, seed=5)
+    fs = [pkg.SVPF(512, 8, 30.0) for _ in range(3)]
+    for f in fs:
+        f.configure(**pkg.production_config(30.0, 8).to_dict())
+        f.initialize(0.97, 0.15, -1.0, 0.0, seed=7)
+    out = np.zeros((3, 20, 3), np.float32)
+    yp = 0.0
+    for t in range(20):
+        vals = [[C.c_float() for _ in range(3)] for _ in range(3)]
+        L.svpf_step_graph(fs[0]._s, float(ys[t]), yp, C.byref(fs[0].params), *[C.byref(v) for v in vals[0]])
+        L.svpf_step_adaptive(fs[1]._s, float(ys[t]), yp, C.byref(fs[1].params), *[C.byref(v) for v in vals[1]])
+        L.svpf_step_optimized(fs[2]._s, float(ys[t]), yp, C.byref(fs[2].params), C.byref(vals[2][0]),
+                              C.byref(vals[2][1]))
+        vals[2][2].value = fs[2].last_output().h_mean
+        for k in range(3):
+            out[k, t] = [v.value for v in vals[k]]
+            assert L.svpf_last_error(fs[k]._s) == 0
+        yp = float(ys[t])
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
+    for f in fs:
+        f.close()
