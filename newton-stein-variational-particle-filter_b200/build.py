@@ -27,7 +27,8 @@ SOURCES = ["svpf_kernels.cu", "svpf_single_small.cu", "svpf_single_large.cu", "s
            "svpf_batch_kernel.cu", "svpf_capi.cu", "svpf_batch.cu", "svpf_noalloc.cu", "svpf_grad.cu",
            "svpf_stream.cu", "svpf_v2.cu",
            "svpf_multiscale.cu", "svpf_estimator.cu", "svpf_calib.cu"]
-HEADERS = ["svpf_device.cuh", "svpf_tick.cuh", "svpf_tick2f.cuh", "svpf_internal.h", "svpf_single.cuh", "svpf_math.h"]
+HEADERS = ["svpf_device.cuh", "svpf_tick.cuh", "svpf_tick2f.cuh", "svpf_internal.h", "svpf_single.cuh", "svpf_math.h",
+           "svpf_trace.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
 

@@ -19,6 +19,7 @@
 
 #include "svpf.h"
 #include "svpf_internal.h"
+#include "svpf_trace.h"
 
 using namespace svpf;
 
@@ -159,6 +160,7 @@ extern "C" {
 
 svpf_batch_t* svpf_batch_create(int F, const int* ns, const svpf_config_t* cfgs, const SVPFParams* prms,
                                 cudaStream_t stream) {
+    SVPF_TRACE();
     if (F < 1 || !ns || !cfgs || !prms) return nullptr;
     int n_max = 0, n_max1 = 0, n_max2 = 0, F1 = 0, heun = 0, prod = 1;
     for (int f = 0; f < F; ++f) {
@@ -281,6 +283,7 @@ void svpf_batch_destroy(svpf_batch_t* b) {
 
 // svpf_initialize for every filter (svpf_optimized_graph.cu:349-451)
 int svpf_batch_initialize(svpf_batch_t* b, unsigned long long seed) {
+    SVPF_TRACE();
     if (!b) return SVPF_ERR_INVALID_ARG;
     b->seed = seed;
     if (b->F2 > 0 && b->tape_n && b->slots_n < 3) return SVPF_ERR_TAPE_SHORT;
@@ -370,6 +373,7 @@ int svpf_batch_initialize(svpf_batch_t* b, unsigned long long seed) {
 
 int svpf_batch_step(svpf_batch_t* b, const float* y_t, const float* y_prev, float* loglik, float* vol,
                     float* h_mean) {
+    SVPF_TRACE();
     if (!b || !y_t || !y_prev) return SVPF_ERR_INVALID_ARG;
     const size_t F = (size_t)b->F;
     std::memcpy(b->h_stage, y_t, F * sizeof(float));
@@ -392,11 +396,13 @@ int svpf_batch_step(svpf_batch_t* b, const float* y_t, const float* y_prev, floa
 }
 
 int svpf_batch_step_device(svpf_batch_t* b, const float* d_yt, const float* d_yp, svpf_out_t* d_out) {
+    SVPF_TRACE();
     if (!b || !d_yt || !d_yp) return SVPF_ERR_INVALID_ARG;
     return enqueue_tick(b, d_yt, d_yp, d_out);
 }
 
 int svpf_batch_graph_launch(svpf_batch_t* b, const float* d_yt, const float* d_yp, svpf_out_t* d_out) {
+    SVPF_TRACE();
     if (!b || !d_yt || !d_yp) return SVPF_ERR_INVALID_ARG;
     if (b->gexec && (b->g_yt != d_yt || b->g_yp != d_yp || b->g_out != d_out)) drop_graph(b);
     if (!b->gexec) {
@@ -605,6 +611,7 @@ int tune_one(int n, int ticks, int* best_tile) {
 }  // namespace
 
 int svpf_autotune(const int* ns, int count, int ticks) {
+    SVPF_TRACE();
     if (!ns || count < 1) return SVPF_ERR_INVALID_ARG;
     ticks = std::max(ticks, 1);
     for (int k = 0; k < count; ++k)

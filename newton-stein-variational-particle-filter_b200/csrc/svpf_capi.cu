@@ -13,6 +13,7 @@
 
 #include "svpf.h"
 #include "svpf_internal.h"
+#include "svpf_trace.h"
 
 using namespace svpf;
 
@@ -350,6 +351,7 @@ void step_impl(SVPFState* s, float y_t, float y_prev, const SVPFParams* params,
 extern "C" {
 
 SVPFState* svpf_create(int n_particles, int n_stein_steps, float nu, cudaStream_t stream) {
+    SVPF_TRACE();
     if (n_particles < 1 || n_particles > SVPF_MAX_PARTICLES) return nullptr;
     int dev_count = 0;
     if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count < 1) return nullptr;
@@ -411,6 +413,7 @@ void svpf_destroy(SVPFState* s) {
 
 // svpf_initialize (svpf_optimized_graph.cu:349-451)
 void svpf_initialize(SVPFState* s, const SVPFParams* p, unsigned long long seed) {
+    SVPF_TRACE();
     Impl* im = impl_of(s);
     if (!s || !im || !p) {
         if (s) set_err(s, SVPF_ERR_INVALID_ARG);
@@ -480,21 +483,25 @@ void svpf_initialize(SVPFState* s, const SVPFParams* p, unsigned long long seed)
 
 void svpf_step_graph(SVPFState* s, float y_t, float y_prev, const SVPFParams* p, float* ll, float* vol,
                      float* hm) {
+    SVPF_TRACE();
     Impl* im = impl_of(s);
     step_impl(s, y_t, y_prev, p, im ? im->seed : 0ull, ll, vol, hm);
 }
 
 void svpf_step_adaptive(SVPFState* s, float y_t, float y_prev, const SVPFParams* p, float* ll, float* vol,
                         float* hm) {
+    SVPF_TRACE();
     svpf_step_graph(s, y_t, y_prev, p, ll, vol, hm);
 }
 
 void svpf_step_optimized(SVPFState* s, float y_t, float y_prev, const SVPFParams* p, float* ll, float* vol) {
+    SVPF_TRACE();
     svpf_step_graph(s, y_t, y_prev, p, ll, vol, nullptr);
 }
 
 // svpf_step (svpf_optimized_graph.cu:1396-1407)
 void svpf_step(SVPFState* s, float y_t, const SVPFParams* p, SVPFResult* r) {
+    SVPF_TRACE();
     if (!s) return;
     float ll = 0.0f, vol = 0.0f, hm = 0.0f;
     svpf_step_graph(s, y_t, s->y_prev, p, &ll, &vol, &hm);
@@ -510,6 +517,7 @@ void svpf_step(SVPFState* s, float y_t, const SVPFParams* p, SVPFResult* r) {
 
 void svpf_step_seeded(SVPFState* s, float y_t, const SVPFParams* p, unsigned long long rng_seed,
                       SVPFResult* r) {
+    SVPF_TRACE();
     if (!s) return;
     float ll = 0.0f, vol = 0.0f, hm = 0.0f;
     step_impl(s, y_t, s->y_prev, p, rng_seed, &ll, &vol, &hm);
@@ -525,6 +533,7 @@ void svpf_step_seeded(SVPFState* s, float y_t, const SVPFParams* p, unsigned lon
 
 void svpf_run_sequence(SVPFState* s, const float* obs, int T, const SVPFParams* p, float* ll_out,
                        float* vol_out) {
+    SVPF_TRACE();
     if (!s || !obs || T < 0) {
         if (s) set_err(s, SVPF_ERR_INVALID_ARG);
         return;
@@ -541,6 +550,7 @@ void svpf_run_sequence(SVPFState* s, const float* obs, int T, const SVPFParams* 
 
 void svpf_run_sequence_device(SVPFState* s, const float* d_obs, int T, const SVPFParams* p, float* d_ll,
                               float* d_vol) {
+    SVPF_TRACE();
     if (!s || !d_obs || T < 0) {
         if (s) set_err(s, SVPF_ERR_INVALID_ARG);
         return;

@@ -40,6 +40,7 @@
 #include "svpf_device.cuh"
 #include "svpf_internal.h"
 #include "svpf_math.h"
+#include "svpf_trace.h"
 
 namespace svpf {
 namespace est {
@@ -538,6 +539,7 @@ long long svpf_estimator_tape_floats(int n_particles, int T) {
 
 svpf_estimator_t* svpf_estimator_create(int n_filters, int n_particles, int n_stein_steps, float stein_lr,
                                         int T_max, int checkpoint_every, int truncate_every, cudaStream_t stream) {
+    SVPF_TRACE();
     if (n_filters < 1 || n_particles < 2 || (n_particles & 1) || n_particles > SVPF_MAX_PARTICLES ||
         n_stein_steps < 0 || n_stein_steps > 64 || T_max < 1 || checkpoint_every < 1 || truncate_every < 0 ||
         !std::isfinite(stein_lr))
@@ -605,6 +607,7 @@ void svpf_estimator_destroy(svpf_estimator_t* e) {
 
 int svpf_estimator_forward_device(svpf_estimator_t* e, const float* d_theta, const float* d_y, int T,
                                   unsigned long long seed, const float* d_tape, float* d_loglik, float* d_vol) {
+    SVPF_TRACE();
     if (!e || !d_theta || !d_y || T < 1 || T > e->T_max) return SVPF_ERR_INVALID_ARG;
     e->T = T;
     e->seed = seed;
@@ -623,6 +626,7 @@ int svpf_estimator_forward_device(svpf_estimator_t* e, const float* d_theta, con
 }
 
 int svpf_estimator_backward_device(svpf_estimator_t* e, const float* d_w, double* d_grad) {
+    SVPF_TRACE();
     if (!e || !e->forward_done) return SVPF_ERR_NOT_INITIALIZED;
     if (cudaMemsetAsync(e->d_ax, 0, (size_t)e->F * e->np * sizeof(float), e->stream) != cudaSuccess ||
         cudaMemsetAsync(e->d_ath, 0, (size_t)e->F * 4 * sizeof(double), e->stream) != cudaSuccess)
@@ -641,6 +645,7 @@ int svpf_estimator_backward_device(svpf_estimator_t* e, const float* d_w, double
 
 int svpf_estimator_forward(svpf_estimator_t* e, const float* theta, const float* y, int T, unsigned long long seed,
                            const float* tape, float* loglik, float* vol, double* loglik_sum) {
+    SVPF_TRACE();
     if (!e || !theta || !y || T < 1 || T > e->T_max) return SVPF_ERR_INVALID_ARG;
     const size_t F = (size_t)e->F;
     for (size_t f = 0; f < F; ++f)
@@ -687,6 +692,7 @@ int svpf_estimator_get_status(svpf_estimator_t* e, int* status) {
 }
 
 int svpf_estimator_backward(svpf_estimator_t* e, const float* w, double* grad) {
+    SVPF_TRACE();
     if (!e || !grad) return SVPF_ERR_INVALID_ARG;
     if (!e->forward_done) return SVPF_ERR_NOT_INITIALIZED;
     const size_t F = (size_t)e->F;

@@ -46,6 +46,7 @@
 #include "svpf_device.cuh"
 #include "svpf_internal.h"
 #include "svpf_math.h"
+#include "svpf_trace.h"
 
 namespace svpf {
 namespace grad {
@@ -1511,6 +1512,7 @@ int svpf_grad_supported(const svpf_config_t* c) {
 
 svpf_grad_t* svpf_grad_create(int F, const int* ns, const svpf_config_t* cfgs, int T_max, int k,
                               cudaStream_t stream) {
+    SVPF_TRACE();
     if (F < 1 || !ns || !cfgs || T_max < 1 || k < 1) return nullptr;
     int n_max = 0, bmax = 1;
     for (int f = 0; f < F; ++f) {
@@ -1609,6 +1611,7 @@ void svpf_grad_destroy(svpf_grad_t* g) {
 
 int svpf_grad_forward_device(svpf_grad_t* g, const float* d_theta, const float* d_gamma, const float* d_y, int T,
                              unsigned long long seed, float* d_loglik) {
+    SVPF_TRACE();
     if (!g || !d_theta || !d_y || T < 1 || T > g->T_max) return SVPF_ERR_INVALID_ARG;
     g->T = T;
     g->seed = seed;
@@ -1626,6 +1629,7 @@ int svpf_grad_forward_device(svpf_grad_t* g, const float* d_theta, const float* 
 }
 
 int svpf_grad_backward_device(svpf_grad_t* g, const float* d_w, double* d_grad) {
+    SVPF_TRACE();
     if (!g || !g->forward_done) return SVPF_ERR_NOT_INITIALIZED;
     // statuses are the backward's own from here (parameter domain, overflow)
     if (cudaMemsetAsync(g->d_status, 0, g->F * sizeof(int), g->stream) != cudaSuccess ||
@@ -1651,6 +1655,7 @@ int svpf_grad_backward_device(svpf_grad_t* g, const float* d_w, double* d_grad) 
 
 int svpf_grad_forward(svpf_grad_t* g, const float* theta, const float* gamma, const float* y, int T,
                       unsigned long long seed, float* loglik, double* loglik_sum) {
+    SVPF_TRACE();
     if (!g || !theta || !y || T < 1 || T > g->T_max) return SVPF_ERR_INVALID_ARG;
     const size_t F = (size_t)g->F;
     for (size_t f = 0; f < F; ++f) {
@@ -1680,6 +1685,7 @@ int svpf_grad_forward(svpf_grad_t* g, const float* theta, const float* gamma, co
 }
 
 int svpf_grad_backward(svpf_grad_t* g, const float* w, double* grad) {
+    SVPF_TRACE();
     if (!g || !grad) return SVPF_ERR_INVALID_ARG;
     if (!g->forward_done) return SVPF_ERR_NOT_INITIALIZED;
     const size_t F = (size_t)g->F;

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "svpf.h"
+#include "svpf_trace.h"
 
 struct svpf_ms_batch {
     int F = 0;
@@ -85,6 +86,7 @@ svpf_ms_config_t svpf_ms_default_config(void) {
 
 svpf_ms_batch_t* svpf_ms_batch_create(int F, const svpf_ms_config_t* cfg_in, const SVPFParams* base,
                                       cudaStream_t stream) {
+    SVPF_TRACE();
     if (F < 1 || !base) return nullptr;
     svpf_ms_batch* m = new svpf_ms_batch();
     m->F = F;
@@ -135,6 +137,7 @@ void svpf_ms_batch_destroy(svpf_ms_batch_t* m) {
 // 0.10, :269-270, :388-390) -- its stationary draw, EKF variance and effective
 // sigma_z -- while its ticks use the instrument's base parameters (:468).
 int svpf_ms_batch_init(svpf_ms_batch_t* m, float initial_vol, unsigned long long seed) {
+    SVPF_TRACE();
     if (!m) return SVPF_ERR_INVALID_ARG;
     const int F = m->F;
     std::vector<SVPFParams> base(F);
@@ -158,6 +161,7 @@ int svpf_ms_batch_init(svpf_ms_batch_t* m, float initial_vol, unsigned long long
 
 // ms_svpf_step (:408-536) for every instrument
 int svpf_ms_batch_step(svpf_ms_batch_t* m, const float* y, svpf_ms_output_t* out) {
+    SVPF_TRACE();
     if (!m || !y || !out) return SVPF_ERR_INVALID_ARG;
     const int F = m->F;
     for (int i = 0; i < F; ++i) {

@@ -15,6 +15,7 @@
 #include "svpf.h"
 #include "svpf_device.cuh"
 #include "svpf_internal.h"
+#include "svpf_trace.h"
 
 namespace svpf {
 namespace {
@@ -144,6 +145,7 @@ int svpf_batch_tick_noalloc(int n_filters, const int* d_n, const long long* d_of
                             float* d_v, float* d_log_w, const float* d_y_t, const float* d_y_prev,
                             svpf_out_t* d_out, int n_max, int any_heun, unsigned long long seed,
                             cudaStream_t stream) {
+    SVPF_TRACE();
     if (n_filters < 1 || n_filters > SVPF_NOALLOC_MAX_FILTERS) return SVPF_ERR_INVALID_ARG;
     if (n_max < 1 || n_max > SVPF_MAX_PARTICLES) return SVPF_ERR_INVALID_ARG;
     if (!d_n || !d_off || !d_cfg || !d_params || !d_ctl || !d_h || !d_h_prev || !d_v || !d_log_w || !d_y_t ||

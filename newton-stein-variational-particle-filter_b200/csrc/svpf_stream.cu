@@ -24,6 +24,7 @@
 #include "svpf.h"
 #include "svpf_device.cuh"
 #include "svpf_internal.h"
+#include "svpf_trace.h"
 
 using namespace svpf;
 
@@ -179,6 +180,7 @@ int launch_round(svpf_stream* s, int c1, int c2, const int* d_req, const float* 
 extern "C" {
 
 svpf_stream_t* svpf_stream_create(int max_instruments, size_t hbm_budget_bytes, int n_max, cudaStream_t stream) {
+    SVPF_TRACE();
     if (max_instruments < 1 || n_max < 1 || n_max > SVPF_MAX_PARTICLES) return nullptr;
     svpf_stream* s = new svpf_stream();
     s->cap = max_instruments;
@@ -270,6 +272,7 @@ void svpf_stream_set_seed(svpf_stream_t* s, unsigned long long seed) {
 
 int svpf_stream_admit(svpf_stream_t* s, int n, const svpf_config_t* cfg, const SVPFParams* p,
                       unsigned long long seed) {
+    SVPF_TRACE();
     if (!s || !cfg || !p || n < 1 || n > s->n_max) return -SVPF_ERR_INVALID_ARG;
     if (cfg->use_heun) return -SVPF_ERR_UNSUPPORTED;   // the loop's shared-memory layout has no Heun buffers
     if (!cfg->use_two_factor && s->grid1 < 1) return -SVPF_ERR_UNSUPPORTED;
@@ -353,6 +356,7 @@ int svpf_stream_admit(svpf_stream_t* s, int n, const svpf_config_t* cfg, const S
 }
 
 int svpf_stream_evict(svpf_stream_t* s, int slot) {
+    SVPF_TRACE();
     if (!s || slot < 0 || slot >= s->cap || !s->active[slot]) return SVPF_ERR_INVALID_ARG;
     cudaStreamSynchronize(s->stream);
     long long at = s->off[slot], L = s->len[slot];
@@ -385,6 +389,7 @@ size_t svpf_stream_bytes_in_use(const svpf_stream_t* s) {
 size_t svpf_stream_bytes_budget(const svpf_stream_t* s) { return s ? s->budget : 0; }
 
 int svpf_stream_process(svpf_stream_t* s, int count, const int* slots, const float* y, svpf_out_t* out) {
+    SVPF_TRACE();
     if (!s || count < 0 || (count > 0 && (!slots || !y))) return SVPF_ERR_INVALID_ARG;
     for (int r = 0; r < count; ++r)
         if (slots[r] < 0 || slots[r] >= s->cap || !s->active[slots[r]]) return SVPF_ERR_INVALID_ARG;
@@ -433,6 +438,7 @@ int svpf_stream_process(svpf_stream_t* s, int count, const int* slots, const flo
 
 int svpf_stream_process_device(svpf_stream_t* s, int count1, int count2, const int* d_slots, const float* d_y,
                                svpf_out_t* d_out) {
+    SVPF_TRACE();
     if (!s || count1 < 0 || count2 < 0 || count1 + count2 > s->cap || !d_slots || !d_y || !d_out)
         return SVPF_ERR_INVALID_ARG;
     if (count1 + count2 == 0) return SVPF_OK;

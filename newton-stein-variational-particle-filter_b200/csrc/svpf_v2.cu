@@ -30,6 +30,7 @@
 #include "svpf.h"
 #include "svpf_device.cuh"
 #include "svpf_internal.h"
+#include "svpf_trace.h"
 
 namespace svpf {
 namespace v2 {
@@ -604,6 +605,7 @@ cudaError_t svpf_fully_fused_step_v2(
     float mu_ema_alpha, int use_adaptive_sigma, float sigma_boost_threshold, float sigma_boost_max,
     float step_size, float temperature, float rmsprop_rho, float rmsprop_eps, int n_stein_steps,
     int n_anneal_steps, int stein_sign_mode, int n, int timestep, cudaStream_t stream) {
+    SVPF_TRACE();
     if (!svpf_fully_fused_v2_supported(n)) return cudaErrorInvalidConfiguration;
     if (n_stein_steps > SVPF_MAX_STEIN_STEPS || n_anneal_steps > SVPF_MAX_ANNEAL_STEPS)
         return cudaErrorInvalidValue;   // bounded loop counts: no call keeps the kernel running for long
