@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(kThreads, 2) batch_tick_kernel(const __grid_co
             case 4: run_tick<2, 1, false, PROD>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
             default: run_tick<4, 1, false, PROD>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
         }
-        if (a.req_y && threadIdx.x == 0) ctl.y_prev = yt;
+        if (a.req_y && threadIdx.x == 0 && isfinite(yt)) ctl.y_prev = yt;   // a refused y_t is not kept
         __syncthreads();
         copy_words(&a.ctl[f], &ctl);
         if (a.out != nullptr) copy_words(&a.out[a.req_y ? w : f], &out);
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(kThreads, 2) batch_tick_2f_kernel(const __grid
             case 4: run_tick_2f<2, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
             default: run_tick_2f<4, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
         }
-        if (a.req_y && threadIdx.x == 0) ctl.y_prev = yt;
+        if (a.req_y && threadIdx.x == 0 && isfinite(yt)) ctl.y_prev = yt;   // a refused y_t is not kept
         __syncthreads();
         copy_words(&a.ctl[f], &ctl);
         if (a.out != nullptr) copy_words(&a.out[a.req_y ? w : f], &out);
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(kThreads) batch_tick_2f_cluster_kernel(const _
         if ((n + C - 1) / C <= kThreads) run_tick_2f<1, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out);
         else run_tick_2f<2, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out);
         if (team.rank == 0) {
-            if (a.req_y && threadIdx.x == 0) ctl.y_prev = yt;
+            if (a.req_y && threadIdx.x == 0 && isfinite(yt)) ctl.y_prev = yt;   // a refused y_t is not kept
             __syncthreads();
             copy_words(&a.ctl[f], &ctl);
             if (a.out != nullptr) copy_words(&a.out[a.req_y ? w : f], &out);

@@ -512,7 +512,7 @@ void svpf_step(SVPFState* s, float y_t, const SVPFParams* p, SVPFResult* r) {
         r->vol_std = 0.0f;
         r->mu_estimate = (s->use_adaptive_mu || !p) ? s->mu_state : p->mu;
     }
-    s->y_prev = y_t;
+    if (std::isfinite(y_t)) s->y_prev = y_t;   // a refused observation is not the next tick's y_prev
 }
 
 void svpf_step_seeded(SVPFState* s, float y_t, const SVPFParams* p, unsigned long long rng_seed,
@@ -528,7 +528,7 @@ void svpf_step_seeded(SVPFState* s, float y_t, const SVPFParams* p, unsigned lon
         r->vol_std = 0.0f;
         r->mu_estimate = (s->use_adaptive_mu || !p) ? s->mu_state : p->mu;
     }
-    s->y_prev = y_t;
+    if (std::isfinite(y_t)) s->y_prev = y_t;   // a refused observation is not the next tick's y_prev
 }
 
 void svpf_run_sequence(SVPFState* s, const float* obs, int T, const SVPFParams* p, float* ll_out,
@@ -544,7 +544,7 @@ void svpf_run_sequence(SVPFState* s, const float* obs, int T, const SVPFParams* 
         svpf_step_graph(s, obs[t], y_prev, p, &ll, &vol, &hm);
         if (ll_out) ll_out[t] = ll;
         if (vol_out) vol_out[t] = vol;
-        y_prev = obs[t];
+        if (std::isfinite(obs[t])) y_prev = obs[t];   // a refused observation is not the next y_prev
     }
 }
 

@@ -57,6 +57,27 @@ __device__ __forceinline__ void ksd_publish(float ksd_thread, Plan& pl, const Te
     if (threadIdx.x == 0) team.at(pl.ksd_slot, 0)[team.rank] = v[0];
 }
 
+// A non-finite observation is refused: the tick leaves the filter's state as
+// it was (particles, moments, control record, log-likelihood sum, timestep)
+// and reports SVPF_ERR_NONFINITE with NaN outputs.  The reference runs such a
+// tick: its fminf/fmaxf clamps pin the particles to a bound and the EKF and
+// bandwidth EMAs carry the NaN, so its later ticks report finite nonsense.
+// Every member of a team sees the same y_t, so all members return together.
+__device__ __forceinline__ bool refuse_nonfinite(float y_t, const svpf_ctl_t& ctl, svpf_out_t& out,
+                                                 svpf_ctl_t& ctl_out) {
+    if (isfinite(y_t)) return false;
+    if (threadIdx.x == 0) {
+        const float qnan = __int_as_float(0x7fc00000);
+        ctl_out.status = SVPF_ERR_NONFINITE;
+        out.loglik = out.vol = out.h_mean = out.h_mean_raw = qnan;
+        out.bw = ctl.bw;
+        out.ksd = ctl.ksd_last;
+        out.steps_used = 0;
+        out.rejuv_fired = 0;
+    }
+    return true;
+}
+
 // The tick.  cfg/prm/ctl are shared-memory copies owned by the caller; only
 // thread 0 of rank 0 mutates ctl after make_plan.  Returns on every member; the
 // caller stores ctl/out from rank 0 thread 0.  SCAN: the mixture's row
@@ -71,6 +92,10 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
                          const Team& team, svpf_out_t& out) {
     const int tid = threadIdx.x;
     const int n = sm.n;
+    if (refuse_nonfinite(y_t, ctl, out, ctl)) return;
+    // a non-finite previous observation is read as 0 (no leverage) and flagged
+    const bool y_prev_bad = !isfinite(y_prev);
+    if (y_prev_bad) y_prev = 0.0f;
     if (tid == 0) {
         pl.flag = 0;
         make_plan(cfg, prm, ctl, y_t, y_prev, pl);
@@ -375,10 +400,8 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
         }
         ctl.loglik_sum += (double)ll;
         ctl.timestep += 1;
-        // The reference's clamps (fmaxf/fminf) turn a NaN observation into finite
-        // particles; the tick runs the same way here and the status reports it.
         int status = pl.flag;
-        if (status == SVPF_OK && !(isfinite(y_t) && isfinite(y_prev) && isfinite(ll) && isfinite(vol) && isfinite(hm)))
+        if (status == SVPF_OK && (y_prev_bad || !(isfinite(ll) && isfinite(vol) && isfinite(hm))))
             status = SVPF_ERR_NONFINITE;
         ctl.status = status;
         out.loglik = ll;
