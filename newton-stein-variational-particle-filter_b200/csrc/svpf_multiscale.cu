@@ -181,8 +181,11 @@ int svpf_ms_batch_step(svpf_ms_batch_t* m, const float* y, svpf_ms_output_t* out
         o.loglik_reactive = r.loglik;
         o.ksd_reactive = r.ksd;
         o.stein_steps_reactive = r.steps_used;
+        // a non-finite observation is refused by both scales (their states are
+        // left as they were); the composition's own state is left too
+        const bool ok = std::isfinite(y[i]);
         const float surprise = std::fabs(y[i]) / std::max(m->vol_prev[i], 1e-6f);
-        m->surprise_ema[i] = 0.3f * surprise + 0.7f * m->surprise_ema[i];
+        if (ok) m->surprise_ema[i] = 0.3f * surprise + 0.7f * m->surprise_ema[i];
         o.surprise_reactive = surprise;
         o.cross_scale_boost = 0;
         o.mim_prob_inertial_used = m->mim_base;
@@ -201,8 +204,10 @@ int svpf_ms_batch_step(svpf_ms_batch_t* m, const float* y, svpf_ms_output_t* out
         o.is_transient = (r.vol > vol_elevated) && (o.transient_ratio > ratio_transient) && (n.vol < vol_elevated);
         o.is_regime_shift = (r.vol > vol_elevated) && (n.vol > vol_elevated);
         o.is_calm = (r.vol < vol_elevated) && (n.vol < vol_elevated);
-        m->vol_prev[i] = o.vol_combined;
-        m->y_prev[i] = y[i];
+        if (ok) {
+            m->vol_prev[i] = o.vol_combined;
+            m->y_prev[i] = y[i];
+        }
     }
     return SVPF_OK;
 }

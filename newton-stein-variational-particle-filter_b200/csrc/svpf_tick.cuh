@@ -63,12 +63,11 @@ __device__ __forceinline__ void ksd_publish(float ksd_thread, Plan& pl, const Te
 // tick: its fminf/fmaxf clamps pin the particles to a bound and the EKF and
 // bandwidth EMAs carry the NaN, so its later ticks report finite nonsense.
 // Every member of a team sees the same y_t, so all members return together.
-__device__ __forceinline__ bool refuse_nonfinite(float y_t, const svpf_ctl_t& ctl, svpf_out_t& out,
-                                                 svpf_ctl_t& ctl_out) {
+__device__ __forceinline__ bool refuse_nonfinite(float y_t, svpf_ctl_t& ctl, svpf_out_t& out) {
     if (isfinite(y_t)) return false;
     if (threadIdx.x == 0) {
         const float qnan = __int_as_float(0x7fc00000);
-        ctl_out.status = SVPF_ERR_NONFINITE;
+        ctl.status = SVPF_ERR_NONFINITE;
         out.loglik = out.vol = out.h_mean = out.h_mean_raw = qnan;
         out.bw = ctl.bw;
         out.ksd = ctl.ksd_last;
@@ -92,7 +91,7 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
                          const Team& team, svpf_out_t& out) {
     const int tid = threadIdx.x;
     const int n = sm.n;
-    if (refuse_nonfinite(y_t, ctl, out, ctl)) return;
+    if (refuse_nonfinite(y_t, ctl, out)) return;
     // a non-finite previous observation is read as 0 (no leverage) and flagged
     const bool y_prev_bad = !isfinite(y_prev);
     if (y_prev_bad) y_prev = 0.0f;

@@ -100,7 +100,7 @@ __device__ void run_tick_2f(const svpf_config_t& cfg, const SVPFParams& prm, svp
     const int tid = threadIdx.x;
     const int n = io.n;
     const int np = sm.f[0].np;
-    if (refuse_nonfinite(y_t, ctl, out, ctl)) return;   // state untouched (svpf_tick.cuh)
+    if (refuse_nonfinite(y_t, ctl, out)) return;   // state untouched (svpf_tick.cuh)
     const bool y_prev_bad = !isfinite(y_prev);          // read as 0 and flagged
     if (y_prev_bad) y_prev = 0.0f;
     if (tid == 0) {

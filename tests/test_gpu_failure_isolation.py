@@ -129,3 +129,73 @@ def test_single_filter_refuses_nonfinite_observation(pkg):
     assert np.array_equal(a.get_particles().view(np.uint32), b.get_particles().view(np.uint32))
     for f in fs:
         f.close()
+
+
+def test_request_loop_refuses_nonfinite_request(pkg):
+    """The request loop keeps each instrument's previous observation on the
+    device; a refused (NaN) request leaves it, and the instrument's state, as
+    they were, so the instrument's next request equals the request of a twin
+    loop that never received the NaN, bit for bit.  The two-factor
+    instrument is refused the same way."""
+    ns = [256, 512, 384]
+    c1 = pkg.production_config(7.0, 8)
+    c2 = pkg.default_config(4, 7.0)
+    c2.update(**dict(cases.TWO_FACTOR_TEST, n_anneal_steps=2))
+    cfgs = [c1, c1, c2]
+    prm = pkg.Params(*PARAMS)
+    loops = []
+    for _ in range(2):
+        s = pkg.Stream(4, 32 << 20, 512, seed=9)
+        for f in range(3):
+            assert s.admit(ns[f], cfgs[f], prm, seed=9) == f
+        loops.append(s)
+    a, b = loops
+    slots = np.arange(3, dtype=np.int32)
+    for y in (0.01, -0.02):
+        for s in loops:
+            s.process(slots, np.full(3, y, np.float32))
+    before = [(bytes(a.ctl(f)), a.particles(f).tobytes()) for f in range(3)]
+    out = a.process(np.array([0, 2], np.int32), np.array([np.nan, np.nan], np.float32))
+    for r, f in enumerate((0, 2)):
+        assert np.isnan(out[r].loglik), f
+        c = a.ctl(f)
+        assert c.status == NONFINITE, f
+        c.status = pkg.Ctl.from_buffer_copy(before[f][0]).status
+        assert bytes(c) == before[f][0], f              # y_prev, tick counter and the rest untouched
+        assert a.particles(f).tobytes() == before[f][1], f
+    ya = a.process(slots, np.full(3, 0.03, np.float32))
+    yb = b.process(slots, np.full(3, 0.03, np.float32))
+    for f in range(3):
+        assert a.ctl(f).status == 0 and bytes(a.ctl(f)) == bytes(b.ctl(f)), f
+        assert a.particles(f).tobytes() == b.particles(f).tobytes(), f
+        assert (ya[f].loglik, ya[f].h_mean) == (yb[f].loglik, yb[f].h_mean), f
+    for s in loops:
+        s.close()
+
+
+def test_multiscale_refuses_nonfinite_return(pkg):
+    """The two-scale composition: a NaN return is refused by both scales of
+    its instrument and leaves the composition's own state (surprise EMA,
+    previous volatility and return) as it was, so the instrument's next step
+    equals, bit for bit, the step of a twin that never received the NaN; the
+    other instrument is untouched by it."""
+    base = [pkg.Params(0.97, 0.15, -1.0, 0.0), pkg.Params(0.95, 0.2, -0.5, 0.0)]
+    ms = []
+    for _ in range(3):
+        m = pkg.MultiScale(base)
+        m.init(0.01, seed=5)
+        ms.append(m)
+    a, b, c = ms
+    for y in ((0.01, -0.02), (-0.015, 0.03)):
+        for m in ms:
+            m.step(np.array(y, np.float32))
+    oa = a.step(np.array([np.nan, 0.02], np.float32))
+    ob = b.step(np.array([0.0, 0.02], np.float32))
+    assert np.isnan(oa[0].h_combined) and np.isnan(oa[0].vol_combined)
+    assert bytes(oa[1]) == bytes(ob[1])     # the other instrument: the same bits
+    # c never sees the NaN step (instrument 1 of c then differs: not compared)
+    oa = a.step(np.array([0.01, 0.01], np.float32))
+    oc = c.step(np.array([0.01, 0.01], np.float32))
+    assert np.isfinite(oa[0].h_combined) and bytes(oa[0]) == bytes(oc[0])
+    for m in ms:
+        m.close()
