@@ -52,12 +52,16 @@ __global__ void __launch_bounds__(kThreads, 2) batch_tick_kernel(const __grid_co
         const float yt = a.req_y ? a.req_y[w] : a.y_t[f];
         const float yp = a.req_y ? ctl.y_prev : a.y_prev[f];
         if (threadIdx.x == 0) pl.have_consts = 0;   // make_plan computes the per-tick constants
-        switch (a.tile[f]) {
-            case 1: run_tick<1, 4, false, PROD>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
-            case 2: run_tick<1, 2, false, PROD>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
-            case 3: run_tick<1, 1, false, PROD>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
-            case 4: run_tick<2, 1, false, PROD>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
-            default: run_tick<4, 1, false, PROD>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
+        if (!refuse_nonfinite(yt, ctl, out)) {   // a refused tick leaves the filter as it was
+            const float ypr = readable_y_prev(yp);
+            switch (a.tile[f]) {
+                case 1: run_tick<1, 4, false, PROD>(cfg, prm, ctl, yt, ypr, io, nz, sm, pl, team, out); break;
+                case 2: run_tick<1, 2, false, PROD>(cfg, prm, ctl, yt, ypr, io, nz, sm, pl, team, out); break;
+                case 3: run_tick<1, 1, false, PROD>(cfg, prm, ctl, yt, ypr, io, nz, sm, pl, team, out); break;
+                case 4: run_tick<2, 1, false, PROD>(cfg, prm, ctl, yt, ypr, io, nz, sm, pl, team, out); break;
+                default: run_tick<4, 1, false, PROD>(cfg, prm, ctl, yt, ypr, io, nz, sm, pl, team, out); break;
+            }
+            flag_y_prev(yp, ctl);
         }
         if (a.req_y && threadIdx.x == 0 && isfinite(yt)) ctl.y_prev = yt;   // a refused y_t is not kept
         __syncthreads();
@@ -96,12 +100,16 @@ __global__ void __launch_bounds__(kThreads, 2) batch_tick_2f_kernel(const __grid
         // request mode: y_t from the request, y_prev from the filter's record
         const float yt = a.req_y ? a.req_y[w] : a.y_t[f];
         const float yp = a.req_y ? ctl.y_prev : a.y_prev[f];
-        switch (a.tile[f]) {
-            case 1: run_tick_2f<1, 4>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
-            case 2: run_tick_2f<1, 2>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
-            case 3: run_tick_2f<1, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
-            case 4: run_tick_2f<2, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
-            default: run_tick_2f<4, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out); break;
+        if (!refuse_nonfinite(yt, ctl, out)) {   // a refused tick leaves the filter as it was
+            const float ypr = readable_y_prev(yp);
+            switch (a.tile[f]) {
+                case 1: run_tick_2f<1, 4>(cfg, prm, ctl, yt, ypr, io, nz, sm, pl, team, out); break;
+                case 2: run_tick_2f<1, 2>(cfg, prm, ctl, yt, ypr, io, nz, sm, pl, team, out); break;
+                case 3: run_tick_2f<1, 1>(cfg, prm, ctl, yt, ypr, io, nz, sm, pl, team, out); break;
+                case 4: run_tick_2f<2, 1>(cfg, prm, ctl, yt, ypr, io, nz, sm, pl, team, out); break;
+                default: run_tick_2f<4, 1>(cfg, prm, ctl, yt, ypr, io, nz, sm, pl, team, out); break;
+            }
+            flag_y_prev(yp, ctl);
         }
         if (a.req_y && threadIdx.x == 0 && isfinite(yt)) ctl.y_prev = yt;   // a refused y_t is not kept
         __syncthreads();
@@ -148,8 +156,12 @@ __global__ void __launch_bounds__(kThreads) batch_tick_2f_cluster_kernel(const _
                        a.slots_n, a.slots_u, a.tape_stride, &pl.flag};
         const float yt = a.req_y ? a.req_y[w] : a.y_t[f];
         const float yp = a.req_y ? ctl.y_prev : a.y_prev[f];
-        if ((n + C - 1) / C <= kThreads) run_tick_2f<1, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out);
-        else run_tick_2f<2, 1>(cfg, prm, ctl, yt, yp, io, nz, sm, pl, team, out);
+        if (!refuse_nonfinite(yt, ctl, out)) {   // every member sees the same y_t
+            const float ypr = readable_y_prev(yp);
+            if ((n + C - 1) / C <= kThreads) run_tick_2f<1, 1>(cfg, prm, ctl, yt, ypr, io, nz, sm, pl, team, out);
+            else run_tick_2f<2, 1>(cfg, prm, ctl, yt, ypr, io, nz, sm, pl, team, out);
+            flag_y_prev(yp, ctl);
+        }
         if (team.rank == 0) {
             if (a.req_y && threadIdx.x == 0 && isfinite(yt)) ctl.y_prev = yt;   // a refused y_t is not kept
             __syncthreads();

@@ -51,7 +51,11 @@ __global__ void __launch_bounds__(kThreads, 1) single_tick_kernel(const __grid_c
         pl.stc = a.stc;
         pl.log_y2 = a.log_y2;
     }
-    run_tick<R, S, SCAN, PROD, kClusterUnroll>(cfg, prm, ctl, a.y_t, a.y_prev, io, nz, sm, pl, team, out);
+    if (!refuse_nonfinite(a.y_t, ctl, out)) {   // every member sees the same y_t
+        run_tick<R, S, SCAN, PROD, kClusterUnroll>(cfg, prm, ctl, a.y_t, readable_y_prev(a.y_prev), io, nz, sm, pl,
+                                                   team, out);
+        flag_y_prev(a.y_prev, ctl);
+    }
     if (team.rank == 0) {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -81,7 +85,10 @@ __global__ void __launch_bounds__(kThreads, 1) single_tick_2f_kernel(const __gri
     const Noise nz{philox_key(a.seed, 0), (uint32_t)ctl.timestep, a.tape_n, a.tape_u,
                    a.slots_n, a.slots_u, a.n, &pl.flag};
     const FilterIO io{a.h, a.hp, a.v, a.lw, a.n};
-    run_tick_2f<R, S>(cfg, prm, ctl, a.y_t, a.y_prev, io, nz, sm, pl, team, out);
+    if (!refuse_nonfinite(a.y_t, ctl, out)) {   // every member sees the same y_t
+        run_tick_2f<R, S>(cfg, prm, ctl, a.y_t, readable_y_prev(a.y_prev), io, nz, sm, pl, team, out);
+        flag_y_prev(a.y_prev, ctl);
+    }
     if (team.rank == 0) {
         __syncthreads();
         if (threadIdx.x == 0) {

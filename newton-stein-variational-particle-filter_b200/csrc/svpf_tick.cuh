@@ -62,7 +62,8 @@ __device__ __forceinline__ void ksd_publish(float ksd_thread, Plan& pl, const Te
 // and reports SVPF_ERR_NONFINITE with NaN outputs.  The reference runs such a
 // tick: its fminf/fmaxf clamps pin the particles to a bound and the EKF and
 // bandwidth EMAs carry the NaN, so its later ticks report finite nonsense.
-// Every member of a team sees the same y_t, so all members return together.
+// The kernels call it before the tick; every member of a team sees the same
+// y_t, so all members skip the tick together.
 __device__ __forceinline__ bool refuse_nonfinite(float y_t, svpf_ctl_t& ctl, svpf_out_t& out) {
     if (isfinite(y_t)) return false;
     if (threadIdx.x == 0) {
@@ -75,6 +76,13 @@ __device__ __forceinline__ bool refuse_nonfinite(float y_t, svpf_ctl_t& ctl, svp
         out.rejuv_fired = 0;
     }
     return true;
+}
+
+// A non-finite previous observation is read as 0 (no leverage): the kernels
+// pass the returned value to the tick and then flag the tick's status.
+__device__ __forceinline__ float readable_y_prev(float y_prev) { return isfinite(y_prev) ? y_prev : 0.0f; }
+__device__ __forceinline__ void flag_y_prev(float y_prev, svpf_ctl_t& ctl) {
+    if (threadIdx.x == 0 && !isfinite(y_prev) && ctl.status == SVPF_OK) ctl.status = SVPF_ERR_NONFINITE;
 }
 
 // The tick.  cfg/prm/ctl are shared-memory copies owned by the caller; only
@@ -91,10 +99,6 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
                          const Team& team, svpf_out_t& out) {
     const int tid = threadIdx.x;
     const int n = sm.n;
-    if (refuse_nonfinite(y_t, ctl, out)) return;
-    // a non-finite previous observation is read as 0 (no leverage) and flagged
-    const bool y_prev_bad = !isfinite(y_prev);
-    if (y_prev_bad) y_prev = 0.0f;
     if (tid == 0) {
         pl.flag = 0;
         make_plan(cfg, prm, ctl, y_t, y_prev, pl);
@@ -399,8 +403,10 @@ __device__ void run_tick(const svpf_config_t& cfg, const SVPFParams& prm, svpf_c
         }
         ctl.loglik_sum += (double)ll;
         ctl.timestep += 1;
+        // The reference's clamps (fmaxf/fminf) turn a NaN observation into finite
+        // particles; the tick runs the same way here and the status reports it.
         int status = pl.flag;
-        if (status == SVPF_OK && (y_prev_bad || !(isfinite(ll) && isfinite(vol) && isfinite(hm))))
+        if (status == SVPF_OK && !(isfinite(y_t) && isfinite(y_prev) && isfinite(ll) && isfinite(vol) && isfinite(hm)))
             status = SVPF_ERR_NONFINITE;
         ctl.status = status;
         out.loglik = ll;

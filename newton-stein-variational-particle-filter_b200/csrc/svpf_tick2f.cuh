@@ -100,9 +100,6 @@ __device__ void run_tick_2f(const svpf_config_t& cfg, const SVPFParams& prm, svp
     const int tid = threadIdx.x;
     const int n = io.n;
     const int np = sm.f[0].np;
-    if (refuse_nonfinite(y_t, ctl, out)) return;   // state untouched (svpf_tick.cuh)
-    const bool y_prev_bad = !isfinite(y_prev);          // read as 0 and flagged
-    if (y_prev_bad) y_prev = 0.0f;
     if (tid == 0) {
         pl.flag = 0;
         make_plan_2f(cfg, prm, ctl, y_t, y_prev, pl);
@@ -251,7 +248,7 @@ __device__ void run_tick_2f(const svpf_config_t& cfg, const SVPFParams& prm, svp
         ctl.loglik_sum += (double)ll;
         ctl.timestep += 1;
         int status = pl.flag;
-        if (status == SVPF_OK && (y_prev_bad || !(isfinite(ll) && isfinite(vol) && isfinite(hm))))
+        if (status == SVPF_OK && !(isfinite(y_t) && isfinite(y_prev) && isfinite(ll) && isfinite(vol) && isfinite(hm)))
             status = SVPF_ERR_NONFINITE;
         ctl.status = status;
         out.loglik = ll;
