@@ -52,7 +52,8 @@ extern "C" {
 #define SVPF_ERR_NOT_INITIALIZED   3
 #define SVPF_ERR_TAPE_SHORT        4   /* noise tape has fewer slots than the tick draws */
 #define SVPF_ERR_NONFINITE         5   /* NaN/Inf y_t: the tick is refused (the filter's state is
-                                           left exactly as it was, outputs NaN); NaN/Inf y_prev: read
+                                           left exactly as it was; loglik, vol and h_mean NaN,
+                                           steps_used 0); NaN/Inf y_prev: read
                                            as 0 and the tick runs; or NaN/Inf in the outputs */
 #define SVPF_ERR_UNSUPPORTED       6
 #define SVPF_ERR_BUDGET            7   /* request loop: the instrument's state does not fit the HBM budget */
