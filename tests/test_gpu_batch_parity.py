@@ -35,17 +35,21 @@ TILES = [(1, 4), (1, 2), (1, 1), (2, 1), (4, 1)]
 SIZES = [64, 100, 256, 300, 1024, 2048, 4096]
 
 
-def _twin(oracle_mod, batch, f, cfg, params):
+def _twin(oracle_mod, batch, f, cfg, params, precision=0):
     ctl, h, hp, v, lw = batch.get_state(f)
     o = oracle_mod.OracleFilter(h.shape[0], oracle_mod.config_from_dict(cfg.to_dict()),
-                                oracle_mod.OracleParams(*params))
-    o.ctl = oracle_mod.ctl_from_dict({k: getattr(ctl, k) for k, _ in ctl._fields_ if not k.startswith("smooth_")})
+                                oracle_mod.OracleParams(*params), precision)
+    # every field, the smoother's ring buffers and head included
+    o.ctl = oracle_mod.ctl_from_dict({k: getattr(ctl, k) for k, _ in ctl._fields_})
     o.h, o.h_prev, o.v, o.log_w = (a.astype(np.float64) for a in (h, hp, v, lw))
     return o
 
 
-def _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks, tiles=None, tape_seed=31):
-    """Tick a batch through svpf_batch_graph_launch and the oracle side by side."""
+def _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks, tiles=None, tape_seed=31, slots=None, sensitivity=False):
+    """Tick a batch through svpf_batch_graph_launch and the oracle side by side.
+    sensitivity: also step the oracle's FP32 mirror from the same state and
+    widen each filter's tolerance to four times its deviation from the FP64
+    result where that is larger (ticks that are ill-conditioned in FP32)."""
     import torch
 
     F = len(ns)
@@ -57,7 +61,8 @@ def _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks, tiles=None, tape_seed=31)
         for f, (R, S) in enumerate(tiles):
             b.set_tile(f, R, S)
     used = [b.tile_of_filter(f) for f in range(F)]
-    slots = 2 + max(c.stein_max_steps for c in cfgs) + 7
+    if slots is None:
+        slots = 2 + max(c.stein_max_steps for c in cfgs) + 7
     nrm, uni = tape.tape(tape_seed + 1, 0, n_max, slots, 2)
     b.set_noise_tape(nrm, uni)   # one tape for every tick: the graph is captured once, then replayed
     d_yt = torch.empty(F, dtype=torch.float32, device="cuda")
@@ -67,6 +72,7 @@ def _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks, tiles=None, tape_seed=31)
     pool = cf.ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1))
     for t in range(ticks):
         twins = [_twin(oracle_mod, b, f, cfgs[f], params[f]) for f in range(F)]
+        twins32 = [_twin(oracle_mod, b, f, cfgs[f], params[f], 1) for f in range(F)] if sensitivity else None
         yp = ys[t - 1] if t > 0 else np.zeros(F, np.float32)
         d_yt.copy_(torch.from_numpy(np.ascontiguousarray(ys[t])))
         d_yp.copy_(torch.from_numpy(np.ascontiguousarray(yp)))
@@ -78,6 +84,8 @@ def _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks, tiles=None, tape_seed=31)
         rejuv = out.view(np.int32)[:, 7]
         # the oracle's ticks run in threads: each is a ctypes call, which releases the GIL
         oo = list(pool.map(lambda f: twins[f].step(ys[t, f], yp[f], nrm[:, :ns[f]], uni[:, :ns[f]]), range(F)))
+        oo32 = list(pool.map(lambda f: twins32[f].step(ys[t, f], yp[f], nrm[:, :ns[f]], uni[:, :ns[f]]),
+                             range(F))) if sensitivity else None
         ctl = b.ctl()
         for f in range(F):
             tag = (t, f, ns[f], used[f])
@@ -85,11 +93,19 @@ def _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks, tiles=None, tape_seed=31)
             assert steps[f] == oo[f].steps_used, tag
             assert rejuv[f] == oo[f].rejuv_fired, tag
             h = b.get_particles(f)
-            assert rel_err(h, twins[f].h) < TOL, (tag, rel_err(h, twins[f].h))
+
+            def tol(base, dev):
+                return max(base, 4 * dev) if sensitivity else base
+
+            th = tol(TOL, rel_err(twins32[f].h, twins[f].h) if sensitivity else 0.0)
+            assert rel_err(h, twins[f].h) < th, (tag, rel_err(h, twins[f].h), th)
             for col, name in ((0, "loglik"), (1, "vol"), (2, "h_mean")):
                 want = getattr(oo[f], name)
-                assert abs(out[f, col] - want) < TOL * max(1.0, abs(want)), (tag, name, out[f, col], want)
-            assert abs(out[f, 5] - oo[f].ksd) < 1e-3 * max(1.0, abs(oo[f].ksd)), (tag, out[f, 5], oo[f].ksd)
+                dev = abs(getattr(oo32[f], name) - want) / max(1.0, abs(want)) if sensitivity else 0.0
+                assert abs(out[f, col] - want) < tol(TOL, dev) * max(1.0, abs(want)), (tag, name, out[f, col], want)
+            want = oo[f].ksd
+            dev = abs(oo32[f].ksd - want) / max(1.0, abs(want)) if sensitivity else 0.0
+            assert abs(out[f, 5] - want) < tol(1e-3, dev) * max(1.0, abs(want)), (tag, out[f, 5], want)
     pool.shutdown()
     # one captured launch per tick, replayed: no more kernels than ticks
     assert b.kernel_launches - launches0 == ticks

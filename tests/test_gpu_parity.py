@@ -114,8 +114,7 @@ def oracle_twin(oracle_mod, pkg, f, params):
     o = oracle_mod.OracleFilter(f.n_particles, oracle_mod.config_from_dict(f.config.to_dict()),
                                 oracle_mod.OracleParams(*params))
     ctl, h, hp, v, lw = f.get_state()
-    d = {k: getattr(ctl, k) for k, _ in ctl._fields_ if not k.startswith("smooth_")}
-    o.ctl = oracle_mod.ctl_from_dict(d)
+    o.ctl = oracle_mod.ctl_from_dict({k: getattr(ctl, k) for k, _ in ctl._fields_})   # smoother included
     o.h, o.h_prev, o.v, o.log_w = (a.astype(np.float64) for a in (h, hp, v, lw))
     return o
 

@@ -1,0 +1,132 @@
+"""Randomised configurations against the FP64 oracle.
+
+The fixture families pin the reference's knob sets one family at a time.
+Here every filter of one batch draws its own combination of the knobs a
+caller may set (predict: MIM, asymmetric rho, guided predict, local
+parameters, Student-t state noise; guide: preserving or blending, adaptive
+strength; Stein loop: vanilla / Newton / full Newton, repulsion sign, fixed
+or adaptive beta, annealing stages, SVLD, Heun, exact or approximate
+likelihood score, budget bounds; rejuvenation; adaptive mu and sigma; the
+smoother; Fan mode) and its own particle count, including ragged ones.  The
+batch is ticked through svpf_batch_graph_launch with a noise tape for 12
+ticks (across t = 10, where the KSD-driven budget and rejuvenation switch
+on), each tick compared with the oracle from the engine's re-synced state
+(tolerances as in test_gpu_batch_parity: 1e-4 relative, KSD 1e-3, Stein
+steps and rejuvenation decisions exact; where a tick is ill-conditioned in
+FP32 -- the first tick after initialisation starts from zero RMSProp moments,
+and without SVLD noise some knob sets amplify rounding there -- four times
+the oracle's own FP32 mirror's deviation from its FP64 result on the same
+state and tape).  Seeded, so a failure reproduces.
+"""
+import numpy as np
+import pytest
+
+from test_gpu_batch_parity import _run
+
+pytestmark = pytest.mark.gpu
+
+
+def _random_config(pkg, rng, p_fan=0.1):
+    n_stein = int(rng.integers(3, 9))
+    nu = float(rng.uniform(4.0, 30.0))
+    c = pkg.default_config(n_stein, nu)
+    b = lambda p=0.5: int(rng.random() < p)   # noqa: E731
+    newton = b(0.7)
+    hi = int(rng.integers(3, 9))
+    kw = dict(
+        use_svld=b(0.7), temperature=float(rng.uniform(0.2, 0.6)),
+        use_annealing=b(0.8), n_anneal_steps=int(rng.integers(1, 5)), use_adaptive_beta=b(),
+        use_mim=b(0.6), mim_jump_prob=float(rng.uniform(0.05, 0.3)), mim_jump_scale=float(rng.uniform(2.0, 9.0)),
+        use_asymmetric_rho=b(), use_local_params=b(0.3), delta_rho=float(rng.uniform(0.0, 0.02)),
+        delta_sigma=float(rng.uniform(0.0, 0.1)),
+        use_guided=b(0.4), use_guide=b(0.7), use_guide_preserving=b(), use_adaptive_guide=b(0.3),
+        use_newton=newton, use_full_newton=int(newton and rng.random() < 0.6),
+        stein_repulsive_sign=b(), use_exact_gradient=b(),
+        use_rejuvenation=b(0.6), rejuv_ksd_threshold=float(rng.uniform(0.02, 0.2)),
+        use_adaptive_mu=b(0.3), use_adaptive_sigma=b(0.3),
+        use_student_t_state=b(0.2), nu_state=float(rng.uniform(4.0, 9.0)),
+        use_heun=b(0.2), use_smoothing=b(0.3), smooth_lag=int(rng.integers(2, 7)),
+        smooth_output_lag=int(rng.integers(0, 2)), use_fan_mode=b(p_fan),
+        stein_min_steps=int(rng.integers(1, hi + 1)), stein_max_steps=hi,
+    )
+    c.update(**kw)
+    return c
+
+
+SMALL = [1, 2, 33, 64, 100, 257, 512]
+LARGE = [256, 700, 1024, 2048]
+
+
+@pytest.mark.parametrize("seed,sizes,p_fan", [(20261204, SMALL, 0.1), (7, SMALL, 0.1), (99, SMALL, 0.1),
+                                              (5, SMALL, 0.4), (13, LARGE, 0.1), (21, LARGE, 0.4)])
+def test_random_configurations_match_oracle(pkg, oracle_mod, seed, sizes, p_fan):
+    rng = np.random.default_rng(seed)
+    F = 24
+    ns = [int(x) for x in rng.choice(sizes, size=F)]
+    cfgs = [_random_config(pkg, rng, p_fan) for _ in range(F)]
+    params = [(float(rng.uniform(0.9, 0.99)), float(rng.uniform(0.08, 0.3)), float(rng.uniform(-2.0, -0.5)),
+               float(rng.choice([0.0, -0.3]))) for _ in range(F)]
+    T = 12
+    h = np.array([p[2] for p in params], np.float32)
+    ys = (np.exp(0.5 * h)[None, :] * rng.standard_normal((T, F))).astype(np.float32)
+    # noise slots: predict (1 + Student-t state draws), one per Stein iteration
+    # (and one per Heun corrector), rejuvenation, with margin
+    nu_state = max((c.nu_state for c in cfgs if c.use_student_t_state), default=0.0)
+    slots = 4 + int(nu_state + 1.5) + 2 * max(c.stein_max_steps for c in cfgs)
+    _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks=T, slots=slots, sensitivity=True)
+
+
+@pytest.mark.parametrize("seed", [3, 11, 42])
+def test_random_configurations_single_filter_match_oracle(pkg, oracle_mod, seed):
+    """The same random knob sets through svpf_step_graph: the single-filter
+    cluster kernels (the latency kernels, with their own tiles, the min-pass
+    row maximum at N <= 1024 and the kernel compiled for the production
+    configuration alone), cluster sizes from the engine's choice or forced,
+    12 ticks each against the oracle from the engine's re-synced state.
+    Where a tick is ill-conditioned in FP32 (the first tick after
+    initialisation starts from zero RMSProp moments; without SVLD noise a
+    few knob sets amplify rounding there), the tolerance is widened to four
+    times the oracle's own FP32 mirror's deviation from its FP64 result on
+    the same state and tape, as the size sweeps do."""
+    import tape
+    from test_gpu_parity import oracle_twin
+    from test_oracle import TOL, rel_err
+
+    rng = np.random.default_rng(seed)
+    for k in range(6):
+        cfg = _random_config(pkg, rng)
+        n = int(rng.choice([1, 2, 33, 100, 257, 512, 1000]))
+        clusters = [0] + [c for c in (1, 2, 4, 8, 16) if 32 * c <= n]
+        cluster = int(rng.choice(clusters))
+        params = (float(rng.uniform(0.9, 0.99)), float(rng.uniform(0.08, 0.3)), float(rng.uniform(-2.0, -0.5)),
+                  float(rng.choice([0.0, -0.3])))
+        slots = 4 + int(cfg.nu_state + 1.5) * cfg.use_student_t_state + 2 * cfg.stein_max_steps
+        f = pkg.SVPF(n, cfg.n_stein_steps, cfg.nu)
+        f.configure(**cfg.to_dict())
+        if cluster:
+            f.set_cluster_size(cluster)
+        f.initialize(*params, seed=seed + k)
+        yp = 0.0
+        for t in range(12):
+            y = float(np.exp(0.5 * params[2]) * rng.standard_normal())
+            o = oracle_twin(oracle_mod, pkg, f, params)
+            o32 = oracle_mod.OracleFilter(n, o.cfg, oracle_mod.OracleParams(*params), 1)   # FP32 mirror
+            o32.ctl = oracle_mod.OracleCtl.from_buffer_copy(o.ctl)
+            o32.h, o32.h_prev, o32.v, o32.log_w = o.h.copy(), o.h_prev.copy(), o.v.copy(), o.log_w.copy()
+            nrm, uni = tape.tape(1000 * seed + k, t, n, slots, 2)
+            f.set_noise_tape(nrm, uni)
+            rc, out = f.step_raw(y, yp)
+            oo = o.step(y, yp, nrm, uni)
+            o32o = o32.step(y, yp, nrm, uni)
+            tag = (k, t, n, cluster)
+            assert rc == 0, tag
+            assert out.steps_used == oo.steps_used and out.rejuv_fired == oo.rejuv_fired, tag
+            tol = max(TOL, 4 * rel_err(o32.h, o.h))
+            assert rel_err(f.get_particles(), o.h) < tol, (tag, rel_err(f.get_particles(), o.h), tol)
+            for name in ("loglik", "vol", "h_mean"):
+                a, b, c = getattr(out, name), getattr(oo, name), getattr(o32o, name)
+                tol = max(TOL, 4 * abs(c - b) / max(1.0, abs(b)))
+                assert abs(a - b) < tol * max(1.0, abs(b)), (tag, name, a, b, tol)
+            assert abs(out.ksd - oo.ksd) < 1e-3 * max(1.0, abs(oo.ksd)), (tag, out.ksd, oo.ksd)
+            yp = y
+        f.close()
