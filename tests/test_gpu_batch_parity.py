@@ -37,7 +37,8 @@ SIZES = [64, 100, 256, 300, 1024, 2048, 4096]
 
 def _twin(oracle_mod, batch, f, cfg, params, precision=0):
     ctl, h, hp, v, lw = batch.get_state(f)
-    o = oracle_mod.OracleFilter(h.shape[0], oracle_mod.config_from_dict(cfg.to_dict()),
+    # particle count: the log-weights hold n values (h, h_prev, v hold 2n for two factors)
+    o = oracle_mod.OracleFilter(lw.shape[0], oracle_mod.config_from_dict(cfg.to_dict()),
                                 oracle_mod.OracleParams(*params), precision)
     # every field, the smoother's ring buffers and head included
     o.ctl = oracle_mod.ctl_from_dict({k: getattr(ctl, k) for k, _ in ctl._fields_})
@@ -47,15 +48,19 @@ def _twin(oracle_mod, batch, f, cfg, params, precision=0):
 
 def _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks, tiles=None, tape_seed=31, slots=None, sensitivity=False):
     """Tick a batch through svpf_batch_graph_launch and the oracle side by side.
-    sensitivity: also step the oracle's FP32 mirror from the same state and
-    widen each filter's tolerance to four times its deviation from the FP64
-    result where that is larger (ticks that are ill-conditioned in FP32)."""
+    sensitivity: also step the oracle's FP32 mirror from the same state, and
+    from that state with the positions moved by about two FP32 ulps either way (three
+    rounding paths), and widen each filter's tolerance to four times the
+    largest deviation from the FP64 result where that is larger (ticks that
+    are ill-conditioned in FP32)."""
     import torch
 
     F = len(ns)
     n_max = max(ns)
     b = pkg.Batch(ns, cfgs, [pkg.Params(*p) for p in params])
-    b.set_noise_tape(tape.init_normals(tape_seed, n_max)[None, :], np.ones((1, n_max), np.float32))
+    two_factor = any(c.use_two_factor for c in cfgs)   # a two-factor initialisation draws 3 slots
+    init = tape.init_normals(tape_seed, n_max, 3 if two_factor else 1)
+    b.set_noise_tape(init if two_factor else init[None, :], np.ones((1, n_max), np.float32))
     b.initialize(seed=1)
     if tiles is not None:
         for f, (R, S) in enumerate(tiles):
@@ -72,7 +77,13 @@ def _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks, tiles=None, tape_seed=31,
     pool = cf.ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1))
     for t in range(ticks):
         twins = [_twin(oracle_mod, b, f, cfgs[f], params[f]) for f in range(F)]
-        twins32 = [_twin(oracle_mod, b, f, cfgs[f], params[f], 1) for f in range(F)] if sensitivity else None
+        mirrors = []
+        if sensitivity:
+            for nudge in (0.0, 2.0 ** -22, -(2.0 ** -22)):
+                m = [_twin(oracle_mod, b, f, cfgs[f], params[f], 1) for f in range(F)]
+                for o in m:
+                    o.h = o.h * (1.0 + nudge)
+                mirrors.append(m)
         yp = ys[t - 1] if t > 0 else np.zeros(F, np.float32)
         d_yt.copy_(torch.from_numpy(np.ascontiguousarray(ys[t])))
         d_yp.copy_(torch.from_numpy(np.ascontiguousarray(yp)))
@@ -84,8 +95,8 @@ def _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks, tiles=None, tape_seed=31,
         rejuv = out.view(np.int32)[:, 7]
         # the oracle's ticks run in threads: each is a ctypes call, which releases the GIL
         oo = list(pool.map(lambda f: twins[f].step(ys[t, f], yp[f], nrm[:, :ns[f]], uni[:, :ns[f]]), range(F)))
-        oo32 = list(pool.map(lambda f: twins32[f].step(ys[t, f], yp[f], nrm[:, :ns[f]], uni[:, :ns[f]]),
-                             range(F))) if sensitivity else None
+        outs32 = [list(pool.map(lambda f: m[f].step(ys[t, f], yp[f], nrm[:, :ns[f]], uni[:, :ns[f]]), range(F)))
+                  for m in mirrors]
         ctl = b.ctl()
         for f in range(F):
             tag = (t, f, ns[f], used[f])
@@ -97,18 +108,23 @@ def _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks, tiles=None, tape_seed=31,
             def tol(base, dev):
                 return max(base, 4 * dev) if sensitivity else base
 
-            th = tol(TOL, rel_err(twins32[f].h, twins[f].h) if sensitivity else 0.0)
+            def dev(name):   # largest deviation of the FP32 mirrors from the FP64 result
+                want = getattr(oo[f], name)
+                return max((abs(getattr(o[f], name) - want) / max(1.0, abs(want)) for o in outs32), default=0.0)
+
+            th = tol(TOL, max((rel_err(m[f].h, twins[f].h) for m in mirrors), default=0.0))
             assert rel_err(h, twins[f].h) < th, (tag, rel_err(h, twins[f].h), th)
             for col, name in ((0, "loglik"), (1, "vol"), (2, "h_mean")):
                 want = getattr(oo[f], name)
-                dev = abs(getattr(oo32[f], name) - want) / max(1.0, abs(want)) if sensitivity else 0.0
-                assert abs(out[f, col] - want) < tol(TOL, dev) * max(1.0, abs(want)), (tag, name, out[f, col], want)
+                assert abs(out[f, col] - want) < tol(TOL, dev(name)) * max(1.0, abs(want)), (tag, name, out[f, col],
+                                                                                              want)
             want = oo[f].ksd
-            dev = abs(oo32[f].ksd - want) / max(1.0, abs(want)) if sensitivity else 0.0
-            assert abs(out[f, 5] - want) < tol(1e-3, dev) * max(1.0, abs(want)), (tag, out[f, 5], want)
+            assert abs(out[f, 5] - want) < tol(1e-3, dev("ksd")) * max(1.0, abs(want)), (tag, out[f, 5], want)
     pool.shutdown()
-    # one captured launch per tick, replayed: no more kernels than ticks
-    assert b.kernel_launches - launches0 == ticks
+    # one captured graph per tick, replayed: one persistent launch per tick for
+    # each kind of filter in the batch (single-factor, two-factor)
+    kinds = int(any(not c.use_two_factor for c in cfgs)) + int(any(c.use_two_factor for c in cfgs))
+    assert b.kernel_launches - launches0 == kinds * ticks
     b.close()
     return used
 

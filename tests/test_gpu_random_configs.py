@@ -130,3 +130,40 @@ def test_random_configurations_single_filter_match_oracle(pkg, oracle_mod, seed)
             assert abs(out.ksd - oo.ksd) < 1e-3 * max(1.0, abs(oo.ksd)), (tag, out.ksd, oo.ksd)
             yp = y
         f.close()
+
+
+def _random_config_2f(pkg, rng):
+    n_stein = int(rng.integers(2, 9))
+    c = pkg.default_config(n_stein, float(rng.uniform(4.0, 30.0)))
+    b = lambda p=0.5: int(rng.random() < p)   # noqa: E731
+    c.update(use_two_factor=1, rho_fast=float(rng.uniform(0.7, 0.95)), sigma_fast=float(rng.uniform(0.1, 0.35)),
+             rho_slow=float(rng.uniform(0.98, 0.998)), sigma_slow=float(rng.uniform(0.03, 0.08)),
+             bw_floor_fast=0.01, bw_floor_slow=0.05, use_svld=b(0.7), temperature=float(rng.uniform(0.2, 0.6)),
+             use_annealing=b(0.8), n_anneal_steps=int(rng.integers(1, 5)), use_mim=b(0.6),
+             mim_jump_prob=float(rng.uniform(0.05, 0.3)), mim_jump_scale=float(rng.uniform(2.0, 9.0)),
+             use_guide=b(0.7), use_guide_preserving=b(), guide_strength=float(rng.uniform(0.05, 0.3)),
+             use_exact_gradient=b(), lik_offset=float(rng.uniform(0.2, 0.4)), stein_repulsive_sign=b())
+    return c
+
+
+@pytest.mark.parametrize("seed", [31, 57])
+def test_random_two_factor_configurations_match_oracle(pkg, oracle_mod, seed):
+    """Two-factor filters (h = mu + h_fast + h_slow) with random factor
+    dynamics, annealing, SVLD, MIM, guide and score knobs, mixed with
+    single-factor filters in one batch (two persistent launches per tick),
+    12 graph-replayed ticks against the oracle, as above."""
+    rng = np.random.default_rng(seed)
+    F = 24
+    ns = [int(x) for x in rng.choice(SMALL, size=F)]
+    cfgs = [_random_config_2f(pkg, rng) if f % 3 else _random_config(pkg, rng) for f in range(F)]
+    params = [(float(rng.uniform(0.9, 0.99)), float(rng.uniform(0.08, 0.3)), float(rng.uniform(-4.0, -2.0)),
+               0.0) for _ in range(F)]
+    T = 12
+    h = np.array([p[2] for p in params], np.float32)
+    ys = (np.exp(0.5 * h)[None, :] * rng.standard_normal((T, F))).astype(np.float32)
+    nu_state = max((c.nu_state for c in cfgs if c.use_student_t_state and not c.use_two_factor), default=0.0)
+    steps_2f = max((c.n_stein_steps * (c.n_anneal_steps if c.use_annealing else 1) for c in cfgs
+                    if c.use_two_factor), default=0)
+    steps_1f = max((c.stein_max_steps for c in cfgs if not c.use_two_factor), default=0)
+    slots = 4 + max(int(nu_state + 1.5) + 2 * steps_1f, 2 * steps_2f)
+    _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks=T, slots=slots, sensitivity=True)
