@@ -167,3 +167,68 @@ def test_random_two_factor_configurations_match_oracle(pkg, oracle_mod, seed):
     steps_1f = max((c.stein_max_steps for c in cfgs if not c.use_two_factor), default=0)
     slots = 4 + max(int(nu_state + 1.5) + 2 * steps_1f, 2 * steps_2f)
     _run(pkg, oracle_mod, ns, cfgs, params, ys, ticks=T, slots=slots, sensitivity=True)
+
+
+def _random_v2(rng):
+    import cases
+    b = lambda p=0.5: int(rng.random() < p)   # noqa: E731
+    mu, rho, sz = float(rng.uniform(-4.5, -0.5)), float(rng.uniform(0.9, 0.99)), float(rng.uniform(0.08, 0.3))
+    newton = b(0.7)
+    p = dict(cases.V2_REFERENCE_TEST, mu=mu, rho=rho, sigma_z=sz, nu=float(rng.uniform(4.0, 30.0)),
+             gamma=float(rng.choice([0.0, -0.3])), delta_rho=float(rng.uniform(0.0, 0.02)) * b(0.3),
+             delta_sigma=float(rng.uniform(0.0, 0.1)) * b(0.3), mim_jump_prob=float(rng.uniform(0.0, 0.3)),
+             mim_jump_scale=float(rng.uniform(2.0, 9.0)), use_guide=b(0.7), use_guided_predict=b(0.5),
+             use_guide_preserving=b(), use_newton=newton, use_full_newton=int(rng.random() < 0.5),
+             use_rejuvenation=b(0.6), rejuv_ksd_threshold=float(rng.uniform(0.0, 0.1)),
+             use_adaptive_mu=b(0.3), mu_ema_alpha=float(rng.uniform(0.01, 0.1)), use_adaptive_sigma=b(0.5),
+             step_size=float(rng.uniform(0.05, 0.3)), temperature=float(rng.uniform(0.2, 1.0)) * b(0.7),
+             n_stein_steps=int(rng.integers(1, 9)), n_anneal_steps=int(rng.integers(1, 5)),
+             stein_sign_mode=b())
+    return p, (mu, rho, sz)
+
+
+@pytest.mark.parametrize("seed", [2, 17])
+def test_random_v2_configurations_match_oracle(pkg, oracle_mod, seed):
+    """svpf_fully_fused_step_v2 (the reference's second entry point) with
+    random knobs and sizes, 4 ticks each from the engine's re-synced state
+    against the oracle's restatement of its kernel; the tolerance is widened
+    to four times the oracle's own sensitivity where that is larger (its FP32
+    mirror, and its response to a 1e-7 relative change of the positions), as
+    the v2 size sweep does."""
+    import tape
+    from test_gpu_v2 import check_against, load_state
+    from test_oracle import TOL, rel_err
+    from test_oracle_v2 import v2_params
+
+    rng = np.random.default_rng(seed)
+    for k in range(6):
+        praw, (mu, rho, sz) = _random_v2(rng)
+        n = int(rng.choice([1, 31, 100, 257, 512, 1000]))
+        p = v2_params(oracle_mod, praw)
+        params = p.to_dict()
+        slots = 4 + max(praw["n_stein_steps"], 1) + 1
+        st = oracle_mod.V2State(n)
+        st.h[:] = np.clip(mu + sz / np.sqrt(1 - rho * rho) * tape.init_normals(5 + k, n), -15, 5).astype(np.float32)
+        st.mu_state[0] = mu
+        _, ys = tape.sv_path(5, mu, rho, sz, seed=100 * seed + k)
+        f = pkg.FusedV2(n)
+        yp, hmp, volp, ksdp = 0.0, mu, float(np.exp(mu / 2)), 0.1
+        for t in range(4):
+            load_state(f, oracle_mod, st)
+            nrm, uni = tape.tape(1000 * seed + k, t, n, slots, 2)
+            f.set_tape(nrm, uni)
+            assert f.step(params, ys[t], yp, hmp, volp, ksdp, 12 + t) == 0, (k, t)
+            s32, spert = st.copy(), st.copy()
+            spert.h = spert.h * (1 + 1e-7 * np.random.default_rng(t).standard_normal(n))
+            out = oracle_mod.v2_tick(p, st, ys[t], yp, hmp, volp, ksdp, 12 + t, nrm, uni)
+            oracle_mod.v2_tick(p, s32, ys[t], yp, hmp, volp, ksdp, 12 + t, nrm, uni, precision=1)
+            oracle_mod.v2_tick(p, spert, ys[t], yp, hmp, volp, ksdp, 12 + t, nrm, uni)
+            sens = max(rel_err(s32.h, st.h), rel_err(spert.h, st.h), rel_err(s32.lw, st.lw), rel_err(spert.lw, st.lw))
+            check_against(f, oracle_mod, st, out, tol=max(TOL, 4 * sens))
+            st = oracle_mod.V2State(n)
+            for a in oracle_mod.V2State.ARRAYS:
+                setattr(st, a, f.get(a).astype(np.float64))
+            st.guide_mean[0], st.guide_var[0] = f.get("guide_mean"), f.get("guide_var")
+            st.mu_state[0] = f.get("mu_state")
+            yp, hmp, volp, ksdp = float(ys[t]), out.h_mean, out.vol, out.ksd
+        f.close()
