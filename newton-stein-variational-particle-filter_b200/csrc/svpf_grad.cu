@@ -289,6 +289,20 @@ __device__ __forceinline__ float flip_sign(float v, float s) {
     return __int_as_float(__float_as_int(v) ^ (__float_as_int(s) & 0x80000000));
 }
 
+// The pair loops form u = x_j (-1/bw) + x_i/bw in one FMA: the column's
+// product is exact, the row's x_i/bw was rounded once, so a row's own column
+// (j = i) enters with u = that rounding error instead of 0.  Its terms that
+// are odd in u (u K^2 and what it weights) are then spurious: with one
+// particle at the bandwidth floor (1/bw = 100) the repulsion picks up
+// 2 u / bw ~ 1e-3.  self_uk2 gives the loop's own value of u K^2 for j = i
+// (and K, for the Hessian term), so the row sums can take it back out.
+__device__ __forceinline__ float2 self_uk2(float2 xr, float2 xi2, float ib, float2& K) {
+    const float2 u = fma2(xr, f2(-ib), xi2);
+    const float2 b = fma2(u, u, f2(1.0f));
+    K = make_float2(rcp_approx(b.x), rcp_approx(b.y));
+    return mul2(u, mul2(K, K));
+}
+
 // Transport adjoint row sums (the row and column terms of one Stein
 // iteration, see the header), with K^2 |3u^2-1| = K |3-4K| and
 // uK^2 (6 sgn - 4 K |3u^2-1|) = sgn(3-4K) uK^2 (16K - 6).  Accumulators:
@@ -637,6 +651,12 @@ __device__ float fwd_tick(const svpf_config_t& c, int n, int np, float* x, float
                 if (last) transport_rows<false, true>(x, g, curv, nk4, xi2, ib, kg, gk, ks, kc, nk, gdk, ht);
                 else transport_rows<false, false>(x, g, curv, nk4, xi2, ib, kg, gk, ks, kc, nk, gdk, ht);
             }
+            {   // the row's own column: u = 0 exactly (self_uk2)
+                float2 Ks;
+                const float2 s1 = self_uk2(make_float2(x[i0], x[i1]), xi2, ib, Ks);
+                gk = fma2(s1, f2(-1.0f), gk);
+                if (last) gdk = fma2(make_float2(-g[i0], -g[i1]), s1, gdk);
+            }
 #pragma unroll
             for (int r = 0; r < 2; ++r) {
                 if (r == 1 && !two) break;
@@ -824,6 +844,25 @@ __device__ void bwd_tick(const svpf_config_t& c, int n, int np, float* xb, float
             const float2 xi2 = make_float2(xs[i0] * ib, xs[i1] * ib);
             if (full) adjoint_rows<true>(xs, g, a, cv, hwb, knb, nk4, xi2, ib, acc);
             else adjoint_rows<false>(xs, g, a, cv, hwb, knb, nk4, xi2, ib, acc);
+            {   // the row's own column: u = 0 exactly (self_uk2); its terms odd in u leave the sums
+                float2 Ks;
+                const float2 s1 = self_uk2(make_float2(xs[i0], xs[i1]), xi2, ib, Ks);
+                const float2 ns1 = make_float2(-s1.x, -s1.y);
+                acc[0] = fma2(make_float2(g[i0], g[i1]), ns1, acc[0]);
+                acc[2] = fma2(make_float2(a[i0], a[i1]), ns1, acc[2]);
+                acc[5] = add2(acc[5], ns1);
+                if (full) {
+                    const float2 t = fma2(Ks, f2(-4.0f), f2(3.0f));
+                    const float2 f6u = mul2(s1, fma2(Ks, f2(16.0f), f2(-6.0f)));
+                    const float2 nf6 = make_float2(-flip_sign(f6u.x, t.x), -flip_sign(f6u.y, t.y));
+                    const float2 hb2 = make_float2(hwb[i0], hwb[i1]);
+                    acc[6] = fma2(make_float2(cv[i0], cv[i1]), ns1, acc[6]);
+                    acc[7] = add2(acc[7], nf6);
+                    acc[8] = fma2(hb2, ns1, acc[8]);
+                    acc[9] = fma2(hb2, nf6, acc[9]);
+                    acc[10] = fma2(make_float2(knb[i0], knb[i1]), ns1, acc[10]);
+                }
+            }
 #pragma unroll
             for (int r = 0; r < 2; ++r) {
                 if (r == 1 && !two) break;

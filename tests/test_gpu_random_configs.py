@@ -232,3 +232,39 @@ def test_random_v2_configurations_match_oracle(pkg, oracle_mod, seed):
             st.mu_state[0] = f.get("mu_state")
             yp, hmp, volp, ksdp = float(ys[t]), out.h_mean, out.vol, out.ksd
         f.close()
+
+
+def _random_grad_config(pkg, rng):
+    """A random member of the differentiable configuration set."""
+    b = lambda p=0.5: int(rng.random() < p)   # noqa: E731
+    n_stein = int(rng.integers(1, 9))
+    c = pkg.grad_config(n_stein, 12.0, full_newton=bool(b(0.6)))
+    c.update(use_mim=b(0.6), mim_jump_prob=float(rng.uniform(0.05, 0.3)), mim_jump_scale=float(rng.uniform(2.0, 9.0)),
+             use_guide=b(0.7), use_guide_preserving=b(), guide_strength=float(rng.uniform(0.02, 0.3)),
+             use_exact_gradient=b(), lik_offset=float(rng.uniform(0.2, 0.4)), use_svld=b(0.7),
+             temperature=float(rng.uniform(0.2, 0.6)), use_annealing=b(0.8), n_anneal_steps=int(rng.integers(1, 5)),
+             stein_repulsive_sign=b())
+    return c
+
+
+@pytest.mark.parametrize("seed", [4, 9])
+def test_random_differentiable_configurations_match_oracle(pkg, oracle_mod, seed):
+    """The adjoint engine on random members of its differentiable set (predict
+    with or without MIM, guide preserving or blending, exact or approximate
+    score, vanilla or full-Newton transport, SVLD, annealing stages, budget,
+    repulsion sign), both objectives, with or without truncation, random
+    checkpoint intervals: per-tick log-likelihoods and gradients against the
+    FP64 forward-mode oracle, tolerances as in test_gpu_grad."""
+    from test_gpu_grad import check_against_oracle
+
+    rng = np.random.default_rng(seed)
+    for _ in range(3):
+        cfg = _random_grad_config(pkg, rng)
+        assert pkg.lib().svpf_grad_supported(cfg)
+        # a single particle sits at the bandwidth floor (1/bw = 100), where the
+        # adjoint's 1/bw^2 terms cancel in FP32 to ~3e-4 of the gradient: N = 1
+        # is checked by test_gpu_grad's size sweep on its own configuration
+        ns = [int(x) for x in rng.choice([2, 33, 100, 257], size=3)]
+        T = int(rng.integers(6, 13))
+        check_against_oracle(pkg, oracle_mod, cfg, ns, T=T, k=int(rng.integers(1, 9)), seed=int(rng.integers(1, 99)),
+                             objective=int(rng.integers(0, 2)), trunc=int(rng.choice([0, 0, 4])))
