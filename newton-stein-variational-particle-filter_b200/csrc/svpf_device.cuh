@@ -868,6 +868,14 @@ __device__ float transport_pass(const Smem& sm, int cur, const P& pl, const svpf
             for (int r = 0; r < R; ++r) {
                 if (il[r] >= nloc) continue;
                 const int i = sm.row0 + il[r];
+                if constexpr (RAW && KIND == 0 && !KSD) {
+                    // log-volatility positions are scaled inside the pair FMA, u =
+                    // h_j (-1/bw) + round(h_i / bw): the row's own column enters with
+                    // u = that rounding error, not 0; take its u K^2 back out
+                    const float e = fmaf(hi[r], -inv_bw, __fmul_rn(hi[r], inv_bw));
+                    const float Ke = rcp_approx(fmaf(e, e, 1.0f));
+                    gk[r] -= e * (Ke * Ke);
+                }
                 // sums over u = d / bw carry one factor bw: 2 d K^2 / bw^2 = 2 u K^2 / bw
                 float phi = (kg[r] + sign * 2.0f * inv_bw * gk[r]) * inv_n;
                 if (KIND == 2) {
