@@ -268,3 +268,41 @@ def test_random_differentiable_configurations_match_oracle(pkg, oracle_mod, seed
         T = int(rng.integers(6, 13))
         check_against_oracle(pkg, oracle_mod, cfg, ns, T=T, k=int(rng.integers(1, 9)), seed=int(rng.integers(1, 99)),
                              objective=int(rng.integers(0, 2)), trunc=int(rng.choice([0, 0, 4])))
+
+
+@pytest.mark.parametrize("seed", [6, 23])
+def test_random_estimator_configurations_match_oracle(pkg, seed):
+    """The reference's torch estimator model as its CUDA engine, with random
+    particle counts, Stein steps and step sizes, truncation and checkpoint
+    intervals, tick weights and theta, against the FP64 oracle restatement
+    (tolerances as in test_gpu_estimator)."""
+    import oracle
+    from test_gpu_estimator import G_TOL, LL_TOL, _random_case, sensitivity
+
+    rng = np.random.default_rng(seed)
+    for _ in range(3):
+        n = int(rng.choice([2, 8, 64, 130, 512]))
+        S = int(rng.integers(0, 5))
+        lr = float(rng.uniform(0.05, 0.3))
+        T = int(rng.integers(8, 25))
+        trunc = int(rng.choice([0, 0, 3, 7]))
+        k = int(rng.integers(1, 9))
+        F = 3
+        thetas = np.stack([rng.uniform(-4, -2, F), rng.uniform(0.85, 0.98, F), rng.uniform(0.1, 0.3, F),
+                           rng.uniform(5, 20, F)], 1)
+        cases = [_random_case(n, T, int(rng.integers(1, 1 << 30))) for _ in range(F)]
+        w = rng.uniform(-1, 1, (F, T))
+        e = pkg.Estimator(F, n, S, lr, T_max=T, checkpoint_every=k, truncate_every=trunc)
+        tape = np.stack([pkg.Estimator.make_tape(c[1], c[2]) for c in cases])
+        ll, vol, _ = e.forward(thetas, np.stack([c[0] for c in cases]), tape=tape)
+        g = e.backward(w.astype(np.float32))
+        e.close()
+        for f in range(F):
+            ys, ti, tt = cases[f]
+            oll, ovol, og = oracle.estimator_run(n, S, lr, thetas[f], ys, ti, tt, trunc, w[f])
+            sl, sv, sg = sensitivity(n, S, lr, thetas[f], ys, ti, tt, trunc, w[f])
+            tag = (n, S, lr, T, trunc, k, f)
+            assert np.max(np.abs(ll[f] - oll) / np.maximum(1.0, np.abs(oll))) < max(LL_TOL, 4 * sl), tag
+            assert np.max(np.abs(vol[f] - ovol) / ovol) < max(LL_TOL, 4 * sv), tag
+            err = np.abs(g[f] - og) / np.maximum(np.abs(og), 1e-3)
+            assert np.all(err < max(G_TOL, 4 * sg)), (tag, g[f], og, err, sg)
