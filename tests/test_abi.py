@@ -65,6 +65,22 @@ def test_ctypes_layouts_match_c(pkg, oracle_mod):
     assert pkg.Ctl.status.offset == status_off
 
 
+@pytest.mark.parametrize("lang,std", [("c", "-std=c99"), ("c", "-std=c11"), ("c++", "-std=c++11"),
+                                      ("c++", "-std=c++17")])
+def test_header_compiles_as_c_and_cpp(lang, std):
+    """include/svpf.h (and the svpf.cuh shim a reference caller includes) is a
+    plain C header: it compiles in C and C++ translation units with warnings
+    as errors, the way a caller's own build would include it."""
+    cc = "gcc" if lang == "c" else "g++"
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "t." + ("c" if lang == "c" else "cpp"))
+        open(src, "w").write('#include "svpf.cuh"\nint svpf_header_probe(void) { return SVPF_OK; }\n')
+        r = subprocess.run([cc, "-x", lang, std, "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-I",
+                            os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include", src],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+
+
 def test_config_fields_follow_header_order(pkg, oracle_mod):
     text = open(HEADER).read()
     block = text[text.index("#define SVPF_CONFIG_FIELDS"):text.index("#define SVPF_DECL_INT_")]
